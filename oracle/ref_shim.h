@@ -1,0 +1,89 @@
+/* C-ABI shim over the reference's own CPU linear-solve path (DelFEM, built from
+ * its sources by oracle/Makefile into oracle/_ref/libdfm_refshim.so).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker and the timed CPU
+ * baseline; nothing in the product (delfem_b200/) links or calls it.
+ *
+ * Two levels:
+ *  - field level: a mesh goes through Fem::Field::CFieldWorld::AddMesh,
+ *    Fem::Ls::CLinearSystem_Field / CZLinearSystem, LsSol::CPreconditioner_ILU /
+ *    CZPreconditioner_ILU and LsSol::Solve_PCG / Solve_PBiCGSTAB /
+ *    Fem::Ls::Solve_PCOCG, in the call order of
+ *    src/femeqn/eqnsys_scalar.cpp:213-359 and test_glut/helmholtz2d/main.cpp:82-121;
+ *  - matrix level: arbitrary block-CRS arrays go into MatVec::CMatDia_BlkCrs /
+ *    CMatDiaFrac_BlkCrs and LsSol::CLinearSystem directly.
+ *
+ * Array layout everywhere is the reference's: rowptr[N+1] (m_colInd_Blk),
+ * colind[ncrs] (m_rowPtr_Blk, off-diagonal only, ascending per row), diagonal
+ * blocks diag[N*b*b], off-diagonal blocks off[ncrs*b*b], each block row-major.
+ * Complex values are interleaved (re, im) doubles.
+ * All functions return 0 on success, non-zero on failure. */
+#ifndef DFM_REF_SHIM_H
+#define DFM_REF_SHIM_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DFM_REF_POISSON2D = 1,   /* Fem::Eqn::AddLinSys_Poisson, P1 triangles, b=1      */
+  DFM_REF_SOLID2D = 2,     /* Fem::Eqn::AddLinSys_LinearSolid2D_Static, P1, b=2   */
+  DFM_REF_SOLID3D = 3,     /* Fem::Eqn::AddLinSys_LinearSolid3D_Static, P1 tet, b=3 */
+  DFM_REF_HELMHOLTZ2D = 4  /* Fem::Eqn::AddLinSys_Helmholtz + SommerfeltRadiationBC, complex b=1 */
+};
+enum { DFM_REF_PCG = 0, DFM_REF_PBICGSTAB = 1, DFM_REF_PCOCG = 2 };
+
+typedef struct dfm_ref_sys dfm_ref_sys;
+
+/* Mesh: coord[nnode*ndim]; elem[nelem*nnoel] (TRI nnoel=3, TET nnoel=4);
+ * bnd[nbnd*bnd_nnoel] (BAR 2 / TRI 3, or nbnd=0).  The boundary array is a
+ * Dirichlet partial field (all DOFs fixed) for the real kinds and carries the
+ * Sommerfeld radiation condition for DFM_REF_HELMHOLTZ2D. */
+dfm_ref_sys* dfm_ref_create(int kind, int ndim, int nnode, const double* coord,
+                            int nnoel, int nelem, const int* elem,
+                            int bnd_nnoel, int nbnd, const int* bnd);
+void dfm_ref_destroy(dfm_ref_sys* s);
+int dfm_ref_dims(const dfm_ref_sys* s, unsigned* N, unsigned* b, unsigned* ncrs);
+int dfm_ref_pattern(const dfm_ref_sys* s, unsigned* rowptr, unsigned* colind);
+/* params: POISSON2D {alpha, source}; SOLID2D {lambda, myu, rho, gx, gy};
+ * SOLID3D {lambda, myu, rho, gx, gy, gz}; HELMHOLTZ2D {wave_length}.
+ * elem_coef (may be NULL; POISSON2D/SOLID2D only): per-element multiplier of the
+ * element matrix, assembled by a restatement of the element loop into the
+ * reference's own matrix through CMatDia_BlkCrs::Mearge.
+ * nodal_load (may be NULL): added to the residual before FinalizeMarge. */
+int dfm_ref_assemble(dfm_ref_sys* s, const double* params, const double* elem_coef,
+                     const double* nodal_load, double* res_norm, double* seconds);
+int dfm_ref_get_system(const dfm_ref_sys* s, double* diag, double* off, double* rhs);
+int dfm_ref_get_bcflag(const dfm_ref_sys* s, int* flags);
+int dfm_ref_ilu(dfm_ref_sys* s, double* seconds);
+int dfm_ref_get_ilu(const dfm_ref_sys* s, double* diag, double* off);
+/* Restores r = b (saved after assembly), runs the solver, copies the update x. */
+int dfm_ref_solve(dfm_ref_sys* s, int method, double tol, unsigned maxit,
+                  unsigned* iters, double* conv, double* x, double* seconds);
+
+/* ---- matrix level (real, fixed block size b) ---- */
+int dfm_ref_mat_spmv(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                     const double* diag, const double* off, double alpha, const double* x,
+                     double beta, double* y);
+/* Returns 0 if DoILUDecomp succeeded, 1 if it gave up (more than 10 singular pivots). */
+int dfm_ref_mat_ilu0(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                     const double* diag, const double* off, double* fdiag, double* foff);
+int dfm_ref_mat_precond(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                        const double* fdiag, const double* foff, double* vec);
+/* LsSol::CLinearSystem + CPreconditioner_ILU(0) + Solve_PCG / Solve_PBiCGSTAB.
+ * Returns 0 when the solver reported convergence, 3 when it did not, 1 on ILU failure. */
+int dfm_ref_mat_solve(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                      const double* diag, const double* off, const double* rhs, int method,
+                      double tol, unsigned maxit, unsigned* iters, double* conv, double* x,
+                      double* t_ilu, double* t_solve);
+
+/* ---- matrix level (complex, b = 1) ---- */
+int dfm_ref_zmat_spmv(unsigned N, const unsigned* rowptr, const unsigned* colind,
+                      const double* diag, const double* off, double alpha, const double* x,
+                      double beta, double* y);
+int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind,
+                      const double* diag, const double* off, double* fdiag, double* foff);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,190 @@
+"""ctypes binding of oracle/_ref/libdfm_refshim.so - the reference's own CPU
+implementation of the linear-solve path (DelFEM sources compiled by
+oracle/Makefile).  TEST INFRASTRUCTURE ONLY: tests, fixture generation and the
+bench's CPU-baseline leg use it as the checker / timed baseline."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libdfm_refshim.so")
+REF_DIR = "/root/reference"
+
+POISSON2D, SOLID2D, SOLID3D, HELMHOLTZ2D = 1, 2, 3, 4
+PCG, PBICGSTAB, PCOCG = 0, 1, 2
+
+_lib = None
+
+
+def build(ref_dir: str = REF_DIR) -> bool:
+    """Compile the reference + shim into oracle/_ref (needs the reference tree)."""
+    if not os.path.isdir(ref_dir):
+        return os.path.exists(LIB_PATH)
+    r = subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}", "ref", "-j8"],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference build failed:\n" + r.stdout + r.stderr)
+    return True
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        dp, up, ip = C.POINTER(C.c_double), C.POINTER(C.c_uint), C.POINTER(C.c_int)
+        L.dfm_ref_create.restype = P
+        L.dfm_ref_create.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_int, C.c_int, ip, C.c_int, C.c_int, ip]
+        L.dfm_ref_destroy.argtypes = [P]
+        L.dfm_ref_dims.argtypes = [P, up, up, up]
+        L.dfm_ref_pattern.argtypes = [P, up, up]
+        L.dfm_ref_assemble.argtypes = [P, dp, dp, dp, dp, dp]
+        L.dfm_ref_get_system.argtypes = [P, dp, dp, dp]
+        L.dfm_ref_get_bcflag.argtypes = [P, ip]
+        L.dfm_ref_ilu.argtypes = [P, dp]
+        L.dfm_ref_get_ilu.argtypes = [P, dp, dp]
+        L.dfm_ref_solve.argtypes = [P, C.c_int, C.c_double, C.c_uint, up, dp, dp, dp]
+        L.dfm_ref_mat_spmv.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
+        L.dfm_ref_mat_ilu0.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, dp]
+        L.dfm_ref_mat_precond.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp]
+        L.dfm_ref_mat_solve.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
+                                        C.c_uint, up, dp, dp, dp, dp]
+        L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
+        L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _u(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint))
+
+
+def _i(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+class RefSystem:
+    """Field-level reference system built from a :class:`delfem_b200.meshes.Mesh`."""
+
+    def __init__(self, kind: int, mesh):
+        L = lib()
+        self.kind = kind
+        coord = np.ascontiguousarray(mesh.coord, dtype=np.float64)
+        elem = np.ascontiguousarray(mesh.elem, dtype=np.int32)
+        bnd = np.ascontiguousarray(mesh.bnd, dtype=np.int32)
+        self._keep = (coord, elem, bnd)
+        self.h = L.dfm_ref_create(kind, mesh.ndim, mesh.nnode, _d(coord), mesh.nnoel, elem.shape[0], _i(elem),
+                                  bnd.shape[1] if bnd.size else 0, bnd.shape[0], _i(bnd) if bnd.size else None)
+        if not self.h:
+            raise RuntimeError("dfm_ref_create failed")
+        N, b, n = C.c_uint(), C.c_uint(), C.c_uint()
+        L.dfm_ref_dims(self.h, C.byref(N), C.byref(b), C.byref(n))
+        self.N, self.b, self.ncrs = N.value, b.value, n.value
+        self.cplx = kind == HELMHOLTZ2D
+        self.vw = 2 if self.cplx else self.b * self.b     # doubles per block
+        self.xw = 2 if self.cplx else self.b              # doubles per block row of a vector
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dfm_ref_destroy(self.h)
+            self.h = None
+
+    def pattern(self):
+        rp = np.zeros(self.N + 1, np.uint32)
+        ci = np.zeros(max(self.ncrs, 1), np.uint32)
+        lib().dfm_ref_pattern(self.h, _u(rp), _u(ci))
+        return rp, ci[: self.ncrs]
+
+    def assemble(self, params, coef=None, load=None):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        c = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64)
+        l_ = None if load is None else np.ascontiguousarray(load, dtype=np.float64).ravel()
+        res, sec = C.c_double(), C.c_double()
+        rc = lib().dfm_ref_assemble(self.h, _d(p), _d(c), _d(l_), C.byref(res), C.byref(sec))
+        if rc:
+            raise RuntimeError("assemble failed")
+        return res.value, sec.value
+
+    def system(self):
+        d = np.zeros(self.N * self.vw)
+        o = np.zeros(max(self.ncrs, 1) * self.vw)
+        r = np.zeros(self.N * self.xw)
+        lib().dfm_ref_get_system(self.h, _d(d), _d(o), _d(r))
+        return d, o[: self.ncrs * self.vw], r
+
+    def bcflag(self):
+        f = np.zeros(self.N * self.b, np.int32)
+        lib().dfm_ref_get_bcflag(self.h, _i(f))
+        return f
+
+    def ilu(self):
+        sec = C.c_double()
+        rc = lib().dfm_ref_ilu(self.h, C.byref(sec))
+        return rc, sec.value
+
+    def ilu_factor(self):
+        d = np.zeros(self.N * self.vw)
+        o = np.zeros(max(self.ncrs, 1) * self.vw)
+        rc = lib().dfm_ref_get_ilu(self.h, _d(d), _d(o))
+        return rc, d, o[: self.ncrs * self.vw]
+
+    def solve(self, method=PCG, tol=1e-10, maxit=10000):
+        x = np.zeros(self.N * self.xw)
+        it, conv, sec = C.c_uint(), C.c_double(), C.c_double()
+        rc = lib().dfm_ref_solve(self.h, method, tol, maxit, C.byref(it), C.byref(conv), _d(x), C.byref(sec))
+        return rc, x, it.value, conv.value, sec.value
+
+
+def mat_spmv(N, b, rowptr, colind, diag, off, alpha, x, beta, y):
+    y = np.array(y, dtype=np.float64, copy=True)
+    lib().dfm_ref_mat_spmv(N, b, _u(rowptr), _u(colind), _d(diag), _d(off), alpha, _d(np.ascontiguousarray(x)), beta, _d(y))
+    return y
+
+
+def mat_ilu0(N, b, rowptr, colind, diag, off):
+    fd = np.zeros_like(diag)
+    fo = np.zeros(max(off.size, 1))
+    rc = lib().dfm_ref_mat_ilu0(N, b, _u(rowptr), _u(colind), _d(diag), _d(off if off.size else fo), _d(fd), _d(fo))
+    return rc, fd, fo[: off.size]
+
+
+def mat_precond(N, b, rowptr, colind, fdiag, foff, vec):
+    v = np.array(vec, dtype=np.float64, copy=True)
+    fo = foff if foff.size else np.zeros(1)
+    lib().dfm_ref_mat_precond(N, b, _u(rowptr), _u(colind), _d(fdiag), _d(fo), _d(v))
+    return v
+
+
+def mat_solve(N, b, rowptr, colind, diag, off, rhs, method=PCG, tol=1e-10, maxit=10000):
+    x = np.zeros(N * b)
+    it, conv, ti, ts = C.c_uint(), C.c_double(), C.c_double(), C.c_double()
+    rc = lib().dfm_ref_mat_solve(N, b, _u(rowptr), _u(colind), _d(diag), _d(off), _d(np.ascontiguousarray(rhs)),
+                                 method, tol, maxit, C.byref(it), C.byref(conv), _d(x), C.byref(ti), C.byref(ts))
+    return rc, x, it.value, conv.value, ti.value, ts.value
+
+
+def zmat_ilu0(N, rowptr, colind, diag, off):
+    fd = np.zeros_like(diag)
+    fo = np.zeros(max(off.size, 1))
+    lib().dfm_ref_zmat_ilu0(N, _u(rowptr), _u(colind), _d(diag), _d(off if off.size else fo), _d(fd), _d(fo))
+    return fd, fo[: off.size]
+
+
+def zmat_spmv(N, rowptr, colind, diag, off, alpha, x, beta, y):
+    y = np.array(y, dtype=np.float64, copy=True)
+    lib().dfm_ref_zmat_spmv(N, _u(rowptr), _u(colind), _d(diag), _d(off), alpha, _d(np.ascontiguousarray(x)), beta, _d(y))
+    return y
