@@ -1,0 +1,445 @@
+// C ABI entry points (include/dfm_b200.h): handle lifetimes, host-side
+// validation of patterns, the symbolic ILU(0) (m_DiaInd + level sets), and
+// dispatch to the kernels.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "dfm_internal.h"
+
+namespace dfm {
+void pcg_release(dfm_ilu M);
+
+int cuda_fail(cudaError_t e, const char* what) {
+  (void)what;
+  if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); return DFM_ERR_NOMEM; }
+  return DFM_ERR_CUDA;
+}
+
+template <typename T>
+static int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  DFM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+  return DFM_OK;
+}
+
+static int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t s) {
+  if (bytes == 0) return DFM_OK;
+  if (!src || !dst) return DFM_ERR_INVALID;
+  DFM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  if (where == DFM_HOST) DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFM_OK;
+}
+
+// Reads and clears the device status code (a timed-out wait, ...).
+int take_code(dfm_ctx c) {
+  DevStatus h = {};
+  DFM_CUDA_TRY(cudaMemcpyAsync(&h, c->d_status, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (h.code) {
+    DFM_CUDA_TRY(cudaMemsetAsync(&c->d_status->code, 0, sizeof(int), c->stream));
+    DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  return h.code;
+}
+
+static int copy_out(void* dst, const void* src, size_t bytes, int where, cudaStream_t s) {
+  if (bytes == 0) return DFM_OK;
+  if (!src || !dst) return DFM_ERR_INVALID;
+  DFM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, where == DFM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+  DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFM_OK;
+}
+
+// Level sets of the natural ordering: lev(i) = 1 + max lev(j) over the rows the
+// sweep reads (j in L(i) forward, j in U(i) backward), 0 for none.  Rows are
+// then listed level by level, ascending inside a level.
+static unsigned make_levels(unsigned N, const std::vector<unsigned>& rowptr, const std::vector<unsigned>& colind,
+                            const std::vector<unsigned>& diaind, bool fwd, std::vector<unsigned>& lev,
+                            std::vector<unsigned>& order, std::vector<unsigned>& lvlptr) {
+  lev.assign(N, 0);
+  unsigned nl = 0;
+  for (unsigned t = 0; t < N; t++) {
+    const unsigned i = fwd ? t : N - 1 - t;
+    const unsigned s0 = fwd ? rowptr[i] : diaind[i], s1 = fwd ? diaind[i] : rowptr[i + 1];
+    unsigned l = 0;
+    for (unsigned s = s0; s < s1; s++) l = std::max(l, lev[colind[s]] + 1);
+    lev[i] = l;
+    nl = std::max(nl, l + 1);
+  }
+  if (N == 0) nl = 0;
+  lvlptr.assign(nl + 1, 0);
+  for (unsigned i = 0; i < N; i++) lvlptr[lev[i] + 1]++;
+  for (unsigned l = 0; l < nl; l++) lvlptr[l + 1] += lvlptr[l];
+  order.assign(N, 0);
+  std::vector<unsigned> fill(lvlptr.begin(), lvlptr.end() - (nl ? 1 : 0));
+  for (unsigned i = 0; i < N; i++) order[fill[lev[i]]++] = i;
+  return nl;
+}
+
+}  // namespace dfm
+
+using namespace dfm;
+
+extern "C" {
+
+const char* dfm_status_string(int s) {
+  switch (s) {
+    case DFM_OK: return "ok";
+    case DFM_ERR_INVALID: return "invalid argument";
+    case DFM_ERR_CUDA: return "CUDA error";
+    case DFM_ERR_NOMEM: return "out of device memory";
+    case DFM_NOT_CONVERGED: return "not converged";
+    case DFM_BREAKDOWN: return "breakdown";
+    case DFM_SINGULAR_PIVOT: return "singular pivot";
+    case DFM_WAIT_TIMEOUT: return "device wait timeout";
+    case DFM_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown";
+  }
+}
+
+int dfm_abi_version(void) { return DFM_ABI_VERSION; }
+
+int dfm_ctx_create(int device, dfm_ctx* out) {
+  if (!out) return DFM_ERR_INVALID;
+  *out = nullptr;
+  DFM_CUDA_TRY(cudaSetDevice(device));
+  dfm_ctx c = new (std::nothrow) dfm_ctx_s();
+  if (!c) return DFM_ERR_NOMEM;
+  c->device = device;
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+  int rc = DFM_OK;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) rc = DFM_ERR_CUDA;
+  c->stream = c->own;
+  if (!rc) rc = dalloc(&c->d_status, 1);
+  if (!rc) rc = dalloc(&c->d_part, (size_t)8 * kMaxBlocks);
+  if (!rc) rc = dalloc(&c->d_scal, 1);
+  if (!rc && cudaMallocHost((void**)&c->h_scal, sizeof(KrylovScalars)) != cudaSuccess) rc = DFM_ERR_CUDA;
+  if (!rc && cudaMemset(c->d_status, 0, sizeof(DevStatus)) != cudaSuccess) rc = DFM_ERR_CUDA;
+  if (!rc && cudaMemset(c->d_scal, 0, sizeof(KrylovScalars)) != cudaSuccess) rc = DFM_ERR_CUDA;
+  if (rc) { dfm_ctx_destroy(c); return rc; }
+  *out = c;
+  return DFM_OK;
+}
+
+int dfm_ctx_destroy(dfm_ctx c) {
+  if (!c) return DFM_OK;
+  cudaSetDevice(c->device);
+  if (c->own) cudaStreamSynchronize(c->own);
+  cudaFree(c->d_status);
+  cudaFree(c->d_part);
+  cudaFree(c->d_scal);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return DFM_OK;
+}
+
+int dfm_ctx_set_stream(dfm_ctx c, void* stream) {
+  if (!c) return DFM_ERR_INVALID;
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return DFM_OK;
+}
+
+int dfm_ctx_sync(dfm_ctx c) {
+  if (!c) return DFM_ERR_INVALID;
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFM_OK;
+}
+
+int dfm_ctx_set_wait_limit(dfm_ctx c, unsigned long long ns) {
+  if (!c || ns == 0) return DFM_ERR_INVALID;
+  c->wait_ns = ns;
+  return DFM_OK;
+}
+
+int dfm_ctx_take_error(dfm_ctx c, int* code, int* where) {
+  if (!c) return DFM_ERR_INVALID;
+  DevStatus h = {};
+  DFM_CUDA_TRY(cudaMemcpyAsync(&h, c->d_status, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (code) *code = h.code;
+  if (where) *where = h.where;
+  h.code = 0;
+  h.where = 0;
+  DFM_CUDA_TRY(cudaMemcpyAsync(c->d_status, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFM_OK;
+}
+
+int dfm_ctx_wait_selftest(dfm_ctx c, unsigned long long limit_ns) {
+  if (!c || limit_ns == 0 || limit_ns > 10000000000ull) return DFM_ERR_INVALID;
+  int rc = ilu_wait_selftest(c, limit_ns);
+  if (rc) return rc;
+  int code = 0, where = 0;
+  rc = dfm_ctx_take_error(c, &code, &where);
+  if (rc) return rc;
+  return code;  // DFM_WAIT_TIMEOUT expected
+}
+
+// ------------------------------------------------------------------ matrix
+int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* rowptr, const unsigned* colind,
+                   dfm_mat* out) {
+  if (!c || !out || !rowptr) return DFM_ERR_INVALID;
+  *out = nullptr;
+  if (vt != DFM_REAL && vt != DFM_COMPLEX) return DFM_ERR_INVALID;
+  if (vt == DFM_REAL && (b < 1 || b > 3)) return DFM_ERR_UNSUPPORTED;
+  if (vt == DFM_COMPLEX && b != 1) return DFM_ERR_UNSUPPORTED;
+  if (rowptr[0] != 0) return DFM_ERR_INVALID;
+  for (unsigned i = 0; i < N; i++)
+    if (rowptr[i + 1] < rowptr[i]) return DFM_ERR_INVALID;
+  const unsigned ncrs = rowptr[N];
+  if (ncrs && !colind) return DFM_ERR_INVALID;
+  for (unsigned i = 0; i < N; i++)
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) {
+      if (colind[s] >= N || colind[s] == i) return DFM_ERR_INVALID;
+      if (s > rowptr[i] && colind[s] <= colind[s - 1]) return DFM_ERR_INVALID;
+    }
+  cudaSetDevice(c->device);
+  dfm_mat A = new (std::nothrow) dfm_mat_s();
+  if (!A) return DFM_ERR_NOMEM;
+  A->ctx = c;
+  A->N = N;
+  A->b = b;
+  A->vt = vt;
+  A->ncrs = ncrs;
+  A->h_rowptr.assign(rowptr, rowptr + N + 1);
+  A->h_colind.assign(colind, colind + ncrs);
+  int rc = dalloc(&A->d_rowptr, N + 1);
+  if (!rc) rc = dalloc(&A->d_colind, ncrs);
+  if (!rc) rc = dalloc(&A->d_diag, (size_t)N * A->vw());
+  if (!rc) rc = dalloc(&A->d_off, (size_t)ncrs * A->vw());
+  if (!rc) rc = copy_in(A->d_rowptr, rowptr, sizeof(unsigned) * (N + 1), DFM_HOST, c->stream);
+  if (!rc) rc = copy_in(A->d_colind, colind, sizeof(unsigned) * ncrs, DFM_HOST, c->stream);
+  if (!rc) rc = dfm_mat_set_zero(A);
+  if (rc) { dfm_mat_destroy(A); return rc; }
+  *out = A;
+  return DFM_OK;
+}
+
+int dfm_mat_destroy(dfm_mat A) {
+  if (!A) return DFM_OK;
+  cudaStreamSynchronize(A->ctx->stream);
+  cudaFree(A->d_rowptr);
+  cudaFree(A->d_colind);
+  cudaFree(A->d_diag);
+  cudaFree(A->d_off);
+  delete A;
+  return DFM_OK;
+}
+
+int dfm_mat_info(dfm_mat A, unsigned* N, unsigned* b, unsigned* ncrs, int* vt) {
+  if (!A) return DFM_ERR_INVALID;
+  if (N) *N = A->N;
+  if (b) *b = A->b;
+  if (ncrs) *ncrs = A->ncrs;
+  if (vt) *vt = A->vt;
+  return DFM_OK;
+}
+
+int dfm_mat_set_zero(dfm_mat A) {
+  if (!A) return DFM_ERR_INVALID;
+  cudaStream_t s = A->ctx->stream;
+  DFM_CUDA_TRY(cudaMemsetAsync(A->d_diag, 0, sizeof(double) * A->vw() * std::max(A->N, 1u), s));
+  DFM_CUDA_TRY(cudaMemsetAsync(A->d_off, 0, sizeof(double) * A->vw() * std::max(A->ncrs, 1u), s));
+  return DFM_OK;
+}
+
+int dfm_mat_set_values(dfm_mat A, const double* diag, const double* off, int where) {
+  if (!A) return DFM_ERR_INVALID;
+  int rc = copy_in(A->d_diag, diag, sizeof(double) * A->vw() * A->N, where, A->ctx->stream);
+  if (!rc) rc = copy_in(A->d_off, off, sizeof(double) * A->vw() * A->ncrs, where, A->ctx->stream);
+  return rc;
+}
+
+int dfm_mat_get_values(dfm_mat A, double* diag, double* off, int where) {
+  if (!A) return DFM_ERR_INVALID;
+  int rc = DFM_OK;
+  if (diag) rc = copy_out(diag, A->d_diag, sizeof(double) * A->vw() * A->N, where, A->ctx->stream);
+  if (!rc && off) rc = copy_out(off, A->d_off, sizeof(double) * A->vw() * A->ncrs, where, A->ctx->stream);
+  return rc;
+}
+
+int dfm_mat_values_device(dfm_mat A, double** diag, double** off) {
+  if (!A) return DFM_ERR_INVALID;
+  if (diag) *diag = A->d_diag;
+  if (off) *off = A->d_off;
+  return DFM_OK;
+}
+
+int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes) {
+  if (!A) return DFM_ERR_INVALID;
+  if (lanes != 0 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return DFM_ERR_INVALID;
+  A->lanes = lanes;
+  return DFM_OK;
+}
+
+int dfm_mat_get_spmv_lanes(dfm_mat A, int* lanes) {
+  if (!A || !lanes) return DFM_ERR_INVALID;
+  *lanes = A->lanes;
+  return DFM_OK;
+}
+
+int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, double* y) {
+  if (!A || (!x && A->N) || (!y && A->N)) return DFM_ERR_INVALID;
+  int rc = spmv_autotune(A);
+  if (rc) return rc;
+  rc = spmv_launch(A, alpha, x, beta, y, nullptr, 0, nullptr, A->lanes);
+  if (rc) return rc;
+  DFM_CUDA_TRY(cudaStreamSynchronize(A->ctx->stream));
+  return DFM_OK;
+}
+
+// -------------------------------------------------------------------- ILU
+int dfm_ilu_create(dfm_mat A, dfm_ilu* out) {
+  if (!A || !out) return DFM_ERR_INVALID;
+  *out = nullptr;
+  dfm_ilu M = new (std::nothrow) dfm_ilu_s();
+  if (!M) return DFM_ERR_NOMEM;
+  M->ctx = A->ctx;
+  M->A = A;
+  M->N = A->N;
+  M->b = A->b;
+  M->ncrs = A->ncrs;
+  M->vt = A->vt;
+  const unsigned N = A->N;
+  M->h_diaind.resize(N);
+  for (unsigned i = 0; i < N; i++) {  // CMatDiaFrac_BlkCrs ctor, src/matvec/matdiafrac_blkcrs.cpp:263-278
+    M->h_diaind[i] = A->h_rowptr[i + 1];
+    for (unsigned s = A->h_rowptr[i]; s < A->h_rowptr[i + 1]; s++)
+      if (A->h_colind[s] > i) { M->h_diaind[i] = s; break; }
+  }
+  std::vector<unsigned> of, ob, lf, lb;
+  M->nlev_f = make_levels(N, A->h_rowptr, A->h_colind, M->h_diaind, true, M->lev_f, of, lf);
+  M->nlev_b = make_levels(N, A->h_rowptr, A->h_colind, M->h_diaind, false, M->lev_b, ob, lb);
+  cudaStream_t s = A->ctx->stream;
+  int rc = dalloc(&M->d_diaind, N);
+  if (!rc) rc = dalloc(&M->d_order_f, N);
+  if (!rc) rc = dalloc(&M->d_order_b, N);
+  if (!rc) rc = dalloc(&M->d_lvl_f, lf.size());
+  if (!rc) rc = dalloc(&M->d_lvl_b, lb.size());
+  if (!rc) rc = dalloc(&M->d_fdiag, (size_t)N * M->vw());
+  if (!rc) rc = dalloc(&M->d_foff, (size_t)M->ncrs * M->vw());
+  if (!rc) rc = dalloc(&M->d_flags, N);
+  if (!rc) rc = dalloc(&M->d_tmp, (size_t)N * M->xw());
+  if (!rc) rc = copy_in(M->d_diaind, M->h_diaind.data(), sizeof(unsigned) * N, DFM_HOST, s);
+  if (!rc) rc = copy_in(M->d_order_f, of.data(), sizeof(unsigned) * N, DFM_HOST, s);
+  if (!rc) rc = copy_in(M->d_order_b, ob.data(), sizeof(unsigned) * N, DFM_HOST, s);
+  if (!rc) rc = copy_in(M->d_lvl_f, lf.data(), sizeof(unsigned) * lf.size(), DFM_HOST, s);
+  if (!rc) rc = copy_in(M->d_lvl_b, lb.data(), sizeof(unsigned) * lb.size(), DFM_HOST, s);
+  if (!rc && cudaMemsetAsync(M->d_flags, 0, sizeof(unsigned) * std::max(N, 1u), s) != cudaSuccess) rc = DFM_ERR_CUDA;
+  if (rc) { dfm_ilu_destroy(M); return rc; }
+  *out = M;
+  return DFM_OK;
+}
+
+int dfm_ilu_destroy(dfm_ilu M) {
+  if (!M) return DFM_OK;
+  cudaStreamSynchronize(M->ctx->stream);
+  pcg_release(M);
+  cudaFree(M->d_diaind);
+  cudaFree(M->d_order_f);
+  cudaFree(M->d_order_b);
+  cudaFree(M->d_lvl_f);
+  cudaFree(M->d_lvl_b);
+  cudaFree(M->d_fdiag);
+  cudaFree(M->d_foff);
+  cudaFree(M->d_flags);
+  cudaFree(M->d_tmp);
+  delete M;
+  return DFM_OK;
+}
+
+int dfm_ilu_levels(dfm_ilu M, unsigned* nf, unsigned* nb, unsigned* lev_f, unsigned* lev_b) {
+  if (!M) return DFM_ERR_INVALID;
+  if (nf) *nf = M->nlev_f;
+  if (nb) *nb = M->nlev_b;
+  if (lev_f) std::copy(M->lev_f.begin(), M->lev_f.end(), lev_f);
+  if (lev_b) std::copy(M->lev_b.begin(), M->lev_b.end(), lev_b);
+  return DFM_OK;
+}
+
+int dfm_ilu_factor(dfm_ilu M, dfm_mat A, unsigned* n_singular) {
+  if (!M || !A || A->N != M->N || A->ncrs != M->ncrs || A->b != M->b || A->vt != M->vt) return DFM_ERR_INVALID;
+  int rc = ilu_factor_launch(M, A);
+  if (rc) return rc;
+  DevStatus h = {};
+  DFM_CUDA_TRY(cudaMemcpyAsync(&h, M->ctx->d_status, sizeof(h), cudaMemcpyDeviceToHost, M->ctx->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(M->ctx->stream));
+  if (n_singular) *n_singular = h.nsing;
+  if (h.code) return take_code(M->ctx);
+  M->factored = true;
+  if (M->vt == DFM_REAL && h.nsing > 10) return DFM_SINGULAR_PIVOT;  // nmax_sing, :774
+  return DFM_OK;
+}
+
+int dfm_ilu_get_values(dfm_ilu M, double* diag, double* off, int where) {
+  if (!M) return DFM_ERR_INVALID;
+  int rc = DFM_OK;
+  if (diag) rc = copy_out(diag, M->d_fdiag, sizeof(double) * M->vw() * M->N, where, M->ctx->stream);
+  if (!rc && off) rc = copy_out(off, M->d_foff, sizeof(double) * M->vw() * M->ncrs, where, M->ctx->stream);
+  return rc;
+}
+
+int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int where) {
+  if (!M) return DFM_ERR_INVALID;
+  int rc = copy_in(M->d_fdiag, diag, sizeof(double) * M->vw() * M->N, where, M->ctx->stream);
+  if (!rc) rc = copy_in(M->d_foff, off, sizeof(double) * M->vw() * M->ncrs, where, M->ctx->stream);
+  if (!rc) M->factored = true;
+  return rc;
+}
+
+int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
+  if (!M || mode < 0 || mode > 2) return DFM_ERR_INVALID;
+  M->sweep = mode;
+  return DFM_OK;
+}
+
+int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {
+  if (!M || !mode) return DFM_ERR_INVALID;
+  *mode = M->sweep;
+  return DFM_OK;
+}
+
+int dfm_ilu_apply(dfm_ilu M, const double* r, double* z) {
+  if (!M || (M->N && (!r || !z)) || r == z) return DFM_ERR_INVALID;
+  int rc = ilu_autotune(M);
+  if (rc) return rc;
+  const size_t n = (size_t)M->N * M->xw();
+  if ((rc = ilu_fill_sentinel(M, M->d_tmp, n))) return rc;
+  if ((rc = ilu_fill_sentinel(M, z, n))) return rc;
+  if ((rc = ilu_fwd_launch(M, r, M->d_tmp, nullptr, M->sweep))) return rc;
+  if ((rc = ilu_bwd_launch(M, M->d_tmp, z, nullptr, nullptr, nullptr, M->sweep))) return rc;
+  return take_code(M->ctx);
+}
+
+// ---------------------------------------------------------------- solvers
+int dfm_solve_pcg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                  double* conv) {
+  if (!A || !M || M->A != A || A->vt != DFM_REAL || (A->N && (!r || !x))) return DFM_ERR_INVALID;
+  if (!M->factored) return DFM_ERR_INVALID;
+  return pcg_solve(A, M, r, x, tol, maxit, iters, conv);
+}
+
+int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol, unsigned maxit,
+                       unsigned* iters, double* conv) {
+  if (!A || !M || (A->N && (!b_host || !x_host))) return DFM_ERR_INVALID;
+  const size_t n = (size_t)A->N * A->xw();
+  cudaStream_t s = A->ctx->stream;
+  double *r = nullptr, *x = nullptr;
+  int rc = dalloc(&r, n);
+  if (!rc) rc = dalloc(&x, n);
+  if (!rc && cudaMemcpyAsync(r, b_host, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) rc = DFM_ERR_CUDA;
+  if (!rc) rc = dfm_solve_pcg(A, M, r, x, tol, maxit, iters, conv);
+  if ((rc == DFM_OK || rc == DFM_NOT_CONVERGED) &&
+      cudaMemcpyAsync(x_host, x, n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = DFM_ERR_CUDA;
+  cudaStreamSynchronize(s);
+  cudaFree(r);
+  cudaFree(x);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Host-side objects behind the C ABI handles (include/dfm_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dfm_b200.h"
+#include "common.cuh"
+
+#define DFM_CUDA_TRY(expr)                                 \
+  do {                                                     \
+    cudaError_t e__ = (expr);                              \
+    if (e__ != cudaSuccess) return dfm::cuda_fail(e__, #expr); \
+  } while (0)
+
+namespace dfm {
+
+int cuda_fail(cudaError_t e, const char* what);
+int take_code(dfm_ctx c);
+
+// Scalars of one Krylov solve, in device memory so a captured CUDA graph can
+// run many iterations without the host.
+struct KrylovScalars {
+  int done;        // 0 running, else final dfm_status + 100 (so DFM_OK is distinguishable)
+  unsigned it;     // iterations completed (0-based index of the next one)
+  unsigned maxit;
+  unsigned conv_it;
+  double tol2;     // tol^2
+  double inv0;     // 1 / |r0|^2
+  double rz;       // (r, z) of the current direction
+  double conv;     // final sqrt(|r|^2 / |r0|^2)
+  double alpha, beta, omega, rho;  // BiCGSTAB / COCG extras
+  double zr[4];    // complex scalars (re, im pairs)
+};
+
+// Upper bound of blocks of the grid-stride kernels (partials arrays length).
+constexpr int kMaxBlocks = 148 * 16;
+
+}  // namespace dfm
+
+struct dfm_ctx_s;
+struct dfm_ctx_s {
+  int device = 0;
+  int nsm = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  DevStatus* d_status = nullptr;
+  unsigned long long wait_ns = 2000000000ull;
+  double* d_part = nullptr;                 // 8 partial arrays of kMaxBlocks doubles
+  dfm::KrylovScalars* d_scal = nullptr;
+  dfm::KrylovScalars* h_scal = nullptr;     // pinned mirror
+  double* part(int k) { return d_part + (size_t)k * dfm::kMaxBlocks; }
+};
+
+struct dfm_mat_s {
+  dfm_ctx ctx = nullptr;
+  unsigned N = 0, b = 1, ncrs = 0;
+  int vt = DFM_REAL;
+  unsigned* d_rowptr = nullptr;
+  unsigned* d_colind = nullptr;
+  double* d_diag = nullptr;
+  double* d_off = nullptr;
+  std::vector<unsigned> h_rowptr, h_colind;
+  int lanes = 0;            // SpMV lanes per block row (0 = not tuned yet)
+  size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }   // doubles per block
+  size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }               // doubles per vector block
+};
+
+struct dfm_ilu_s {
+  dfm_ctx ctx = nullptr;
+  dfm_mat A = nullptr;      // pattern owner (rowptr/colind shared)
+  unsigned N = 0, b = 1, ncrs = 0;
+  int vt = DFM_REAL;
+  unsigned* d_diaind = nullptr;
+  // rows sorted by forward / backward level (ascending row within a level)
+  unsigned* d_order_f = nullptr;
+  unsigned* d_order_b = nullptr;
+  unsigned* d_lvl_f = nullptr;   // level pointers into order_f (nlev_f + 1)
+  unsigned* d_lvl_b = nullptr;
+  std::vector<unsigned> lev_f, lev_b, h_diaind;
+  unsigned nlev_f = 0, nlev_b = 0;
+  double* d_fdiag = nullptr;     // D^-1 blocks
+  double* d_foff = nullptr;      // L and D^-1 U blocks
+  unsigned* d_flags = nullptr;   // per-row completion epochs of the numeric factorisation
+  unsigned epoch = 0;
+  double* d_tmp = nullptr;       // N*xw scratch: forward-sweep output of dfm_ilu_apply
+  int sweep = 0;                 // 0 untuned, 1 sync-free grid, 2 single CTA
+  bool factored = false;
+  size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }
+  size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }
+};
+
+namespace dfm {
+// spmv.cu
+int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
+                int nblocks_hint, KrylovScalars* sc, int lanes);
+int spmv_autotune(dfm_mat A);
+int spmv_grid(dfm_mat A);
+// ilu.cu
+int ilu_factor_launch(dfm_ilu M, dfm_mat A);
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep);
+int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part,
+                   KrylovScalars* sc, int sweep);
+int ilu_fill_sentinel(dfm_ilu M, double* v, size_t n);
+int ilu_autotune(dfm_ilu M);
+int sweep_grid(dfm_ilu M, int sweep);
+int ilu_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns);
+// krylov.cu
+int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+              double* conv);
+}  // namespace dfm

@@ -1,0 +1,800 @@
+// ILU(0) on the device: numeric factorisation and the two triangular sweeps,
+// scheduled by the level sets of the reference's natural ordering.
+//
+// Reference: CMatDiaFrac_BlkCrs (src/matvec/matdiafrac_blkcrs.cpp):
+//   DoILUDecomp :769-1102  row i -= L_ik (D^-1 U)_kj over the pattern, k ascending;
+//                          D_i <- D_i^-1 (closed forms); U_i <- D_i^-1 U_i
+//   ForwardSubstitution :332-503   y_i = D_i^-1 (r_i - sum_{j<i} L_ij y_j)
+//   BackwardSubstitution :505-663  z_i = y_i - sum_{j>i} (D^-1 U)_ij z_j
+// complex twin: CZMatDiaFrac_BlkCrs (src/matvec/zmatdiafrac_blkcrs.cpp:116-261).
+//
+// Scheduling.  Rows are processed in level order (order_f / order_b: rows
+// sorted by level, ascending row inside a level).  Two sweep schedules:
+//  * sync-free (mode 1): a persistent, co-resident grid; worker w takes level-
+//    order positions w, w+W, ...; a row waits only for the rows it reads, by
+//    polling their outputs, which start out as a NaN sentinel.  Because every
+//    dependency sits at an earlier position, and a worker's earlier positions
+//    are all smaller, every wait ends (induction on the position).
+//  * one CTA with level barriers (mode 2): for long dependency chains with few
+//    rows per level the whole sweep runs on one SM with __syncthreads between
+//    levels, so a level costs a CTA barrier instead of a trip through L2.
+// The factorisation uses the sync-free schedule with per-row completion epochs
+// and reproduces the reference's arithmetic exactly (no FMA contraction).
+#include <algorithm>
+
+#include "dfm_internal.h"
+
+namespace dfm {
+
+// ------------------------------------------------------------------ waits
+DFM_DEVINL int ld_status(const DevStatus* st) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(&st->code) : "memory");
+  return v;
+}
+
+template <typename T>
+DFM_DEVINL T poll_value(const T* p, DevStatus* st, uint64_t wait_ns, int where) {
+  T v = ld_relaxed(p);
+  if (!Sent<T>::is(v)) return v;
+  uint64_t deadline = 0;
+  unsigned n = 0;
+  for (;;) {
+    v = ld_relaxed(p);
+    if (!Sent<T>::is(v)) return v;
+    if ((++n & 31u) == 0) {
+      const uint64_t now = globaltimer_ns();
+      if (deadline == 0) deadline = now + wait_ns;
+      if (now > deadline || ld_status(st) != 0) {
+        raise_error(st, DFM_WAIT_TIMEOUT, where);
+        return v;
+      }
+    }
+  }
+}
+
+DFM_DEVINL void wait_epoch(const unsigned* flag, unsigned epoch, DevStatus* st, uint64_t wait_ns, int where) {
+  if (ld_acquire_u32(flag) == epoch) return;
+  uint64_t deadline = 0;
+  unsigned n = 0;
+  for (;;) {
+    if (ld_acquire_u32(flag) == epoch) return;
+    if ((++n & 31u) == 0) {
+      const uint64_t now = globaltimer_ns();
+      if (deadline == 0) deadline = now + wait_ns;
+      if (now > deadline || ld_status(st) != 0) {
+        raise_error(st, DFM_WAIT_TIMEOUT, where);
+        return;
+      }
+    }
+  }
+}
+
+// --------------------------------------------------- numeric factorisation
+DFM_DEVINL long find_slot(const unsigned* colind, unsigned s0, unsigned s1, unsigned j) {
+  while (s0 < s1) {  // strictly ascending columns
+    const unsigned m = (s0 + s1) >> 1;
+    const unsigned c = __ldg(colind + m);
+    if (c == j) return (long)m;
+    if (c < j) s0 = m + 1; else s1 = m;
+  }
+  return -1;
+}
+
+// D <- D^-1 with the reference's closed forms; returns false if singular.
+template <int B>
+DFM_DEVINL bool invert_pivot(double* d);
+template <>
+DFM_DEVINL bool invert_pivot<1>(double* d) {
+  const double v = d[0];
+  if (fabs(v) > 1.0e-30) { d[0] = __ddiv_rn(1.0, v); return true; }
+  return false;
+}
+template <>
+DFM_DEVINL bool invert_pivot<2>(double* d) {
+  const double det = sub_rn(mul_rn(d[0], d[3]), mul_rn(d[1], d[2]));
+  if (!(fabs(det) > 1.0e-30)) return false;
+  const double inv = __ddiv_rn(1.0, det);
+  const double t = d[0];
+  d[0] = mul_rn(inv, d[3]);
+  d[1] = mul_rn(-inv, d[1]);
+  d[2] = mul_rn(-inv, d[2]);
+  d[3] = mul_rn(inv, t);
+  return true;
+}
+DFM_DEVINL double det3(const double* a) {
+  double v = mul_rn(mul_rn(a[0], a[4]), a[8]);
+  v = add_rn(v, mul_rn(mul_rn(a[3], a[7]), a[2]));
+  v = add_rn(v, mul_rn(mul_rn(a[6], a[1]), a[5]));
+  v = sub_rn(v, mul_rn(mul_rn(a[0], a[7]), a[5]));
+  v = sub_rn(v, mul_rn(mul_rn(a[6], a[4]), a[2]));
+  v = sub_rn(v, mul_rn(mul_rn(a[3], a[1]), a[8]));
+  return v;
+}
+template <>
+DFM_DEVINL bool invert_pivot<3>(double* a) {
+  const double det = det3(a);
+  if (!(fabs(det) > 1.0e-30)) return false;
+  const double inv = __ddiv_rn(1.0, det);
+  double t[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) t[q] = a[q];
+  a[0] = mul_rn(inv, sub_rn(mul_rn(t[4], t[8]), mul_rn(t[5], t[7])));
+  a[1] = mul_rn(inv, sub_rn(mul_rn(t[2], t[7]), mul_rn(t[1], t[8])));
+  a[2] = mul_rn(inv, sub_rn(mul_rn(t[1], t[5]), mul_rn(t[2], t[4])));
+  a[3] = mul_rn(inv, sub_rn(mul_rn(t[5], t[6]), mul_rn(t[3], t[8])));
+  a[4] = mul_rn(inv, sub_rn(mul_rn(t[0], t[8]), mul_rn(t[2], t[6])));
+  a[5] = mul_rn(inv, sub_rn(mul_rn(t[2], t[3]), mul_rn(t[0], t[5])));
+  a[6] = mul_rn(inv, sub_rn(mul_rn(t[3], t[7]), mul_rn(t[4], t[6])));
+  a[7] = mul_rn(inv, sub_rn(mul_rn(t[1], t[6]), mul_rn(t[0], t[7])));
+  a[8] = mul_rn(inv, sub_rn(mul_rn(t[0], t[4]), mul_rn(t[1], t[3])));
+  return true;
+}
+
+// One warp per row.  Values are read/written with .cg (L2) accesses: another
+// SM may have finished a row whose bytes share an L1 line this SM cached.
+template <int B>
+__global__ void __launch_bounds__(256)
+k_ilu0_factor(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+              const unsigned* __restrict__ diaind, const unsigned* __restrict__ order, double* fdiag,
+              double* foff, unsigned* flags, unsigned epoch, DevStatus* st, uint64_t wait_ns) {
+  constexpr int BB = B * B;
+  const int lane = threadIdx.x & 31;
+  const unsigned w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned p = w0; p < N; p += nw) {
+    const unsigned i = __ldg(order + p);
+    const unsigned s0 = __ldg(rowptr + i), s1 = __ldg(rowptr + i + 1), di = __ldg(diaind + i);
+    for (unsigned ik = s0; ik < di; ik++) {
+      const unsigned k = __ldg(colind + ik);
+      wait_epoch(flags + k, epoch, st, wait_ns, 1);  // every lane acquires row k
+      __syncwarp();
+      const unsigned u0 = __ldg(diaind + k), u1 = __ldg(rowptr + k + 1);
+      const unsigned nq = (u1 - u0) * BB;
+      for (unsigned q = lane; q < nq; q += 32) {
+        const unsigned kj = u0 + q / BB;
+        const int e = q % BB, r = e / B, c = e % B;
+        const unsigned j = __ldg(colind + kj);
+        double* tgt;
+        if (j == i) tgt = fdiag + (size_t)i * BB + e;
+        else {
+          const long t = find_slot(colind, s0, s1, j);
+          if (t < 0) continue;  // no fill-in in ILU(0)
+          tgt = foff + (size_t)t * BB + e;
+        }
+        const double* l = foff + (size_t)ik * BB + r * B;
+        const double* u = foff + (size_t)kj * BB + c;
+        double acc = mul_rn(__ldcg(l), __ldcg(u));
+#pragma unroll
+        for (int m = 1; m < B; m++) acc = add_rn(acc, mul_rn(__ldcg(l + m), __ldcg(u + m * B)));
+        __stcg(tgt, sub_rn(__ldcg(tgt), acc));
+      }
+      __syncwarp();
+    }
+    __shared__ double s_d[8][BB];
+    double* d = s_d[threadIdx.x >> 5];
+    if (lane < BB) d[lane] = __ldcg(fdiag + (size_t)i * BB + lane);
+    __syncwarp();
+    if (lane == 0) {
+      if (!invert_pivot<B>(d)) atomicAdd(&st->nsing, 1u);
+    }
+    __syncwarp();
+    if (lane < BB) __stcg(fdiag + (size_t)i * BB + lane, d[lane]);
+    for (unsigned ij = di + lane; ij < s1; ij += 32) {
+      double* u = foff + (size_t)ij * BB;
+      double t[BB];
+#pragma unroll
+      for (int q = 0; q < BB; q++) t[q] = __ldcg(u + q);
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          double v = mul_rn(d[r * B], t[c]);
+#pragma unroll
+          for (int m = 1; m < B; m++) v = add_rn(v, mul_rn(d[r * B + m], t[m * B + c]));
+          __stcg(u + r * B + c, v);
+        }
+    }
+    __syncwarp();
+    __threadfence();
+    if (lane == 0) st_release_u32(flags + i, epoch);
+  }
+}
+
+// complex b = 1 (CZMatDiaFrac_BlkCrs::DoILUDecomp)
+DFM_DEVINL double2 zmul_rn(double2 a, double2 b) {
+  return make_double2(sub_rn(mul_rn(a.x, b.x), mul_rn(a.y, b.y)), add_rn(mul_rn(a.x, b.y), mul_rn(a.y, b.x)));
+}
+__global__ void __launch_bounds__(256)
+k_zilu0_factor(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+               const unsigned* __restrict__ diaind, const unsigned* __restrict__ order, double2* fdiag,
+               double2* foff, unsigned* flags, unsigned epoch, DevStatus* st, uint64_t wait_ns) {
+  const int lane = threadIdx.x & 31;
+  const unsigned w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned p = w0; p < N; p += nw) {
+    const unsigned i = __ldg(order + p);
+    const unsigned s0 = __ldg(rowptr + i), s1 = __ldg(rowptr + i + 1), di = __ldg(diaind + i);
+    for (unsigned ik = s0; ik < di; ik++) {
+      const unsigned k = __ldg(colind + ik);
+      wait_epoch(flags + k, epoch, st, wait_ns, 2);
+      __syncwarp();
+      const double2 ikv = __ldcg(foff + ik);
+      const unsigned u0 = __ldg(diaind + k), u1 = __ldg(rowptr + k + 1);
+      for (unsigned kj = u0 + lane; kj < u1; kj += 32) {
+        const unsigned j = __ldg(colind + kj);
+        double2* tgt;
+        if (j == i) tgt = fdiag + i;
+        else {
+          const long t = find_slot(colind, s0, s1, j);
+          if (t < 0) continue;
+          tgt = foff + t;
+        }
+        const double2 pr = zmul_rn(ikv, __ldcg(foff + kj));
+        const double2 a = __ldcg(tgt);
+        __stcg(tgt, make_double2(sub_rn(a.x, pr.x), sub_rn(a.y, pr.y)));
+      }
+      __syncwarp();
+    }
+    __shared__ double2 s_inv[8];
+    if (lane == 0) {
+      const double2 piv = __ldcg(fdiag + i);
+      const double n2 = add_rn(mul_rn(piv.x, piv.x), mul_rn(piv.y, piv.y));
+      if (n2 < 1.0e-20) atomicAdd(&st->nsing, 1u);  // the reference stops for a key press here
+      const double fact = __ddiv_rn(1.0, n2);
+      const double2 inv = make_double2(mul_rn(fact, piv.x), mul_rn(-fact, piv.y));
+      __stcg(fdiag + i, inv);
+      s_inv[threadIdx.x >> 5] = inv;
+    }
+    __syncwarp();
+    const double2 inv = s_inv[threadIdx.x >> 5];
+    for (unsigned ij = di + lane; ij < s1; ij += 32) __stcg(foff + ij, zmul_rn(__ldcg(foff + ij), inv));
+    __syncwarp();
+    __threadfence();
+    if (lane == 0) st_release_u32(flags + i, epoch);
+  }
+}
+
+// ------------------------------------------------------------ sweep helpers
+// Convergence guard run at the top of the forward sweep inside a Krylov
+// iteration: every block reduces the (r, r) partials of the previous kernel
+// and returns early once |r|^2/|r0|^2 < tol^2 (block 0 records the result).
+DFM_DEVINL bool converged_guard(KrylovScalars* sc, const double* rr_part, int nparts) {
+  if (!sc) return false;
+  if (block_flag(&sc->done)) return true;
+  const double rr = reduce_partials(rr_part, nparts);
+  if (rr * sc->inv0 < sc->tol2) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      sc->conv = sqrt(rr * sc->inv0);
+      sc->conv_it = sc->it;
+      sc->done = 100 + DFM_OK;
+    }
+    return true;
+  }
+  return false;
+}
+
+// Real b x b block row: acc_r = sum_c m[r*B+c] * v[c]
+template <int B, typename TV, typename TX>
+DFM_DEVINL void block_mv(double* acc, const TV* m, const TX* v) {
+#pragma unroll
+  for (int r = 0; r < B; r++)
+#pragma unroll
+    for (int c = 0; c < B; c++) acc[r] += (double)m[r * B + c] * (double)v[c];
+}
+
+// ------------------------------------------------------- sync-free sweeps
+// FWD: out_i = D_i^-1 (in_i - sum_{L} m * out_j);  BWD: out_i = in_i - sum_{U} m * out_j.
+// DOT (BWD only): partial of rdot . out, for the Krylov (r, z).
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
+__global__ void __launch_bounds__(256)
+k_sweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned* __restrict__ rowptr,
+                 const unsigned* __restrict__ colind, const unsigned* __restrict__ diaind,
+                 const double* __restrict__ fdiag, const TV* __restrict__ foff, const TX* __restrict__ in,
+                 TX* out, const TX* __restrict__ rdot, double* part, KrylovScalars* sc,
+                 const double* rr_part, int rr_nparts, DevStatus* st, uint64_t wait_ns) {
+  if (FWD) {
+    if (converged_guard(sc, rr_part, rr_nparts)) return;
+  } else if (sc && block_flag(&sc->done)) {
+    return;
+  }
+  constexpr int BB = B * B;
+  const int lane = threadIdx.x % LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned g0 = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+  const unsigned ng = gridDim.x * blockDim.x / LPR;
+  double dacc = 0.0;
+  for (unsigned p = g0; p < N; p += ng) {
+    const unsigned i = __ldg(order + p);
+    unsigned s0, s1;
+    if (FWD) { s0 = __ldg(rowptr + i); s1 = __ldg(diaind + i); }
+    else { s0 = __ldg(diaind + i); s1 = __ldg(rowptr + i + 1); }
+    double acc[B];
+#pragma unroll
+    for (int r = 0; r < B; r++) acc[r] = 0.0;
+    for (unsigned s = s0 + lane; s < s1; s += LPR) {
+      const unsigned col = __ldg(colind + s);
+      TV mv[BB];
+#pragma unroll
+      for (int e = 0; e < BB; e++) mv[e] = __ldcs(foff + (size_t)s * BB + e);
+      TX xv[B];
+#pragma unroll
+      for (int c = 0; c < B; c++) xv[c] = poll_value(out + (size_t)col * B + c, st, wait_ns, FWD ? 3 : 4);
+      block_mv<B>(acc, mv, xv);
+    }
+#pragma unroll
+    for (int r = 0; r < B; r++)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+    if (lane == 0) {
+      double t[B];
+#pragma unroll
+      for (int r = 0; r < B; r++) t[r] = (double)in[(size_t)i * B + r] - acc[r];
+      double o[B];
+      if (FWD) {
+        const double* d = fdiag + (size_t)i * BB;
+#pragma unroll
+        for (int r = 0; r < B; r++) {
+          o[r] = 0.0;
+#pragma unroll
+          for (int c = 0; c < B; c++) o[r] += d[r * B + c] * t[c];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < B; r++) o[r] = t[r];
+      }
+#pragma unroll
+      for (int r = 0; r < B; r++) {
+        const TX v = (TX)o[r];
+        st_relaxed(out + (size_t)i * B + r, v);
+        if (DOT) dacc += (double)rdot[(size_t)i * B + r] * (double)v;
+      }
+    }
+  }
+  if (DOT) block_partial<256>(dacc, part);
+}
+
+// complex b = 1
+template <int LPR, bool FWD, bool DOT>
+__global__ void __launch_bounds__(256)
+k_zsweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned* __restrict__ rowptr,
+                  const unsigned* __restrict__ colind, const unsigned* __restrict__ diaind,
+                  const double2* __restrict__ fdiag, const double2* __restrict__ foff,
+                  const double2* __restrict__ in, double2* out, const double2* __restrict__ rdot, double* part,
+                  KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st, uint64_t wait_ns) {
+  if (FWD) {
+    if (converged_guard(sc, rr_part, rr_nparts)) return;
+  } else if (sc && block_flag(&sc->done)) {
+    return;
+  }
+  const int lane = threadIdx.x % LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned g0 = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+  const unsigned ng = gridDim.x * blockDim.x / LPR;
+  double dre = 0.0, dim = 0.0;
+  double* o64 = reinterpret_cast<double*>(out);
+  for (unsigned p = g0; p < N; p += ng) {
+    const unsigned i = __ldg(order + p);
+    unsigned s0, s1;
+    if (FWD) { s0 = __ldg(rowptr + i); s1 = __ldg(diaind + i); }
+    else { s0 = __ldg(diaind + i); s1 = __ldg(rowptr + i + 1); }
+    double re = 0.0, im = 0.0;
+    for (unsigned s = s0 + lane; s < s1; s += LPR) {
+      const unsigned col = __ldg(colind + s);
+      const double2 m = __ldcs(foff + s);
+      const double xr = poll_value(o64 + 2 * (size_t)col, st, wait_ns, FWD ? 5 : 6);
+      const double xi = poll_value(o64 + 2 * (size_t)col + 1, st, wait_ns, FWD ? 5 : 6);
+      re += m.x * xr - m.y * xi;
+      im += m.x * xi + m.y * xr;
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(gmask, re, o);
+      im += __shfl_xor_sync(gmask, im, o);
+    }
+    if (lane == 0) {
+      const double2 v_in = in[i];
+      double tr = v_in.x - re, ti = v_in.y - im;
+      if (FWD) {
+        const double2 d = fdiag[i];
+        const double a = d.x * tr - d.y * ti, b = d.x * ti + d.y * tr;
+        tr = a; ti = b;
+      }
+      st_relaxed(o64 + 2 * (size_t)i, tr);
+      st_relaxed(o64 + 2 * (size_t)i + 1, ti);
+      if (DOT) {  // unconjugated r^T z
+        const double2 rv = rdot[i];
+        dre += rv.x * tr - rv.y * ti;
+        dim += rv.x * ti + rv.y * tr;
+      }
+    }
+  }
+  if (DOT) {
+    block_partial<256>(dre, part);
+    block_partial<256>(dim, part + kMaxBlocks);
+  }
+}
+
+// ------------------------------------------------- single-CTA level sweeps
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
+__global__ void __launch_bounds__(1024)
+k_sweep_cta(unsigned nlev, const unsigned* __restrict__ lvl, const unsigned* __restrict__ order,
+            const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+            const unsigned* __restrict__ diaind, const double* __restrict__ fdiag, const TV* __restrict__ foff,
+            const TX* __restrict__ in, TX* out, const TX* __restrict__ rdot, double* part, KrylovScalars* sc,
+            const double* rr_part, int rr_nparts) {
+  if (FWD) {
+    if (converged_guard(sc, rr_part, rr_nparts)) return;
+  } else if (sc && block_flag(&sc->done)) {
+    return;
+  }
+  constexpr int BB = B * B;
+  const int lane = threadIdx.x % LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned g = threadIdx.x / LPR, ng = blockDim.x / LPR;
+  double dacc = 0.0;
+  for (unsigned l = 0; l < nlev; l++) {
+    const unsigned p0 = __ldg(lvl + l), p1 = __ldg(lvl + l + 1);
+    for (unsigned pb = p0; pb < p1; pb += ng) {
+      const unsigned p = pb + g;
+      const bool valid = p < p1;
+      unsigned i = 0, s0 = 0, s1 = 0;
+      if (valid) {
+        i = __ldg(order + p);
+        if (FWD) { s0 = __ldg(rowptr + i); s1 = __ldg(diaind + i); }
+        else { s0 = __ldg(diaind + i); s1 = __ldg(rowptr + i + 1); }
+      }
+      double acc[B];
+#pragma unroll
+      for (int r = 0; r < B; r++) acc[r] = 0.0;
+      for (unsigned s = s0 + lane; s < s1; s += LPR) {
+        const unsigned col = __ldg(colind + s);
+        TV mv[BB];
+#pragma unroll
+        for (int e = 0; e < BB; e++) mv[e] = __ldg(foff + (size_t)s * BB + e);
+        TX xv[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = out[(size_t)col * B + c];
+        block_mv<B>(acc, mv, xv);
+      }
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+      if (valid && lane == 0) {
+        double t[B];
+#pragma unroll
+        for (int r = 0; r < B; r++) t[r] = (double)in[(size_t)i * B + r] - acc[r];
+#pragma unroll
+        for (int r = 0; r < B; r++) {
+          double o = t[r];
+          if (FWD) {
+            const double* d = fdiag + (size_t)i * BB + r * B;
+            o = 0.0;
+#pragma unroll
+            for (int c = 0; c < B; c++) o += d[c] * t[c];
+          }
+          const TX v = (TX)o;
+          out[(size_t)i * B + r] = v;
+          if (DOT) dacc += (double)rdot[(size_t)i * B + r] * (double)v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (DOT) block_partial<1024>(dacc, part);
+}
+
+template <int LPR, bool FWD, bool DOT>
+__global__ void __launch_bounds__(1024)
+k_zsweep_cta(unsigned nlev, const unsigned* __restrict__ lvl, const unsigned* __restrict__ order,
+             const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+             const unsigned* __restrict__ diaind, const double2* __restrict__ fdiag,
+             const double2* __restrict__ foff, const double2* __restrict__ in, double2* out,
+             const double2* __restrict__ rdot, double* part, KrylovScalars* sc, const double* rr_part,
+             int rr_nparts) {
+  if (FWD) {
+    if (converged_guard(sc, rr_part, rr_nparts)) return;
+  } else if (sc && block_flag(&sc->done)) {
+    return;
+  }
+  const int lane = threadIdx.x % LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned g = threadIdx.x / LPR, ng = blockDim.x / LPR;
+  double dre = 0.0, dim = 0.0;
+  for (unsigned l = 0; l < nlev; l++) {
+    const unsigned p0 = __ldg(lvl + l), p1 = __ldg(lvl + l + 1);
+    for (unsigned pb = p0; pb < p1; pb += ng) {
+      const unsigned p = pb + g;
+      const bool valid = p < p1;
+      unsigned i = 0, s0 = 0, s1 = 0;
+      if (valid) {
+        i = __ldg(order + p);
+        if (FWD) { s0 = __ldg(rowptr + i); s1 = __ldg(diaind + i); }
+        else { s0 = __ldg(diaind + i); s1 = __ldg(rowptr + i + 1); }
+      }
+      double re = 0.0, im = 0.0;
+      for (unsigned s = s0 + lane; s < s1; s += LPR) {
+        const double2 m = __ldg(foff + s);
+        const double2 xv = out[__ldg(colind + s)];
+        re += m.x * xv.x - m.y * xv.y;
+        im += m.x * xv.y + m.y * xv.x;
+      }
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(gmask, re, o);
+        im += __shfl_xor_sync(gmask, im, o);
+      }
+      if (valid && lane == 0) {
+        const double2 v_in = in[i];
+        double tr = v_in.x - re, ti = v_in.y - im;
+        if (FWD) {
+          const double2 d = fdiag[i];
+          const double a = d.x * tr - d.y * ti, b = d.x * ti + d.y * tr;
+          tr = a; ti = b;
+        }
+        out[i] = make_double2(tr, ti);
+        if (DOT) {
+          const double2 rv = rdot[i];
+          dre += rv.x * tr - rv.y * ti;
+          dim += rv.x * ti + rv.y * tr;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (DOT) {
+    block_partial<1024>(dre, part);
+    block_partial<1024>(dim, part + kMaxBlocks);
+  }
+}
+
+// -------------------------------------------------------------- utilities
+__global__ void k_fill_sentinel(double* v, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    v[k] = Sent<double>::value();
+}
+
+__global__ void k_wait_selftest(const double* never, DevStatus* st, uint64_t wait_ns) {
+  (void)poll_value(never, st, wait_ns, 99);
+}
+
+// ---------------------------------------------------------------- launches
+static int coop_grid(const void* fn, int threads, int nsm, int cap) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0) != cudaSuccess) return -1;
+  per_sm = std::max(1, std::min(per_sm, 8));
+  return std::max(1, std::min(per_sm * nsm, cap));
+}
+
+// Co-resident persistent launch (cooperative attribute: all blocks resident).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_coop(void (*fn)(KArgs...), int grid, int threads, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fn, static_cast<KArgs>(args)...);
+}
+
+int ilu_factor_launch(dfm_ilu M, dfm_mat A) {
+  dfm_ctx c = M->ctx;
+  cudaStream_t s = c->stream;
+  const size_t vw = M->vw();
+  DFM_CUDA_TRY(cudaMemcpyAsync(M->d_fdiag, A->d_diag, sizeof(double) * vw * M->N, cudaMemcpyDeviceToDevice, s));
+  if (M->ncrs)
+    DFM_CUDA_TRY(cudaMemcpyAsync(M->d_foff, A->d_off, sizeof(double) * vw * M->ncrs, cudaMemcpyDeviceToDevice, s));
+  DFM_CUDA_TRY(cudaMemsetAsync(&c->d_status->nsing, 0, sizeof(unsigned), s));
+  M->epoch++;
+  if (M->epoch == 0) {  // wrapped: clear the epochs
+    DFM_CUDA_TRY(cudaMemsetAsync(M->d_flags, 0, sizeof(unsigned) * M->N, s));
+    M->epoch = 1;
+  }
+  if (M->N == 0) return DFM_OK;
+  cudaError_t e;
+  if (M->vt == DFM_COMPLEX) {
+    const int grid = coop_grid((const void*)k_zilu0_factor, 256, c->nsm, (M->N + 7) / 8);
+    e = launch_coop(k_zilu0_factor, grid, 256, s, M->N, (const unsigned*)M->A->d_rowptr,
+                    (const unsigned*)M->A->d_colind, (const unsigned*)M->d_diaind, (const unsigned*)M->d_order_f,
+                    reinterpret_cast<double2*>(M->d_fdiag), reinterpret_cast<double2*>(M->d_foff), M->d_flags,
+                    M->epoch, c->d_status, (uint64_t)c->wait_ns);
+  } else {
+#define DFM_ILU_CASE(BV)                                                                                      \
+  case BV: {                                                                                                  \
+    const int grid = coop_grid((const void*)k_ilu0_factor<BV>, 256, c->nsm, (M->N + 7) / 8);                  \
+    e = launch_coop(k_ilu0_factor<BV>, grid, 256, s, M->N, (const unsigned*)M->A->d_rowptr,                   \
+                    (const unsigned*)M->A->d_colind, (const unsigned*)M->d_diaind,                           \
+                    (const unsigned*)M->d_order_f, M->d_fdiag, M->d_foff, M->d_flags, M->epoch, c->d_status, \
+                    (uint64_t)c->wait_ns);                                                                    \
+  } break;
+    switch (M->b) {
+      DFM_ILU_CASE(1)
+      DFM_ILU_CASE(2)
+      DFM_ILU_CASE(3)
+      default: return DFM_ERR_UNSUPPORTED;
+    }
+#undef DFM_ILU_CASE
+  }
+  DFM_CUDA_TRY(e);
+  return DFM_OK;
+}
+
+int ilu_fill_sentinel(dfm_ilu M, double* v, size_t n) {
+  if (n == 0) return DFM_OK;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)M->ctx->nsm * 8);
+  k_fill_sentinel<<<grid, 256, 0, M->ctx->stream>>>(v, n);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+static int sweep_lanes(dfm_ilu M) { return M->b == 3 ? 16 : 8; }
+
+template <int B, int LPR, bool FWD, bool DOT>
+static const void* syncfree_fn() { return (const void*)k_sweep_syncfree<B, LPR, double, double, FWD, DOT>; }
+
+int sweep_grid(dfm_ilu M, int sweep) {
+  if (sweep == 2) return 1;
+  // every sync-free kernel here has the same resource profile class; size by the B=3 bwd+dot one
+  const void* fn = (M->vt == DFM_COMPLEX) ? (const void*)k_zsweep_syncfree<8, false, true>
+                                          : syncfree_fn<3, 16, false, true>();
+  const int lpr = sweep_lanes(M);
+  const int rows_per_block = 256 / lpr;
+  const int g = coop_grid(fn, 256, M->ctx->nsm, (int)std::min<unsigned>((M->N + rows_per_block - 1) / rows_per_block, kMaxBlocks));
+  return std::max(1, g);
+}
+
+template <int B, int LPR, bool FWD>
+static cudaError_t sweep_real(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
+                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  dfm_ctx c = M->ctx;
+  const unsigned* order = FWD ? M->d_order_f : M->d_order_b;
+  if (sweep == 2) {
+    const unsigned* lvl = FWD ? M->d_lvl_f : M->d_lvl_b;
+    const unsigned nlev = FWD ? M->nlev_f : M->nlev_b;
+    if (part)
+      k_sweep_cta<B, LPR, double, double, FWD, true><<<1, 1024, 0, c->stream>>>(
+          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, M->d_foff, in, out, rdot, part,
+          sc, rr_part, rr_n);
+    else
+      k_sweep_cta<B, LPR, double, double, FWD, false><<<1, 1024, 0, c->stream>>>(
+          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, M->d_foff, in, out, rdot,
+          nullptr, sc, rr_part, rr_n);
+    return cudaGetLastError();
+  }
+  const int grid = sweep_grid(M, 1);
+  if (part)
+    return launch_coop(k_sweep_syncfree<B, LPR, double, double, FWD, true>, grid, 256, c->stream, M->N, order,
+                       (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
+                       (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, (const double*)M->d_foff, in, out,
+                       rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+  return launch_coop(k_sweep_syncfree<B, LPR, double, double, FWD, false>, grid, 256, c->stream, M->N, order,
+                     (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
+                     (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, (const double*)M->d_foff, in, out,
+                     rdot, (double*)nullptr, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+}
+
+template <int LPR, bool FWD>
+static cudaError_t sweep_cplx(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
+                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  dfm_ctx c = M->ctx;
+  const unsigned* order = FWD ? M->d_order_f : M->d_order_b;
+  auto* fd = reinterpret_cast<const double2*>(M->d_fdiag);
+  auto* fo = reinterpret_cast<const double2*>(M->d_foff);
+  auto* vi = reinterpret_cast<const double2*>(in);
+  auto* vo = reinterpret_cast<double2*>(out);
+  auto* rd = reinterpret_cast<const double2*>(rdot);
+  if (sweep == 2) {
+    const unsigned* lvl = FWD ? M->d_lvl_f : M->d_lvl_b;
+    const unsigned nlev = FWD ? M->nlev_f : M->nlev_b;
+    if (part)
+      k_zsweep_cta<LPR, FWD, true><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr, M->A->d_colind,
+                                                              M->d_diaind, fd, fo, vi, vo, rd, part, sc, rr_part,
+                                                              rr_n);
+    else
+      k_zsweep_cta<LPR, FWD, false><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr, M->A->d_colind,
+                                                               M->d_diaind, fd, fo, vi, vo, rd, nullptr, sc,
+                                                               rr_part, rr_n);
+    return cudaGetLastError();
+  }
+  const int grid = sweep_grid(M, 1);
+  if (part)
+    return launch_coop(k_zsweep_syncfree<LPR, FWD, true>, grid, 256, c->stream, M->N, order,
+                       (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
+                       (const unsigned*)M->d_diaind, fd, fo, vi, vo, rd, part, sc, rr_part, rr_n, c->d_status,
+                       (uint64_t)c->wait_ns);
+  return launch_coop(k_zsweep_syncfree<LPR, FWD, false>, grid, 256, c->stream, M->N, order,
+                     (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind, (const unsigned*)M->d_diaind,
+                     fd, fo, vi, vo, rd, (double*)nullptr, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+}
+
+static int sweep_dispatch(dfm_ilu M, bool fwd, int sweep, const double* in, double* out, const double* rdot,
+                          double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  if (M->N == 0) return DFM_OK;
+  if (sweep <= 0) sweep = M->sweep > 0 ? M->sweep : 1;
+  cudaError_t e;
+  if (M->vt == DFM_COMPLEX) {
+    e = fwd ? sweep_cplx<8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
+            : sweep_cplx<8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+  } else if (M->b == 1) {
+    e = fwd ? sweep_real<1, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
+            : sweep_real<1, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+  } else if (M->b == 2) {
+    e = fwd ? sweep_real<2, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
+            : sweep_real<2, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+  } else {
+    e = fwd ? sweep_real<3, 16, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
+            : sweep_real<3, 16, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+  }
+  DFM_CUDA_TRY(e);
+  return DFM_OK;
+}
+
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep) {
+  return sweep_dispatch(M, true, sweep, r, y, nullptr, nullptr, sc, sc ? M->ctx->part(2) : nullptr,
+                        sc ? spmv_grid(M->A) : 0);
+}
+
+int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part, KrylovScalars* sc,
+                   int sweep) {
+  return sweep_dispatch(M, false, sweep, y, z, rdot, dot_part, sc, nullptr, 0);
+}
+
+// Autotuner for the sweep schedule: times one forward+backward application
+// with each schedule (best of 3) and keeps the faster one.
+int ilu_autotune(dfm_ilu M) {
+  if (M->sweep > 0) return DFM_OK;
+  if (M->N == 0) { M->sweep = 1; return DFM_OK; }
+  cudaStream_t s = M->ctx->stream;
+  const size_t n = (size_t)M->N * M->xw();
+  double *r = nullptr, *z = nullptr;
+  DFM_CUDA_TRY(cudaMallocAsync(&r, n * sizeof(double), s));
+  DFM_CUDA_TRY(cudaMallocAsync(&z, n * sizeof(double), s));
+  DFM_CUDA_TRY(cudaMemsetAsync(r, 0, n * sizeof(double), s));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_mode = 1;
+  for (int mode = 1; mode <= 2; mode++) {
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      int rc = ilu_fill_sentinel(M, M->d_tmp, n);
+      rc |= ilu_fill_sentinel(M, z, n);
+      cudaEventRecord(e0, s);
+      rc |= ilu_fwd_launch(M, r, M->d_tmp, nullptr, mode);
+      rc |= ilu_bwd_launch(M, M->d_tmp, z, nullptr, nullptr, nullptr, mode);
+      cudaEventRecord(e1, s);
+      if (rc) return rc;
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) tmin = std::min(tmin, ms);
+    }
+    if (tmin < best) { best = tmin; best_mode = mode; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(r, s);
+  cudaFreeAsync(z, s);
+  DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  M->sweep = best_mode;
+  return DFM_OK;
+}
+
+int ilu_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns) {
+  double* flag = nullptr;
+  DFM_CUDA_TRY(cudaMallocAsync(&flag, sizeof(double), ctx->stream));
+  k_fill_sentinel<<<1, 32, 0, ctx->stream>>>(flag, 1);
+  k_wait_selftest<<<1, 1, 0, ctx->stream>>>(flag, ctx->d_status, (uint64_t)limit_ns);
+  DFM_CUDA_TRY(cudaGetLastError());
+  DFM_CUDA_TRY(cudaFreeAsync(flag, ctx->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return DFM_OK;
+}
+
+}  // namespace dfm

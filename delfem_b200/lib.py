@@ -1,0 +1,289 @@
+"""ctypes binding of the C ABI (include/dfm_b200.h) and thin Python handles.
+
+The CUDA library is required: importing works without it, but every call that
+needs it raises if delfem_b200/_lib/libdfm_b200.so is missing or no CUDA device
+is visible.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED = range(9)
+REAL, COMPLEX = 0, 1
+HOST, DEVICE = 0, 1
+
+_lib = None
+
+_vp, _u, _i, _d = C.c_void_p, C.c_uint, C.c_int, C.c_double
+_up, _dp, _ip = C.POINTER(C.c_uint), C.POINTER(C.c_double), C.POINTER(C.c_int)
+
+# name -> (restype, argtypes); every symbol declared in include/dfm_b200.h
+PROTOS = {
+    "dfm_status_string": (C.c_char_p, [_i]),
+    "dfm_abi_version": (_i, []),
+    "dfm_ctx_create": (_i, [_i, C.POINTER(_vp)]),
+    "dfm_ctx_destroy": (_i, [_vp]),
+    "dfm_ctx_set_stream": (_i, [_vp, _vp]),
+    "dfm_ctx_sync": (_i, [_vp]),
+    "dfm_ctx_set_wait_limit": (_i, [_vp, C.c_ulonglong]),
+    "dfm_ctx_take_error": (_i, [_vp, _ip, _ip]),
+    "dfm_ctx_wait_selftest": (_i, [_vp, C.c_ulonglong]),
+    "dfm_mat_create": (_i, [_vp, _u, _u, _i, _up, _up, C.POINTER(_vp)]),
+    "dfm_mat_destroy": (_i, [_vp]),
+    "dfm_mat_info": (_i, [_vp, _up, _up, _up, _ip]),
+    "dfm_mat_set_zero": (_i, [_vp]),
+    "dfm_mat_set_values": (_i, [_vp, _vp, _vp, _i]),
+    "dfm_mat_get_values": (_i, [_vp, _vp, _vp, _i]),
+    "dfm_mat_values_device": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
+    "dfm_mat_set_spmv_lanes": (_i, [_vp, _i]),
+    "dfm_mat_get_spmv_lanes": (_i, [_vp, _ip]),
+    "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
+    "dfm_ilu_create": (_i, [_vp, C.POINTER(_vp)]),
+    "dfm_ilu_destroy": (_i, [_vp]),
+    "dfm_ilu_levels": (_i, [_vp, _up, _up, _up, _up]),
+    "dfm_ilu_factor": (_i, [_vp, _vp, _up]),
+    "dfm_ilu_get_values": (_i, [_vp, _vp, _vp, _i]),
+    "dfm_ilu_set_values": (_i, [_vp, _vp, _vp, _i]),
+    "dfm_ilu_apply": (_i, [_vp, _vp, _vp]),
+    "dfm_ilu_set_sweep": (_i, [_vp, _i]),
+    "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
+    "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_pcg_host": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+}
+
+
+class DfmError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = code
+        msg = lib().dfm_status_string(code).decode() if _lib is not None else str(code)
+        super().__init__(f"{where}: {msg} ({code})")
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (no GPU needed for loading)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing; build it with `python -m delfem_b200.build`")
+        L = C.CDLL(path)
+        for name, (res, args) in PROTOS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def lib():
+    return load()
+
+
+def check(rc: int, where: str = "", allow=(OK,)):
+    if rc not in allow:
+        raise DfmError(rc, where)
+    return rc
+
+
+def _ptr(t):
+    """Device (or host) address of a torch tensor / numpy array."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return t.ctypes.data_as(C.c_void_p)
+
+
+def _sync_torch():
+    """Order the caller's torch work (default stream) before a library call,
+    which runs on the context's own stream."""
+    import torch
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.current_stream().synchronize()
+
+
+def _require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("delfem_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+class Context:
+    def __init__(self, device: int = 0, use_torch_stream: bool = False):
+        torch = _require_cuda()
+        self.device = device
+        h = C.c_void_p()
+        check(lib().dfm_ctx_create(device, C.byref(h)), "dfm_ctx_create")
+        self.h = h
+        if use_torch_stream:
+            s = torch.cuda.current_stream(device).cuda_stream
+            check(lib().dfm_ctx_set_stream(self.h, C.c_void_p(s)), "dfm_ctx_set_stream")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(lib().dfm_ctx_sync(self.h), "dfm_ctx_sync")
+
+    def take_error(self):
+        code, where = C.c_int(), C.c_int()
+        check(lib().dfm_ctx_take_error(self.h, C.byref(code), C.byref(where)))
+        return code.value, where.value
+
+    def set_wait_limit(self, ns: int):
+        check(lib().dfm_ctx_set_wait_limit(self.h, ns))
+
+    def wait_selftest(self, ns: int) -> int:
+        return lib().dfm_ctx_wait_selftest(self.h, ns)
+
+
+class Matrix:
+    """MatVec::CMatDia_BlkCrs on the device (reference block-CRS layout)."""
+
+    def __init__(self, ctx: Context, rowptr, colind, b: int, vtype: int = REAL):
+        self.ctx = ctx
+        rp = np.ascontiguousarray(rowptr, np.uint32)
+        ci = np.ascontiguousarray(colind, np.uint32)
+        ci_ = ci if ci.size else np.zeros(1, np.uint32)
+        h = C.c_void_p()
+        check(lib().dfm_mat_create(ctx.h, rp.size - 1, b, vtype, rp.ctypes.data_as(_up), ci_.ctypes.data_as(_up),
+                                   C.byref(h)), "dfm_mat_create")
+        self.h = h
+        self.N, self.b, self.ncrs, self.vtype = rp.size - 1, b, ci.size, vtype
+        self.rowptr, self.colind = rp, ci
+        self.vw = 2 if vtype == COMPLEX else b * b
+        self.xw = 2 if vtype == COMPLEX else b
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_mat_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_values(self, diag, off):
+        where = DEVICE if hasattr(diag, "data_ptr") and diag.is_cuda else HOST
+        if where == HOST:
+            diag = np.ascontiguousarray(diag, np.float64)
+            off = np.ascontiguousarray(off, np.float64)
+        if where == DEVICE:
+            _sync_torch()
+        check(lib().dfm_mat_set_values(self.h, _ptr(diag), _ptr(off), where), "dfm_mat_set_values")
+
+    def get_values(self):
+        d = np.zeros(self.N * self.vw)
+        o = np.zeros(max(self.ncrs, 1) * self.vw)
+        check(lib().dfm_mat_get_values(self.h, _ptr(d), _ptr(o), HOST), "dfm_mat_get_values")
+        return d, o[: self.ncrs * self.vw]
+
+    def spmv(self, alpha, x, beta, y):
+        _sync_torch()
+        check(lib().dfm_spmv(self.h, alpha, _ptr(x), beta, _ptr(y)), "dfm_spmv")
+        return y
+
+    @property
+    def lanes(self):
+        v = C.c_int()
+        check(lib().dfm_mat_get_spmv_lanes(self.h, C.byref(v)))
+        return v.value
+
+    @lanes.setter
+    def lanes(self, v):
+        check(lib().dfm_mat_set_spmv_lanes(self.h, int(v)))
+
+
+class ILU:
+    """LsSol::CPreconditioner_ILU(0) on the device."""
+
+    def __init__(self, A: Matrix):
+        self.A = A
+        h = C.c_void_p()
+        check(lib().dfm_ilu_create(A.h, C.byref(h)), "dfm_ilu_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_ilu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def levels(self):
+        nf, nb = C.c_uint(), C.c_uint()
+        lf = np.zeros(max(self.A.N, 1), np.uint32)
+        lb = np.zeros(max(self.A.N, 1), np.uint32)
+        check(lib().dfm_ilu_levels(self.h, C.byref(nf), C.byref(nb), lf.ctypes.data_as(_up),
+                                   lb.ctypes.data_as(_up)))
+        return lf[: self.A.N], nf.value, lb[: self.A.N], nb.value
+
+    def factor(self, A: Matrix | None = None, allow=(OK,)):
+        ns = C.c_uint()
+        rc = lib().dfm_ilu_factor(self.h, (A or self.A).h, C.byref(ns))
+        check(rc, "dfm_ilu_factor", allow)
+        return rc, ns.value
+
+    def get_values(self):
+        d = np.zeros(self.A.N * self.A.vw)
+        o = np.zeros(max(self.A.ncrs, 1) * self.A.vw)
+        check(lib().dfm_ilu_get_values(self.h, _ptr(d), _ptr(o), HOST), "dfm_ilu_get_values")
+        return d, o[: self.A.ncrs * self.A.vw]
+
+    def set_values(self, diag, off):
+        diag = np.ascontiguousarray(diag, np.float64)
+        off = np.ascontiguousarray(off if np.size(off) else np.zeros(1), np.float64)
+        check(lib().dfm_ilu_set_values(self.h, _ptr(diag), _ptr(off), HOST), "dfm_ilu_set_values")
+
+    def apply(self, r, z):
+        _sync_torch()
+        check(lib().dfm_ilu_apply(self.h, _ptr(r), _ptr(z)), "dfm_ilu_apply")
+        return z
+
+    @property
+    def sweep(self):
+        v = C.c_int()
+        check(lib().dfm_ilu_get_sweep(self.h, C.byref(v)))
+        return v.value
+
+    @sweep.setter
+    def sweep(self, v):
+        check(lib().dfm_ilu_set_sweep(self.h, int(v)))
+
+
+def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """LsSol::Solve_PCG on device vectors; returns (status, iters, conv)."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_pcg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pcg", allow)
+    return rc, it.value, conv.value
+
+
+def solve_pcg_host(A: Matrix, M: ILU, b, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b)
+    it, conv = C.c_uint(), C.c_double()
+    rc = lib().dfm_solve_pcg_host(A.h, M.h, _ptr(b), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pcg_host", allow)
+    return rc, x, it.value, conv.value

@@ -1,0 +1,133 @@
+/* dfm_b200.h - C ABI of the B200-native DelFEM linear-solve path.
+ *
+ * One shared library (delfem_b200/_lib/libdfm_b200.so, sm_100a) replaces the
+ * reference's CPU hot path behind its own interfaces:
+ *   LsSol::ILinearSystem(Preconditioner)_Sol  include/delfem/ls/linearsystem_interface_solver.h:39-82
+ *   LsSol::CPreconditioner(_ILU)               include/delfem/ls/preconditioner.h:46-108
+ *   LsSol::Solve_PCG / Solve_PBiCGSTAB         include/delfem/ls/solver_ls_iter.h:35-45
+ *   Fem::Ls::Solve_PCOCG                       include/delfem/femls/zsolver_ls_iter.h:53-54
+ *   MatVec::CMatDia_BlkCrs / CMatDiaFrac_BlkCrs include/delfem/matvec/matdia_blkcrs.h:44-118,
+ *                                              include/delfem/matvec/matdiafrac_blkcrs.h:40-313
+ * The C++ adapters in include/dfm_b200_lsol.hpp mirror those classes on top of
+ * this ABI.
+ *
+ * Conventions
+ *  - Storage is the reference's block-CRS with a separate diagonal: rowptr[N+1]
+ *    (its m_colInd_Blk), colind[ncrs] (its m_rowPtr_Blk: off-diagonal columns,
+ *    strictly ascending per row), diag[N*b*b], off[ncrs*b*b], each b x b block
+ *    row-major; complex matrices (b = 1) store interleaved (re, im) doubles.
+ *  - Vectors passed to compute calls are DEVICE pointers (cudaMalloc'd or
+ *    torch tensors) of N*b doubles (2*N for complex).  Calls ending in _host
+ *    take host pointers and include the copies.
+ *  - Every call returns a dfm_status; nothing exits, asserts or waits for input.
+ *  - Calls on one context are issued on its stream and are not re-entrant.
+ */
+#ifndef DFM_B200_H
+#define DFM_B200_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define DFM_API __attribute__((visibility("default")))
+#else
+#define DFM_API
+#endif
+
+typedef enum dfm_status {
+  DFM_OK = 0,
+  DFM_ERR_INVALID = 1,       /* bad argument or inconsistent pattern (validated on the host) */
+  DFM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  DFM_ERR_NOMEM = 3,         /* device allocation failed */
+  DFM_NOT_CONVERGED = 4,     /* max_iter reached (the reference's `false` of Solve_PCG) */
+  DFM_BREAKDOWN = 5,         /* p.Ap <= 0, rho == 0 or a non-finite scalar */
+  DFM_SINGULAR_PIVOT = 6,    /* more than 10 singular ILU pivots (reference nmax_sing) */
+  DFM_WAIT_TIMEOUT = 7,      /* a bounded device-side wait ran out */
+  DFM_ERR_UNSUPPORTED = 8    /* block size / value type not supported by this entry */
+} dfm_status;
+
+enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
+enum { DFM_HOST = 0, DFM_DEVICE = 1 };
+
+typedef struct dfm_ctx_s* dfm_ctx;
+typedef struct dfm_mat_s* dfm_mat;
+typedef struct dfm_ilu_s* dfm_ilu;
+
+DFM_API const char* dfm_status_string(int status);
+DFM_API int dfm_abi_version(void);
+
+/* ---- context: device, stream, device status word ---------------------- */
+DFM_API int dfm_ctx_create(int device, dfm_ctx* out);
+DFM_API int dfm_ctx_destroy(dfm_ctx ctx);
+/* Issue work on `stream` (a cudaStream_t; NULL restores the context's own). */
+DFM_API int dfm_ctx_set_stream(dfm_ctx ctx, void* stream);
+DFM_API int dfm_ctx_sync(dfm_ctx ctx);
+/* Time limit of every device-side spin-wait (default 2 s). */
+DFM_API int dfm_ctx_set_wait_limit(dfm_ctx ctx, unsigned long long ns);
+/* First device-side error since the last call (code, kernel id); clears it. */
+DFM_API int dfm_ctx_take_error(dfm_ctx ctx, int* code, int* where);
+/* Failure-detection self test: one kernel waits on a flag nothing sets, under
+ * the given limit, and must come back with DFM_WAIT_TIMEOUT. */
+DFM_API int dfm_ctx_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns);
+
+/* ---- matrix: CMatDia_BlkCrs on the device ------------------------------ */
+/* Pattern from host arrays; validated (monotone rowptr, in-range, strictly
+ * ascending off-diagonal columns, no diagonal entry) as CMatDia_BlkCrs::AddPattern
+ * (src/matvec/matdia_blkcrs.cpp:346-505) requires.  b in {1,2,3} (real) or 1 (complex). */
+DFM_API int dfm_mat_create(dfm_ctx ctx, unsigned N, unsigned b, int value_type,
+                   const unsigned* rowptr, const unsigned* colind, dfm_mat* out);
+DFM_API int dfm_mat_destroy(dfm_mat A);
+DFM_API int dfm_mat_info(dfm_mat A, unsigned* N, unsigned* b, unsigned* ncrs, int* value_type);
+/* CMatDia_BlkCrs::SetZero (src/matvec/matdia_blkcrs.cpp:139-163). */
+DFM_API int dfm_mat_set_zero(dfm_mat A);
+DFM_API int dfm_mat_set_values(dfm_mat A, const double* diag, const double* off, int where);
+DFM_API int dfm_mat_get_values(dfm_mat A, double* diag, double* off, int where);
+/* Device addresses of the value arrays (owned by A). */
+DFM_API int dfm_mat_values_device(dfm_mat A, double** diag, double** off);
+/* Lanes per block row of the SpMV (4, 8, 16, 32); 0 = autotuned on first use. */
+DFM_API int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes);
+DFM_API int dfm_mat_get_spmv_lanes(dfm_mat A, int* lanes);
+
+/* y = beta*y + alpha*A x  (CMatDia_BlkCrs::MatVec, src/matvec/matdia_blkcrs.cpp:921-1094;
+ * complex: CZMatDia_BlkCrs::MatVec, src/matvec/zmatdia_blkcrs.cpp:737-801).
+ * beta == 0 writes y without reading it. */
+DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, double* y);
+
+/* ---- ILU(0): CPreconditioner_ILU / CMatDiaFrac_BlkCrs ------------------- */
+/* Symbolic ILU(0) (CMatDiaFrac_BlkCrs(0, A), src/matvec/matdiafrac_blkcrs.cpp:227-287)
+ * plus the level sets of both sweeps in the natural order. */
+DFM_API int dfm_ilu_create(dfm_mat A, dfm_ilu* out);
+DFM_API int dfm_ilu_destroy(dfm_ilu M);
+/* Level counts; lev_fwd / lev_bwd (host, N entries each, nullable) get the level of every row. */
+DFM_API int dfm_ilu_levels(dfm_ilu M, unsigned* nlev_fwd, unsigned* nlev_bwd, unsigned* lev_fwd,
+                   unsigned* lev_bwd);
+/* Numeric ILU(0) of A on the device (DoILUDecomp, :769-1102), bit-identical to the
+ * reference.  Returns DFM_SINGULAR_PIVOT when more than 10 pivots are singular. */
+DFM_API int dfm_ilu_factor(dfm_ilu M, dfm_mat A, unsigned* n_singular);
+DFM_API int dfm_ilu_get_values(dfm_ilu M, double* diag, double* off, int where);
+DFM_API int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int where);
+/* z = U^-1 L^-1 r (ForwardSubstitution + BackwardSubstitution, :332-663).  r != z. */
+DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
+/* Sweep schedule: 0 = autotuned, 1 = sync-free across the GPU, 2 = one CTA with
+ * level barriers. */
+DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
+DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
+
+/* ---- Krylov solvers ------------------------------------------------------ */
+/* LsSol::Solve_PCG (src/ls/solver_ls_iter.cpp:100-172) preconditioned by M:
+ * r holds b on entry and the recursive residual on exit, x receives the
+ * solution (x = 0 initial guess).  *iters follows the reference: the 0-based
+ * index of the converged iteration.  DFM_NOT_CONVERGED at maxit. */
+DFM_API int dfm_solve_pcg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
+                  unsigned* iters, double* conv);
+/* The same with host buffers: copies b in, x out (end-to-end call). */
+DFM_API int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol,
+                       unsigned maxit, unsigned* iters, double* conv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,77 @@
+"""Seeded problem builders shared by the tests: each returns the mesh and the
+oracle system (oracle/dfm_oracle.c) assembled with the reference's kernels,
+Dirichlet elimination applied."""
+from __future__ import annotations
+
+import numpy as np
+
+from delfem_b200 import meshes
+from oracle import port as P
+
+NU = 0.3
+LAM3 = 1.0 * NU / ((1 + NU) * (1 - 2 * NU))
+MYU3 = 1.0 / (2 * (1 + NU))
+LAM2_PS = NU / (1 - NU * NU)        # plane-stress lambda* at E = 1
+MYU2 = 1.0 / (2 * (1 + NU))
+WAVE_LENGTH = 2 * 3.1416 / 20       # k = 20 with the reference's truncated pi
+
+
+def poisson(n, coef=None):
+    m = meshes.unit_square_tri(n)
+    rp, ci = P.pattern(m.nnode, m.elem)
+    S = P.System(rp, ci, 1)
+    S.asm_poisson(m, 1.0, 1.0, coef)
+    S.apply_bc(P.bc_flags_from_bnd(m.nnode, 1, m.bnd))
+    return m, S
+
+
+def solid2d(n, theta=None):
+    m = meshes.unit_square_tri(n, bnd="left")
+    rp, ci = P.pattern(m.nnode, m.elem)
+    S = P.System(rp, ci, 2)
+    S.asm_solid2d(m, LAM2_PS, MYU2, 0.0, 0.0, 0.0, theta)
+    S.rhs += meshes.right_edge_traction(m, n).ravel()
+    S.apply_bc(P.bc_flags_from_bnd(m.nnode, 2, m.bnd))
+    return m, S
+
+
+def solid3d(nx, ny, nz):
+    m = meshes.box_tet(nx, ny, nz)
+    rp, ci = P.pattern(m.nnode, m.elem)
+    S = P.System(rp, ci, 3)
+    S.asm_solid3d(m, LAM3, MYU3, 1.0, 0.0, 0.0, -1.0)
+    S.apply_bc(P.bc_flags_from_bnd(m.nnode, 3, m.bnd))
+    return m, S
+
+
+def helmholtz(nring):
+    m = meshes.unit_disk_tri(nring)
+    rp, ci = P.pattern(m.nnode, m.elem)
+    S = P.System(rp, ci, 1, cplx=True)
+    S.asm_helmholtz(m, WAVE_LENGTH)
+    S.rhs += meshes.gaussian_source_load(m).ravel()
+    return m, S
+
+
+def random_spd_like(N, b, seed=0, density=6):
+    """A random block pattern (symmetric) with diagonally dominant values."""
+    rng = np.random.default_rng(seed)
+    rows = [set() for _ in range(N)]
+    for i in range(N):
+        for j in rng.integers(0, N, size=rng.integers(0, density + 1)):
+            if j != i:
+                rows[i].add(int(j))
+                rows[int(j)].add(i)
+    rp = np.zeros(N + 1, np.uint32)
+    for i in range(N):
+        rp[i + 1] = rp[i] + len(rows[i])
+    ci = np.concatenate([np.array(sorted(r), np.uint32) for r in rows]) if rp[-1] else np.zeros(0, np.uint32)
+    S = P.System(rp, ci, b)
+    bb = b * b
+    S.off[:] = rng.standard_normal(S.off.size) * 0.1
+    d = np.zeros((N, b, b))
+    for i in range(N):
+        d[i] = np.eye(b) * (2.0 + rng.random()) + rng.standard_normal((b, b)) * 0.05
+    S.diag[:] = d.reshape(-1)
+    S.rhs[:] = rng.standard_normal(N * b)
+    return S
