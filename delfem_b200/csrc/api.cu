@@ -339,6 +339,8 @@ int dfm_ilu_destroy(dfm_ilu M) {
   if (!M) return DFM_OK;
   cudaStreamSynchronize(M->ctx->stream);
   pcg_release(M);
+  sweep_plan_free(&M->plan_f);
+  sweep_plan_free(&M->plan_b);
   cudaFree(M->d_diaind);
   cudaFree(M->d_order_f);
   cudaFree(M->d_order_b);
@@ -392,9 +394,16 @@ int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int whe
 }
 
 int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
-  if (!M || mode < 0 || mode > 2) return DFM_ERR_INVALID;
+  if (!M || mode < 0 || mode > 3) return DFM_ERR_INVALID;
+  if (mode == 3) return ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm);
   M->sweep = mode;
   return DFM_OK;
+}
+
+int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) {
+  if (!M || max_blocks < 0 || poll_sleep_ns > 100000) return DFM_ERR_INVALID;
+  M->sweep_blocks = max_blocks;
+  return set_poll_sleep(poll_sleep_ns);
 }
 
 int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {

@@ -3,7 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/dfm_b200.h"
+#include "dfm_b200.h"
 
 #define DFM_DEVINL __device__ __forceinline__
 
@@ -74,13 +74,26 @@ DFM_DEVINL void raise_error(DevStatus* st, int code, int where) {
   if (atomicCAS(&st->code, 0, code) == 0) st->where = where;
 }
 
-// Every spin-wait has a time limit (ns).  When it runs out the wait records
-// DFM_WAIT_TIMEOUT and returns false; the caller then stops waiting and the
-// kernel drains normally, so the context stays usable.
-struct WaitBudget {
-  uint64_t deadline;
-  DFM_DEVINL void start(uint64_t limit_ns) { deadline = globaltimer_ns() + limit_ns; }
-  DFM_DEVINL bool expired() const { return globaltimer_ns() > deadline; }
+// Every spin-wait has a time limit.  When it runs out the wait records
+// DFM_WAIT_TIMEOUT and gives up; the caller then stops waiting and the kernel
+// drains normally, so the context stays usable.  The limit is counted with the
+// SM cycle counter (a %globaltimer read costs far more than one poll and would
+// sit on the critical path of every hand-off), checked every 64 polls, as
+// 2 cycles per requested ns: never shorter than asked for at SM clocks up to
+// 2 GHz.
+DFM_DEVINL long long sm_clock() {
+#ifdef __CUDA_ARCH__
+  return clock64();
+#else
+  return 0;
+#endif
+}
+struct SpinGuard {
+  long long t0 = 0, budget = 0;
+  unsigned n = 0;
+  DFM_DEVINL explicit SpinGuard(uint64_t limit_ns) : t0(sm_clock()), budget((long long)(2 * limit_ns)) {}
+  // true once the budget is spent (evaluated every 64th call)
+  DFM_DEVINL bool expired() { return ((++n & 63u) == 0) && (sm_clock() - t0 > budget); }
 };
 
 // ---------------------------------------------------------------- reductions

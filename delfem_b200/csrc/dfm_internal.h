@@ -6,8 +6,9 @@
 #include <string>
 #include <vector>
 
-#include "../../include/dfm_b200.h"
+#include "dfm_b200.h"
 #include "common.cuh"
+#include "sweep.h"
 
 #define DFM_CUDA_TRY(expr)                                 \
   do {                                                     \
@@ -86,7 +87,10 @@ struct dfm_ilu_s {
   unsigned* d_flags = nullptr;   // per-row completion epochs of the numeric factorisation
   unsigned epoch = 0;
   double* d_tmp = nullptr;       // N*xw scratch: forward-sweep output of dfm_ilu_apply
-  int sweep = 0;                 // 0 untuned, 1 sync-free grid, 2 single CTA
+  int sweep = 0;                 // 0 untuned, 1 sync-free grid, 2 single CTA, 3 CTA row ranges
+  int sweep_blocks = 0;          // sync-free grid size cap (0 = all co-resident blocks)
+  dfm::SweepPlan plan_f, plan_b; // mode 3 plans (forward / backward)
+  float sweep_ms = 0.f;          // autotuned fwd+bwd time
   bool factored = false;
   size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }
   size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }
@@ -107,6 +111,15 @@ int ilu_fill_sentinel(dfm_ilu M, double* v, size_t n);
 int ilu_autotune(dfm_ilu M);
 int sweep_grid(dfm_ilu M, int sweep);
 int ilu_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns);
+int set_poll_sleep(unsigned ns);
+// sweep.cu
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P,
+                     bool direct_remote = true);
+void sweep_plan_free(SweepPlan* P);
+int sweep_plan_refresh(dfm_ilu M, SweepPlan* P);
+int ilu_set_ranges(dfm_ilu M, int G);
+int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
+                        KrylovScalars* sc, const double* rr_part, int rr_n);
 // krylov.cu
 int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
               double* conv);

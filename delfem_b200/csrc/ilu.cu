@@ -33,39 +33,36 @@ DFM_DEVINL int ld_status(const DevStatus* st) {
   return v;
 }
 
+// Back-off between polls (ns) of a sync-free sweep; 0 spins without sleeping.
+// Thousands of waiting lanes polling L2 back to back starve the stores that
+// would release them, so waiting lanes sleep briefly between polls.
+__constant__ unsigned c_poll_sleep_ns = 0;
+
 template <typename T>
 DFM_DEVINL T poll_value(const T* p, DevStatus* st, uint64_t wait_ns, int where) {
   T v = ld_relaxed(p);
   if (!Sent<T>::is(v)) return v;
-  uint64_t deadline = 0;
-  unsigned n = 0;
+  SpinGuard g(wait_ns);
+  const unsigned nap = c_poll_sleep_ns;
   for (;;) {
+    if (nap) __nanosleep(nap);
     v = ld_relaxed(p);
     if (!Sent<T>::is(v)) return v;
-    if ((++n & 31u) == 0) {
-      const uint64_t now = globaltimer_ns();
-      if (deadline == 0) deadline = now + wait_ns;
-      if (now > deadline || ld_status(st) != 0) {
-        raise_error(st, DFM_WAIT_TIMEOUT, where);
-        return v;
-      }
+    if (g.expired() || ((g.n & 1023u) == 0 && ld_status(st) != 0)) {
+      raise_error(st, DFM_WAIT_TIMEOUT, where);
+      return v;
     }
   }
 }
 
 DFM_DEVINL void wait_epoch(const unsigned* flag, unsigned epoch, DevStatus* st, uint64_t wait_ns, int where) {
   if (ld_acquire_u32(flag) == epoch) return;
-  uint64_t deadline = 0;
-  unsigned n = 0;
+  SpinGuard g(wait_ns);
   for (;;) {
     if (ld_acquire_u32(flag) == epoch) return;
-    if ((++n & 31u) == 0) {
-      const uint64_t now = globaltimer_ns();
-      if (deadline == 0) deadline = now + wait_ns;
-      if (now > deadline || ld_status(st) != 0) {
-        raise_error(st, DFM_WAIT_TIMEOUT, where);
-        return;
-      }
+    if (g.expired() || ((g.n & 1023u) == 0 && ld_status(st) != 0)) {
+      raise_error(st, DFM_WAIT_TIMEOUT, where);
+      return;
     }
   }
 }
@@ -590,6 +587,8 @@ int ilu_factor_launch(dfm_ilu M, dfm_mat A) {
   if (M->ncrs)
     DFM_CUDA_TRY(cudaMemcpyAsync(M->d_foff, A->d_off, sizeof(double) * vw * M->ncrs, cudaMemcpyDeviceToDevice, s));
   DFM_CUDA_TRY(cudaMemsetAsync(&c->d_status->nsing, 0, sizeof(unsigned), s));
+  M->plan_f.stale = true;  // packed sweep values are re-gathered on next use
+  M->plan_b.stale = true;
   M->epoch++;
   if (M->epoch == 0) {  // wrapped: clear the epochs
     DFM_CUDA_TRY(cudaMemsetAsync(M->d_flags, 0, sizeof(unsigned) * M->N, s));
@@ -639,13 +638,21 @@ static const void* syncfree_fn() { return (const void*)k_sweep_syncfree<B, LPR, 
 
 int sweep_grid(dfm_ilu M, int sweep) {
   if (sweep == 2) return 1;
+  if (sweep == 3) return std::max(1, M->plan_b.G);  // the backward sweep writes the (r, z) partials
   // every sync-free kernel here has the same resource profile class; size by the B=3 bwd+dot one
   const void* fn = (M->vt == DFM_COMPLEX) ? (const void*)k_zsweep_syncfree<8, false, true>
                                           : syncfree_fn<3, 16, false, true>();
   const int lpr = sweep_lanes(M);
   const int rows_per_block = 256 / lpr;
-  const int g = coop_grid(fn, 256, M->ctx->nsm, (int)std::min<unsigned>((M->N + rows_per_block - 1) / rows_per_block, kMaxBlocks));
+  int cap = (int)std::min<unsigned>((M->N + rows_per_block - 1) / rows_per_block, kMaxBlocks);
+  if (M->sweep_blocks > 0) cap = std::min(cap, M->sweep_blocks);
+  const int g = coop_grid(fn, 256, M->ctx->nsm, cap);
   return std::max(1, g);
+}
+
+int set_poll_sleep(unsigned ns) {
+  DFM_CUDA_TRY(cudaMemcpyToSymbol(c_poll_sleep_ns, &ns, sizeof(ns)));
+  return DFM_OK;
 }
 
 template <int B, int LPR, bool FWD>
@@ -716,6 +723,7 @@ static int sweep_dispatch(dfm_ilu M, bool fwd, int sweep, const double* in, doub
                           double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
   if (M->N == 0) return DFM_OK;
   if (sweep <= 0) sweep = M->sweep > 0 ? M->sweep : 1;
+  if (sweep == 3) return sweep_ranges_launch(M, fwd, in, out, rdot, part, sc, rr_part, rr_n);
   cudaError_t e;
   if (M->vt == DFM_COMPLEX) {
     e = fwd ? sweep_cplx<8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
@@ -758,16 +766,14 @@ int ilu_autotune(dfm_ilu M) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  float best = 1e30f;
-  int best_mode = 1;
-  for (int mode = 1; mode <= 2; mode++) {
+  auto time_mode = [&](int mode, float* out_ms) -> int {
     float tmin = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
       int rc = ilu_fill_sentinel(M, M->d_tmp, n);
       rc |= ilu_fill_sentinel(M, z, n);
       cudaEventRecord(e0, s);
-      rc |= ilu_fwd_launch(M, r, M->d_tmp, nullptr, mode);
-      rc |= ilu_bwd_launch(M, M->d_tmp, z, nullptr, nullptr, nullptr, mode);
+      if (!rc) rc = ilu_fwd_launch(M, r, M->d_tmp, nullptr, mode);
+      if (!rc) rc = ilu_bwd_launch(M, M->d_tmp, z, nullptr, nullptr, nullptr, mode);
       cudaEventRecord(e1, s);
       if (rc) return rc;
       cudaEventSynchronize(e1);
@@ -775,7 +781,68 @@ int ilu_autotune(dfm_ilu M) {
       cudaEventElapsedTime(&ms, e0, e1);
       if (rep > 0) tmin = std::min(tmin, ms);
     }
-    if (tmin < best) { best = tmin; best_mode = mode; }
+    *out_ms = tmin;
+    return take_code(M->ctx);
+  };
+  float best = 1e30f;
+  int best_mode = 1;
+  for (int mode = 1; mode <= 2; mode++) {
+    float ms;
+    int rc = time_mode(mode, &ms);
+    if (rc) return rc;
+    if (ms < best) { best = ms; best_mode = mode; }
+  }
+  // range-partitioned schedule: every CTA count whose slice fits in shared memory
+  if (M->vt == DFM_REAL) {
+    sweep_plan_free(&M->plan_f);
+    sweep_plan_free(&M->plan_b);
+    SweepPlan best_f, best_b;  // owned here until the end
+    const int nsm = M->ctx->nsm;
+    const int cand[] = {nsm, nsm / 2, nsm / 4, 16, 8, 4, 2, 1};
+    int last = -1;
+    for (int G : cand) {
+      if (G < 1 || G == last) continue;
+      last = G;
+      SweepPlan pf, pb;
+      if (sweep_plan_build(M, true, G, 8, 8, &pf) != DFM_OK || sweep_plan_build(M, false, G, 8, 8, &pb) != DFM_OK) {
+        sweep_plan_free(&pf);
+        sweep_plan_free(&pb);
+        cudaGetLastError();
+        continue;  // slice does not fit in shared memory at this CTA count
+      }
+      std::swap(M->plan_f, pf);  // M holds the candidate
+      std::swap(M->plan_b, pb);
+      float ms = 1e30f;
+      int rc = DFM_OK, best_lpr = 1;
+      for (int lpr : {1, 2, 4, 8}) {  // consumer lanes per row
+        M->plan_f.lpr = M->plan_b.lpr = lpr;
+        float t = 1e30f;
+        rc = time_mode(3, &t);
+        if (rc) break;
+        if (t < ms) { ms = t; best_lpr = lpr; }
+      }
+      M->plan_f.lpr = M->plan_b.lpr = best_lpr;
+      std::swap(M->plan_f, pf);  // candidate back in pf/pb, M empty
+      std::swap(M->plan_b, pb);
+      if (rc == DFM_OK && ms < best) {
+        best = ms;
+        best_mode = 3;
+        sweep_plan_free(&best_f);
+        sweep_plan_free(&best_b);
+        std::swap(best_f, pf);
+        std::swap(best_b, pb);
+      } else {
+        sweep_plan_free(&pf);
+        sweep_plan_free(&pb);
+        if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
+          sweep_plan_free(&best_f);
+          sweep_plan_free(&best_b);
+          return rc;
+        }
+      }
+    }
+    std::swap(M->plan_f, best_f);
+    std::swap(M->plan_b, best_b);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -783,6 +850,25 @@ int ilu_autotune(dfm_ilu M) {
   cudaFreeAsync(z, s);
   DFM_CUDA_TRY(cudaStreamSynchronize(s));
   M->sweep = best_mode;
+  M->sweep_ms = best;
+  return DFM_OK;
+}
+
+int ilu_set_ranges(dfm_ilu M, int G) {
+  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
+  SweepPlan pf, pb;
+  int rc = sweep_plan_build(M, true, G, 8, 8, &pf);
+  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb);
+  if (rc) {
+    sweep_plan_free(&pf);
+    sweep_plan_free(&pb);
+    return rc;
+  }
+  sweep_plan_free(&M->plan_f);
+  sweep_plan_free(&M->plan_b);
+  std::swap(M->plan_f, pf);
+  std::swap(M->plan_b, pb);
+  M->sweep = 3;
   return DFM_OK;
 }
 

@@ -1,0 +1,507 @@
+// Range-partitioned ILU(0) triangular sweeps (schedule mode 3).
+//
+// The rows are split into G contiguous ranges, one per CTA (a persistent,
+// co-resident grid).  A CTA walks its range level by level (a level's rows are
+// independent): a dependency on a row of its own range is always on an earlier
+// level and is read from the CTA's shared-memory copy of the range's vector
+// slice; a dependency on another range is polled in global memory, where the
+// owning CTA publishes each row as soon as it is computed (the output vector
+// starts as a NaN sentinel).  With the reference's natural FEM ordering most
+// dependencies are local, so most steps of the critical path cost a CTA
+// barrier plus shared-memory latency instead of a round trip through L2.
+//
+// Everything a level needs (a 16-byte descriptor per row, the shared-memory
+// offset or global row of every block's operand, factor blocks, D^-1 for the
+// forward sweep) is packed per "chunk" (a level, or a slice of one) into one
+// contiguous, 16-byte aligned blob in chunk order and streamed into a ring of
+// shared-memory stages by TMA bulk copies (cp.async.bulk, no multicast)
+// completing on mbarriers, several chunks ahead.  Thread 0 alone drives the
+// ring: before each level barrier it makes sure the next chunk has landed, and
+// after it refills the stage just released.  The per-level path of every other
+// thread is one descriptor load, its blocks, and the barrier.  The blob's
+// values are re-gathered from the factor after every numeric factorisation.
+//
+// Every row waits only for rows of lower level, each CTA handles its chunks in
+// increasing level order and all CTAs are co-resident, so every wait ends
+// (induction on the level); all waits are also bounded.
+#include <algorithm>
+#include <cstring>
+
+#include "dfm_internal.h"
+#include "sweep.h"
+
+namespace dfm {
+
+// ------------------------------------------------------------ PTX helpers
+DFM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+DFM_DEVINL void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+DFM_DEVINL void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+DFM_DEVINL void mbar_arrive_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+DFM_DEVINL bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 1-D bulk copy global -> this CTA's shared memory (addresses and size 16-byte multiples).
+DFM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+DFM_DEVINL int ld_status2(const DevStatus* st) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(&st->code) : "memory");
+  return v;
+}
+
+template <typename T>
+DFM_DEVINL T poll_remote(const T* p, DevStatus* st, uint64_t wait_ns, int where) {
+  T v = ld_relaxed(p);
+  if (!Sent<T>::is(v)) return v;
+  SpinGuard g(wait_ns);
+  for (;;) {
+    v = ld_relaxed(p);
+    if (!Sent<T>::is(v)) return v;
+    if (g.expired() || ((g.n & 1023u) == 0 && ld_status2(st) != 0)) {
+      raise_error(st, DFM_WAIT_TIMEOUT, where);
+      return v;
+    }
+  }
+}
+
+// Waits for a stage phase; false (after recording the error) if it never completes.
+DFM_DEVINL bool wait_stage(uint64_t* bar, unsigned parity, DevStatus* st, uint64_t wait_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  SpinGuard g(wait_ns);
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (g.expired()) {
+      raise_error(st, DFM_WAIT_TIMEOUT, 10);
+      return false;
+    }
+  }
+}
+
+// --------------------------------------------------------------- kernel
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
+__global__ void __launch_bounds__(kSweepThreads)
+k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
+               const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
+               int nstage, unsigned x_bytes, const TX* __restrict__ in, TX* out, const TX* __restrict__ rdot,
+               double* part, KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st,
+               uint64_t wait_ns) {
+  constexpr int BB = B * B;
+  extern __shared__ __align__(128) char smem[];
+  __shared__ int s_alive;
+  // guards (block-uniform)
+  if (sc) {
+    if (block_flag(&sc->done)) return;
+    if (FWD) {
+      const double rr = reduce_partials(rr_part, rr_nparts);
+      if (rr * sc->inv0 < sc->tol2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          sc->conv = sqrt(rr * sc->inv0);
+          sc->conv_it = sc->it;
+          sc->done = 100 + DFM_OK;
+        }
+        return;
+      }
+    }
+  }
+  const unsigned a0 = range[blockIdx.x], a1 = range[blockIdx.x + 1];
+  const unsigned q0 = cta_chunk[blockIdx.x], q1 = cta_chunk[blockIdx.x + 1];
+  const unsigned len = a1 - a0;
+  TX* X = reinterpret_cast<TX*>(smem);
+  char* stages = smem + x_bytes;
+  uint64_t* bar_data = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
+
+  // X slice <- in[a0:a1) (rows overwrite their entry with the output)
+  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[(size_t)a0 * B + k];
+  unsigned issued_end = q0;  // thread 0: chunks [q0, issued_end) requested
+  if (threadIdx.x == 0) {
+    s_alive = 1;
+    for (int s = 0; s < nstage; s++) mbar_init(&bar_data[s], 1);
+    fence_mbar_init();
+    for (unsigned q = q0; q < q1 && q < q0 + (unsigned)nstage; q++) {
+      const ChunkDesc cd = chunks[q];
+      const int s = (int)((q - q0) % (unsigned)nstage);
+      mbar_arrive_tx(&bar_data[s], cd.bytes);
+      bulk_g2s(stages + (size_t)s * stage_bytes, blob + cd.off, cd.bytes, &bar_data[s]);
+      issued_end = q + 1;
+    }
+    if (q0 < q1 && !wait_stage(&bar_data[0], 0u, st, wait_ns)) s_alive = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x % LPR;
+  const unsigned g = threadIdx.x / LPR, ng = kSweepThreads / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  for (unsigned q = q0; q < q1; q++) {
+    const unsigned k = q - q0;
+    const int s = (int)(k % (unsigned)nstage);
+    const char* sb = stages + (size_t)s * stage_bytes;
+    if (s_alive) {
+      const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+      const unsigned nrows = hdr->nrows;
+      const uint4* rdesc = reinterpret_cast<const uint4*>(sb + 32);
+      const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+      const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+      const double* dinv = reinterpret_cast<const double*>(sb + hdr->dinv);
+      for (unsigned r = g; r < nrows; r += ng) {  // uniform within a group (lanes share r)
+        const uint4 rd = rdesc[r];
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) acc[c] = 0.0;
+        for (unsigned kk = rd.y + lane; kk < rd.z; kk += LPR) {
+          const unsigned xo = xoff[kk];
+          TX xv[B];
+          if (xo & 0x80000000u) {  // another range's row: poll its published value
+            const unsigned col = xo & 0x7fffffffu;
+#pragma unroll
+            for (int c = 0; c < B; c++) xv[c] = ld_relaxed(out + (size_t)col * B + c);
+#pragma unroll
+            for (int c = 0; c < B; c++)
+              if (Sent<TX>::is(xv[c])) xv[c] = poll_remote(out + (size_t)col * B + c, st, wait_ns, FWD ? 11 : 12);
+          } else {
+#pragma unroll
+            for (int c = 0; c < B; c++) xv[c] = X[xo + c];
+          }
+          const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+          for (int rr = 0; rr < B; rr++)
+#pragma unroll
+            for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)xv[c];
+        }
+        if (LPR > 1) {
+#pragma unroll
+          for (int rr = 0; rr < B; rr++)
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
+        }
+        if (lane == 0) {
+          TX* xi = X + rd.x * B;
+          double t[B];
+#pragma unroll
+          for (int rr = 0; rr < B; rr++) t[rr] = (double)xi[rr] - acc[rr];
+          TX o[B];
+          if (FWD) {
+            const double* d = dinv + (size_t)r * BB;
+#pragma unroll
+            for (int rr = 0; rr < B; rr++) {
+              double v = 0.0;
+#pragma unroll
+              for (int c = 0; c < B; c++) v += d[rr * B + c] * t[c];
+              o[rr] = (TX)v;
+            }
+          } else {
+#pragma unroll
+            for (int rr = 0; rr < B; rr++) o[rr] = (TX)t[rr];
+          }
+#pragma unroll
+          for (int rr = 0; rr < B; rr++) {
+            xi[rr] = o[rr];
+            st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+          }
+        }
+      }
+    }
+    // thread 0: the next level's chunk must have landed before the barrier
+    if (threadIdx.x == 0 && s_alive && q + 1 < q1) {
+      const unsigned k1 = k + 1;
+      if (!wait_stage(&bar_data[k1 % (unsigned)nstage], (k1 / (unsigned)nstage) & 1u, st, wait_ns)) s_alive = 0;
+    }
+    __syncthreads();  // level done: slice entries visible, stage s free
+    if (threadIdx.x == 0 && s_alive) {
+      const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+      if (hdr->next_bytes) {
+        mbar_arrive_tx(&bar_data[s], hdr->next_bytes);
+        bulk_g2s(stages + (size_t)s * stage_bytes, blob + hdr->next_off, hdr->next_bytes, &bar_data[s]);
+        issued_end = q + nstage + 1;
+      }
+    }
+  }
+  if (DOT) {  // (rdot, out) over this CTA's range, from the finished slice
+    double dacc = 0.0;
+    for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
+      dacc += (double)rdot[(size_t)a0 * B + k] * (double)X[k];
+    block_partial<kSweepThreads>(dacc, part);
+  }
+  // after an aborted wait, copies already requested must land before the CTA exits
+  if (threadIdx.x == 0 && !s_alive) {
+    for (unsigned q = q0; q < issued_end; q++) {
+      const unsigned k = q - q0;
+      (void)wait_stage(&bar_data[k % (unsigned)nstage], (k / (unsigned)nstage) & 1u, st, wait_ns);
+    }
+  }
+}
+
+// Refreshes the blob's values from the factor after a numeric factorisation:
+// one CTA per chunk copies its blocks (and D^-1 rows for the forward sweep).
+template <typename TV>
+__global__ void k_gather_blob(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ blk_src,
+                              int bb, const double* __restrict__ fdiag, const double* __restrict__ foff,
+                              char* blob, int with_dinv) {
+  const ChunkDesc cd = chunks[blockIdx.x];
+  char* base = blob + cd.off;
+  TV* vals = reinterpret_cast<TV*>(base + cd.vals_off);
+  const unsigned* src = blk_src + cd.blk0;
+  for (unsigned e = threadIdx.x; e < cd.nblk_pad * (unsigned)bb; e += blockDim.x) {
+    const unsigned kk = e / bb, q = e % bb;
+    const unsigned sl = src[kk];
+    vals[e] = (sl == 0xffffffffu) ? (TV)0 : (TV)foff[(size_t)sl * bb + q];
+  }
+  if (with_dinv) {
+    const uint4* rd = reinterpret_cast<const uint4*>(base + 32);
+    double* dinv = reinterpret_cast<double*>(base + cd.dinv_off);
+    for (unsigned e = threadIdx.x; e < cd.nrows * (unsigned)bb; e += blockDim.x)
+      dinv[e] = fdiag[((size_t)cd.row0 + rd[e / bb].x) * bb + e % bb];
+  }
+}
+
+// ------------------------------------------------------------- host plan
+void sweep_plan_free(SweepPlan* P) {
+  if (!P) return;
+  cudaFree(P->d_chunks);
+  cudaFree(P->d_cta_chunk);
+  cudaFree(P->d_range);
+  cudaFree(P->d_blob);
+  cudaFree(P->d_blk_src);
+  *P = SweepPlan();
+}
+
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool) {
+  const unsigned N = M->N;
+  const unsigned b = M->b;
+  const unsigned bb = b * b;
+  const unsigned vblk = (unsigned)val_bytes * bb;     // bytes per packed block
+  const unsigned drow = fwd ? 8u * bb : 0u;           // D^-1 bytes per row (FP64)
+  const std::vector<unsigned>& rp = M->A->h_rowptr;
+  const std::vector<unsigned>& ci = M->A->h_colind;
+  const std::vector<unsigned>& dia = M->h_diaind;
+  const std::vector<unsigned>& lev = fwd ? M->lev_f : M->lev_b;
+  sweep_plan_free(P);
+  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
+  if (N >= 0x80000000u) return DFM_ERR_UNSUPPORTED;
+  if (G < 1) G = 1;
+  if ((unsigned)G > std::max(N, 1u)) G = std::max(N, 1u);
+  // balanced contiguous ranges by (dependency blocks + 1) per row
+  std::vector<unsigned long long> wpre(N + 1, 0);
+  for (unsigned i = 0; i < N; i++) {
+    const unsigned nb = fwd ? dia[i] - rp[i] : rp[i + 1] - dia[i];
+    wpre[i + 1] = wpre[i] + nb + 1;
+  }
+  std::vector<unsigned> range(G + 1, N);
+  range[0] = 0;
+  for (int c = 1; c < G; c++) {
+    const unsigned long long target = wpre[N] * (unsigned long long)c / (unsigned)G;
+    range[c] = (unsigned)(std::lower_bound(wpre.begin(), wpre.end(), target) - wpre.begin());
+    range[c] = std::max(range[c], range[c - 1]);
+  }
+  unsigned maxlen = 0;
+  for (int c = 0; c < G; c++) maxlen = std::max(maxlen, range[c + 1] - range[c]);
+  const size_t x_bytes = ((size_t)maxlen * b * vec_bytes + 127) & ~(size_t)127;
+  if (x_bytes + 4 * 1024 > kSweepSmemBudget) return DFM_ERR_UNSUPPORTED;  // use more CTAs
+
+  struct Pend {
+    std::vector<uint4> rd;
+    std::vector<unsigned> xo;
+  };
+  std::vector<ChunkDesc> chunks;
+  std::vector<Pend> pend;
+  std::vector<unsigned> cta_chunk(G + 1, 0);
+  std::vector<unsigned> blk_src;
+  size_t blob_size = 0;
+  unsigned stage_max = 0;
+  for (int c = 0; c < G; c++) {
+    cta_chunk[c] = (unsigned)chunks.size();
+    const unsigned a0 = range[c], a1 = range[c + 1];
+    std::vector<unsigned> rows(a1 - a0);
+    for (unsigned i = a0; i < a1; i++) rows[i - a0] = fwd ? i : (a1 - 1 - (i - a0));
+    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return lev[x] < lev[y]; });
+    size_t p = 0;
+    while (p < rows.size()) {
+      const unsigned L = lev[rows[p]];
+      // one chunk: rows of level L, capped in rows and bytes
+      Pend pd;
+      unsigned nblk = 0;
+      while (p < rows.size() && lev[rows[p]] == L) {
+        const unsigned i = rows[p];
+        const unsigned s0 = fwd ? rp[i] : dia[i], s1 = fwd ? dia[i] : rp[i + 1];
+        const unsigned nb = s1 - s0;
+        const ChunkLayout est = chunk_layout((unsigned)pd.rd.size() + 1, ((nblk + nb) + 3) & ~3u, 0u, vblk, drow);
+        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) break;
+        pd.rd.push_back(make_uint4(i - a0, nblk, nblk + nb, 0u));
+        for (unsigned s = s0; s < s1; s++) {
+          const unsigned col = ci[s];
+          pd.xo.push_back((col >= a0 && col < a1) ? (col - a0) * b : (0x80000000u | col));
+          blk_src.push_back(s);
+        }
+        nblk += nb;
+        p++;
+      }
+      const unsigned nblk_pad = (nblk + 3) & ~3u;
+      for (unsigned k = nblk; k < nblk_pad; k++) {
+        pd.xo.push_back(0);  // padding: never referenced (outside every row's block range)
+        blk_src.push_back(0xffffffffu);
+      }
+      ChunkDesc cd = {};
+      cd.nrows = (unsigned)pd.rd.size();
+      cd.nblk_pad = nblk_pad;
+      cd.blk0 = (unsigned)(blk_src.size() - nblk_pad);
+      cd.row0 = a0;
+      const ChunkLayout cl = chunk_layout(cd.nrows, nblk_pad, 0u, vblk, drow);
+      cd.vals_off = cl.vals;
+      cd.dinv_off = cl.dinv;
+      cd.bytes = cl.bytes;
+      cd.off = blob_size;
+      blob_size += cl.bytes;
+      stage_max = std::max(stage_max, cl.bytes);
+      chunks.push_back(cd);
+      pend.push_back(std::move(pd));
+    }
+  }
+  cta_chunk[G] = (unsigned)chunks.size();
+  const unsigned stage_bytes = (std::max(stage_max, 32u) + 15u) & ~15u;
+  const size_t bar_bytes = 8 * (size_t)kMaxStages;
+  int ns = 0;
+  for (int t = kMaxStages; t >= 2; t--)
+    if (x_bytes + (size_t)t * stage_bytes + bar_bytes <= kSweepSmemBudget) { ns = t; break; }
+  if (ns < 2) return DFM_ERR_UNSUPPORTED;  // the slice does not fit: use more CTAs
+
+  std::vector<char> hblob(std::max<size_t>(blob_size, 16), 0);
+  for (int c = 0; c < G; c++) {
+    for (unsigned q = cta_chunk[c]; q < cta_chunk[c + 1]; q++) {
+      const ChunkDesc& cd = chunks[q];
+      const ChunkLayout cl = chunk_layout(cd.nrows, cd.nblk_pad, 0u, vblk, drow);
+      char* base = hblob.data() + cd.off;
+      ChunkHeader hdr = {};
+      hdr.nrows = cd.nrows;
+      hdr.xoff = cl.xoff;
+      hdr.vals = cl.vals;
+      hdr.dinv = cl.dinv;
+      if (q + ns < cta_chunk[c + 1]) {
+        hdr.next_off = chunks[q + ns].off;
+        hdr.next_bytes = chunks[q + ns].bytes;
+      }
+      std::memcpy(base, &hdr, sizeof(hdr));
+      std::memcpy(base + cl.roff, pend[q].rd.data(), 16 * pend[q].rd.size());
+      std::memcpy(base + cl.xoff, pend[q].xo.data(), 4 * pend[q].xo.size());
+    }
+  }
+  P->G = G;
+  P->fwd = fwd;
+  P->nchunks = (unsigned)chunks.size();
+  P->stage_bytes = stage_bytes;
+  P->x_bytes = (unsigned)x_bytes;
+  P->val_bytes = val_bytes;
+  P->vec_bytes = vec_bytes;
+  P->nstage = ns;
+  P->smem = x_bytes + (size_t)ns * stage_bytes + bar_bytes;
+  P->lpr = (b == 3) ? 4 : 1;
+  cudaStream_t s = M->ctx->stream;
+  DFM_CUDA_TRY(cudaMalloc(&P->d_chunks, sizeof(ChunkDesc) * std::max<size_t>(chunks.size(), 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_cta_chunk, sizeof(unsigned) * (G + 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_range, sizeof(unsigned) * (G + 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_blob, hblob.size()));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_blk_src, sizeof(unsigned) * std::max<size_t>(blk_src.size(), 1)));
+  if (!chunks.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_chunks, chunks.data(), sizeof(ChunkDesc) * chunks.size(), cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_cta_chunk, cta_chunk.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_range, range.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blob, hblob.data(), hblob.size(), cudaMemcpyHostToDevice, s));
+  if (!blk_src.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blk_src, blk_src.data(), sizeof(unsigned) * blk_src.size(), cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  P->valid = true;
+  P->stale = true;
+  return DFM_OK;
+}
+
+int sweep_plan_refresh(dfm_ilu M, SweepPlan* P) {
+  if (!P->valid || P->nchunks == 0) { P->stale = false; return DFM_OK; }
+  const int bb = (int)M->vw();
+  if (P->val_bytes == 8)
+    k_gather_blob<double><<<P->nchunks, 256, 0, M->ctx->stream>>>(P->d_chunks, P->d_blk_src, bb, M->d_fdiag,
+                                                                  M->d_foff, P->d_blob, P->fwd ? 1 : 0);
+  else
+    k_gather_blob<float><<<P->nchunks, 256, 0, M->ctx->stream>>>(P->d_chunks, P->d_blk_src, bb, M->d_fdiag,
+                                                                 M->d_foff, P->d_blob, P->fwd ? 1 : 0);
+  DFM_CUDA_TRY(cudaGetLastError());
+  P->stale = false;
+  return DFM_OK;
+}
+
+template <int B, int LPR, typename TV, typename TX, bool FWD>
+static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX* out, const TX* rdot,
+                                 double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  dfm_ctx c = M->ctx;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P->G);
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.dynamicSmemBytes = P->smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (part) {
+    auto fn = k_sweep_ranges<B, LPR, TV, TX, FWD, true>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
+    return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
+                              (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
+                              P->x_bytes, in, out, rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+  }
+  auto fn = k_sweep_ranges<B, LPR, TV, TX, FWD, false>;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
+  return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
+                            (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
+                            P->x_bytes, in, out, rdot, (double*)nullptr, sc, rr_part, rr_n, c->d_status,
+                            (uint64_t)c->wait_ns);
+}
+
+template <int B, typename TV, typename TX, bool FWD>
+static cudaError_t launch_ranges_lpr(dfm_ilu M, const SweepPlan* P, const TX* in, TX* out, const TX* rdot,
+                                     double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  switch (P->lpr) {
+    case 1: return launch_ranges<B, 1, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 2: return launch_ranges<B, 2, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 4: return launch_ranges<B, 4, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    default: return launch_ranges<B, 8, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  }
+}
+
+int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
+                        KrylovScalars* sc, const double* rr_part, int rr_n) {
+  SweepPlan* P = fwd ? &M->plan_f : &M->plan_b;
+  if (!P->valid || P->val_bytes != 8 || P->vec_bytes != 8) return DFM_ERR_INVALID;
+  if (P->stale) {
+    int rc = sweep_plan_refresh(M, P);
+    if (rc) return rc;
+  }
+  if (M->vt == DFM_COMPLEX) return DFM_ERR_UNSUPPORTED;
+  cudaError_t e;
+  switch (M->b) {
+    case 1: e = fwd ? launch_ranges_lpr<1, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                    : launch_ranges_lpr<1, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
+    case 2: e = fwd ? launch_ranges_lpr<2, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                    : launch_ranges_lpr<2, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
+    default: e = fwd ? launch_ranges_lpr<3, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                     : launch_ranges_lpr<3, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
+  }
+  DFM_CUDA_TRY(e);
+  return DFM_OK;
+}
+
+}  // namespace dfm

@@ -53,6 +53,7 @@ PROTOS = {
     "dfm_ilu_apply": (_i, [_vp, _vp, _vp]),
     "dfm_ilu_set_sweep": (_i, [_vp, _i]),
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
+    "dfm_ilu_set_sweep_tuning": (_i, [_vp, _i, _u]),
     "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_host": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
 }

@@ -112,9 +112,14 @@ DFM_API int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off,
 /* z = U^-1 L^-1 r (ForwardSubstitution + BackwardSubstitution, :332-663).  r != z. */
 DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
 /* Sweep schedule: 0 = autotuned, 1 = sync-free across the GPU, 2 = one CTA with
- * level barriers. */
+ * level barriers, 3 = contiguous row ranges per CTA (shared-memory slice, TMA-
+ * streamed level data; the CTA count is the max_blocks of
+ * dfm_ilu_set_sweep_tuning, default one per SM).  Real matrices only for 3. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
+/* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all
+ * that fit) and the back-off between polls of a waiting lane in ns (global). */
+DFM_API int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns);
 
 /* ---- Krylov solvers ------------------------------------------------------ */
 /* LsSol::Solve_PCG (src/ls/solver_ls_iter.cpp:100-172) preconditioned by M:

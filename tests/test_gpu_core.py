@@ -69,10 +69,12 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2])
+@pytest.mark.parametrize("sweep", [1, 2, 3])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
+    if sweep == 3 and S.cplx:
+        pytest.skip("range-partitioned sweep is real-only")
     A = make(ctx, S)
     M = lib.ILU(A)
     M.factor()
@@ -88,7 +90,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2])
+@pytest.mark.parametrize("sweep", [1, 2, 3])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -108,6 +110,32 @@ def test_pcg_matches_oracle(ctx, name, sweep):
     assert err <= 1e-8, (name, err)
     # the recursive residual returned in r satisfies the stop test
     assert conv < 1e-10
+
+
+@pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1"])
+@pytest.mark.parametrize("ctas", [1, 3, 7, 148])
+def test_range_sweep_cta_counts(ctx, name, ctas):
+    """Mode 3 with every CTA count: same result as the oracle's sweeps."""
+    from delfem_b200 import lib
+    S = SYSTEMS[name]()
+    A = make(ctx, S)
+    M = lib.ILU(A)
+    M.factor()
+    lib.check(lib.lib().dfm_ilu_set_sweep_tuning(M.h, ctas, 64))
+    M.sweep = 3
+    _, fd, fo = S.ilu0()
+    r = np.random.default_rng(5).standard_normal(S.N * S.xw)
+    ref = S.precond(fd, fo, r)
+    z = torch.zeros(S.N * S.xw, dtype=torch.float64, device="cuda")
+    M.apply(dev(r), z)
+    assert np.allclose(z.cpu().numpy(), ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
+    # refactor with new values: the packed sweep data must follow the factor
+    A.set_values(S.diag * 2.0, S.off * 2.0)
+    M.factor()
+    z2 = torch.zeros_like(z)
+    M.apply(dev(r), z2)
+    assert np.allclose(z2.cpu().numpy(), ref / 2.0, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
+    lib.check(lib.lib().dfm_ilu_set_sweep_tuning(M.h, 0, 64))
 
 
 def test_pcg_maxit_and_zero_rhs(ctx):
