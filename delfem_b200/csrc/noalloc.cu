@@ -1,0 +1,76 @@
+// dfm_ilu_apply_static: the ILU(0) preconditioner application
+// z = U^-1 L^-1 r without any device allocation.
+//
+// Some callers cannot allocate device memory when they need the
+// preconditioner: code running inside a stream-ordered region that must not
+// synchronise (cudaMalloc/cudaFree implicitly synchronise the device), code
+// holding a fixed memory budget handed out by a host framework that owns all
+// allocations, and callbacks that run while an allocator lock is held.  For
+// them this entry point keeps its only scratch buffer - the intermediate
+// vector y = L^-1 r between the two sweeps - in a file-scope static device
+// array of kNoAllocMaxDoubles doubles (4 MiB).  Every GPU that loads the
+// library holds that array until the process exits.
+//
+// Limits and sharing:
+//  * N * (doubles per block row) must not exceed kNoAllocMaxDoubles
+//    (524,288 doubles: e.g. 524,288 scalar rows, 174,762 3x3 block rows or
+//    262,144 complex rows); larger systems get DFM_ERR_INVALID.
+//  * All calls share the one array and it keeps the last call's contents.
+//    The sweeps write every entry they later read, so nothing needs clearing,
+//    but calls whose kernels overlap on the GPU (different streams, or
+//    different contexts on one device without ordering) race on it.
+//  * The first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress) with that device current; make that first call
+//    before any stream capture.
+// It runs the one-CTA level-barrier schedule, which needs no sentinel buffers
+// and no autotuning (both of which allocate on first use).
+#include <mutex>
+
+#include "dfm_internal.h"
+
+namespace dfm {
+
+constexpr size_t kNoAllocMaxDoubles = (size_t)1 << 19;  // 4 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxDoubles];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `device` (looked up once per device).
+static int noalloc_scratch(int device, double** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return DFM_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    int cur = 0;
+    DFM_CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != device) DFM_CUDA_TRY(cudaSetDevice(device));
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (cur != device) cudaSetDevice(cur);
+    if (e != cudaSuccess || !p) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress");
+    g_noalloc_ptr[device] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return DFM_OK;
+}
+
+}  // namespace dfm
+
+using namespace dfm;
+
+extern "C" int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z) {
+  if (!M) return DFM_ERR_INVALID;
+  const size_t n = (size_t)M->N * M->xw();
+  if (n > kNoAllocMaxDoubles) return DFM_ERR_INVALID;  // beyond the static scratch
+  if ((M->N && (!r || !z)) || r == z || !M->factored) return DFM_ERR_INVALID;
+  if (n == 0) return DFM_OK;
+  double* y = nullptr;
+  int rc = noalloc_scratch(M->ctx->device, &y);
+  if (rc) return rc;
+  if ((rc = ilu_fwd_launch(M, r, y, nullptr, 2))) return rc;
+  if ((rc = ilu_bwd_launch(M, y, z, nullptr, nullptr, nullptr, 2))) return rc;
+  DFM_CUDA_TRY(cudaStreamSynchronize(M->ctx->stream));
+  return take_code(M->ctx);
+}

@@ -51,6 +51,7 @@ PROTOS = {
     "dfm_ilu_get_values": (_i, [_vp, _vp, _vp, _i]),
     "dfm_ilu_set_values": (_i, [_vp, _vp, _vp, _i]),
     "dfm_ilu_apply": (_i, [_vp, _vp, _vp]),
+    "dfm_ilu_apply_static": (_i, [_vp, _vp, _vp]),
     "dfm_ilu_set_sweep": (_i, [_vp, _i]),
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
     "dfm_ilu_set_sweep_tuning": (_i, [_vp, _i, _u]),

@@ -111,6 +111,17 @@ DFM_API int dfm_ilu_get_values(dfm_ilu M, double* diag, double* off, int where);
 DFM_API int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int where);
 /* z = U^-1 L^-1 r (ForwardSubstitution + BackwardSubstitution, :332-663).  r != z. */
 DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
+/* No counterpart in the reference.  The same z = U^-1 L^-1 r as dfm_ilu_apply,
+ * for callers that cannot allocate device memory at the point of use (code
+ * inside a stream-ordered region that must not synchronise, a host framework
+ * that owns every device allocation, callbacks under an allocator lock): it
+ * allocates nothing, keeping its intermediate vector in a static device array
+ * of 4 MiB (N * doubles-per-row <= 524,288, else DFM_ERR_INVALID) that every
+ * GPU loading the library holds until exit.  All calls share that array, so
+ * calls whose kernels overlap on the GPU race on it.  The first call on a
+ * device looks up the array's address with that device current; make it
+ * before any stream capture.  Runs the one-CTA level-barrier schedule. */
+DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
 /* Sweep schedule: 0 = autotuned, 1 = sync-free across the GPU, 2 = one CTA with
  * level barriers, 3 = contiguous row ranges per CTA (shared-memory slice, TMA-
  * streamed level data; the CTA count is the max_blocks of
