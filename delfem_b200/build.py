@@ -20,6 +20,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-warn-spills"]
+# Element assembly must add and multiply exactly as the reference's element
+# loops do (no fused multiply-add) for its bit-identical results.
+FILE_FLAGS = {"assemble.cu": ["-fmad=false"], "adjoint.cu": ["-fmad=false"]}
 
 
 def sources():
@@ -47,7 +50,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in sources():
         obj = os.path.join(OUT_DIR, "obj", os.path.basename(src) + ".o")
         objs.append(obj)
-        cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), "-I",
+               os.path.join(ROOT, "include"), "-c", src, "-o", obj]
         procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
     for cmd, p in procs:
         out, _ = p.communicate()

@@ -9,7 +9,6 @@
 #include "dfm_internal.h"
 
 namespace dfm {
-void pcg_release(dfm_ilu M);
 
 int cuda_fail(cudaError_t e, const char* what) {
   (void)what;
@@ -207,6 +206,7 @@ int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* ro
   A->ncrs = ncrs;
   A->h_rowptr.assign(rowptr, rowptr + N + 1);
   A->h_colind.assign(colind, colind + ncrs);
+  for (unsigned i = 0; i < N; i++) A->max_row = std::max(A->max_row, rowptr[i + 1] - rowptr[i]);
   int rc = dalloc(&A->d_rowptr, N + 1);
   if (!rc) rc = dalloc(&A->d_colind, ncrs);
   if (!rc) rc = dalloc(&A->d_diag, (size_t)N * A->vw());
@@ -338,7 +338,7 @@ int dfm_ilu_create(dfm_mat A, dfm_ilu* out) {
 int dfm_ilu_destroy(dfm_ilu M) {
   if (!M) return DFM_OK;
   cudaStreamSynchronize(M->ctx->stream);
-  pcg_release(M);
+  solve_release(M);
   sweep_plan_free(&M->plan_f);
   sweep_plan_free(&M->plan_b);
   cudaFree(M->d_diaind);
@@ -425,30 +425,45 @@ int dfm_ilu_apply(dfm_ilu M, const double* r, double* z) {
 }
 
 // ---------------------------------------------------------------- solvers
+static int solve_args(dfm_mat A, dfm_ilu M, int method, const void* b, const void* x) {
+  if (!A || !M || M->A != A || (A->N && (!b || !x))) return DFM_ERR_INVALID;
+  if (method == DFM_PCOCG ? A->vt != DFM_COMPLEX : A->vt != DFM_REAL) return DFM_ERR_INVALID;
+  if (!M->factored) return DFM_ERR_INVALID;
+  return DFM_OK;
+}
+
 int dfm_solve_pcg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
                   double* conv) {
-  if (!A || !M || M->A != A || A->vt != DFM_REAL || (A->N && (!r || !x))) return DFM_ERR_INVALID;
-  if (!M->factored) return DFM_ERR_INVALID;
-  return pcg_solve(A, M, r, x, tol, maxit, iters, conv);
+  const int rc = solve_args(A, M, DFM_PCG, r, x);
+  if (rc) return rc;
+  return krylov_solve(A, M, DFM_PCG, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
+int dfm_solve_pbicgstab(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                        double* conv) {
+  const int rc = solve_args(A, M, DFM_PBICGSTAB, r, x);
+  if (rc) return rc;
+  return krylov_solve(A, M, DFM_PBICGSTAB, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
+int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                    double* conv) {
+  const int rc = solve_args(A, M, DFM_PCOCG, r, x);
+  if (rc) return rc;
+  return krylov_solve(A, M, DFM_PCOCG, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
+int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
+                   unsigned maxit, unsigned* iters, double* conv) {
+  if (method != DFM_PCG && method != DFM_PBICGSTAB && method != DFM_PCOCG) return DFM_ERR_INVALID;
+  const int rc = solve_args(A, M, method, b_host, x_host);
+  if (rc) return rc;
+  return krylov_solve(A, M, method, b_host, DFM_HOST, x_host, DFM_HOST, nullptr, tol, maxit, iters, conv);
 }
 
 int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol, unsigned maxit,
                        unsigned* iters, double* conv) {
-  if (!A || !M || (A->N && (!b_host || !x_host))) return DFM_ERR_INVALID;
-  const size_t n = (size_t)A->N * A->xw();
-  cudaStream_t s = A->ctx->stream;
-  double *r = nullptr, *x = nullptr;
-  int rc = dalloc(&r, n);
-  if (!rc) rc = dalloc(&x, n);
-  if (!rc && cudaMemcpyAsync(r, b_host, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) rc = DFM_ERR_CUDA;
-  if (!rc) rc = dfm_solve_pcg(A, M, r, x, tol, maxit, iters, conv);
-  if ((rc == DFM_OK || rc == DFM_NOT_CONVERGED) &&
-      cudaMemcpyAsync(x_host, x, n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    rc = DFM_ERR_CUDA;
-  cudaStreamSynchronize(s);
-  cudaFree(r);
-  cudaFree(x);
-  return rc;
+  return dfm_solve_host(A, M, DFM_PCG, b_host, x_host, tol, maxit, iters, conv);
 }
 
 }  // extern "C"

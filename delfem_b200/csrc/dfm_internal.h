@@ -64,6 +64,7 @@ struct dfm_mat_s {
   double* d_diag = nullptr;
   double* d_off = nullptr;
   std::vector<unsigned> h_rowptr, h_colind;
+  unsigned max_row = 0;     // most off-diagonal blocks in one row
   int lanes = 0;            // SpMV lanes per block row (0 = not tuned yet)
   size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }   // doubles per block
   size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }               // doubles per vector block
@@ -98,13 +99,17 @@ struct dfm_ilu_s {
 
 namespace dfm {
 // spmv.cu
+// dot_part: partials of (dot_w ? dot_w : x) . y; dot_part2: partials of y . y (real only).
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
-                int nblocks_hint, KrylovScalars* sc, int lanes);
+                int nblocks_hint, KrylovScalars* sc, int lanes, const double* dot_w = nullptr,
+                double* dot_part2 = nullptr);
 int spmv_autotune(dfm_mat A);
 int spmv_grid(dfm_mat A);
 // ilu.cu
 int ilu_factor_launch(dfm_ilu M, dfm_mat A);
-int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep);
+// With sc, a forward sweep first stops the solve when |r|^2/|r0|^2 < tol^2
+// (partials in part(2)) unless rr_check is false.
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check = true);
 int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part,
                    KrylovScalars* sc, int sweep);
 int ilu_fill_sentinel(dfm_ilu M, double* v, size_t n);
@@ -121,6 +126,8 @@ int ilu_set_ranges(dfm_ilu M, int G);
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
                         KrylovScalars* sc, const double* rr_part, int rr_n);
 // krylov.cu
-int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
-              double* conv);
+// method: DFM_PCG / DFM_PBICGSTAB / DFM_PCOCG; b and x at DFM_HOST or DFM_DEVICE.
+int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where, double* x, int x_where,
+                 double* r_out, double tol, unsigned maxit, unsigned* iters, double* conv);
+void solve_release(dfm_ilu M);
 }  // namespace dfm

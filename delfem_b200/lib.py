@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED = range(9)
 REAL, COMPLEX = 0, 1
 HOST, DEVICE = 0, 1
+PCG, PBICGSTAB, PCOCG = 0, 1, 2
 
 _lib = None
 
@@ -44,6 +45,13 @@ PROTOS = {
     "dfm_mat_set_spmv_lanes": (_i, [_vp, _i]),
     "dfm_mat_get_spmv_lanes": (_i, [_vp, _ip]),
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
+    "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
+    "dfm_mesh_destroy": (_i, [_vp]),
+    "dfm_assemble_poisson2d": (_i, [_vp, _vp, _d, _d, _vp, _vp, _vp, _vp]),
+    "dfm_assemble_solid2d": (_i, [_vp, _vp, _d, _d, _d, _d, _d, _vp, _vp, _vp, _vp]),
+    "dfm_assemble_solid3d": (_i, [_vp, _vp, _d, _d, _d, _d, _d, _d, _vp, _vp, _vp]),
+    "dfm_assemble_helmholtz2d": (_i, [_vp, _vp, _d, _vp, _vp, _vp]),
+    "dfm_apply_dirichlet": (_i, [_vp, _vp, _vp]),
     "dfm_ilu_create": (_i, [_vp, C.POINTER(_vp)]),
     "dfm_ilu_destroy": (_i, [_vp]),
     "dfm_ilu_levels": (_i, [_vp, _up, _up, _up, _up]),
@@ -56,6 +64,9 @@ PROTOS = {
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
     "dfm_ilu_set_sweep_tuning": (_i, [_vp, _i, _u]),
     "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_pbicgstab": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_pcocg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_host": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
 }
 
@@ -212,6 +223,69 @@ class Matrix:
         check(lib().dfm_mat_set_spmv_lanes(self.h, int(v)))
 
 
+class Mesh:
+    """A P1 mesh on the device (triangles or tetrahedra, optional boundary bars)
+    for the gather assembly kernels."""
+
+    def __init__(self, ctx: Context, coord, elem, bars=None):
+        self.ctx = ctx
+        coord = np.ascontiguousarray(coord, np.float64)
+        elem = np.ascontiguousarray(elem, np.int32)
+        ndim = coord.shape[1]
+        nnoel = elem.shape[1]
+        bars = np.zeros((0, 2), np.int32) if bars is None else np.ascontiguousarray(bars, np.int32).reshape(-1, 2)
+        b_ = bars if bars.size else np.zeros((1, 2), np.int32)
+        e_ = elem if elem.size else np.zeros((1, nnoel), np.int32)
+        h = C.c_void_p()
+        check(lib().dfm_mesh_create(ctx.h, ndim, coord.shape[0], coord.ctypes.data_as(_dp), nnoel, elem.shape[0],
+                                    e_.ctypes.data_as(_ip), bars.shape[0], b_.ctypes.data_as(_ip), C.byref(h)),
+              "dfm_mesh_create")
+        self.h = h
+        self.ndim, self.nnode, self.nnoel, self.nelem, self.nbar = ndim, coord.shape[0], nnoel, elem.shape[0], \
+            bars.shape[0]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def assemble_poisson(self, A: Matrix, alpha, source, rhs, coef=None, u=None, load=None):
+        _sync_torch()
+        check(lib().dfm_assemble_poisson2d(self.h, A.h, alpha, source, _ptr(coef), _ptr(u), _ptr(load), _ptr(rhs)),
+              "dfm_assemble_poisson2d")
+        return rhs
+
+    def assemble_solid2d(self, A: Matrix, lam, myu, rho, gx, gy, rhs, coef=None, u=None, load=None):
+        _sync_torch()
+        check(lib().dfm_assemble_solid2d(self.h, A.h, lam, myu, rho, gx, gy, _ptr(coef), _ptr(u), _ptr(load),
+                                         _ptr(rhs)), "dfm_assemble_solid2d")
+        return rhs
+
+    def assemble_solid3d(self, A: Matrix, lam, myu, rho, gx, gy, gz, rhs, u=None, load=None):
+        _sync_torch()
+        check(lib().dfm_assemble_solid3d(self.h, A.h, lam, myu, rho, gx, gy, gz, _ptr(u), _ptr(load), _ptr(rhs)),
+              "dfm_assemble_solid3d")
+        return rhs
+
+    def assemble_helmholtz(self, A: Matrix, wave_length, rhs, u=None, load=None):
+        _sync_torch()
+        check(lib().dfm_assemble_helmholtz2d(self.h, A.h, wave_length, _ptr(u), _ptr(load), _ptr(rhs)),
+              "dfm_assemble_helmholtz2d")
+        return rhs
+
+
+def apply_dirichlet(A: Matrix, flags, rhs=None):
+    """Dirichlet elimination with device int32 flags[N*b] (nonzero = fixed)."""
+    _sync_torch()
+    check(lib().dfm_apply_dirichlet(A.h, _ptr(flags), _ptr(rhs)), "dfm_apply_dirichlet")
+
+
 class ILU:
     """LsSol::CPreconditioner_ILU(0) on the device."""
 
@@ -280,6 +354,34 @@ def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CO
     rc = lib().dfm_solve_pcg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_pcg", allow)
     return rc, it.value, conv.value
+
+
+def solve_pbicgstab(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """LsSol::Solve_PBiCGSTAB on device vectors; returns (status, iters, conv)."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_pbicgstab(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pbicgstab", allow)
+    return rc, it.value, conv.value
+
+
+def solve_pcocg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """Fem::Ls::Solve_PCOCG on device vectors (interleaved complex); returns (status, iters, conv)."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_pcocg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pcocg", allow)
+    return rc, it.value, conv.value
+
+
+def solve_host(A: Matrix, M: ILU, b, method=PCG, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """End-to-end solve from host b to host x; returns (status, x, iters, conv)."""
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b)
+    it, conv = C.c_uint(), C.c_double()
+    rc = lib().dfm_solve_host(A.h, M.h, method, _ptr(b), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_host", allow)
+    return rc, x, it.value, conv.value
 
 
 def solve_pcg_host(A: Matrix, M: ILU, b, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):

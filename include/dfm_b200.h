@@ -51,10 +51,12 @@ typedef enum dfm_status {
 
 enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
 enum { DFM_HOST = 0, DFM_DEVICE = 1 };
+enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2 };
 
 typedef struct dfm_ctx_s* dfm_ctx;
 typedef struct dfm_mat_s* dfm_mat;
 typedef struct dfm_ilu_s* dfm_ilu;
+typedef struct dfm_mesh_s* dfm_mesh;
 
 DFM_API const char* dfm_status_string(int status);
 DFM_API int dfm_abi_version(void);
@@ -96,6 +98,43 @@ DFM_API int dfm_mat_get_spmv_lanes(dfm_mat A, int* lanes);
  * beta == 0 writes y without reading it. */
 DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, double* y);
 
+/* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
+/* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]
+ * (triangles nnoel = 3 in 2D, tetrahedra 4 in 3D) and optional boundary bars
+ * bar[nbar*2] (the Sommerfeld boundary of the Helmholtz problem).  Host arrays;
+ * the node -> element adjacency used by the gather assembly is built here. */
+DFM_API int dfm_mesh_create(dfm_ctx ctx, int ndim, unsigned nnode, const double* coord, unsigned nnoel,
+                    unsigned nelem, const int* elem, unsigned nbar, const int* bar, dfm_mesh* out);
+DFM_API int dfm_mesh_destroy(dfm_mesh mesh);
+/* Each assemble call is InitializeMarge (matrix and residual zeroed,
+ * src/ls/linearsystem.cpp:74-89) + the element loop + nodal loads
+ * added to the residual afterwards.  A's pattern must hold every element's node
+ * pairs (dfm pattern from the same mesh); entries outside it are skipped as in
+ * CMatDia_BlkCrs::Mearge (src/matvec/matdia_blkcrs.cpp:165-258).  Results are
+ * bit-identical to the reference's.  Device pointers: elem_coef[nelem]
+ * (per-element multiplier of the material constants, nullable), u (current
+ * field, nullable = 0: res = f - K u), load (nodal loads, nullable), rhs (out,
+ * N*b doubles, 2N for complex).  Row length <= 63 off-diagonal blocks. */
+/* AddLinearSystem_Poisson2D_P1, src/femeqn/eqn_poisson.cpp:49-125 (b = 1). */
+DFM_API int dfm_assemble_poisson2d(dfm_mesh mesh, dfm_mat A, double alpha, double source,
+                           const double* elem_coef, const double* u, const double* load, double* rhs);
+/* AddLinSys_LinearSolid2D_Static_P1, src/femeqn/eqn_linear_solid2d.cpp:505-598 (b = 2). */
+DFM_API int dfm_assemble_solid2d(dfm_mesh mesh, dfm_mat A, double lambda, double myu, double rho, double gx,
+                         double gy, const double* elem_coef, const double* u, const double* load, double* rhs);
+/* AddLinSys_LinearSolid3D_Static_P1, src/femeqn/eqn_linear_solid3d.cpp:241-334 (b = 3). */
+DFM_API int dfm_assemble_solid3d(dfm_mesh mesh, dfm_mat A, double lambda, double myu, double rho, double gx,
+                         double gy, double gz, const double* u, const double* load, double* rhs);
+/* AddLinearSystem_Helmholtz2D_P1 (src/femeqn/eqn_helmholtz.cpp:51-137) followed by
+ * AddLinearSystem_SommerfeltRadiationBC2D_B1 (:437-512) on the mesh's bars; complex A. */
+DFM_API int dfm_assemble_helmholtz2d(dfm_mesh mesh, dfm_mat A, double wave_length, const double* u,
+                             const double* load, double* rhs);
+/* Dirichlet elimination of FinalizeMarge (src/ls/linearsystem.cpp:92-122:
+ * CMatDia_BlkCrs::SetBoundaryCondition, src/matvec/matdia_blkcrs.cpp:261-343,
+ * and CBCFlag::SetZeroToBCDof): rows and
+ * columns of fixed DOFs zeroed, unit diagonal, residual zeroed.  flags: device
+ * int[N*b], nonzero = fixed; rhs nullable.  Real matrices. */
+DFM_API int dfm_apply_dirichlet(dfm_mat A, const int* flags, double* rhs);
+
 /* ---- ILU(0): CPreconditioner_ILU / CMatDiaFrac_BlkCrs ------------------- */
 /* Symbolic ILU(0) (CMatDiaFrac_BlkCrs(0, A), src/matvec/matdiafrac_blkcrs.cpp:227-287)
  * plus the level sets of both sweeps in the natural order. */
@@ -133,13 +172,30 @@ DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 DFM_API int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns);
 
 /* ---- Krylov solvers ------------------------------------------------------ */
-/* LsSol::Solve_PCG (src/ls/solver_ls_iter.cpp:100-172) preconditioned by M:
- * r holds b on entry and the recursive residual on exit, x receives the
- * solution (x = 0 initial guess).  *iters follows the reference: the 0-based
- * index of the converged iteration.  DFM_NOT_CONVERGED at maxit. */
+/* Common to the solvers: x = 0 initial guess; r holds b on entry and the
+ * recursive residual on exit; *conv = |r|/|r0| at exit; the stop test is the
+ * reference's |r|^2/|r0|^2 < tol^2 on the recursive residual.  Reductions are
+ * deterministic (same inputs, same bits), the iterations run as replays of a
+ * captured CUDA graph with all scalars on the device.  DFM_NOT_CONVERGED at
+ * max_iter (where the reference's PBiCGSTAB and PCOCG still return true),
+ * DFM_BREAKDOWN on a non-finite step. */
+/* LsSol::Solve_PCG (src/ls/solver_ls_iter.cpp:100-172) preconditioned by M.
+ * *iters follows the reference: the 0-based index of the converged iteration. */
 DFM_API int dfm_solve_pcg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                   unsigned* iters, double* conv);
-/* The same with host buffers: copies b in, x out (end-to-end call). */
+/* LsSol::Solve_PBiCGSTAB (src/ls/solver_ls_iter.cpp:291-408): shadow residual
+ * r0, *iters 1-based.  Real matrices. */
+DFM_API int dfm_solve_pbicgstab(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
+                        unsigned* iters, double* conv);
+/* Fem::Ls::Solve_PCOCG (src/femls/zsolver_ls_iter.cpp:171-267): complex
+ * symmetric CG with unconjugated products, *iters 1-based.  Complex matrices;
+ * r and x are interleaved (re, im). */
+DFM_API int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
+                    unsigned* iters, double* conv);
+/* End-to-end variants with HOST buffers (b copied in, x copied out, inside the
+ * call); method is DFM_PCG, DFM_PBICGSTAB or DFM_PCOCG. */
+DFM_API int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
+                   unsigned maxit, unsigned* iters, double* conv);
 DFM_API int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol,
                        unsigned maxit, unsigned* iters, double* conv);
 
