@@ -397,12 +397,14 @@ int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
   if (!M || mode < 0 || mode > 3) return DFM_ERR_INVALID;
   if (mode == 3) return ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm);
   M->sweep = mode;
+  M->plan_gen++;
   return DFM_OK;
 }
 
 int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) {
   if (!M || max_blocks < 0 || poll_sleep_ns > 100000) return DFM_ERR_INVALID;
   M->sweep_blocks = max_blocks;
+  M->plan_gen++;
   return set_poll_sleep(poll_sleep_ns);
 }
 

@@ -91,6 +91,7 @@ struct dfm_ilu_s {
   int sweep = 0;                 // 0 untuned, 1 sync-free grid, 2 single CTA, 3 CTA row ranges
   int sweep_blocks = 0;          // sync-free grid size cap (0 = all co-resident blocks)
   dfm::SweepPlan plan_f, plan_b; // mode 3 plans (forward / backward)
+  unsigned plan_gen = 0;         // bumped whenever the schedule or its plans change
   float sweep_ms = 0.f;          // autotuned fwd+bwd time
   bool factored = false;
   size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }

@@ -259,6 +259,7 @@ k_zilu0_factor(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* 
 DFM_DEVINL bool converged_guard(KrylovScalars* sc, const double* rr_part, int nparts) {
   if (!sc) return false;
   if (block_flag(&sc->done)) return true;
+  if (!rr_part) return false;  // solver checks convergence elsewhere
   const double rr = reduce_partials(rr_part, nparts);
   if (rr * sc->inv0 < sc->tol2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -742,9 +743,10 @@ static int sweep_dispatch(dfm_ilu M, bool fwd, int sweep, const double* in, doub
   return DFM_OK;
 }
 
-int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep) {
-  return sweep_dispatch(M, true, sweep, r, y, nullptr, nullptr, sc, sc ? M->ctx->part(2) : nullptr,
-                        sc ? spmv_grid(M->A) : 0);
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check) {
+  const bool chk = sc && rr_check;
+  return sweep_dispatch(M, true, sweep, r, y, nullptr, nullptr, sc, chk ? M->ctx->part(2) : nullptr,
+                        chk ? spmv_grid(M->A) : 0);
 }
 
 int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part, KrylovScalars* sc,
@@ -843,6 +845,7 @@ int ilu_autotune(dfm_ilu M) {
     }
     std::swap(M->plan_f, best_f);
     std::swap(M->plan_b, best_b);
+    M->plan_gen++;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -869,6 +872,7 @@ int ilu_set_ranges(dfm_ilu M, int G) {
   std::swap(M->plan_f, pf);
   std::swap(M->plan_b, pb);
   M->sweep = 3;
+  M->plan_gen++;
   return DFM_OK;
 }
 

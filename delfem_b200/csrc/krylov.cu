@@ -1,19 +1,25 @@
-// ILU(0)-preconditioned CG on the device, LsSol::Solve_PCG
-// (src/ls/solver_ls_iter.cpp:100-172), with the reference's stop test
-// (recursive residual, |r|^2/|r0|^2 < tol^2) and iteration convention.
+// ILU(0)-preconditioned Krylov solvers on the device, with the reference's
+// stop tests and iteration conventions:
+//   PCG        LsSol::Solve_PCG        src/ls/solver_ls_iter.cpp:100-172
+//              (x = 0; stop on |r|^2/|r0|^2 < tol^2; *iters = 0-based index)
+//   PBiCGSTAB  LsSol::Solve_PBiCGSTAB  src/ls/solver_ls_iter.cpp:291-408
+//              (shadow residual r2 = r0; 1-based iterations; max_iter reached
+//              is still `true` in the reference, DFM_NOT_CONVERGED here)
+//   PCOCG      Fem::Ls::Solve_PCOCG    src/femls/zsolver_ls_iter.cpp:171-267
+//              (complex symmetric, unconjugated products; 1-based iterations)
 //
-// One iteration = 5 kernels, all scalars in device memory (KrylovScalars):
-//   K1 q = A p, partial (p, q)                     [SpMV + fused dot]
-//   K2 alpha = (r,z)/(p,q); r -= alpha q; x += alpha p; partial (r, r);
-//      pre-fill the sweep outputs with the sentinel
-//   K3 y = L^-1 r   (first: stop if |r|^2/|r0|^2 < tol^2)
-//   K4 z = U^-1 y, partial (r, z)
-//   K5 beta = (r,z)_new/(r,z); p = beta p + z; it++
-// Every reduction is a fixed-order sum of per-block partials, so a solve is
+// Every scalar lives in device memory (KrylovScalars); every reduction is a
+// fixed-order sum of per-block partials (ctx part(k) arrays), so a solve is
 // bit-reproducible run to run.  A CUDA graph of kIterPerGraph iterations is
-// replayed until the device sets `done` (converged, maxit, breakdown).
+// replayed until the device sets `done` (converged, max_iter, breakdown).
+// Kernels after `done` return at once.  A scalar that one kernel derives and a
+// later kernel needs is written by block 0 of the producer and read by the
+// consumer kernel only, never within the kernel that writes it.
+//
+// Partial slots: 0,1 SpMV dots; 2 (r, r); 3,4 preconditioned dots.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "dfm_internal.h"
 
@@ -24,10 +30,22 @@ constexpr int kVecThreads = 256;
 
 static int vec_grid(dfm_mat A) { return spmv_grid(A); }
 
+#define GRID_LOOP(k, n) \
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < (n); k += (size_t)gridDim.x * blockDim.x)
+
+DFM_DEVINL void finish(KrylovScalars* sc, int status, double conv) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->conv = conv;
+    sc->conv_it = sc->it;
+    sc->done = 100 + status;
+  }
+}
+
+// ============================================================== PCG (real)
 __global__ void __launch_bounds__(kVecThreads)
 k_pcg_start(size_t n, const double* __restrict__ r, double* __restrict__ x, double* y, double* z, double* part_rr) {
   double acc = 0.0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+  GRID_LOOP(k, n) {
     const double rv = r[k];
     acc += rv * rv;
     x[k] = 0.0;
@@ -52,33 +70,23 @@ k_pcg_start2(size_t n, KrylovScalars* sc, const double* part_rr, int np_rr, cons
       sc->done = 0;
     }
   }
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    p[k] = z[k];
+  GRID_LOOP(k, n) p[k] = z[k];
 }
 
 __global__ void __launch_bounds__(kVecThreads)
 k_pcg_update_xr(size_t n, KrylovScalars* sc, const double* part_pq, int np_pq, const double* part_rz, int np_rz,
-                double* part_rr_prev_and_new, int np_rr, double* __restrict__ q_then_z, const double* __restrict__ p,
+                double* part_rr, int np_rr, double* __restrict__ q_then_z, const double* __restrict__ p,
                 double* __restrict__ r, double* __restrict__ x, double* __restrict__ y) {
   if (block_flag(&sc->done)) return;
   if (sc->it >= sc->maxit) {  // reference: loop ends, conv from the last (r, r)
-    const double rr = reduce_partials(part_rr_prev_and_new, np_rr);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      sc->conv = sqrt(rr * sc->inv0);
-      sc->conv_it = sc->it;
-      sc->done = 100 + DFM_NOT_CONVERGED;
-    }
+    finish(sc, DFM_NOT_CONVERGED, sqrt(reduce_partials(part_rr, np_rr) * sc->inv0));
     return;
   }
   const double rz = reduce_partials(part_rz, np_rz);
   const double pq = reduce_partials(part_pq, np_pq);
   const double alpha = rz / pq;
   if (!isfinite(alpha)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      sc->conv_it = sc->it;
-      sc->conv = NAN;
-      sc->done = 100 + DFM_BREAKDOWN;
-    }
+    finish(sc, DFM_BREAKDOWN, NAN);
     return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -86,7 +94,7 @@ k_pcg_update_xr(size_t n, KrylovScalars* sc, const double* part_pq, int np_pq, c
     sc->alpha = alpha;
   }
   double acc = 0.0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+  GRID_LOOP(k, n) {
     const double qv = q_then_z[k];
     const double rv = r[k] - alpha * qv;
     r[k] = rv;
@@ -95,7 +103,7 @@ k_pcg_update_xr(size_t n, KrylovScalars* sc, const double* part_pq, int np_pq, c
     y[k] = Sent<double>::value();
     q_then_z[k] = Sent<double>::value();
   }
-  block_partial<kVecThreads>(acc, part_rr_prev_and_new);
+  block_partial<kVecThreads>(acc, part_rr);
 }
 
 __global__ void __launch_bounds__(kVecThreads)
@@ -104,55 +112,440 @@ k_pcg_update_p(size_t n, KrylovScalars* sc, const double* part_rz, int np_rz, co
   if (block_flag(&sc->done)) return;
   const double rz_new = reduce_partials(part_rz, np_rz);
   const double beta = rz_new / sc->rz;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    p[k] = p[k] * beta + z[k];
+  GRID_LOOP(k, n) p[k] = p[k] * beta + z[k];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     sc->beta = beta;
     sc->it = sc->it + 1;
   }
 }
 
-// Solve workspace kept on the ILU object: vectors, and the captured graph of
-// kIterPerGraph iterations for the (A, M) pair it was built with.
-struct PcgPlan {
-  dfm_mat A = nullptr;
-  double *r = nullptr, *x = nullptr, *p = nullptr, *z = nullptr, *y = nullptr;
-  size_t n = 0;
+// ======================================================== PBiCGSTAB (real)
+// start: x = 0, r2 = r, p = r, partials of (r, r) into slot 2 and (r, r2) into slot 3
+__global__ void __launch_bounds__(kVecThreads)
+k_bicg_start(size_t n, const double* __restrict__ r, double* __restrict__ x, double* __restrict__ r2,
+             double* __restrict__ p, double* y, double* Mp, double* part_rr, double* part_rr2) {
+  double acc = 0.0;
+  GRID_LOOP(k, n) {
+    const double rv = r[k];
+    acc += rv * rv;
+    x[k] = 0.0;
+    r2[k] = rv;
+    p[k] = rv;
+    y[k] = Sent<double>::value();
+    Mp[k] = Sent<double>::value();
+  }
+  block_partial<kVecThreads>(acc, part_rr);
+  block_partial<kVecThreads>(acc, part_rr2);
+}
+
+__global__ void k_bicg_start2(KrylovScalars* sc, const double* part_rr, int np_rr) {
+  const double rr0 = reduce_partials(part_rr, np_rr);
+  if (threadIdx.x == 0) {
+    sc->it = 1;
+    if (rr0 < 1.0e-60) {  // reference: conv_ratio = sqrt(sq0), iteration = 0, return true
+      sc->conv = sqrt(rr0);
+      sc->conv_it = 0;
+      sc->done = 100 + DFM_OK;
+    } else {
+      sc->inv0 = 1.0 / rr0;
+      sc->done = 0;
+    }
+  }
+}
+
+// alpha = (r, r2) / (AMp, r2); s = r - alpha AMp
+__global__ void __launch_bounds__(kVecThreads)
+k_bicg_s(size_t n, KrylovScalars* sc, const double* part_amp_r2, int np_spmv, const double* part_r_r2, int np_vec,
+         const double* part_rr, const double* __restrict__ r, const double* __restrict__ AMp,
+         double* __restrict__ s, double* y, double* Ms) {
+  if (block_flag(&sc->done)) return;
+  if (sc->it >= sc->maxit) {
+    finish(sc, DFM_NOT_CONVERGED, sqrt(reduce_partials(part_rr, np_vec) * sc->inv0));
+    return;
+  }
+  const double r_r2 = reduce_partials(part_r_r2, np_vec);
+  const double alpha = r_r2 / reduce_partials(part_amp_r2, np_spmv);
+  if (!isfinite(alpha)) {
+    finish(sc, DFM_BREAKDOWN, NAN);
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->rho = r_r2;
+    sc->alpha = alpha;
+  }
+  GRID_LOOP(k, n) {
+    s[k] = r[k] - alpha * AMp[k];
+    y[k] = Sent<double>::value();
+    Ms[k] = Sent<double>::value();
+  }
+}
+
+// omega = (s, AMs) / (AMs, AMs); x += alpha Mp + omega Ms; r = s - omega AMs;
+// partials of (r, r) and (r, r2)
+__global__ void __launch_bounds__(kVecThreads)
+k_bicg_xr(size_t n, KrylovScalars* sc, const double* part_num, const double* part_den, int np_spmv,
+          double* part_rr, double* part_r_r2, const double* __restrict__ Mp, const double* __restrict__ Ms,
+          const double* __restrict__ s, const double* __restrict__ AMs, const double* __restrict__ r2,
+          double* __restrict__ x, double* __restrict__ r) {
+  if (block_flag(&sc->done)) return;
+  const double omega = reduce_partials(part_num, np_spmv) / reduce_partials(part_den, np_spmv);
+  if (!isfinite(omega)) {
+    finish(sc, DFM_BREAKDOWN, NAN);
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->omega = omega;
+  const double alpha = sc->alpha;
+  double a_rr = 0.0, a_rr2 = 0.0;
+  GRID_LOOP(k, n) {
+    x[k] = (x[k] + alpha * Mp[k]) + omega * Ms[k];
+    const double rv = s[k] - omega * AMs[k];
+    r[k] = rv;
+    a_rr += rv * rv;
+    a_rr2 += rv * r2[k];
+  }
+  block_partial<kVecThreads>(a_rr, part_rr);
+  block_partial<kVecThreads>(a_rr2, part_r_r2);
+}
+
+// stop test; beta = (r, r2)_new alpha / ((r, r2) omega); p = beta p + r - beta omega AMp
+__global__ void __launch_bounds__(kVecThreads)
+k_bicg_p(size_t n, KrylovScalars* sc, const double* part_rr, const double* part_r_r2, int np_vec,
+         const double* __restrict__ r, const double* __restrict__ AMp, double* __restrict__ p, double* y,
+         double* Mp) {
+  if (block_flag(&sc->done)) return;
+  const double rr = reduce_partials(part_rr, np_vec);
+  if (rr * sc->inv0 < sc->tol2) {
+    finish(sc, DFM_OK, sqrt(rr * sc->inv0));
+    return;
+  }
+  const double tmp1 = reduce_partials(part_r_r2, np_vec);
+  const double alpha = sc->alpha, omega = sc->omega;
+  const double beta = tmp1 * alpha / (sc->rho * omega);
+  const double bo = -beta * omega;
+  GRID_LOOP(k, n) {
+    p[k] = (p[k] * beta + r[k]) + bo * AMp[k];
+    y[k] = Sent<double>::value();
+    Mp[k] = Sent<double>::value();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->beta = beta;
+    sc->it = sc->it + 1;
+  }
+}
+
+// ========================================================== PCOCG (complex)
+DFM_DEVINL double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+DFM_DEVINL double2 zdiv(double2 a, double2 b) {  // Com::Complex operator/ (include/delfem/complex.h)
+  const double f = 1.0 / (b.x * b.x + b.y * b.y);
+  return make_double2((a.x * b.x + a.y * b.y) * f, (-a.x * b.y + a.y * b.x) * f);
+}
+
+// start: x = 0, partials of |r|^2 (slot 2), y and w to the sentinel
+__global__ void __launch_bounds__(kVecThreads)
+k_cocg_start(size_t n2, const double* __restrict__ r, double* __restrict__ x, double* y, double* w, double* part_rr) {
+  double acc = 0.0;
+  GRID_LOOP(k, n2) {
+    const double rv = r[k];
+    acc += rv * rv;
+    x[k] = 0.0;
+    y[k] = Sent<double>::value();
+    w[k] = Sent<double>::value();
+  }
+  block_partial<kVecThreads>(acc, part_rr);
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+k_cocg_start2(size_t n2, KrylovScalars* sc, const double* part_rr, int np_rr, const double* __restrict__ w,
+              double* __restrict__ p) {
+  const double rr0 = reduce_partials(part_rr, np_rr);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->it = 1;
+    if (rr0 < 1.0e-30) {
+      sc->conv = 0.0;
+      sc->conv_it = 0;
+      sc->done = 100 + DFM_OK;
+    } else {
+      sc->inv0 = 1.0 / rr0;
+      sc->done = 0;
+    }
+  }
+  GRID_LOOP(k, n2) p[k] = w[k];
+}
+
+// alpha = (r, w) / (p, Ap) (unconjugated); x += alpha p; r -= alpha Ap; partials of |r|^2
+__global__ void __launch_bounds__(kVecThreads)
+k_cocg_xr(size_t N, KrylovScalars* sc, const double* part_pap, int np_spmv, const double* part_rw, int np_rw,
+          double* part_rr, int np_vec, const double2* __restrict__ p, const double2* __restrict__ Ap,
+          double2* __restrict__ x, double2* __restrict__ r, double2* y, double2* w) {
+  if (block_flag(&sc->done)) return;
+  if (sc->it >= sc->maxit) {
+    finish(sc, DFM_NOT_CONVERGED, sqrt(reduce_partials(part_rr, np_vec) * sc->inv0));
+    return;
+  }
+  const double2 rw = make_double2(reduce_partials(part_rw, np_rw), reduce_partials(part_rw + kMaxBlocks, np_rw));
+  const double2 pap =
+      make_double2(reduce_partials(part_pap, np_spmv), reduce_partials(part_pap + kMaxBlocks, np_spmv));
+  const double2 alpha = zdiv(rw, pap);
+  if (!isfinite(alpha.x) || !isfinite(alpha.y)) {
+    finish(sc, DFM_BREAKDOWN, NAN);
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->zr[0] = rw.x;
+    sc->zr[1] = rw.y;
+    sc->zr[2] = alpha.x;
+    sc->zr[3] = alpha.y;
+  }
+  const double2 sent = make_double2(Sent<double>::value(), Sent<double>::value());
+  double acc = 0.0;
+  GRID_LOOP(k, N) {
+    const double2 pk = p[k], ak = Ap[k];
+    const double2 ap = zmul(alpha, pk), aa = zmul(alpha, ak);
+    double2 xv = x[k], rv = r[k];
+    xv.x += ap.x; xv.y += ap.y;
+    rv.x -= aa.x; rv.y -= aa.y;
+    x[k] = xv;
+    r[k] = rv;
+    acc += rv.x * rv.x + rv.y * rv.y;
+    y[k] = sent;
+    w[k] = sent;
+  }
+  block_partial<kVecThreads>(acc, part_rr);
+}
+
+// beta = (r, w)_new / (r, w); p = beta p + w
+__global__ void __launch_bounds__(kVecThreads)
+k_cocg_p(size_t N, KrylovScalars* sc, const double* part_rw, int np_rw, const double2* __restrict__ w,
+         double2* __restrict__ p) {
+  if (block_flag(&sc->done)) return;
+  const double2 rw2 = make_double2(reduce_partials(part_rw, np_rw), reduce_partials(part_rw + kMaxBlocks, np_rw));
+  const double2 beta = zdiv(rw2, make_double2(sc->zr[0], sc->zr[1]));
+  GRID_LOOP(k, N) {
+    const double2 t = zmul(p[k], beta), wk = w[k];
+    p[k] = make_double2(t.x + wk.x, t.y + wk.y);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->it = sc->it + 1;
+}
+
+// ============================================================ solve plans
+// vectors: PCG uses R X P Z Y; PCOCG adds Q (= Ap); PBiCGSTAB uses all
+// (Z = Mp, Q = AMp).
+enum { kVecR, kVecX, kVecP, kVecZ, kVecY, kVecQ, kVecR2, kVecS, kVecMs, kVecAMs, kNumVec };
+
+static int vectors_of(int method) {
+  return method == DFM_PBICGSTAB ? kNumVec : method == DFM_PCOCG ? kVecQ + 1 : kVecY + 1;
+}
+
+// Workspace of one (M, method) pair: vectors and the captured graph, with the
+// launch configuration the graph was captured with.
+struct SolvePlan {
+  dfm_ilu M = nullptr;
+  int method = 0;
+  size_t n = 0;  // doubles per vector
+  double* v[kNumVec] = {};
   cudaGraphExec_t exec = nullptr;
   bool graph_failed = false;
+  // capture key: everything the captured kernel arguments depend on
+  int key_sweep = -1, key_lanes = -1;
+  unsigned key_gen = ~0u;
+  unsigned long long key_wait = 0;
 };
 
-static PcgPlan* plan_of(dfm_ilu M);
+static std::mutex g_plan_mu;
+static std::vector<SolvePlan*>& registry() {
+  static std::vector<SolvePlan*> r;
+  return r;
+}
 
-static int enqueue_iteration(dfm_mat A, dfm_ilu M, PcgPlan* P, KrylovScalars* sc) {
+static void plan_drop_graph(SolvePlan* P) {
+  if (P->exec) cudaGraphExecDestroy(P->exec);
+  P->exec = nullptr;
+  P->graph_failed = false;
+}
+
+static int plan_of(dfm_ilu M, int method, SolvePlan** out) {
+  std::lock_guard<std::mutex> lock(g_plan_mu);
+  for (auto* e : registry())
+    if (e->M == M && e->method == method) {
+      *out = e;
+      return DFM_OK;
+    }
+  auto* P = new (std::nothrow) SolvePlan();
+  if (!P) return DFM_ERR_NOMEM;
+  P->M = M;
+  P->method = method;
+  P->n = (size_t)M->N * M->xw();
+  const size_t bytes = std::max<size_t>(P->n, 1) * sizeof(double);
+  for (int k = 0; k < vectors_of(method); k++)
+    if (cudaMalloc(&P->v[k], bytes) != cudaSuccess) {
+      cudaGetLastError();
+      for (int j = 0; j < k; j++) cudaFree(P->v[j]);
+      delete P;
+      return DFM_ERR_NOMEM;
+    }
+  registry().push_back(P);
+  *out = P;
+  return DFM_OK;
+}
+
+void solve_release(dfm_ilu M) {
+  std::lock_guard<std::mutex> lock(g_plan_mu);
+  auto& r = registry();
+  for (size_t k = 0; k < r.size();) {
+    if (r[k]->M != M) { k++; continue; }
+    SolvePlan* P = r[k];
+    plan_drop_graph(P);
+    for (double* v : P->v) cudaFree(v);
+    delete P;
+    r.erase(r.begin() + k);
+  }
+}
+
+// -------------------------------------------------- one iteration per method
+static int enqueue_pcg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   dfm_ctx c = A->ctx;
-  const int gv = vec_grid(A);
-  const int gs = sweep_grid(M, M->sweep);
-  int rc = spmv_launch(A, 1.0, P->p, 0.0, P->z, c->part(0), gv, sc, A->lanes);
+  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *z = P->v[kVecZ], *y = P->v[kVecY];
+  int rc = spmv_launch(A, 1.0, p, 0.0, z, c->part(0), gv, sc, A->lanes);
   if (rc) return rc;
-  k_pcg_update_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(1), gs, c->part(2), gv, P->z,
-                                                    P->p, P->r, P->x, P->y);
+  k_pcg_update_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv, z, p,
+                                                    r, x, y);
   DFM_CUDA_TRY(cudaGetLastError());
-  rc = ilu_fwd_launch(M, P->r, P->y, sc, M->sweep);
-  if (rc) return rc;
-  rc = ilu_bwd_launch(M, P->y, P->z, P->r, c->part(1), sc, M->sweep);
-  if (rc) return rc;
-  k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(1), gs, P->z, P->p);
+  if ((rc = ilu_fwd_launch(M, r, y, sc, M->sweep))) return rc;
+  if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), sc, M->sweep))) return rc;
+  k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(3), gs, z, p);
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;
 }
 
-int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
-              double* conv) {
+static int enqueue_bicg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  const int gv = vec_grid(A);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *Mp = P->v[kVecZ], *y = P->v[kVecY];
+  double *AMp = P->v[kVecQ], *r2 = P->v[kVecR2], *s = P->v[kVecS], *Ms = P->v[kVecMs], *AMs = P->v[kVecAMs];
+  int rc;
+  // Mp = M^-1 p; AMp = A Mp with (r2, AMp)
+  if ((rc = ilu_fwd_launch(M, p, y, sc, M->sweep, false))) return rc;
+  if ((rc = ilu_bwd_launch(M, y, Mp, nullptr, nullptr, sc, M->sweep))) return rc;
+  if ((rc = spmv_launch(A, 1.0, Mp, 0.0, AMp, c->part(0), gv, sc, A->lanes, r2))) return rc;
+  k_bicg_s<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(3), gv, c->part(2), r, AMp, s, y, Ms);
+  DFM_CUDA_TRY(cudaGetLastError());
+  // Ms = M^-1 s; AMs = A Ms with (s, AMs) and (AMs, AMs)
+  if ((rc = ilu_fwd_launch(M, s, y, sc, M->sweep, false))) return rc;
+  if ((rc = ilu_bwd_launch(M, y, Ms, nullptr, nullptr, sc, M->sweep))) return rc;
+  if ((rc = spmv_launch(A, 1.0, Ms, 0.0, AMs, c->part(0), gv, sc, A->lanes, s, c->part(1)))) return rc;
+  k_bicg_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), c->part(1), gv, c->part(2), c->part(3), Mp, Ms,
+                                              s, AMs, r2, x, r);
+  DFM_CUDA_TRY(cudaGetLastError());
+  k_bicg_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(2), c->part(3), gv, r, AMp, p, y, Mp);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *w = P->v[kVecZ], *y = P->v[kVecY];
+  double* Ap = P->v[kVecQ];
+  int rc = spmv_launch(A, 1.0, p, 0.0, Ap, c->part(0), gv, sc, A->lanes);  // (p, Ap) re/im in slots 0/1
+  if (rc) return rc;
+  k_cocg_xr<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv,
+                                              reinterpret_cast<const double2*>(p),
+                                              reinterpret_cast<const double2*>(Ap), reinterpret_cast<double2*>(x),
+                                              reinterpret_cast<double2*>(r), reinterpret_cast<double2*>(y),
+                                              reinterpret_cast<double2*>(w));
+  DFM_CUDA_TRY(cudaGetLastError());
+  if ((rc = ilu_fwd_launch(M, r, y, sc, M->sweep))) return rc;                 // stop test on slot 2
+  if ((rc = ilu_bwd_launch(M, y, w, r, c->part(3), sc, M->sweep))) return rc;  // (r, w) re/im in slots 3/4
+  k_cocg_p<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(3), gs, reinterpret_cast<const double2*>(w),
+                                             reinterpret_cast<double2*>(p));
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  switch (P->method) {
+    case DFM_PBICGSTAB: return enqueue_bicg(A, M, P, sc);
+    case DFM_PCOCG: return enqueue_cocg(A, M, P, sc);
+    default: return enqueue_pcg(A, M, P, sc);
+  }
+}
+
+// ---------------------------------------------------------- initial steps
+static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  cudaStream_t s = c->stream;
+  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *z = P->v[kVecZ], *y = P->v[kVecY];
+  int rc;
+  switch (P->method) {
+    case DFM_PBICGSTAB:
+      k_bicg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, P->v[kVecR2], p, y, z, c->part(2), c->part(3));
+      DFM_CUDA_TRY(cudaGetLastError());
+      k_bicg_start2<<<1, kVecThreads, 0, s>>>(sc, c->part(2), gv);
+      break;
+    case DFM_PCOCG:
+      k_cocg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, y, z, c->part(2));
+      DFM_CUDA_TRY(cudaGetLastError());
+      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep))) return rc;
+      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep))) return rc;
+      k_cocg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, z, p);
+      break;
+    default:
+      k_pcg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, y, z, c->part(2));
+      DFM_CUDA_TRY(cudaGetLastError());
+      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep))) return rc;
+      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep))) return rc;
+      k_pcg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, z, p);
+      break;
+  }
+  (void)gs;
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+// Capture kIterPerGraph iterations once per plan and launch configuration.
+static void ensure_graph(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  const bool same = P->key_sweep == M->sweep && P->key_lanes == A->lanes && P->key_gen == M->plan_gen &&
+                    P->key_wait == c->wait_ns;
+  if (!same) {
+    plan_drop_graph(P);
+    P->key_sweep = M->sweep;
+    P->key_lanes = A->lanes;
+    P->key_gen = M->plan_gen;
+    P->key_wait = c->wait_ns;
+  }
+  if (P->exec || P->graph_failed) return;
+  cudaStream_t s = c->stream;
+  cudaGraph_t g = nullptr;
+  bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  int erc = DFM_OK;
+  if (ok) {
+    for (int k = 0; k < kIterPerGraph && erc == DFM_OK; k++) erc = enqueue_iteration(A, M, P, sc);
+    ok = (cudaStreamEndCapture(s, &g) == cudaSuccess) && erc == DFM_OK;
+  }
+  if (ok) ok = cudaGraphInstantiate(&P->exec, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    P->exec = nullptr;
+    P->graph_failed = true;
+    cudaGetLastError();  // clear a capture error; iterations are then launched directly
+  }
+}
+
+// Runs `method` on A x = b.  b: N*xw doubles at `b_where`; x receives the
+// solution (at x_where); r_out (device, nullable) receives the final residual.
+int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where, double* x, int x_where,
+                 double* r_out, double tol, unsigned maxit, unsigned* iters, double* conv) {
   dfm_ctx c = A->ctx;
   cudaStream_t s = c->stream;
   int rc = spmv_autotune(A);
   if (rc) return rc;
-  rc = ilu_autotune(M);
-  if (rc) return rc;
-  PcgPlan* P = plan_of(M);
-  const size_t n = (size_t)A->N * A->xw();
-  if (P->n != n) return DFM_ERR_INVALID;
+  if ((rc = ilu_autotune(M))) return rc;
+  SolvePlan* P = nullptr;
+  if ((rc = plan_of(M, method, &P))) return rc;
+  const size_t n = P->n;
   KrylovScalars* sc = c->d_scal;
   {
     KrylovScalars h = {};
@@ -160,34 +553,10 @@ int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned m
     h.tol2 = tol * tol;
     DFM_CUDA_TRY(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
   }
-  DFM_CUDA_TRY(cudaMemcpyAsync(P->r, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  const int gv = vec_grid(A);
-  const int gs = sweep_grid(M, M->sweep);
-  // x = 0; (r, r); z = M^-1 r; p = z; (r, z)
-  k_pcg_start<<<gv, kVecThreads, 0, s>>>(n, P->r, P->x, P->y, P->z, c->part(2));
-  DFM_CUDA_TRY(cudaGetLastError());
-  if ((rc = ilu_fwd_launch(M, P->r, P->y, nullptr, M->sweep))) return rc;
-  if ((rc = ilu_bwd_launch(M, P->y, P->z, P->r, c->part(1), nullptr, M->sweep))) return rc;
-  k_pcg_start2<<<gv, kVecThreads, 0, s>>>(n, sc, c->part(2), gv, P->z, P->p);
-  DFM_CUDA_TRY(cudaGetLastError());
-
-  // capture kIterPerGraph iterations once per plan
-  if (!P->exec && !P->graph_failed) {
-    cudaGraph_t g = nullptr;
-    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    int erc = DFM_OK;
-    if (ok) {
-      for (int k = 0; k < kIterPerGraph && erc == DFM_OK; k++) erc = enqueue_iteration(A, M, P, sc);
-      ok = (cudaStreamEndCapture(s, &g) == cudaSuccess) && erc == DFM_OK;
-    }
-    if (ok) ok = cudaGraphInstantiate(&P->exec, g, 0) == cudaSuccess;
-    if (g) cudaGraphDestroy(g);
-    if (!ok) {
-      P->exec = nullptr;
-      P->graph_failed = true;
-      cudaGetLastError();  // clear a capture error; fall back to direct launches
-    }
-  }
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->v[kVecR], b, n * sizeof(double),
+                               b_where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  if ((rc = enqueue_start(A, M, P, sc))) return rc;
+  ensure_graph(A, M, P, sc);
   for (;;) {
     if (P->exec) {
       DFM_CUDA_TRY(cudaGraphLaunch(P->exec, s));
@@ -201,8 +570,13 @@ int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned m
     const int code = take_code(c);
     if (code) return code;
   }
-  DFM_CUDA_TRY(cudaMemcpyAsync(x, P->x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  DFM_CUDA_TRY(cudaMemcpyAsync(r, P->r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  // Solve_PBiCGSTAB returns before zeroing x when |r0|^2 < 1e-60: x is left as given
+  const bool keep_x = method == DFM_PBICGSTAB && c->h_scal->done == 100 + DFM_OK && c->h_scal->conv_it == 0;
+  if (!keep_x)
+    DFM_CUDA_TRY(cudaMemcpyAsync(x, P->v[kVecX], n * sizeof(double),
+                                 x_where == DFM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+  if (r_out) DFM_CUDA_TRY(cudaMemcpyAsync(r_out, P->v[kVecR], n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  DFM_CUDA_TRY(cudaStreamSynchronize(s));
   {
     const int code = take_code(c);
     if (code) return code;
@@ -211,47 +585,6 @@ int pcg_solve(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned m
   if (iters) *iters = h->conv_it;
   if (conv) *conv = h->conv;
   return h->done - 100;
-}
-
-// -------------------------------------------------------------- plan cache
-struct PlanRegistry {
-  dfm_ilu M;
-  PcgPlan plan;
-};
-static std::vector<PlanRegistry*>& registry() {
-  static std::vector<PlanRegistry*> r;
-  return r;
-}
-
-static PcgPlan* plan_of(dfm_ilu M) {
-  for (auto* e : registry())
-    if (e->M == M) return &e->plan;
-  auto* e = new PlanRegistry();
-  e->M = M;
-  PcgPlan& P = e->plan;
-  P.A = M->A;
-  P.n = (size_t)M->N * M->xw();
-  const size_t bytes = std::max<size_t>(P.n, 1) * sizeof(double);
-  cudaMalloc(&P.r, bytes);
-  cudaMalloc(&P.x, bytes);
-  cudaMalloc(&P.p, bytes);
-  cudaMalloc(&P.z, bytes);
-  cudaMalloc(&P.y, bytes);
-  registry().push_back(e);
-  return &P;
-}
-
-void pcg_release(dfm_ilu M) {
-  auto& r = registry();
-  for (size_t k = 0; k < r.size(); k++) {
-    if (r[k]->M != M) continue;
-    PcgPlan& P = r[k]->plan;
-    if (P.exec) cudaGraphExecDestroy(P.exec);
-    cudaFree(P.r); cudaFree(P.x); cudaFree(P.p); cudaFree(P.z); cudaFree(P.y);
-    delete r[k];
-    r.erase(r.begin() + k);
-    return;
-  }
 }
 
 }  // namespace dfm

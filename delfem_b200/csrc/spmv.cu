@@ -7,27 +7,28 @@
 // nnz takes the diagonal block, so a row's contiguous b*b*8-byte blocks are
 // read by consecutive lanes (coalesced, streamed with evict-first hints) while
 // x is gathered through L1/L2.  Partial products are summed inside the group
-// with shuffles; lane 0 writes the b outputs.  An optional fused dot x.y is
-// reduced per block into a deterministic partial array.
+// with shuffles; lane 0 writes the b outputs.  Optional fused dots: w.y
+// (w = x unless given) and y.y, reduced per block into deterministic
+// partial arrays.
 #include <algorithm>
 
 #include "dfm_internal.h"
 
 namespace dfm {
 
-template <int B, int LPR, typename TV, typename TX, bool DOT>
+template <int B, int LPR, typename TV, typename TX, int NDOT>
 __global__ void __launch_bounds__(256)
 k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
        const TV* __restrict__ diag, const TV* __restrict__ off, double alpha,
        const TX* __restrict__ x, double beta, TX* __restrict__ y, double* __restrict__ part,
-       const int* done) {
+       const int* done, const TX* __restrict__ w, double* __restrict__ part2) {
   if (done && block_flag(done)) return;
   constexpr int BB = B * B;
   const int lane = threadIdx.x % LPR;
   const unsigned g0 = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
   const unsigned ng = gridDim.x * blockDim.x / LPR;
   const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
-  double dacc = 0.0;
+  double dacc = 0.0, dacc2 = 0.0;
   for (unsigned i = g0; i < N; i += ng) {
     const unsigned s0 = __ldg(rowptr + i), s1 = __ldg(rowptr + i + 1);
     double acc[B];
@@ -65,11 +66,13 @@ k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restri
         if (beta != 0.0) v += beta * (double)y[(size_t)i * B + r];
         const TX out = (TX)v;
         y[(size_t)i * B + r] = out;
-        if (DOT) dacc += (double)x[(size_t)i * B + r] * (double)out;
+        if (NDOT >= 1) dacc += (double)w[(size_t)i * B + r] * (double)out;
+        if (NDOT >= 2) dacc2 += (double)out * (double)out;
       }
     }
   }
-  if (DOT) block_partial<256>(dacc, part);
+  if (NDOT >= 1) block_partial<256>(dacc, part);
+  if (NDOT >= 2) block_partial<256>(dacc2, part2);
 }
 
 // Complex b = 1: values and vectors interleaved (re, im).
@@ -127,23 +130,28 @@ int spmv_grid(dfm_mat A) {
 
 template <int B, int LPR>
 static void launch_real(dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x, double beta,
-                        double* y, double* part, const int* done) {
-  if (part)
-    k_spmv<B, LPR, double, double, true><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
-                                                              alpha, x, beta, y, part, done);
+                        double* y, double* part, const int* done, const double* w, double* part2) {
+  if (!w) w = x;
+  if (part && part2)
+    k_spmv<B, LPR, double, double, 2><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
+                                                           alpha, x, beta, y, part, done, w, part2);
+  else if (part)
+    k_spmv<B, LPR, double, double, 1><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
+                                                           alpha, x, beta, y, part, done, w, nullptr);
   else
-    k_spmv<B, LPR, double, double, false><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag,
-                                                               A->d_off, alpha, x, beta, y, nullptr, done);
+    k_spmv<B, LPR, double, double, 0><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
+                                                           alpha, x, beta, y, nullptr, done, nullptr, nullptr);
 }
 
 template <int B>
 static void launch_real_lpr(int lanes, dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x,
-                            double beta, double* y, double* part, const int* done) {
+                            double beta, double* y, double* part, const int* done, const double* w,
+                            double* part2) {
   switch (lanes) {
-    case 4: launch_real<B, 4>(A, grid, s, alpha, x, beta, y, part, done); break;
-    case 8: launch_real<B, 8>(A, grid, s, alpha, x, beta, y, part, done); break;
-    case 16: launch_real<B, 16>(A, grid, s, alpha, x, beta, y, part, done); break;
-    default: launch_real<B, 32>(A, grid, s, alpha, x, beta, y, part, done); break;
+    case 4: launch_real<B, 4>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
+    case 8: launch_real<B, 8>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
+    case 16: launch_real<B, 16>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
+    default: launch_real<B, 32>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
   }
 }
 
@@ -162,7 +170,8 @@ static void launch_cplx(dfm_mat A, int grid, cudaStream_t s, double alpha, const
 }
 
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
-                int grid, KrylovScalars* sc, int lanes) {
+                int grid, KrylovScalars* sc, int lanes, const double* dot_w, double* dot_part2) {
+  if (A->vt == DFM_COMPLEX && (dot_w || dot_part2)) return DFM_ERR_UNSUPPORTED;
   if (A->N == 0) return DFM_OK;
   cudaStream_t s = A->ctx->stream;
   if (grid <= 0) grid = spmv_grid(A);
@@ -176,11 +185,11 @@ int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y
       default: launch_cplx<32>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
     }
   } else if (A->b == 1) {
-    launch_real_lpr<1>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done);
+    launch_real_lpr<1>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
   } else if (A->b == 2) {
-    launch_real_lpr<2>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done);
+    launch_real_lpr<2>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
   } else {
-    launch_real_lpr<3>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done);
+    launch_real_lpr<3>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
   }
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;

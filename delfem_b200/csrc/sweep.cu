@@ -108,7 +108,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
   // guards (block-uniform)
   if (sc) {
     if (block_flag(&sc->done)) return;
-    if (FWD) {
+    if (FWD && rr_part) {
       const double rr = reduce_partials(rr_part, rr_nparts);
       if (rr * sc->inv0 < sc->tol2) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -703,9 +703,9 @@ int dfo_pbicgstab(unsigned N, unsigned b, const unsigned* rowptr, const unsigned
     vaxpy(n, 1.0, r, p);
     vaxpy(n, -beta * omega, AMp, p);
   }
-  *conv = sqrt(vdot(n, r, r) * inv0);
+  *conv = tol; /* max_iter reached: the reference leaves conv_ratio at its input (the tolerance) */
   free(w);
-  return 1; /* the reference returns true at max_iter as well */
+  return 1; /* and returns true (src/ls/solver_ls_iter.cpp:327-407) */
 }
 
 /* ---------------------------------------------------------------- complex */
@@ -852,7 +852,7 @@ int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const 
     const zc one = {1.0, 0.0};
     zaxpy(N, one, w, p);
   }
-  *conv = sqrt(znorm2(N, r) * inv0);
+  *conv = tol; /* max_iter reached: conv_ratio keeps its input (the tolerance) */
   free(p); free(Ap); free(w);
-  return 1; /* Solve_PCOCG returns true at max_iter as well */
+  return 1; /* and Solve_PCOCG returns true (src/femls/zsolver_ls_iter.cpp:213-266) */
 }

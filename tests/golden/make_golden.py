@@ -1,0 +1,89 @@
+"""Generate the golden fixtures tests/golden/*.npz from the reference itself.
+
+Each fixture is one small seeded problem run through the reference's own CPU
+code (DelFEM sources compiled by oracle/Makefile, driven through
+oracle/ref_shim.cpp): the block-CRS pattern of CMatDia_BlkCrs, the assembled
+matrix and residual after Dirichlet elimination (CLinearSystem_Field), the
+ILU(0) factor (CPreconditioner_ILU), the reference's solve (Solve_PCG /
+Solve_PBiCGSTAB / Solve_PCOCG: x, iterations, convergence ratio) and one
+matrix-level SpMV and preconditioner application on a seeded vector.
+
+Run where the reference tree and its build are available:
+    make -C oracle REF=<reference tree> ref
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from delfem_b200 import meshes  # noqa: E402
+from oracle import refshim as R  # noqa: E402
+from tests import cases  # noqa: E402
+
+
+def case_list():
+    rng = np.random.default_rng(2024)
+    out = []
+    m = meshes.unit_square_tri(6)
+    out.append(("poisson_n6", R.POISSON2D, m, [1.0, 1.0], None, None, R.PCG))
+    m = meshes.unit_square_tri(6)
+    out.append(("poisson_coef_n6", R.POISSON2D, m, [1.0, 1.0], rng.lognormal(0, 1.0, m.elem.shape[0]), None, R.PCG))
+    m = meshes.unit_square_tri(5, bnd="left")
+    out.append(("solid2d_n5", R.SOLID2D, m, [cases.LAM2_PS, cases.MYU2, 0.0, 0.0, 0.0],
+                rng.lognormal(0, 0.5, m.elem.shape[0]), meshes.right_edge_traction(m, 5), R.PCG))
+    m = meshes.box_tet(4, 2, 2)
+    out.append(("solid3d_4x2x2", R.SOLID3D, m, [cases.LAM3, cases.MYU3, 1.0, 0.0, 0.0, -1.0], None, None, R.PCG))
+    m = meshes.box_tet(4, 2, 2)
+    out.append(("solid3d_bicgstab", R.SOLID3D, m, [cases.LAM3, cases.MYU3, 1.0, 0.0, 0.0, -1.0], None, None,
+                R.PBICGSTAB))
+    m = meshes.unit_disk_tri(8)
+    out.append(("helmholtz_r8_k4", R.HELMHOLTZ2D, m, [2 * 3.1416 / 4], None, meshes.gaussian_source_load(m),
+                R.PCOCG))
+    # under-resolved (k h = 2.5): stops at max_iter, the reference's exit values
+    out.append(("helmholtz_r8_maxit", R.HELMHOLTZ2D, m, [cases.WAVE_LENGTH], None, meshes.gaussian_source_load(m),
+                R.PCOCG))
+    return out
+
+
+def generate(path=HERE):
+    rng = np.random.default_rng(7)
+    for name, kind, m, params, coef, load, method in case_list():
+        S = R.RefSystem(kind, m)
+        rp, ci = S.pattern()
+        S.assemble(params, coef, load)
+        diag, off, rhs = S.system()
+        flags = S.bcflag()
+        S.ilu()
+        _, fd, fo = S.ilu_factor()
+        tol = 1e-10
+        maxit = 60 if name.endswith("maxit") else 2000
+        rc, x, it, conv, _ = S.solve(method, tol, maxit)
+        ok = rc == 0  # the shim returns 0 when the reference's solver returned true
+        v = rng.standard_normal(S.N * S.xw)
+        if S.cplx:
+            y = R.zmat_spmv(S.N, rp, ci, diag, off, 1.0, v, 0.0, np.zeros_like(v))
+            z = np.zeros(0)
+        else:
+            y = R.mat_spmv(S.N, S.b, rp, ci, diag, off, 1.0, v, 0.0, np.zeros_like(v))
+            z = R.mat_precond(S.N, S.b, rp, ci, fd, fo, v)
+        np.savez_compressed(
+            os.path.join(path, f"{name}.npz"),
+            kind=kind, method=method, params=np.asarray(params, np.float64),
+            coord=m.coord, elem=m.elem, bnd=m.bnd,
+            coef=np.zeros(0) if coef is None else coef,
+            load=np.zeros(0) if load is None else np.asarray(load, np.float64).ravel(),
+            rowptr=rp, colind=ci, diag=diag, off=off, rhs=rhs, bcflag=flags,
+            ilu_diag=fd, ilu_off=fo, x=x, iters=it, conv=conv, ok=int(bool(ok)), tol=tol, maxit=maxit,
+            vec=v, spmv=y, precond=z)
+        print(f"{name}: N={S.N} b={S.b} ncrs={S.ncrs} iters={it} conv={conv:.3e}")
+
+
+if __name__ == "__main__":
+    generate()

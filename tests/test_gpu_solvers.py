@@ -1,0 +1,156 @@
+"""PBiCGSTAB (real) and PCOCG (complex) on the device against the oracle's
+restatements of LsSol::Solve_PBiCGSTAB and Fem::Ls::Solve_PCOCG (pinned to the
+reference).  Parity bar: ||x - x_ref|| / ||x_ref|| <= 1e-8 at a relative
+residual of 1e-10, iteration counts within a few of the oracle's (the device
+reductions sum in a different order), and the reference's conventions for
+max_iter, a zero right-hand side and the end-to-end host entry."""
+import numpy as np
+import pytest
+
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+X_TOL = 1e-8
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float64)).cuda()
+
+
+def _gpu(ctx, S, sweep=0):
+    from delfem_b200 import lib
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b, lib.COMPLEX if S.cplx else lib.REAL)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    if sweep:
+        M.sweep = sweep
+    return A, M
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+REAL_SYSTEMS = {
+    "poisson20": lambda: cases.poisson(20)[1],
+    "poisson_coef": lambda: cases.poisson(24, np.random.default_rng(1).lognormal(0, 1.0, 2 * 24 * 24))[1],
+    "solid2d": lambda: cases.solid2d(10, np.random.default_rng(2).lognormal(0, 0.5, 200))[1],
+    "solid3d": lambda: cases.solid3d(6, 2, 2)[1],
+    "random_b1": lambda: cases.random_spd_like(300, 1, seed=3),
+    "random_b3": lambda: cases.random_spd_like(200, 3, seed=4),
+}
+
+
+@pytest.mark.parametrize("name", list(REAL_SYSTEMS))
+@pytest.mark.parametrize("sweep", [1, 2, 3])
+def test_pbicgstab_matches_oracle(ctx, name, sweep):
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS[name]()
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pbicgstab", tol=1e-10, maxit=2000)
+    assert ref["ok"]
+    A, M = _gpu(ctx, S, sweep)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pbicgstab(A, M, r, x, tol=1e-10, maxit=2000)
+    assert rc == lib.OK, (rc, it, conv)
+    assert abs(it - ref["iters"]) <= max(2, ref["iters"] // 20), (it, ref["iters"])
+    assert conv < 1e-10
+    assert _rel(x.cpu().numpy(), ref["x"]) <= X_TOL
+    # r holds the recursive residual on exit
+    res = S.rhs - S.spmv(1.0, x.cpu().numpy(), 0.0, np.zeros_like(S.rhs))
+    assert np.linalg.norm(res) <= 1e-8 * np.linalg.norm(S.rhs)
+
+
+def test_pbicgstab_maxit_and_zero_rhs(ctx):
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS["poisson20"]()
+    ns, fd, fo = S.ilu0()
+    A, M = _gpu(ctx, S)
+    ref = S.solve(fd, fo, method="pbicgstab", tol=1e-12, maxit=4)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pbicgstab(A, M, r, x, tol=1e-12, maxit=4)
+    assert rc == lib.NOT_CONVERGED and it == 4 == ref["iters"]  # the reference returns true here
+    # the reference leaves conv_ratio at the tolerance here; the device reports |r|/|r0|
+    assert ref["conv"] == 1e-12
+    assert conv == pytest.approx(np.linalg.norm(ref["r"]) / np.linalg.norm(S.rhs), rel=1e-6)
+    assert _rel(x.cpu().numpy(), ref["x"]) <= 1e-9
+    r = torch.zeros_like(r)
+    x = torch.full_like(r, 5.0)
+    rc, it, conv = lib.solve_pbicgstab(A, M, r, x)
+    # the reference returns before touching x when |r0|^2 < 1e-60
+    assert rc == lib.OK and it == 0 and float((x - 5.0).abs().max()) == 0.0
+
+
+def test_pbicgstab_host_entry(ctx):
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS["solid2d"]()
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pbicgstab", tol=1e-10, maxit=2000)
+    A, M = _gpu(ctx, S)
+    rc, x, it, conv = lib.solve_host(A, M, S.rhs, lib.PBICGSTAB, tol=1e-10, maxit=2000)
+    assert rc == lib.OK and _rel(x, ref["x"]) <= X_TOL
+
+
+@pytest.mark.parametrize("nring", [40, 60])
+@pytest.mark.parametrize("sweep", [1, 2])
+def test_pcocg_matches_oracle(ctx, nring, sweep):
+    from delfem_b200 import lib
+    m, S = cases.helmholtz(nring)
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcocg", tol=1e-10, maxit=5000)
+    assert ref["ok"] and ref["iters"] < 5000
+    A, M = _gpu(ctx, S, sweep)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcocg(A, M, r, x, tol=1e-10, maxit=5000)
+    assert rc == lib.OK, (rc, it, conv)
+    assert abs(it - ref["iters"]) <= max(3, ref["iters"] // 20), (it, ref["iters"])
+    assert _rel(x.cpu().numpy(), ref["x"]) <= X_TOL
+    rc, xh, it2, conv2 = lib.solve_host(A, M, S.rhs, lib.PCOCG, tol=1e-10, maxit=5000)
+    assert rc == lib.OK and it2 == it and np.array_equal(xh, x.cpu().numpy())  # deterministic
+
+
+def test_pcocg_maxit(ctx):
+    from delfem_b200 import lib
+    m, S = cases.helmholtz(40)
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcocg", tol=1e-10, maxit=7)
+    A, M = _gpu(ctx, S)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcocg(A, M, r, x, tol=1e-10, maxit=7)
+    assert rc == lib.NOT_CONVERGED and it == 7 == ref["iters"]
+    assert conv == pytest.approx(np.linalg.norm(ref["r"]) / np.linalg.norm(S.rhs), rel=1e-6)
+    assert _rel(x.cpu().numpy(), ref["x"]) <= 1e-9
+
+
+def test_method_value_type_mismatch(ctx):
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS["poisson20"]()
+    A, M = _gpu(ctx, S)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    with pytest.raises(lib.DfmError):
+        lib.solve_pcocg(A, M, r, x)
+
+
+def test_switching_sweep_recaptures(ctx):
+    """The captured iteration graph follows the sweep schedule: solving, changing
+    the schedule (which rebuilds the range plans) and solving again must give
+    the oracle's answer both times."""
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS["solid3d"]()
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcg", tol=1e-10, maxit=2000)
+    A, M = _gpu(ctx, S, 3)
+    for mode in (3, 1, 3, 2):
+        M.sweep = mode
+        r = _dev(S.rhs)
+        x = torch.zeros_like(r)
+        rc, it, conv = lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=2000)
+        assert rc == lib.OK and _rel(x.cpu().numpy(), ref["x"]) <= X_TOL, mode
