@@ -22,7 +22,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompil
          "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-warn-spills"]
 # Element assembly must add and multiply exactly as the reference's element
 # loops do (no fused multiply-add) for its bit-identical results.
-FILE_FLAGS = {"assemble.cu": ["-fmad=false"], "adjoint.cu": ["-fmad=false"]}
+FILE_FLAGS = {"assemble.cu": ["-fmad=false"]}
 
 
 def sources():

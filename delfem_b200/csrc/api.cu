@@ -226,6 +226,8 @@ int dfm_mat_destroy(dfm_mat A) {
   cudaFree(A->d_colind);
   cudaFree(A->d_diag);
   cudaFree(A->d_off);
+  cudaFree(A->d_diag32);
+  cudaFree(A->d_off32);
   delete A;
   return DFM_OK;
 }
@@ -341,6 +343,9 @@ int dfm_ilu_destroy(dfm_ilu M) {
   solve_release(M);
   sweep_plan_free(&M->plan_f);
   sweep_plan_free(&M->plan_b);
+  sweep_plan_free(&M->plan32_f);
+  sweep_plan_free(&M->plan32_b);
+  cudaFree(M->d_foff32);
   cudaFree(M->d_diaind);
   cudaFree(M->d_order_f);
   cudaFree(M->d_order_b);
@@ -455,9 +460,16 @@ int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsi
   return krylov_solve(A, M, DFM_PCOCG, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
 }
 
+int dfm_solve_pcg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                        double* conv) {
+  const int rc = solve_args(A, M, DFM_PCG_MIXED, r, x);
+  if (rc) return rc;
+  return krylov_solve(A, M, DFM_PCG_MIXED, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
 int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv) {
-  if (method != DFM_PCG && method != DFM_PBICGSTAB && method != DFM_PCOCG) return DFM_ERR_INVALID;
+  if (method < DFM_PCG || method > DFM_PCG_MIXED) return DFM_ERR_INVALID;
   const int rc = solve_args(A, M, method, b_host, x_host);
   if (rc) return rc;
   return krylov_solve(A, M, method, b_host, DFM_HOST, x_host, DFM_HOST, nullptr, tol, maxit, iters, conv);

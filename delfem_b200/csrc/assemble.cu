@@ -36,6 +36,8 @@ struct dfm_mesh_s {
   unsigned* d_esup = nullptr;
   unsigned* d_bsup_ptr = nullptr;  // node -> boundary bars (ascending)
   unsigned* d_bsup = nullptr;
+  std::vector<int> h_elem;         // host copies for the pattern
+  std::vector<unsigned> h_esup_ptr, h_esup;
 };
 
 namespace dfm {
@@ -379,6 +381,37 @@ __global__ void k_dirichlet(unsigned N, unsigned b, const unsigned* __restrict__
   }
 }
 
+// Adjoint element kernel: grad_e = -lambda_e^T (dK_e/dcoef_e) u_e, where the
+// element matrix is linear in its coefficient (K_e = coef_e K_e^0, K_e^0 the
+// matrix at the base constants P.p, as the assembly computes it).
+template <int KIND>
+__global__ void k_coef_grad(unsigned nelem, AsmParams P, const double* __restrict__ X, const int* __restrict__ elem,
+                            const double* __restrict__ lam, const double* __restrict__ u, double* __restrict__ grad) {
+  using K = Kind<KIND>;
+  constexpr int NNO = K::NNO, BW = K::BW, RW = K::RW;
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    int no[NNO];
+#pragma unroll
+    for (int c = 0; c < NNO; c++) no[c] = elem[(size_t)e * NNO + c];
+    double g = 0.0;
+#pragma unroll
+    for (int a = 0; a < NNO; a++) {
+      double blk[NNO * BW], res[RW];
+      K::row(P, e, no, X, a, blk, res);
+#pragma unroll
+      for (int r = 0; r < RW; r++) {
+        double v = 0.0;  // (K_e^0 u_e) at node a, component r
+#pragma unroll
+        for (int c = 0; c < NNO; c++)
+#pragma unroll
+          for (int s = 0; s < RW; s++) v += blk[c * BW + r * RW + s] * u[(size_t)no[c] * RW + s];
+        g += lam[(size_t)no[a] * RW + r] * v;
+      }
+    }
+    grad[e] = -g;
+  }
+}
+
 static void node_adjacency(unsigned nnode, unsigned nnoel, unsigned nelem, const int* elem, std::vector<unsigned>& ptr,
                            std::vector<unsigned>& lst) {
   ptr.assign(nnode + 1, 0);
@@ -451,7 +484,41 @@ int dfm_mesh_create(dfm_ctx c, int ndim, unsigned nnode, const double* coord, un
     dfm_mesh_destroy(G);
     return rc;
   }
+  G->h_elem.assign(elem, elem + (size_t)nelem * nnoel);
+  G->h_esup_ptr.swap(ep);
+  G->h_esup.swap(el);
   *out = G;
+  return DFM_OK;
+}
+
+// Block pattern of the mesh: node i's row lists every other node sharing an
+// element with it, ascending (CMatDia_BlkCrs::AddPattern over the field's
+// element connectivity, src/matvec/matdia_blkcrs.cpp:346-505).
+int dfm_mesh_pattern(dfm_mesh G, unsigned* rowptr, unsigned* colind, size_t* ncrs) {
+  if (!G || !ncrs) return DFM_ERR_INVALID;
+  const unsigned n = G->nnode, nno = G->nnoel;
+  std::vector<unsigned> mark(n, 0xffffffffu), row;
+  size_t total = 0;
+  if (rowptr) rowptr[0] = 0;
+  for (unsigned i = 0; i < n; i++) {
+    row.clear();
+    for (unsigned k = G->h_esup_ptr[i]; k < G->h_esup_ptr[i + 1]; k++) {
+      const int* no = G->h_elem.data() + (size_t)G->h_esup[k] * nno;
+      for (unsigned a = 0; a < nno; a++) {
+        const unsigned j = (unsigned)no[a];
+        if (j != i && mark[j] != i) {
+          mark[j] = i;
+          row.push_back(j);
+        }
+      }
+    }
+    std::sort(row.begin(), row.end());
+    if (colind) std::copy(row.begin(), row.end(), colind + total);
+    total += row.size();
+    if (total > 0xffffffffull) return DFM_ERR_UNSUPPORTED;
+    if (rowptr) rowptr[i + 1] = (unsigned)total;
+  }
+  *ncrs = total;
   return DFM_OK;
 }
 
@@ -500,6 +567,29 @@ int dfm_assemble_helmholtz2d(dfm_mesh G, dfm_mat A, double wave_length, const do
   AsmParams P = {{wave_length, 0, 0, 0, 0, 0}, nullptr, u};
   if (G->nbar) return launch_asm<K_HELM, K_SOMMER>(G, A, P, P, load, rhs);
   return launch_asm<K_HELM, -1>(G, A, P, P, load, rhs);
+}
+
+int dfm_coef_grad_poisson2d(dfm_mesh G, double alpha, const double* lam, const double* u, double* grad) {
+  if (!G || !lam || !u || !grad || G->ndim != 2) return DFM_ERR_INVALID;
+  if (G->nelem == 0) return DFM_OK;
+  AsmParams P = {{alpha, 0, 0, 0, 0, 0}, nullptr, nullptr};
+  const int grid = (int)std::min<unsigned>((G->nelem + 255) / 256, (unsigned)G->ctx->nsm * 8);
+  k_coef_grad<K_POISSON><<<grid, 256, 0, G->ctx->stream>>>(G->nelem, P, G->d_coord, G->d_elem, lam, u, grad);
+  DFM_CUDA_TRY(cudaGetLastError());
+  DFM_CUDA_TRY(cudaStreamSynchronize(G->ctx->stream));
+  return DFM_OK;
+}
+
+int dfm_coef_grad_solid2d(dfm_mesh G, double lambda, double myu, const double* lam, const double* u,
+                          double* grad) {
+  if (!G || !lam || !u || !grad || G->ndim != 2) return DFM_ERR_INVALID;
+  if (G->nelem == 0) return DFM_OK;
+  AsmParams P = {{lambda, myu, 0, 0, 0, 0}, nullptr, nullptr};
+  const int grid = (int)std::min<unsigned>((G->nelem + 255) / 256, (unsigned)G->ctx->nsm * 8);
+  k_coef_grad<K_SOLID2D><<<grid, 256, 0, G->ctx->stream>>>(G->nelem, P, G->d_coord, G->d_elem, lam, u, grad);
+  DFM_CUDA_TRY(cudaGetLastError());
+  DFM_CUDA_TRY(cudaStreamSynchronize(G->ctx->stream));
+  return DFM_OK;
 }
 
 int dfm_apply_dirichlet(dfm_mat A, const int* flags, double* rhs) {

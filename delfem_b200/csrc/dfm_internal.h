@@ -32,6 +32,8 @@ struct KrylovScalars {
   double inv0;     // 1 / |r0|^2
   double rz;       // (r, z) of the current direction
   double conv;     // final sqrt(|r|^2 / |r0|^2)
+  int conv_code;   // `done` written when the recursive residual meets tol (100 = final, 99 = verify first)
+  int pad_;
   double alpha, beta, omega, rho;  // BiCGSTAB / COCG extras
   double zr[4];    // complex scalars (re, im pairs)
 };
@@ -63,6 +65,8 @@ struct dfm_mat_s {
   unsigned* d_colind = nullptr;
   double* d_diag = nullptr;
   double* d_off = nullptr;
+  float* d_diag32 = nullptr;  // FP32 copies of the values for the mixed-precision solve
+  float* d_off32 = nullptr;
   std::vector<unsigned> h_rowptr, h_colind;
   unsigned max_row = 0;     // most off-diagonal blocks in one row
   int lanes = 0;            // SpMV lanes per block row (0 = not tuned yet)
@@ -85,12 +89,14 @@ struct dfm_ilu_s {
   unsigned nlev_f = 0, nlev_b = 0;
   double* d_fdiag = nullptr;     // D^-1 blocks
   double* d_foff = nullptr;      // L and D^-1 U blocks
+  float* d_foff32 = nullptr;     // FP32 copy of d_foff (mixed precision; D^-1 stays FP64)
   unsigned* d_flags = nullptr;   // per-row completion epochs of the numeric factorisation
   unsigned epoch = 0;
   double* d_tmp = nullptr;       // N*xw scratch: forward-sweep output of dfm_ilu_apply
   int sweep = 0;                 // 0 untuned, 1 sync-free grid, 2 single CTA, 3 CTA row ranges
   int sweep_blocks = 0;          // sync-free grid size cap (0 = all co-resident blocks)
   dfm::SweepPlan plan_f, plan_b; // mode 3 plans (forward / backward)
+  dfm::SweepPlan plan32_f, plan32_b;  // mode 3 plans with FP32 values
   unsigned plan_gen = 0;         // bumped whenever the schedule or its plans change
   float sweep_ms = 0.f;          // autotuned fwd+bwd time
   bool factored = false;
@@ -100,19 +106,37 @@ struct dfm_ilu_s {
 
 namespace dfm {
 // spmv.cu
-// dot_part: partials of (dot_w ? dot_w : x) . y; dot_part2: partials of y . y (real only).
+// Options of one SpMV launch (real matrices only except the defaults):
+//   dot_w  with dot_part: partials of (dot_w ? dot_w : x) . y
+//   dot_part2: partials of y . y beside the first dot
+//   yy: dot_part receives y . y instead (no w)
+//   y0: y = y0 + alpha A x (beta ignored)
+//   f32: multiply with the FP32 copy of the values
+struct SpmvOpts {
+  const double* dot_w = nullptr;
+  double* dot_part2 = nullptr;
+  bool yy = false;
+  const double* y0 = nullptr;
+  bool f32 = false;
+};
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
-                int nblocks_hint, KrylovScalars* sc, int lanes, const double* dot_w = nullptr,
-                double* dot_part2 = nullptr);
+                int nblocks_hint, KrylovScalars* sc, int lanes, const SpmvOpts& o = SpmvOpts());
+int mat_make_f32(dfm_mat A);
+int to_f32(dfm_ctx c, const double* in, float* out, size_t n);
 int spmv_autotune(dfm_mat A);
 int spmv_grid(dfm_mat A);
 // ilu.cu
 int ilu_factor_launch(dfm_ilu M, dfm_mat A);
 // With sc, a forward sweep first stops the solve when |r|^2/|r0|^2 < tol^2
 // (partials in part(2)) unless rr_check is false.
-int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check = true);
+// f32: the sweeps read the FP32 copy of L / D^-1 U (D^-1 itself stays FP64).
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check = true,
+                   bool f32 = false);
 int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part,
-                   KrylovScalars* sc, int sweep);
+                   KrylovScalars* sc, int sweep, bool f32 = false);
+// Brings the packed sweep plans (and, with f32, the FP32 factor copy and its
+// plans) up to date with the factor, outside any stream capture.
+int ilu_prepare(dfm_ilu M, bool f32);
 int ilu_fill_sentinel(dfm_ilu M, double* v, size_t n);
 int ilu_autotune(dfm_ilu M);
 int sweep_grid(dfm_ilu M, int sweep);
@@ -125,7 +149,7 @@ void sweep_plan_free(SweepPlan* P);
 int sweep_plan_refresh(dfm_ilu M, SweepPlan* P);
 int ilu_set_ranges(dfm_ilu M, int G);
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
-                        KrylovScalars* sc, const double* rr_part, int rr_n);
+                        KrylovScalars* sc, const double* rr_part, int rr_n, bool f32 = false);
 // krylov.cu
 // method: DFM_PCG / DFM_PBICGSTAB / DFM_PCOCG; b and x at DFM_HOST or DFM_DEVICE.
 int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where, double* x, int x_where,

@@ -265,7 +265,7 @@ DFM_DEVINL bool converged_guard(KrylovScalars* sc, const double* rr_part, int np
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       sc->conv = sqrt(rr * sc->inv0);
       sc->conv_it = sc->it;
-      sc->done = 100 + DFM_OK;
+      sc->done = sc->conv_code;
     }
     return true;
   }
@@ -590,6 +590,8 @@ int ilu_factor_launch(dfm_ilu M, dfm_mat A) {
   DFM_CUDA_TRY(cudaMemsetAsync(&c->d_status->nsing, 0, sizeof(unsigned), s));
   M->plan_f.stale = true;  // packed sweep values are re-gathered on next use
   M->plan_b.stale = true;
+  M->plan32_f.stale = true;
+  M->plan32_b.stale = true;
   M->epoch++;
   if (M->epoch == 0) {  // wrapped: clear the epochs
     DFM_CUDA_TRY(cudaMemsetAsync(M->d_flags, 0, sizeof(unsigned) * M->N, s));
@@ -656,34 +658,43 @@ int set_poll_sleep(unsigned ns) {
   return DFM_OK;
 }
 
-template <int B, int LPR, bool FWD>
-static cudaError_t sweep_real(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
-                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+template <int B, int LPR, bool FWD, typename TV>
+static cudaError_t sweep_real_tv(dfm_ilu M, const TV* foff, int sweep, const double* in, double* out,
+                                 const double* rdot, double* part, KrylovScalars* sc, const double* rr_part,
+                                 int rr_n) {
   dfm_ctx c = M->ctx;
   const unsigned* order = FWD ? M->d_order_f : M->d_order_b;
   if (sweep == 2) {
     const unsigned* lvl = FWD ? M->d_lvl_f : M->d_lvl_b;
     const unsigned nlev = FWD ? M->nlev_f : M->nlev_b;
     if (part)
-      k_sweep_cta<B, LPR, double, double, FWD, true><<<1, 1024, 0, c->stream>>>(
-          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, M->d_foff, in, out, rdot, part,
-          sc, rr_part, rr_n);
+      k_sweep_cta<B, LPR, TV, double, FWD, true><<<1, 1024, 0, c->stream>>>(
+          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, foff, in, out, rdot, part, sc,
+          rr_part, rr_n);
     else
-      k_sweep_cta<B, LPR, double, double, FWD, false><<<1, 1024, 0, c->stream>>>(
-          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, M->d_foff, in, out, rdot,
-          nullptr, sc, rr_part, rr_n);
+      k_sweep_cta<B, LPR, TV, double, FWD, false><<<1, 1024, 0, c->stream>>>(
+          nlev, lvl, order, M->A->d_rowptr, M->A->d_colind, M->d_diaind, M->d_fdiag, foff, in, out, rdot, nullptr,
+          sc, rr_part, rr_n);
     return cudaGetLastError();
   }
   const int grid = sweep_grid(M, 1);
   if (part)
-    return launch_coop(k_sweep_syncfree<B, LPR, double, double, FWD, true>, grid, 256, c->stream, M->N, order,
+    return launch_coop(k_sweep_syncfree<B, LPR, TV, double, FWD, true>, grid, 256, c->stream, M->N, order,
                        (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
-                       (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, (const double*)M->d_foff, in, out,
-                       rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
-  return launch_coop(k_sweep_syncfree<B, LPR, double, double, FWD, false>, grid, 256, c->stream, M->N, order,
+                       (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, foff, in, out, rdot, part, sc,
+                       rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+  return launch_coop(k_sweep_syncfree<B, LPR, TV, double, FWD, false>, grid, 256, c->stream, M->N, order,
                      (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
-                     (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, (const double*)M->d_foff, in, out,
-                     rdot, (double*)nullptr, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+                     (const unsigned*)M->d_diaind, (const double*)M->d_fdiag, foff, in, out, rdot, (double*)nullptr,
+                     sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+}
+
+template <int B, int LPR, bool FWD>
+static cudaError_t sweep_real(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
+                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n, bool f32) {
+  if (f32)
+    return sweep_real_tv<B, LPR, FWD, float>(M, M->d_foff32, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+  return sweep_real_tv<B, LPR, FWD, double>(M, M->d_foff, sweep, in, out, rdot, part, sc, rr_part, rr_n);
 }
 
 template <int LPR, bool FWD>
@@ -721,37 +732,65 @@ static cudaError_t sweep_cplx(dfm_ilu M, int sweep, const double* in, double* ou
 }
 
 static int sweep_dispatch(dfm_ilu M, bool fwd, int sweep, const double* in, double* out, const double* rdot,
-                          double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+                          double* part, KrylovScalars* sc, const double* rr_part, int rr_n, bool f32) {
   if (M->N == 0) return DFM_OK;
   if (sweep <= 0) sweep = M->sweep > 0 ? M->sweep : 1;
-  if (sweep == 3) return sweep_ranges_launch(M, fwd, in, out, rdot, part, sc, rr_part, rr_n);
+  if (f32 && (M->vt != DFM_REAL || !M->d_foff32)) return DFM_ERR_INVALID;
+  if (sweep == 3) return sweep_ranges_launch(M, fwd, in, out, rdot, part, sc, rr_part, rr_n, f32);
   cudaError_t e;
   if (M->vt == DFM_COMPLEX) {
     e = fwd ? sweep_cplx<8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
             : sweep_cplx<8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
   } else if (M->b == 1) {
-    e = fwd ? sweep_real<1, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
-            : sweep_real<1, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+    e = fwd ? sweep_real<1, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32)
+            : sweep_real<1, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32);
   } else if (M->b == 2) {
-    e = fwd ? sweep_real<2, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
-            : sweep_real<2, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+    e = fwd ? sweep_real<2, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32)
+            : sweep_real<2, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32);
   } else {
-    e = fwd ? sweep_real<3, 16, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
-            : sweep_real<3, 16, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+    e = fwd ? sweep_real<3, 16, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32)
+            : sweep_real<3, 16, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32);
   }
   DFM_CUDA_TRY(e);
   return DFM_OK;
 }
 
-int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check) {
+int ilu_fwd_launch(dfm_ilu M, const double* r, double* y, KrylovScalars* sc, int sweep, bool rr_check, bool f32) {
   const bool chk = sc && rr_check;
   return sweep_dispatch(M, true, sweep, r, y, nullptr, nullptr, sc, chk ? M->ctx->part(2) : nullptr,
-                        chk ? spmv_grid(M->A) : 0);
+                        chk ? spmv_grid(M->A) : 0, f32);
 }
 
 int ilu_bwd_launch(dfm_ilu M, const double* y, double* z, const double* rdot, double* dot_part, KrylovScalars* sc,
-                   int sweep) {
-  return sweep_dispatch(M, false, sweep, y, z, rdot, dot_part, sc, nullptr, 0);
+                   int sweep, bool f32) {
+  return sweep_dispatch(M, false, sweep, y, z, rdot, dot_part, sc, nullptr, 0, f32);
+}
+
+int ilu_prepare(dfm_ilu M, bool f32) {
+  if (M->sweep == 3) {
+    if (M->plan_f.stale && (M->plan_f.valid) && sweep_plan_refresh(M, &M->plan_f)) return DFM_ERR_CUDA;
+    if (M->plan_b.stale && (M->plan_b.valid) && sweep_plan_refresh(M, &M->plan_b)) return DFM_ERR_CUDA;
+  }
+  if (!f32) return DFM_OK;
+  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
+  const size_t no = (size_t)M->ncrs * M->vw();
+  if (!M->d_foff32) DFM_CUDA_TRY(cudaMalloc(&M->d_foff32, std::max<size_t>(no, 1) * sizeof(float)));
+  int rc = to_f32(M->ctx, M->d_foff, M->d_foff32, no);
+  if (rc) return rc;
+  if (M->sweep == 3) {
+    // FP32 plans with the FP64 plans' ranges and lanes
+    for (int f = 0; f < 2; f++) {
+      SweepPlan& P64 = f ? M->plan_b : M->plan_f;
+      SweepPlan& P32 = f ? M->plan32_b : M->plan32_f;
+      if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr) {
+        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32))) return rc;
+        P32.lpr = P64.lpr;
+        M->plan_gen++;  // captured graphs hold the old plan's buffers
+      }
+      if ((rc = sweep_plan_refresh(M, &P32))) return rc;
+    }
+  }
+  return DFM_OK;
 }
 
 // Autotuner for the sweep schedule: times one forward+backward application

@@ -16,6 +16,15 @@
 // later kernel needs is written by block 0 of the producer and read by the
 // consumer kernel only, never within the kernel that writes it.
 //
+// Mixed precision (dfm_solve_pcg_mixed): the PCG recurrences run with the FP32
+// copies of A's values and of L / D^-1 U (D^-1 and every vector, dot and
+// scalar stay FP64), inside FP64 iterative refinement done as residual
+// replacement: every kIterPerGraph-th iteration, and whenever the recursive
+// residual meets the tolerance, r is replaced by the true b - A x computed
+// with the FP64 values.  Only a true residual below the tolerance ends the
+// solve.  Unlike restarting an inner solve per refinement step, this keeps
+// the Krylov space across refinements.
+//
 // Partial slots: 0,1 SpMV dots; 2 (r, r); 3,4 preconditioned dots.
 #include <algorithm>
 #include <cmath>
@@ -333,7 +342,8 @@ k_cocg_p(size_t N, KrylovScalars* sc, const double* part_rw, int np_rw, const do
 enum { kVecR, kVecX, kVecP, kVecZ, kVecY, kVecQ, kVecR2, kVecS, kVecMs, kVecAMs, kNumVec };
 
 static int vectors_of(int method) {
-  return method == DFM_PBICGSTAB ? kNumVec : method == DFM_PCOCG ? kVecQ + 1 : kVecY + 1;
+  return method == DFM_PBICGSTAB ? kNumVec : method == DFM_PCOCG ? kVecQ + 1 : method == DFM_PCG_MIXED ? kVecR2 + 1
+                                                                                                     : kVecY + 1;
 }
 
 // Workspace of one (M, method) pair: vectors and the captured graph, with the
@@ -418,6 +428,63 @@ static int enqueue_pcg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   return DFM_OK;
 }
 
+// r = b - A x with the FP64 values, partials of (r, r) in slot 2
+static int enqueue_true_residual(dfm_mat A, SolvePlan* P, KrylovScalars* sc) {
+  SpmvOpts o;
+  o.yy = true;
+  o.y0 = P->v[kVecR2];
+  return spmv_launch(A, -1.0, P->v[kVecX], 0.0, P->v[kVecR], A->ctx->part(2), vec_grid(A), sc, A->lanes, o);
+}
+
+static int enqueue_pcg_mixed(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, bool replace) {
+  dfm_ctx c = A->ctx;
+  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *z = P->v[kVecZ], *y = P->v[kVecY];
+  SpmvOpts o;
+  o.f32 = true;
+  int rc = spmv_launch(A, 1.0, p, 0.0, z, c->part(0), gv, sc, A->lanes, o);
+  if (rc) return rc;
+  k_pcg_update_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv, z, p,
+                                                    r, x, y);
+  DFM_CUDA_TRY(cudaGetLastError());
+  if (replace && (rc = enqueue_true_residual(A, P, sc))) return rc;
+  if ((rc = ilu_fwd_launch(M, r, y, sc, M->sweep, true, true))) return rc;
+  if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), sc, M->sweep, true))) return rc;
+  k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(3), gs, z, p);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+// After the recursive residual met the tolerance (done == 99): the true
+// residual decides; if it is not small enough the interrupted iteration is
+// completed from the replaced residual and the solve goes on.
+__global__ void k_mp_verify(KrylovScalars* sc, const double* part_rr, int np_rr) {
+  const double rr = reduce_partials(part_rr, np_rr);
+  if (threadIdx.x == 0) {
+    if (rr * sc->inv0 < sc->tol2) {
+      sc->conv = sqrt(rr * sc->inv0);
+      sc->done = 100 + DFM_OK;
+    } else {
+      sc->done = 0;
+    }
+  }
+}
+
+static int mixed_verify(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  int rc = enqueue_true_residual(A, P, nullptr);
+  if (rc) return rc;
+  k_mp_verify<<<1, kVecThreads, 0, c->stream>>>(sc, c->part(2), gv);
+  DFM_CUDA_TRY(cudaGetLastError());
+  // completes the iteration if the solve goes on (kernels skip when done)
+  if ((rc = ilu_fwd_launch(M, P->v[kVecR], P->v[kVecY], sc, M->sweep, false, true))) return rc;
+  if ((rc = ilu_bwd_launch(M, P->v[kVecY], P->v[kVecZ], P->v[kVecR], c->part(3), sc, M->sweep, true))) return rc;
+  k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(3), gs, P->v[kVecZ], P->v[kVecP]);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
 static int enqueue_bicg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   dfm_ctx c = A->ctx;
   const int gv = vec_grid(A);
@@ -427,13 +494,18 @@ static int enqueue_bicg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   // Mp = M^-1 p; AMp = A Mp with (r2, AMp)
   if ((rc = ilu_fwd_launch(M, p, y, sc, M->sweep, false))) return rc;
   if ((rc = ilu_bwd_launch(M, y, Mp, nullptr, nullptr, sc, M->sweep))) return rc;
-  if ((rc = spmv_launch(A, 1.0, Mp, 0.0, AMp, c->part(0), gv, sc, A->lanes, r2))) return rc;
+  SpmvOpts o1;
+  o1.dot_w = r2;
+  if ((rc = spmv_launch(A, 1.0, Mp, 0.0, AMp, c->part(0), gv, sc, A->lanes, o1))) return rc;
   k_bicg_s<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(3), gv, c->part(2), r, AMp, s, y, Ms);
   DFM_CUDA_TRY(cudaGetLastError());
   // Ms = M^-1 s; AMs = A Ms with (s, AMs) and (AMs, AMs)
   if ((rc = ilu_fwd_launch(M, s, y, sc, M->sweep, false))) return rc;
   if ((rc = ilu_bwd_launch(M, y, Ms, nullptr, nullptr, sc, M->sweep))) return rc;
-  if ((rc = spmv_launch(A, 1.0, Ms, 0.0, AMs, c->part(0), gv, sc, A->lanes, s, c->part(1)))) return rc;
+  SpmvOpts o2;
+  o2.dot_w = s;
+  o2.dot_part2 = c->part(1);
+  if ((rc = spmv_launch(A, 1.0, Ms, 0.0, AMs, c->part(0), gv, sc, A->lanes, o2))) return rc;
   k_bicg_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), c->part(1), gv, c->part(2), c->part(3), Mp, Ms,
                                               s, AMs, r2, x, r);
   DFM_CUDA_TRY(cudaGetLastError());
@@ -463,10 +535,12 @@ static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   return DFM_OK;
 }
 
-static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+// k: index of the iteration inside one graph of kIterPerGraph
+static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, int k) {
   switch (P->method) {
     case DFM_PBICGSTAB: return enqueue_bicg(A, M, P, sc);
     case DFM_PCOCG: return enqueue_cocg(A, M, P, sc);
+    case DFM_PCG_MIXED: return enqueue_pcg_mixed(A, M, P, sc, k == kIterPerGraph - 1);
     default: return enqueue_pcg(A, M, P, sc);
   }
 }
@@ -491,13 +565,16 @@ static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
       if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep))) return rc;
       k_cocg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, z, p);
       break;
-    default:
+    default: {
+      const bool f32 = P->method == DFM_PCG_MIXED;
+      if (f32) DFM_CUDA_TRY(cudaMemcpyAsync(P->v[kVecR2], r, P->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
       k_pcg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, y, z, c->part(2));
       DFM_CUDA_TRY(cudaGetLastError());
-      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep))) return rc;
-      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep))) return rc;
+      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep, true, f32))) return rc;
+      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep, f32))) return rc;
       k_pcg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, z, p);
       break;
+    }
   }
   (void)gs;
   DFM_CUDA_TRY(cudaGetLastError());
@@ -522,7 +599,7 @@ static void ensure_graph(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
   bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
   int erc = DFM_OK;
   if (ok) {
-    for (int k = 0; k < kIterPerGraph && erc == DFM_OK; k++) erc = enqueue_iteration(A, M, P, sc);
+    for (int k = 0; k < kIterPerGraph && erc == DFM_OK; k++) erc = enqueue_iteration(A, M, P, sc, k);
     ok = (cudaStreamEndCapture(s, &g) == cudaSuccess) && erc == DFM_OK;
   }
   if (ok) ok = cudaGraphInstantiate(&P->exec, g, 0) == cudaSuccess;
@@ -543,6 +620,9 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
   int rc = spmv_autotune(A);
   if (rc) return rc;
   if ((rc = ilu_autotune(M))) return rc;
+  const bool f32 = method == DFM_PCG_MIXED;
+  if (f32 && (rc = mat_make_f32(A))) return rc;
+  if ((rc = ilu_prepare(M, f32))) return rc;
   SolvePlan* P = nullptr;
   if ((rc = plan_of(M, method, &P))) return rc;
   const size_t n = P->n;
@@ -551,6 +631,7 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
     KrylovScalars h = {};
     h.maxit = maxit;
     h.tol2 = tol * tol;
+    h.conv_code = f32 ? 99 : 100 + DFM_OK;
     DFM_CUDA_TRY(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
   }
   DFM_CUDA_TRY(cudaMemcpyAsync(P->v[kVecR], b, n * sizeof(double),
@@ -562,10 +643,15 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
       DFM_CUDA_TRY(cudaGraphLaunch(P->exec, s));
     } else {
       for (int k = 0; k < kIterPerGraph; k++)
-        if ((rc = enqueue_iteration(A, M, P, sc))) return rc;
+        if ((rc = enqueue_iteration(A, M, P, sc, k))) return rc;
     }
     DFM_CUDA_TRY(cudaMemcpyAsync(c->h_scal, sc, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, s));
     DFM_CUDA_TRY(cudaStreamSynchronize(s));
+    if (c->h_scal->done == 99) {  // mixed precision: confirm with the FP64 residual
+      if ((rc = mixed_verify(A, M, P, sc))) return rc;
+      DFM_CUDA_TRY(cudaMemcpyAsync(c->h_scal, sc, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, s));
+      DFM_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     if (c->h_scal->done) break;
     const int code = take_code(c);
     if (code) return code;

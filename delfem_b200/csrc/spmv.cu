@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(256)
 k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
        const TV* __restrict__ diag, const TV* __restrict__ off, double alpha,
        const TX* __restrict__ x, double beta, TX* __restrict__ y, double* __restrict__ part,
-       const int* done, const TX* __restrict__ w, double* __restrict__ part2) {
+       const int* done, const TX* __restrict__ w, double* __restrict__ part2, const TX* __restrict__ y0) {
   if (done && block_flag(done)) return;
   constexpr int BB = B * B;
   const int lane = threadIdx.x % LPR;
@@ -63,16 +63,18 @@ k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restri
 #pragma unroll
       for (int r = 0; r < B; r++) {
         double v = alpha * acc[r];
-        if (beta != 0.0) v += beta * (double)y[(size_t)i * B + r];
+        if (y0) v += (double)y0[(size_t)i * B + r];
+        else if (beta != 0.0) v += beta * (double)y[(size_t)i * B + r];
         const TX out = (TX)v;
         y[(size_t)i * B + r] = out;
-        if (NDOT >= 1) dacc += (double)w[(size_t)i * B + r] * (double)out;
-        if (NDOT >= 2) dacc2 += (double)out * (double)out;
+        if (NDOT == 1 || NDOT == 2) dacc += (double)w[(size_t)i * B + r] * (double)out;
+        if (NDOT == 2) dacc2 += (double)out * (double)out;
+        if (NDOT == 3) dacc += (double)out * (double)out;
       }
     }
   }
   if (NDOT >= 1) block_partial<256>(dacc, part);
-  if (NDOT >= 2) block_partial<256>(dacc2, part2);
+  if (NDOT == 2) block_partial<256>(dacc2, part2);
 }
 
 // Complex b = 1: values and vectors interleaved (re, im).
@@ -128,30 +130,42 @@ int spmv_grid(dfm_mat A) {
   return std::max(1, std::min(want, kMaxBlocks));
 }
 
+template <int B, int LPR, typename TV>
+static void launch_real_tv(dfm_mat A, const TV* diag, const TV* off, int grid, cudaStream_t s, double alpha,
+                           const double* x, double beta, double* y, double* part, const int* done,
+                           const SpmvOpts& o) {
+  const double* w = o.dot_w ? o.dot_w : x;
+  if (part && o.yy)
+    k_spmv<B, LPR, TV, double, 3><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                       part, done, nullptr, nullptr, o.y0);
+  else if (part && o.dot_part2)
+    k_spmv<B, LPR, TV, double, 2><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                       part, done, w, o.dot_part2, o.y0);
+  else if (part)
+    k_spmv<B, LPR, TV, double, 1><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                       part, done, w, nullptr, o.y0);
+  else
+    k_spmv<B, LPR, TV, double, 0><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                       nullptr, done, nullptr, nullptr, o.y0);
+}
+
 template <int B, int LPR>
 static void launch_real(dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x, double beta,
-                        double* y, double* part, const int* done, const double* w, double* part2) {
-  if (!w) w = x;
-  if (part && part2)
-    k_spmv<B, LPR, double, double, 2><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
-                                                           alpha, x, beta, y, part, done, w, part2);
-  else if (part)
-    k_spmv<B, LPR, double, double, 1><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
-                                                           alpha, x, beta, y, part, done, w, nullptr);
+                        double* y, double* part, const int* done, const SpmvOpts& o) {
+  if (o.f32)
+    launch_real_tv<B, LPR, float>(A, A->d_diag32, A->d_off32, grid, s, alpha, x, beta, y, part, done, o);
   else
-    k_spmv<B, LPR, double, double, 0><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, A->d_diag, A->d_off,
-                                                           alpha, x, beta, y, nullptr, done, nullptr, nullptr);
+    launch_real_tv<B, LPR, double>(A, A->d_diag, A->d_off, grid, s, alpha, x, beta, y, part, done, o);
 }
 
 template <int B>
 static void launch_real_lpr(int lanes, dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x,
-                            double beta, double* y, double* part, const int* done, const double* w,
-                            double* part2) {
+                            double beta, double* y, double* part, const int* done, const SpmvOpts& o) {
   switch (lanes) {
-    case 4: launch_real<B, 4>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
-    case 8: launch_real<B, 8>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
-    case 16: launch_real<B, 16>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
-    default: launch_real<B, 32>(A, grid, s, alpha, x, beta, y, part, done, w, part2); break;
+    case 4: launch_real<B, 4>(A, grid, s, alpha, x, beta, y, part, done, o); break;
+    case 8: launch_real<B, 8>(A, grid, s, alpha, x, beta, y, part, done, o); break;
+    case 16: launch_real<B, 16>(A, grid, s, alpha, x, beta, y, part, done, o); break;
+    default: launch_real<B, 32>(A, grid, s, alpha, x, beta, y, part, done, o); break;
   }
 }
 
@@ -170,8 +184,9 @@ static void launch_cplx(dfm_mat A, int grid, cudaStream_t s, double alpha, const
 }
 
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
-                int grid, KrylovScalars* sc, int lanes, const double* dot_w, double* dot_part2) {
-  if (A->vt == DFM_COMPLEX && (dot_w || dot_part2)) return DFM_ERR_UNSUPPORTED;
+                int grid, KrylovScalars* sc, int lanes, const SpmvOpts& o) {
+  if (A->vt == DFM_COMPLEX && (o.dot_w || o.dot_part2 || o.yy || o.y0 || o.f32)) return DFM_ERR_UNSUPPORTED;
+  if (o.f32 && !A->d_off32) return DFM_ERR_INVALID;
   if (A->N == 0) return DFM_OK;
   cudaStream_t s = A->ctx->stream;
   if (grid <= 0) grid = spmv_grid(A);
@@ -185,14 +200,39 @@ int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y
       default: launch_cplx<32>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
     }
   } else if (A->b == 1) {
-    launch_real_lpr<1>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
+    launch_real_lpr<1>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, o);
   } else if (A->b == 2) {
-    launch_real_lpr<2>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
+    launch_real_lpr<2>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, o);
   } else {
-    launch_real_lpr<3>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, dot_w, dot_part2);
+    launch_real_lpr<3>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, o);
   }
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;
+}
+
+__global__ void k_to_f32(size_t n, const double* __restrict__ in, float* __restrict__ out) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    out[k] = (float)in[k];
+}
+
+int to_f32(dfm_ctx c, const double* in, float* out, size_t n) {
+  if (n == 0) return DFM_OK;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)c->nsm * 8);
+  k_to_f32<<<grid, 256, 0, c->stream>>>(n, in, out);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+// FP32 copy of the values (allocated on first use, refreshed on every call).
+int mat_make_f32(dfm_mat A) {
+  const size_t nd = (size_t)A->N * A->vw(), no = (size_t)A->ncrs * A->vw();
+  if (!A->d_diag32) {
+    DFM_CUDA_TRY(cudaMalloc(&A->d_diag32, std::max<size_t>(nd, 1) * sizeof(float)));
+    DFM_CUDA_TRY(cudaMalloc(&A->d_off32, std::max<size_t>(no, 1) * sizeof(float)));
+  }
+  int rc = to_f32(A->ctx, A->d_diag, A->d_diag32, nd);
+  if (!rc) rc = to_f32(A->ctx, A->d_off, A->d_off32, no);
+  return rc;
 }
 
 // Autotuner: times every lanes-per-row choice on this matrix (CUDA events on

@@ -114,7 +114,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
         if (blockIdx.x == 0 && threadIdx.x == 0) {
           sc->conv = sqrt(rr * sc->inv0);
           sc->conv_it = sc->it;
-          sc->done = 100 + DFM_OK;
+          sc->done = sc->conv_code;
         }
         return;
       }
@@ -483,15 +483,30 @@ static cudaError_t launch_ranges_lpr(dfm_ilu M, const SweepPlan* P, const TX* in
 }
 
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
-                        KrylovScalars* sc, const double* rr_part, int rr_n) {
-  SweepPlan* P = fwd ? &M->plan_f : &M->plan_b;
-  if (!P->valid || P->val_bytes != 8 || P->vec_bytes != 8) return DFM_ERR_INVALID;
+                        KrylovScalars* sc, const double* rr_part, int rr_n, bool f32) {
+  SweepPlan* P = f32 ? (fwd ? &M->plan32_f : &M->plan32_b) : (fwd ? &M->plan_f : &M->plan_b);
+  if (!P->valid || P->val_bytes != (f32 ? 4 : 8) || P->vec_bytes != 8) return DFM_ERR_INVALID;
   if (P->stale) {
     int rc = sweep_plan_refresh(M, P);
     if (rc) return rc;
   }
   if (M->vt == DFM_COMPLEX) return DFM_ERR_UNSUPPORTED;
   cudaError_t e;
+  if (f32) {
+    switch (M->b) {
+      case 1: e = fwd ? launch_ranges_lpr<1, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                      : launch_ranges_lpr<1, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+        break;
+      case 2: e = fwd ? launch_ranges_lpr<2, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                      : launch_ranges_lpr<2, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+        break;
+      default: e = fwd ? launch_ranges_lpr<3, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                       : launch_ranges_lpr<3, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+        break;
+    }
+    DFM_CUDA_TRY(e);
+    return DFM_OK;
+  }
   switch (M->b) {
     case 1: e = fwd ? launch_ranges_lpr<1, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
                     : launch_ranges_lpr<1, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;

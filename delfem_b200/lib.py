@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED = range(9)
 REAL, COMPLEX = 0, 1
 HOST, DEVICE = 0, 1
-PCG, PBICGSTAB, PCOCG = 0, 1, 2
+PCG, PBICGSTAB, PCOCG, PCG_MIXED = 0, 1, 2, 3
 
 _lib = None
 
@@ -47,11 +47,14 @@ PROTOS = {
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
+    "dfm_mesh_pattern": (_i, [_vp, _up, _up, C.POINTER(C.c_size_t)]),
     "dfm_assemble_poisson2d": (_i, [_vp, _vp, _d, _d, _vp, _vp, _vp, _vp]),
     "dfm_assemble_solid2d": (_i, [_vp, _vp, _d, _d, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "dfm_assemble_solid3d": (_i, [_vp, _vp, _d, _d, _d, _d, _d, _d, _vp, _vp, _vp]),
     "dfm_assemble_helmholtz2d": (_i, [_vp, _vp, _d, _vp, _vp, _vp]),
     "dfm_apply_dirichlet": (_i, [_vp, _vp, _vp]),
+    "dfm_coef_grad_poisson2d": (_i, [_vp, _d, _vp, _vp, _vp]),
+    "dfm_coef_grad_solid2d": (_i, [_vp, _d, _d, _vp, _vp, _vp]),
     "dfm_ilu_create": (_i, [_vp, C.POINTER(_vp)]),
     "dfm_ilu_destroy": (_i, [_vp]),
     "dfm_ilu_levels": (_i, [_vp, _up, _up, _up, _up]),
@@ -66,6 +69,12 @@ PROTOS = {
     "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pbicgstab": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcocg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_pcg_mixed": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_batch_create": (_i, [_vp, _u, _up, C.POINTER(_vp)]),
+    "dfm_batch_destroy": (_i, [_vp]),
+    "dfm_batch_set_tuning": (_i, [_vp, _i, _i]),
+    "dfm_batch_get_tuning": (_i, [_vp, _ip, _ip]),
+    "dfm_batch_solve_pcg": (_i, [_vp, _vp, _i, _vp, _i, _d, _u, _up, _dp, _ip]),
     "dfm_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_host": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
 }
@@ -255,6 +264,16 @@ class Mesh:
         except Exception:
             pass
 
+    def pattern(self):
+        """(rowptr, colind) of the mesh's block pattern (host numpy uint32)."""
+        n = C.c_size_t()
+        rp = np.zeros(self.nnode + 1, np.uint32)
+        check(lib().dfm_mesh_pattern(self.h, rp.ctypes.data_as(_up), None, C.byref(n)), "dfm_mesh_pattern")
+        ci = np.zeros(max(n.value, 1), np.uint32)
+        check(lib().dfm_mesh_pattern(self.h, rp.ctypes.data_as(_up), ci.ctypes.data_as(_up), C.byref(n)),
+              "dfm_mesh_pattern")
+        return rp, ci[: n.value]
+
     def assemble_poisson(self, A: Matrix, alpha, source, rhs, coef=None, u=None, load=None):
         _sync_torch()
         check(lib().dfm_assemble_poisson2d(self.h, A.h, alpha, source, _ptr(coef), _ptr(u), _ptr(load), _ptr(rhs)),
@@ -278,6 +297,18 @@ class Mesh:
         check(lib().dfm_assemble_helmholtz2d(self.h, A.h, wave_length, _ptr(u), _ptr(load), _ptr(rhs)),
               "dfm_assemble_helmholtz2d")
         return rhs
+
+
+def coef_grad_solid2d(G: Mesh, lam_e, myu_e, lam, u, grad):
+    _sync_torch()
+    check(lib().dfm_coef_grad_solid2d(G.h, lam_e, myu_e, _ptr(lam), _ptr(u), _ptr(grad)), "dfm_coef_grad_solid2d")
+    return grad
+
+
+def coef_grad_poisson2d(G: Mesh, alpha, lam, u, grad):
+    _sync_torch()
+    check(lib().dfm_coef_grad_poisson2d(G.h, alpha, _ptr(lam), _ptr(u), _ptr(grad)), "dfm_coef_grad_poisson2d")
+    return grad
 
 
 def apply_dirichlet(A: Matrix, flags, rhs=None):
@@ -347,6 +378,58 @@ class ILU:
         check(lib().dfm_ilu_set_sweep(self.h, int(v)))
 
 
+class Batch:
+    """Many independent systems held as one block-diagonal matrix (see dfm_batch_create)."""
+
+    def __init__(self, M: ILU, row_off):
+        self.M = M
+        ro = np.ascontiguousarray(row_off, np.uint32)
+        self.ninst = ro.size - 1
+        self.row_off = ro
+        h = C.c_void_p()
+        check(lib().dfm_batch_create(M.h, self.ninst, ro.ctypes.data_as(_up), C.byref(h)), "dfm_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def tuning(self):
+        a, b = C.c_int(), C.c_int()
+        check(lib().dfm_batch_get_tuning(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    @tuning.setter
+    def tuning(self, v):
+        check(lib().dfm_batch_set_tuning(self.h, int(v[0]), int(v[1])), "dfm_batch_set_tuning")
+
+    def solve(self, b, x=None, tol=1e-8, maxit=10000, allow=(OK, NOT_CONVERGED)):
+        """b, x: device tensors (x written) or host arrays (x returned).  Returns
+        (status, x, iters[ninst], conv[ninst], status[ninst])."""
+        it = np.zeros(self.ninst, np.uint32)
+        cv = np.zeros(self.ninst)
+        st = np.zeros(self.ninst, np.int32)
+        dev = hasattr(b, "data_ptr")
+        if not dev:
+            b = np.ascontiguousarray(b, np.float64)
+            x = np.zeros_like(b)
+        else:
+            _sync_torch()
+        w = DEVICE if dev else HOST
+        rc = lib().dfm_batch_solve_pcg(self.h, _ptr(b), w, _ptr(x), w, tol, maxit, it.ctypes.data_as(_up),
+                                       cv.ctypes.data_as(_dp), st.ctypes.data_as(_ip))
+        check(rc, "dfm_batch_solve_pcg", allow)
+        return rc, x, it, cv, st
+
+
 def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
     """LsSol::Solve_PCG on device vectors; returns (status, iters, conv)."""
     it, conv = C.c_uint(), C.c_double()
@@ -371,6 +454,15 @@ def solve_pcocg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_
     _sync_torch()
     rc = lib().dfm_solve_pcocg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_pcocg", allow)
+    return rc, it.value, conv.value
+
+
+def solve_pcg_mixed(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """PCG with FP32 values inside FP64 residual replacement; returns (status, iters, conv)."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_pcg_mixed(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pcg_mixed", allow)
     return rc, it.value, conv.value
 
 

@@ -184,3 +184,26 @@ def gaussian_source_load(mesh: Mesh, center=(0.3, 0.1), sigma=0.05) -> np.ndarra
     for k in range(3):
         np.add.at(load[:, 0], mesh.elem[:, k], w)
     return load
+
+
+def concat(meshes: list) -> tuple:
+    """Disjoint union of meshes of one element kind, for a batch: node numbers of
+    mesh k are shifted by the nodes of meshes 0..k-1, so the union's pattern is
+    block-diagonal with mesh k's rows in [node_off[k], node_off[k+1]).  Returns
+    (Mesh, node_off, elem_off)."""
+    node_off = np.zeros(len(meshes) + 1, np.int64)
+    elem_off = np.zeros(len(meshes) + 1, np.int64)
+    for k, m in enumerate(meshes):
+        node_off[k + 1] = node_off[k] + m.nnode
+        elem_off[k + 1] = elem_off[k] + m.elem.shape[0]
+    coord = np.concatenate([m.coord for m in meshes])
+    elem = np.concatenate([m.elem + node_off[k] for k, m in enumerate(meshes)]).astype(np.int32)
+    bnd = np.concatenate([m.bnd + node_off[k] for k, m in enumerate(meshes) if m.bnd.size]).astype(np.int32) \
+        if any(m.bnd.size for m in meshes) else np.zeros((0, 2), np.int32)
+    return Mesh(coord, elem, bnd, {}), node_off, elem_off
+
+
+def batch_sizes(count: int, lo: int, hi: int, seed: int) -> np.ndarray:
+    """Grid sides n drawn log-uniformly in [lo, hi] (integers) from the seed."""
+    rng = np.random.default_rng(seed)
+    return np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), count))).astype(np.int64)

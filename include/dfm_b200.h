@@ -51,12 +51,13 @@ typedef enum dfm_status {
 
 enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
 enum { DFM_HOST = 0, DFM_DEVICE = 1 };
-enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2 };
+enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2, DFM_PCG_MIXED = 3 };
 
 typedef struct dfm_ctx_s* dfm_ctx;
 typedef struct dfm_mat_s* dfm_mat;
 typedef struct dfm_ilu_s* dfm_ilu;
 typedef struct dfm_mesh_s* dfm_mesh;
+typedef struct dfm_batch_s* dfm_batch;
 
 DFM_API const char* dfm_status_string(int status);
 DFM_API int dfm_abi_version(void);
@@ -106,6 +107,11 @@ DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, doub
 DFM_API int dfm_mesh_create(dfm_ctx ctx, int ndim, unsigned nnode, const double* coord, unsigned nnoel,
                     unsigned nelem, const int* elem, unsigned nbar, const int* bar, dfm_mesh* out);
 DFM_API int dfm_mesh_destroy(dfm_mesh mesh);
+/* The mesh's block pattern as CMatDia_BlkCrs::AddPattern builds it
+ * (src/matvec/matdia_blkcrs.cpp:346-505): row i lists, ascending, every other
+ * node sharing an element with node i.  Host arrays: rowptr[nnode+1] and
+ * colind[*ncrs]; call with colind NULL first to learn *ncrs. */
+DFM_API int dfm_mesh_pattern(dfm_mesh mesh, unsigned* rowptr, unsigned* colind, size_t* ncrs);
 /* Each assemble call is InitializeMarge (matrix and residual zeroed,
  * src/ls/linearsystem.cpp:74-89) + the element loop + nodal loads
  * added to the residual afterwards.  A's pattern must hold every element's node
@@ -134,6 +140,15 @@ DFM_API int dfm_assemble_helmholtz2d(dfm_mesh mesh, dfm_mat A, double wave_lengt
  * columns of fixed DOFs zeroed, unit diagonal, residual zeroed.  flags: device
  * int[N*b], nonzero = fixed; rhs nullable.  Real matrices. */
 DFM_API int dfm_apply_dirichlet(dfm_mat A, const int* flags, double* rhs);
+/* No counterpart in the reference: the element kernel of the adjoint of
+ * K(coef) u = f, where each element matrix is linear in its coefficient
+ * (K_e = coef_e K_e^0 for the Poisson alpha and the solid lambda, myu pair):
+ * grad[e] = -lambda_e^T K_e^0 u_e with K_e^0 the element matrix at the given
+ * base constants.  lam, u: device vectors (N*b), grad: device nelem. */
+DFM_API int dfm_coef_grad_poisson2d(dfm_mesh mesh, double alpha, const double* lam, const double* u,
+                            double* grad);
+DFM_API int dfm_coef_grad_solid2d(dfm_mesh mesh, double lambda, double myu, const double* lam, const double* u,
+                          double* grad);
 
 /* ---- ILU(0): CPreconditioner_ILU / CMatDiaFrac_BlkCrs ------------------- */
 /* Symbolic ILU(0) (CMatDiaFrac_BlkCrs(0, A), src/matvec/matdiafrac_blkcrs.cpp:227-287)
@@ -192,8 +207,40 @@ DFM_API int dfm_solve_pbicgstab(dfm_mat A, dfm_ilu M, double* r, double* x, doub
  * r and x are interleaved (re, im). */
 DFM_API int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                     unsigned* iters, double* conv);
+/* No counterpart in the reference: PCG whose recurrences use FP32 copies of
+ * A's values and of the ILU(0) L / D^-1 U blocks (D^-1 pivots, vectors, dots
+ * and scalars stay FP64), inside FP64 iterative refinement done as residual
+ * replacement - the true residual b - A x with the FP64 values replaces the
+ * recursive one every 16 iterations and whenever the latter meets tol, and
+ * only a true residual below tol ends the solve.  Same arguments and
+ * conventions as dfm_solve_pcg (x = 0 start, *iters 0-based); real matrices.
+ * It pays where the FP32 copies keep the preconditioned operator's accuracy
+ * (scalar Poisson-type systems); on stiff elasticity systems the FP32 values
+ * cost iterations. */
+DFM_API int dfm_solve_pcg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
+                        unsigned* iters, double* conv);
+/* ---- batched solves (no counterpart in the reference) -------------------- */
+/* A batch of independent systems stored as one block-diagonal matrix: instance
+ * k owns block rows [row_off[k], row_off[k+1]) of M's matrix (row_off: host,
+ * ninst + 1 entries, row_off[ninst] = N) and no entry crosses an instance
+ * boundary (checked).  M's ILU(0) factor is then the per-instance factors. */
+DFM_API int dfm_batch_create(dfm_ilu M, unsigned ninst, const unsigned* row_off, dfm_batch* out);
+DFM_API int dfm_batch_destroy(dfm_batch batch);
+/* Lanes per row of the batched SpMV (4, 8, 16, 32) and rows per chunk (the
+ * tile of the per-instance reductions); 0, 0 = autotuned on the next solve. */
+DFM_API int dfm_batch_set_tuning(dfm_batch batch, int lanes, int chunk_rows);
+DFM_API int dfm_batch_get_tuning(dfm_batch batch, int* lanes, int* chunk_rows);
+/* Every instance runs Solve_PCG's algorithm with its own scalars, stop test
+ * and iteration count, all instances advancing in the same launches; stopped
+ * instances are masked.  b (N*b doubles) and x at DFM_HOST or DFM_DEVICE;
+ * iters, conv, status: host arrays of ninst (nullable), status per instance
+ * (DFM_OK, DFM_NOT_CONVERGED, DFM_BREAKDOWN).  Returns DFM_OK when every
+ * instance converged, else the worst instance status. */
+DFM_API int dfm_batch_solve_pcg(dfm_batch batch, const double* b, int b_where, double* x, int x_where,
+                        double tol, unsigned maxit, unsigned* iters, double* conv, int* status);
+
 /* End-to-end variants with HOST buffers (b copied in, x copied out, inside the
- * call); method is DFM_PCG, DFM_PBICGSTAB or DFM_PCOCG. */
+ * call); method is DFM_PCG, DFM_PBICGSTAB, DFM_PCOCG or DFM_PCG_MIXED. */
 DFM_API int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv);
 DFM_API int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol,

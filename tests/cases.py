@@ -75,3 +75,18 @@ def random_spd_like(N, b, seed=0, density=6):
     S.diag[:] = d.reshape(-1)
     S.rhs[:] = rng.standard_normal(N * b)
     return S
+
+
+def adjoint_case(n, seed=0, nobs=256):
+    """Plane-stress cantilever on the unit square (n x n grid of P1 triangles,
+    nu = 0.3): per-element Young's modulus theta ~ lognormal(0, 0.5), left edge
+    clamped, traction (0, -1) on the right edge; u_target from a second seeded
+    theta field, observed at nobs random nodes (both components)."""
+    m = meshes.unit_square_tri(n, bnd="left")
+    rng = np.random.default_rng(seed)
+    theta = rng.lognormal(0.0, 0.5, m.elem.shape[0])
+    theta_t = rng.lognormal(0.0, 0.5, m.elem.shape[0])
+    obs = rng.choice(m.nnode, size=min(nobs, m.nnode), replace=False)
+    fixed = np.unique(m.bnd.ravel())
+    load = meshes.right_edge_traction(m, n)
+    return m, theta, theta_t, obs, fixed, load

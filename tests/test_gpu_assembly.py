@@ -152,3 +152,16 @@ def test_argument_errors(ctx):
         G.assemble_solid2d(A, 1.0, 1.0, 0.0, 0.0, 0.0, rhs)
     with pytest.raises(lib.DfmError):  # node index out of range
         lib.Mesh(ctx, m.coord, np.array([[0, 1, m.nnode]], np.int32))
+
+
+@pytest.mark.parametrize("mk", [lambda: meshes.unit_square_tri(13), lambda: meshes.box_tet(5, 3, 2),
+                                lambda: meshes.unit_disk_tri(9), lambda: meshes.unit_square_tri(1)],
+                         ids=["square", "box", "disk", "two_tris"])
+def test_mesh_pattern_is_the_references(ctx, mk):
+    """The library's own pattern builder against the oracle's (pinned to AddPattern)."""
+    from delfem_b200 import lib
+    m = mk()
+    G = lib.Mesh(ctx, m.coord, m.elem)
+    rp, ci = G.pattern()
+    prp, pci = P.pattern(m.nnode, m.elem)
+    assert np.array_equal(rp, prp) and np.array_equal(ci, pci)

@@ -1,0 +1,85 @@
+"""Mixed-precision PCG (FP32 values for SpMV and ILU sweeps, FP64 vectors,
+dots, scalars and D^-1, FP64 residual replacement): the answer is judged by
+the TRUE residual b - A x with the FP64 matrix and against the FP64 oracle's
+solution at the same tolerance."""
+import numpy as np
+import pytest
+
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float64)).cuda()
+
+
+SYSTEMS = {
+    "poisson64": lambda: cases.poisson(64)[1],
+    "poisson_coef": lambda: cases.poisson(48, np.random.default_rng(1).lognormal(0, 1.0, 2 * 48 * 48))[1],
+    "solid2d": lambda: cases.solid2d(16, np.random.default_rng(2).lognormal(0, 0.5, 2 * 16 * 16))[1],
+    "solid3d": lambda: cases.solid3d(12, 3, 3)[1],
+}
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+@pytest.mark.parametrize("sweep", [1, 2, 3])
+def test_mixed_true_residual_and_solution(ctx, name, sweep):
+    from delfem_b200 import lib
+    S = SYSTEMS[name]()
+    ns, fd, fo = S.ilu0()
+    tol = 1e-10
+    ref = S.solve(fd, fo, method="pcg", tol=tol, maxit=5000)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    M.sweep = sweep
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcg_mixed(A, M, r, x, tol=tol, maxit=5000)
+    assert rc == lib.OK, (rc, it, conv)
+    xg = x.cpu().numpy()
+    res = S.rhs - S.spmv(1.0, xg, 0.0, np.zeros_like(S.rhs))
+    assert np.linalg.norm(res) < tol * np.linalg.norm(S.rhs)  # FP64 true residual
+    assert conv < tol
+    err = np.linalg.norm(xg - ref["x"]) / np.linalg.norm(ref["x"])
+    assert err <= 1e-7, err
+    # returned r is the final (true) residual
+    assert np.allclose(r.cpu().numpy(), res, rtol=0, atol=1e-12 * np.linalg.norm(S.rhs))
+
+
+def test_mixed_deterministic_and_host_entry(ctx):
+    from delfem_b200 import lib
+    S = SYSTEMS["poisson64"]()
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    out = []
+    for _ in range(2):
+        rc, x, it, conv = lib.solve_host(A, M, S.rhs, lib.PCG_MIXED, tol=1e-9, maxit=5000)
+        assert rc == lib.OK
+        out.append((x, it, conv))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1:] == out[1][1:]
+
+
+def test_mixed_follows_value_updates(ctx):
+    """New values (set_values + refactor) reach the FP32 copies on the next solve."""
+    from delfem_b200 import lib
+    S = SYSTEMS["poisson64"]()
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    lib.solve_pcg_mixed(A, M, r, x, tol=1e-9)
+    A.set_values(S.diag * 2.0, S.off * 2.0)
+    M.factor()
+    r = _dev(S.rhs)
+    x2 = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcg_mixed(A, M, r, x2, tol=1e-9)
+    assert rc == lib.OK
+    assert np.allclose(x2.cpu().numpy() * 2.0, x.cpu().numpy(), rtol=1e-6, atol=1e-9)
