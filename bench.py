@@ -1,17 +1,31 @@
-"""Benchmark of the B200 linear-solve path on the 3D cantilever elasticity
-system (200x40x40 hexes x 6 P1 tets, 337,881 nodes, 1,013,643 DOF, 3x3 blocks).
+"""Benchmark of the B200 linear-solve path.
 
-One step = one complete solve as the reference performs it after assembly:
-numeric ILU(0) of K (CPreconditioner_ILU::SetValue) followed by ILU(0)-PCG to
-relative residual 1e-8 from x = 0 (LsSol::Solve_PCG).  Inputs (K, f) are
-generated once (seeded, deterministic mesh; E = 1, nu = 0.3, body force -z,
-x = 0 face clamped) and are larger than L2 (K is 354 MB).
+Headline workload (the `value`): the 3D cantilever elasticity system, a
+200x40x40 hex grid split into 6 P1 tetrahedra each (337,881 nodes, 1,013,643
+DOF, 3x3 blocks, E = 1, nu = 0.3, body force -z, x = 0 face clamped).  One step
+= one complete solve as the reference performs it after assembly: numeric
+ILU(0) of K (CPreconditioner_ILU::SetValue) and ILU(0)-PCG from x = 0 to
+relative residual 1e-8 (LsSol::Solve_PCG), plain FP64.  The system is
+assembled on the device by the library itself (mesh -> pattern -> element
+assembly -> Dirichlet elimination) before timing; K (354 MB of values) is
+larger than L2.
+
+Beside it, in the same JSON line:
+  mixed    the same c2 solve by dfm_solve_pcg_mixed (FP32 values in SpMV and
+           ILU sweeps, FP64 residual replacement) with its error against the
+           FP64 solve and its speed-up
+  batched  512 uneven 2-D diffusion instances (grid sides log-uniform in
+           [32, 512], per-element kappa ~ lognormal(0, 1)) in one batched solve
+           against a loop of plain single-instance solves (timed on a
+           size-stratified sample of the instances and scaled)
+  spmv     SpMV HBM throughput against the measured peak
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--skip-batched] [--no-cpu-baseline]
 
 Prints one JSON line (rank 0).  Under torchrun every rank solves its own
-replica (the single-system path does not shard: "replicas only"); the value
-is the solves/s of all ranks, timed as the max over ranks.
+replica (a single system does not shard: "replicas only"); the value is the
+solves/s of all ranks over the max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -33,28 +47,19 @@ METRIC = "solve time to rel.res 1e-8: mixed/batched vs plain FP64 GPU PCG; SpMV 
 UNIT = "solves/s (c2, rel.res 1e-8)"
 TOL = 1e-8
 NX, NY, NZ = 200, 40, 40
+NU = 0.3
+LAM3 = NU / ((1 + NU) * (1 - 2 * NU))
+MYU3 = 1.0 / (2 * (1 + NU))
+C3_COUNT, C3_LO, C3_HI, C3_SEED = 512, 32, 512, 3
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-# ------------------------------------------------------------------ workload
-def build_system():
-    from delfem_b200 import meshes
-    from oracle import port as P
-    from tests import cases
-    t0 = time.time()
-    m = meshes.box_tet(NX, NY, NZ)
-    rp, ci = P.pattern(m.nnode, m.elem)
-    S = P.System(rp, ci, 3)
-    S.asm_solid3d(m, cases.LAM3, cases.MYU3, 1.0, 0.0, 0.0, -1.0)
-    S.apply_bc(P.bc_flags_from_bnd(m.nnode, 3, m.bnd))
-    log(f"[bench] c2 system N={S.N} ncrs={S.ncrs} built in {time.time() - t0:.1f}s")
-    return m, S
-
-
 def alg_bytes(N, ncrs, b, sv=8, sx=8):
+    """Algorithmic bytes of one SpMV, one ILU fwd+bwd application and one PCG
+    iteration (values, indices, vectors read/written once)."""
     bb = b * b
     spmv = (ncrs + N) * bb * sv + 4 * ncrs + 4 * (N + 1) + 2 * N * b * sx
     ilu = (ncrs + N) * bb * sv + 4 * ncrs + 4 * (N + 1) + 4 * N + 4 * N * b * sx
@@ -64,7 +69,7 @@ def alg_bytes(N, ncrs, b, sv=8, sx=8):
 
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -104,10 +109,38 @@ class ClockSampler:
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
-                          and "Not" not in r[5 + k]})
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ c2 on the GPU
+def c2_mesh():
+    from delfem_b200 import meshes
+    return meshes.box_tet(NX, NY, NZ)
+
+
+def build_c2(ctx, torch, dev):
+    """Pattern, assembly and Dirichlet elimination through the library."""
+    from delfem_b200 import lib
+    t0 = time.time()
+    m = c2_mesh()
+    G = lib.Mesh(ctx, m.coord, m.elem)
+    rp, ci = G.pattern()
+    A = lib.Matrix(ctx, rp, ci, 3)
+    rhs = torch.empty(3 * m.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+    flags = np.zeros((m.nnode, 3), np.int32)
+    flags[np.unique(m.bnd.ravel())] = 1
+    flags_d = torch.from_numpy(flags.ravel()).cuda(dev)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    G.assemble_solid3d(A, LAM3, MYU3, 1.0, 0.0, 0.0, -1.0, rhs)
+    lib.apply_dirichlet(A, flags_d, rhs)
+    torch.cuda.synchronize()
+    t_asm = time.time() - t1
+    log(f"[bench] c2 N={A.N} ncrs={A.ncrs} set up in {time.time() - t0:.1f}s (device assembly {t_asm * 1e3:.1f} ms)")
+    return m, G, A, rhs, t_asm
 
 
 # ------------------------------------------------------------- reference arm
@@ -116,47 +149,129 @@ def reference_runs():
     return json.load(open(p)) if os.path.exists(p) else {}
 
 
-def cpu_reference_sample(S, sample_iters):
+def cpu_reference_sample(N, b, rowptr, colind, diag, off, rhs, sample_iters):
     """The reference's own ILU(0) + Solve_PCG (oracle/_ref, built from its
-    sources) on a bounded sample: ILU + `sample_iters` PCG iterations, scaled to
-    a full solve with the reference's iteration count to 1e-8."""
+    sources) on a bounded sample: the ILU(0) and `sample_iters` PCG iterations
+    timed on one host core."""
     from oracle import refshim as R
-    rc, x, it, conv, t_ilu, t_solve = R.mat_solve(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, S.rhs,
-                                                  R.PCG, TOL, sample_iters)
-    t_iter = t_solve / max(sample_iters, 1)
-    runs = reference_runs().get("c2", {}).get(f"tol{TOL:g}", {})
-    n_full = runs.get("iterations")
-    return t_ilu, t_iter, n_full
+    rc, x, it, conv, t_ilu, t_solve = R.mat_solve(N, b, rowptr, colind, diag, off, rhs, R.PCG, TOL, sample_iters)
+    return t_ilu, t_solve / max(sample_iters, 1)
 
 
 def run_reference(args, rank):
+    """The reference's stock CPU path on c2 (oracle/_ref): its own pattern,
+    element assembly, ILU(0) and Solve_PCG.  Each step is a bounded sample (the
+    ILU(0) and 5 PCG iterations) scaled to the reference's iteration count to
+    1e-8 (tests/golden/reference_runs.json, measured from the reference)."""
     if rank != 0:
         return
-    _, S = build_system()
     from oracle import refshim as R
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdfm_refshim.so was not built"}))
         return
+    m = c2_mesh()
+    s = R.RefSystem(R.SOLID3D, m)
+    _, t_asm = s.assemble([LAM3, MYU3, 1.0, 0.0, 0.0, -1.0])
+    n_full = reference_runs().get("c2", {}).get(f"tol{TOL:g}", {}).get("iterations")
+    d, o, rhs = s.system()
+    rp, ci = s.pattern()
     per_step = []
-    n_full = None
     for k in range(args.warmup + args.steps):
-        t_ilu, t_iter, n_full = cpu_reference_sample(S, 5)
-        if n_full is None:
-            n_full = 1
+        t_ilu, t_iter = cpu_reference_sample(s.N, s.b, rp, ci, d, o, rhs, 5)
         if k >= args.warmup:
-            per_step.append(t_ilu + n_full * t_iter)
+            per_step.append(t_ilu + (n_full or 1) * t_iter)
     t = statistics.median(per_step)
     v = 1.0 / t
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "c2 3D elasticity 200x40x40x6 tets, ILU(0)+PCG to 1e-8",
-                       "N": S.N, "b": 3, "ncrs": S.ncrs},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"per step: reference ILU(0) + 5 Solve_PCG iterations on one core, "
-                                       f"scaled to the reference's {n_full} iterations to 1e-8"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "c2 3D elasticity 200x40x40x6 tets, ILU(0)+PCG to 1e-8", "N": s.N, "b": 3,
+                   "ncrs": s.ncrs, "reference_assembly_s": t_asm},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"per step: the reference's ILU(0) + 5 Solve_PCG iterations on one core "
+                                   f"(the reference is single-threaded), scaled to its {n_full} iterations to 1e-8"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# --------------------------------------------------------------- c3 batched
+def build_c3(ctx, torch, dev):
+    from delfem_b200 import lib, meshes
+    t0 = time.time()
+    sizes = meshes.batch_sizes(C3_COUNT, C3_LO, C3_HI, C3_SEED)
+    ms = [meshes.unit_square_tri(int(n)) for n in sizes]
+    big, noff, eoff = meshes.concat(ms)
+    kappa = np.random.default_rng(C3_SEED + 1).lognormal(0.0, 1.0, big.elem.shape[0])
+    G = lib.Mesh(ctx, big.coord, big.elem)
+    rp, ci = G.pattern()
+    A = lib.Matrix(ctx, rp, ci, 1)
+    rhs = torch.empty(big.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+    flags = np.zeros(big.nnode, np.int32)
+    flags[np.unique(big.bnd.ravel())] = 1
+    G.assemble_poisson(A, 1.0, 1.0, rhs, coef=torch.from_numpy(kappa).cuda(dev))
+    lib.apply_dirichlet(A, torch.from_numpy(flags).cuda(dev), rhs)
+    M = lib.ILU(A)
+    M.factor()
+    B = lib.Batch(M, noff.astype(np.uint32))
+    torch.cuda.synchronize()
+    log(f"[bench] c3 {C3_COUNT} instances, {big.nnode} nodes, ncrs={A.ncrs}, set up in {time.time() - t0:.1f}s")
+    return sizes, ms, noff, eoff, kappa, A, M, B, rhs
+
+
+def run_c3(ctx, torch, dev, stream, timed, steps):
+    from delfem_b200 import lib
+    sizes, ms, noff, eoff, kappa, A, M, B, rhs = build_c3(ctx, torch, dev)
+    x = torch.zeros_like(rhs)
+    res = {}
+    B.solve(rhs, x, tol=TOL)  # warm-up: autotunes the sweep schedule and the batch tiles
+    t_batch = timed(lambda: B.solve(rhs, x, tol=TOL), max(2, min(steps, 3)))
+    rc, _, it, conv, st = B.solve(rhs, x, tol=TOL)
+    xb = x.cpu().numpy()
+    # looped plain solves on a size-stratified sample (every k-th instance by size)
+    order = np.argsort(sizes, kind="stable")
+    stride = 8
+    sample = order[stride // 2::stride]
+    t_loop_sample = 0.0
+    err = 0.0
+    for k in sample:
+        a0, a1 = int(noff[k]), int(noff[k + 1])
+        m = ms[k]
+        Gk = lib.Mesh(ctx, m.coord, m.elem)
+        rp, ci = Gk.pattern()
+        Ak = lib.Matrix(ctx, rp, ci, 1)
+        rk = torch.empty(m.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+        fl = np.zeros(m.nnode, np.int32)
+        fl[np.unique(m.bnd.ravel())] = 1
+        Gk.assemble_poisson(Ak, 1.0, 1.0, rk, coef=torch.from_numpy(kappa[eoff[k]:eoff[k + 1]]).cuda(dev))
+        lib.apply_dirichlet(Ak, torch.from_numpy(fl).cuda(dev), rk)
+        Mk = lib.ILU(Ak)
+        Mk.factor()
+        bk = rk.clone()
+        xk = torch.zeros_like(bk)
+        rwork = bk.clone()
+        lib.solve_pcg(Ak, Mk, rwork, xk, tol=TOL, maxit=20000)  # warm-up (autotune + graph capture)
+
+        def one():
+            rwork.copy_(bk)
+            lib.solve_pcg(Ak, Mk, rwork, xk, tol=TOL, maxit=20000)
+
+        t_loop_sample += timed(one, 1)
+        xs = xk.cpu().numpy()
+        err = max(err, float(np.linalg.norm(xs - xb[a0:a1]) / max(np.linalg.norm(xs), 1e-300)))
+        for h in (Mk, Ak, Gk):
+            h.close()
+    t_loop = t_loop_sample * (len(sizes) / len(sample))
+    res.update({
+        "instances": int(len(sizes)), "nodes": int(noff[-1]), "grid_sides": [int(sizes.min()), int(sizes.max())],
+        "batched_s": t_batch, "looped_s_estimated": t_loop, "speedup_vs_looped": t_loop / t_batch,
+        "looped_sample": f"{len(sample)} instances (every {stride}th by size) timed one by one with dfm_solve_pcg, "
+                         f"scaled by {len(sizes) / len(sample):.0f}",
+        "max_iterations": int(it.max()), "all_converged": bool((st == lib.OK).all()),
+        "max_rel_diff_vs_single_solves": err, "tuning": list(B.tuning), "sweep": M.sweep,
+    })
+    for h in (B, M, A):
+        h.close()
+    return res
 
 
 # -------------------------------------------------------------------- our arm
@@ -165,15 +280,12 @@ def run_ours(args, rank, world):
     from delfem_b200 import lib
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    _, S = build_system()
-    N, b, ncrs = S.N, S.b, S.ncrs
     stream = torch.cuda.Stream(device=dev)
     ctx = lib.Context(dev)
     lib.check(lib.lib().dfm_ctx_set_stream(ctx.h, lib.C.c_void_p(stream.cuda_stream)))
-    A = lib.Matrix(ctx, S.rowptr, S.colind, b)
-    A.set_values(S.diag, S.off)
+    m, G, A, b_dev, t_asm = build_c2(ctx, torch, dev)
+    N, b, ncrs = A.N, A.b, A.ncrs
     M = lib.ILU(A)
-    b_dev = torch.from_numpy(S.rhs).cuda(dev)
     r = torch.empty_like(b_dev)
     x = torch.empty_like(b_dev)
     torch.cuda.synchronize()
@@ -204,13 +316,13 @@ def run_ours(args, rank, world):
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
         t_step = float(tt.item())
-    x_np = x.cpu().numpy()
+    x64 = x.clone()
 
-    # ---- kernel breakdown (CUDA events on the library stream) ----
     def timed(fn, reps):
         out = []
         for _ in range(reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
             e0.record(stream)
             fn()
             e1.record(stream)
@@ -218,13 +330,22 @@ def run_ours(args, rank, world):
             out.append(e0.elapsed_time(e1) / 1e3)
         return statistics.median(out)
 
+    def true_rel_residual(xv):
+        y = torch.empty_like(b_dev)
+        A.spmv(1.0, xv, 0.0, y)
+        torch.cuda.synchronize()
+        return float(torch.linalg.norm(b_dev - y) / torch.linalg.norm(b_dev))
+
+    rr = true_rel_residual(x64)
+
+    # ---- kernel breakdown (CUDA events on the library stream) ----
     y = torch.empty_like(b_dev)
     t_spmv = timed(lambda: A.spmv(1.0, x, 0.0, y), 20)
     t_apply = timed(lambda: M.apply(r, y), 10)
     t_factor = timed(lambda: M.factor(), 3)
     B_spmv, B_ilu, B_it = alg_bytes(N, ncrs, b)
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peaks_p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_p)) if os.path.exists(peaks_p) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if peaks else "fallback"
     n_it = iters + 1
@@ -235,9 +356,11 @@ def run_ours(args, rank, world):
         "spmv_bcrs_b3": {"ms": t_spmv * 1e3, "alg_bytes": B_spmv, "gbs": B_spmv / t_spmv / 1e9,
                          "frac": B_spmv / t_spmv / 1e9 / hbm, "share_of_step": share_spmv},
         "ilu0_fwd_bwd": {"ms": t_apply * 1e3, "alg_bytes": B_ilu, "gbs": B_ilu / t_apply / 1e9,
-                         "frac": B_ilu / t_apply / 1e9 / hbm, "share_of_step": share_sweep},
+                         "frac": B_ilu / t_apply / 1e9 / hbm, "share_of_step": share_sweep,
+                         "sweep_mode": M.sweep},
         "ilu0_factor": {"ms": t_factor * 1e3},
         "pcg_iteration": {"ms": t_iter * 1e3, "alg_bytes": B_it, "gbs": B_it / t_iter / 1e9},
+        "assembly_c2": {"ms": t_asm * 1e3},
     }
     dom = "ilu0_fwd_bwd" if share_sweep >= share_spmv else "spmv_bcrs_b3"
     dk = kernels[dom]
@@ -246,10 +369,30 @@ def run_ours(args, rank, world):
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
 
+    # ---- mixed precision on the same system ----
+    mixed = {}
+    if not args.skip_mixed:
+        xm = torch.zeros_like(b_dev)
+
+        def mstep():
+            M.factor()
+            r.copy_(b_dev)
+            torch.cuda.synchronize()
+            return lib.solve_pcg_mixed(A, M, r, xm, tol=TOL, maxit=40000)
+
+        mstep()
+        t_mixed = timed(mstep, max(2, min(args.steps, 3)))
+        rc_m, it_m, conv_m = mstep()
+        mixed = {"solve_s": t_mixed, "plain_fp64_solve_s": t_step, "speedup_vs_plain": t_step / t_mixed,
+                 "iterations": it_m + 1, "plain_iterations": n_it, "status": rc_m,
+                 "true_rel_residual": true_rel_residual(xm),
+                 "rel_err_vs_fp64_solution": float(torch.linalg.norm(xm - x64) / torch.linalg.norm(x64))}
+
     # ---- end-to-end through the C ABI with host buffers ----
-    diag_h = torch.from_numpy(S.diag).pin_memory()
-    off_h = torch.from_numpy(S.off).pin_memory()
-    b_h = torch.from_numpy(S.rhs).pin_memory()
+    diag_d, off_d = A.get_values()
+    diag_h = torch.from_numpy(diag_d).pin_memory()
+    off_h = torch.from_numpy(off_d).pin_memory()
+    b_h = b_dev.cpu().pin_memory()
     x_h = torch.empty_like(b_h).pin_memory()
     L = lib.lib()
     it_c, conv_c = lib.C.c_uint(), lib.C.c_double()
@@ -262,26 +405,29 @@ def run_ours(args, rank, world):
 
     e2e_step()
     t_e2e = timed(e2e_step, max(2, min(args.steps, 5)))
-    h2d = (S.diag.nbytes + S.off.nbytes + S.rhs.nbytes)
-    d2h = S.rhs.nbytes
+    h2d = diag_h.numel() * 8 + off_h.numel() * 8 + b_h.numel() * 8
+    d2h = x_h.numel() * 8
 
-    # ---- parity spot check against the oracle's residual (no oracle solve) ----
-    rr = np.linalg.norm(S.rhs - S.spmv(1.0, x_np, 0.0, np.zeros_like(x_np))) / np.linalg.norm(S.rhs)
+    # ---- c3 batched vs looped ----
+    batched = {}
+    if not args.skip_batched and world == 1:
+        batched = run_c3(ctx, torch, dev, stream, timed, args.steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            t_ilu, t_iter_ref, n_full = cpu_reference_sample(S, 30)
-            n_full = n_full or n_it
+            n_full = reference_runs().get("c2", {}).get(f"tol{TOL:g}", {}).get("iterations") or n_it
+            t_ilu, t_iter_ref = cpu_reference_sample(N, b, A.rowptr, A.colind, diag_d, off_d, b_h.numpy(), 30)
             v = 1.0 / (t_ilu + n_full * t_iter_ref)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": f"reference ILU(0) ({t_ilu:.2f}s) + 30 Solve_PCG iterations "
-                             f"({t_iter_ref * 1e3:.1f} ms/it) on one host core, scaled to {n_full} iterations",
+                   "sample": f"the reference's ILU(0) ({t_ilu:.2f}s) + 30 Solve_PCG iterations "
+                             f"({t_iter_ref * 1e3:.1f} ms/it) on one host core (single-threaded code), "
+                             f"scaled to its {n_full} iterations to 1e-8",
                    "t_ilu_s": t_ilu, "t_iter_s": t_iter_ref, "iterations": n_full}
-        except Exception as e:  # the reference build is optional on a box
+        except Exception as e:  # the reference build may be absent
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
 
-    launches = 1 + 4 + 16 * ((n_it + 15) // 16) * 5
+    launches = 2 + 4 + 16 * ((n_it + 15) // 16) * 5
     if rank == 0:
         line = {
             "metric": METRIC, "value": world / t_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -289,15 +435,16 @@ def run_ours(args, rank, world):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "c2 3D elasticity cantilever 200x40x40 hexes x 6 P1 tets, ILU(0) + PCG to "
                                    "rel.res 1e-8 (plain FP64)", "N": N, "b": b, "ncrs": ncrs,
-                       "dof": N * b, "l2": "inputs larger than L2 (K = %.0f MB)" % (S.off.nbytes / 1e6),
+                       "dof": N * b, "l2": "inputs larger than L2 (K = %.0f MB)" % (off_d.nbytes / 1e6),
                        "parallelism": f"replicas x{world}"},
-            "iterations": n_it, "conv": conv, "true_rel_residual": rr,
-            "solve_time_s": t_step,
+            "iterations": n_it, "conv": conv, "true_rel_residual": rr, "solve_time_s": t_step,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
                          "frac": dk["frac"], "traffic": traffic, "peak_source": peak_src},
             "spmv_roofline": {"achieved": kernels["spmv_bcrs_b3"]["gbs"], "peak": hbm, "unit": "GB/s",
                               "frac": kernels["spmv_bcrs_b3"]["frac"]},
             "kernels": kernels,
+            "mixed": mixed,
+            "batched": batched,
             "e2e": {"value": 1.0 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": t_e2e * 1e3},
             "cpu_baseline": cpu,
@@ -314,6 +461,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-mixed", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

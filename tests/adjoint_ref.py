@@ -65,11 +65,26 @@ class Reference:
         ue = u[2 * self.elem[:, :, None] + np.arange(2)]
         return L, -np.einsum("ear,eacrs,ecs->e", le, self.Ke, ue)
 
-    def fd(self, theta, lfun, elems, h=1e-6):
+    def fd(self, theta, idx, ut, elems, h=1e-6):
+        """Central differences (L(theta + h e_k) - L(theta - h e_k)) / 2h of
+        L = 1/2 sum_idx (u - ut)^2, each L(theta +- h e_k) evaluated exactly as
+        L(theta) + (u - ut).d + 1/2 |d|^2 over idx with d = u(theta +- h e_k) - u
+        solved directly from K(theta +- h e_k) d = -(+-h) K_e^0 u (an exact
+        rearrangement: it avoids subtracting two nearly equal losses)."""
+        _, u = self.solve(theta)
+        w = u[idx] - ut[idx]
         out = []
         for e in elems:
-            tp, tm = theta.copy(), theta.copy()
-            tp[e] += h
-            tm[e] -= h
-            out.append((lfun(self.solve(tp)[1]) - lfun(self.solve(tm)[1])) / (2 * h))
+            dofs = (2 * self.elem[e][:, None] + np.arange(2)).ravel()
+            ke = self.Ke[e].transpose(0, 2, 1, 3).reshape(6, 6)
+            du = np.zeros_like(u)
+            du[dofs] = ke @ u[dofs]
+            du[self.fixed] = 0.0
+            dl = []
+            for sgn in (1.0, -1.0):
+                t = theta.copy()
+                t[e] += sgn * h
+                d = spla.splu(self.matrix(t)).solve(-sgn * h * du)
+                dl.append(w @ d[idx] + 0.5 * d[idx] @ d[idx])
+            out.append((dl[0] - dl[1]) / (2 * h))
         return np.array(out)
