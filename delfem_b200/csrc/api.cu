@@ -178,6 +178,41 @@ int dfm_ctx_wait_selftest(dfm_ctx c, unsigned long long limit_ns) {
   return code;  // DFM_WAIT_TIMEOUT expected
 }
 
+// ------------------------------------------------------------- buffers
+int dfm_buf_alloc(dfm_ctx c, size_t bytes, void** out) {
+  if (!c || !out) return DFM_ERR_INVALID;
+  *out = nullptr;
+  DFM_CUDA_TRY(cudaSetDevice(c->device));
+  DFM_CUDA_TRY(cudaMalloc(out, bytes ? bytes : 1));
+  return DFM_OK;
+}
+
+int dfm_buf_free(dfm_ctx c, void* p) {
+  if (!c) return DFM_ERR_INVALID;
+  if (!p) return DFM_OK;
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  DFM_CUDA_TRY(cudaFree(p));
+  return DFM_OK;
+}
+
+int dfm_buf_copy(dfm_ctx c, void* dst, const void* src, size_t bytes, int dir) {
+  if (!c || (bytes && (!dst || !src)) || dir < DFM_H2D || dir > DFM_D2D) return DFM_ERR_INVALID;
+  if (!bytes) return DFM_OK;
+  const cudaMemcpyKind k =
+      dir == DFM_H2D ? cudaMemcpyHostToDevice : dir == DFM_D2H ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  DFM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, c->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFM_OK;
+}
+
+int dfm_buf_zero(dfm_ctx c, void* p, size_t bytes) {
+  if (!c || (bytes && !p)) return DFM_ERR_INVALID;
+  if (!bytes) return DFM_OK;
+  DFM_CUDA_TRY(cudaMemsetAsync(p, 0, bytes, c->stream));
+  DFM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFM_OK;
+}
+
 // ------------------------------------------------------------------ matrix
 int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* rowptr, const unsigned* colind,
                    dfm_mat* out) {

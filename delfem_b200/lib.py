@@ -35,6 +35,10 @@ PROTOS = {
     "dfm_ctx_set_wait_limit": (_i, [_vp, C.c_ulonglong]),
     "dfm_ctx_take_error": (_i, [_vp, _ip, _ip]),
     "dfm_ctx_wait_selftest": (_i, [_vp, C.c_ulonglong]),
+    "dfm_buf_alloc": (_i, [_vp, C.c_size_t, C.POINTER(_vp)]),
+    "dfm_buf_free": (_i, [_vp, _vp]),
+    "dfm_buf_copy": (_i, [_vp, _vp, _vp, C.c_size_t, _i]),
+    "dfm_buf_zero": (_i, [_vp, _vp, C.c_size_t]),
     "dfm_mat_create": (_i, [_vp, _u, _u, _i, _up, _up, C.POINTER(_vp)]),
     "dfm_mat_destroy": (_i, [_vp]),
     "dfm_mat_info": (_i, [_vp, _up, _up, _up, _ip]),

@@ -76,6 +76,14 @@ DFM_API int dfm_ctx_take_error(dfm_ctx ctx, int* code, int* where);
  * the given limit, and must come back with DFM_WAIT_TIMEOUT. */
 DFM_API int dfm_ctx_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns);
 
+/* ---- device buffers (for callers built without the CUDA toolkit) -------- */
+/* dfm_buf_copy directions; the copy is complete when the call returns. */
+enum { DFM_H2D = 0, DFM_D2H = 1, DFM_D2D = 2 };
+DFM_API int dfm_buf_alloc(dfm_ctx ctx, size_t bytes, void** out);
+DFM_API int dfm_buf_free(dfm_ctx ctx, void* p);
+DFM_API int dfm_buf_copy(dfm_ctx ctx, void* dst, const void* src, size_t bytes, int direction);
+DFM_API int dfm_buf_zero(dfm_ctx ctx, void* p, size_t bytes);
+
 /* ---- matrix: CMatDia_BlkCrs on the device ------------------------------ */
 /* Pattern from host arrays; validated (monotone rowptr, in-range, strictly
  * ascending off-diagonal columns, no diagonal entry) as CMatDia_BlkCrs::AddPattern

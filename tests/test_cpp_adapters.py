@@ -1,0 +1,53 @@
+"""The reference-shaped C++ adapters (include/dfm_b200_lsol.hpp): a C++ program
+using only them and the C ABI compiles and links against the library on the
+CPU; on a GPU it solves 2-D Poisson and matches the oracle."""
+import json
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "delfem_b200", "_lib")
+
+
+@pytest.fixture(scope="module")
+def demo(tmp_path_factory):
+    from delfem_b200 import build
+    build.build()
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no C++ compiler")
+    out = str(tmp_path_factory.mktemp("cpp") / "lsol_demo")
+    cmd = [gxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "lsol_demo.cpp"), "-L", LIBDIR, "-ldfm_b200",
+           f"-Wl,-rpath,{LIBDIR}", "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return out
+
+
+def test_adapter_program_compiles_and_links(demo):
+    assert os.path.exists(demo)
+
+
+@pytest.mark.gpu
+def test_adapter_program_matches_oracle(demo):
+    from delfem_b200 import meshes
+    from oracle import port as P
+    r = subprocess.run([demo, "16"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    m = meshes.unit_square_tri(16)
+    S = P.System(*P.pattern(m.nnode, m.elem), 1)
+    S.asm_poisson(m, 1.0, 1.0)
+    S.apply_bc(P.bc_flags_from_bnd(m.nnode, 1, m.bnd))
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcg", tol=1e-10, maxit=1000)
+    refb = S.solve(fd, fo, method="pbicgstab", tol=1e-10, maxit=1000)
+    x = np.array(out["x"])
+    assert out["pcg_ok"] and abs(out["pcg_iters"] - ref["iters"]) <= 1
+    assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
+    assert out["bicg_ok"] and abs(out["bicg_iters"] - refb["iters"]) <= 2
