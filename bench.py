@@ -21,7 +21,9 @@ Beside it, in the same JSON line:
   spmv     SpMV HBM throughput against the measured peak
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--skip-batched] [--no-cpu-baseline]
+                    [--skip-batched] [--skip-mixed] [--no-cpu-baseline]
+    python bench.py --profile-run      # short c2 workload for ncu captures
+
 
 Prints one JSON line (rank 0).  Under torchrun every rank solves its own
 replica (a single system does not shard: "replicas only"); the value is the
@@ -274,6 +276,30 @@ def run_c3(ctx, torch, dev, stream, timed, steps):
     return res
 
 
+# ------------------------------------------------------------- profile run
+def run_profile():
+    """A short c2 workload for profiler captures: device assembly, ILU(0),
+    3 SpMVs, 3 ILU applications and a 32-iteration PCG (no timing output)."""
+    import torch
+    from delfem_b200 import lib
+    ctx = lib.Context(0)
+    m, G, A, b_dev, _ = build_c2(ctx, torch, 0)
+    M = lib.ILU(A)
+    M.factor()
+    x = torch.zeros_like(b_dev)
+    y = torch.empty_like(b_dev)
+    r = b_dev.clone()
+    rc, it, conv = lib.solve_pcg(A, M, r, x, tol=TOL, maxit=32)  # autotunes SpMV lanes and the sweep schedule
+    for _ in range(3):
+        A.spmv(1.0, b_dev, 0.0, y)
+    for _ in range(3):
+        M.apply(b_dev, y)
+    r.copy_(b_dev)
+    lib.solve_pcg(A, M, r, x, tol=TOL, maxit=32)
+    torch.cuda.synchronize()
+    log(f"[profile-run] sweep mode {M.sweep}, lanes {A.lanes}")
+
+
 # -------------------------------------------------------------------- our arm
 def run_ours(args, rank, world):
     import torch
@@ -463,7 +489,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-mixed", action="store_true")
+    ap.add_argument("--profile-run", action="store_true")
     args = ap.parse_args()
+    if args.profile_run:
+        run_profile()
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -469,7 +469,8 @@ int dfm_ilu_apply(dfm_ilu M, const double* r, double* z) {
 // ---------------------------------------------------------------- solvers
 static int solve_args(dfm_mat A, dfm_ilu M, int method, const void* b, const void* x) {
   if (!A || !M || M->A != A || (A->N && (!b || !x))) return DFM_ERR_INVALID;
-  if (method == DFM_PCOCG ? A->vt != DFM_COMPLEX : A->vt != DFM_REAL) return DFM_ERR_INVALID;
+  const bool cplx = method == DFM_PCOCG || method == DFM_PCOCG_MIXED;
+  if (cplx ? A->vt != DFM_COMPLEX : A->vt != DFM_REAL) return DFM_ERR_INVALID;
   if (!M->factored) return DFM_ERR_INVALID;
   return DFM_OK;
 }
@@ -502,9 +503,16 @@ int dfm_solve_pcg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, 
   return krylov_solve(A, M, DFM_PCG_MIXED, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
 }
 
+int dfm_solve_pcocg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                          double* conv) {
+  const int rc = solve_args(A, M, DFM_PCOCG_MIXED, r, x);
+  if (rc) return rc;
+  return krylov_solve(A, M, DFM_PCOCG_MIXED, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
 int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv) {
-  if (method < DFM_PCG || method > DFM_PCG_MIXED) return DFM_ERR_INVALID;
+  if (method < DFM_PCG || method > DFM_PCOCG_MIXED) return DFM_ERR_INVALID;
   const int rc = solve_args(A, M, method, b_host, x_host);
   if (rc) return rc;
   return krylov_solve(A, M, method, b_host, DFM_HOST, x_host, DFM_HOST, nullptr, tol, maxit, iters, conv);

@@ -106,12 +106,14 @@ struct dfm_ilu_s {
 
 namespace dfm {
 // spmv.cu
-// Options of one SpMV launch (real matrices only except the defaults):
-//   dot_w  with dot_part: partials of (dot_w ? dot_w : x) . y
-//   dot_part2: partials of y . y beside the first dot
-//   yy: dot_part receives y . y instead (no w)
+// Options of one SpMV launch:
+//   dot_w  with dot_part: partials of (dot_w ? dot_w : x) . y     (real only)
+//   dot_part2: partials of y . y beside the first dot            (real only)
+//   yy: dot_part receives y . y (|y|^2 for complex) instead
 //   y0: y = y0 + alpha A x (beta ignored)
 //   f32: multiply with the FP32 copy of the values
+// Without options a complex SpMV with dot_part writes the unconjugated x^T y
+// (re in dot_part, im in dot_part + kMaxBlocks).
 struct SpmvOpts {
   const double* dot_w = nullptr;
   double* dot_part2 = nullptr;

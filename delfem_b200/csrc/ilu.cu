@@ -353,11 +353,11 @@ k_sweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned*
 }
 
 // complex b = 1
-template <int LPR, bool FWD, bool DOT>
+template <int LPR, bool FWD, bool DOT, typename TV = double2>
 __global__ void __launch_bounds__(256)
 k_zsweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned* __restrict__ rowptr,
                   const unsigned* __restrict__ colind, const unsigned* __restrict__ diaind,
-                  const double2* __restrict__ fdiag, const double2* __restrict__ foff,
+                  const double2* __restrict__ fdiag, const TV* __restrict__ foff,
                   const double2* __restrict__ in, double2* out, const double2* __restrict__ rdot, double* part,
                   KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st, uint64_t wait_ns) {
   if (FWD) {
@@ -379,7 +379,8 @@ k_zsweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned
     double re = 0.0, im = 0.0;
     for (unsigned s = s0 + lane; s < s1; s += LPR) {
       const unsigned col = __ldg(colind + s);
-      const double2 m = __ldcs(foff + s);
+      const TV mv = __ldcs(foff + s);
+      const double2 m = make_double2((double)mv.x, (double)mv.y);
       const double xr = poll_value(o64 + 2 * (size_t)col, st, wait_ns, FWD ? 5 : 6);
       const double xi = poll_value(o64 + 2 * (size_t)col + 1, st, wait_ns, FWD ? 5 : 6);
       re += m.x * xr - m.y * xi;
@@ -483,12 +484,12 @@ k_sweep_cta(unsigned nlev, const unsigned* __restrict__ lvl, const unsigned* __r
   if (DOT) block_partial<1024>(dacc, part);
 }
 
-template <int LPR, bool FWD, bool DOT>
+template <int LPR, bool FWD, bool DOT, typename TV = double2>
 __global__ void __launch_bounds__(1024)
 k_zsweep_cta(unsigned nlev, const unsigned* __restrict__ lvl, const unsigned* __restrict__ order,
              const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
              const unsigned* __restrict__ diaind, const double2* __restrict__ fdiag,
-             const double2* __restrict__ foff, const double2* __restrict__ in, double2* out,
+             const TV* __restrict__ foff, const double2* __restrict__ in, double2* out,
              const double2* __restrict__ rdot, double* part, KrylovScalars* sc, const double* rr_part,
              int rr_nparts) {
   if (FWD) {
@@ -513,7 +514,8 @@ k_zsweep_cta(unsigned nlev, const unsigned* __restrict__ lvl, const unsigned* __
       }
       double re = 0.0, im = 0.0;
       for (unsigned s = s0 + lane; s < s1; s += LPR) {
-        const double2 m = __ldg(foff + s);
+        const TV mv = __ldg(foff + s);
+        const double2 m = make_double2((double)mv.x, (double)mv.y);
         const double2 xv = out[__ldg(colind + s)];
         re += m.x * xv.x - m.y * xv.y;
         im += m.x * xv.y + m.y * xv.x;
@@ -697,13 +699,13 @@ static cudaError_t sweep_real(dfm_ilu M, int sweep, const double* in, double* ou
   return sweep_real_tv<B, LPR, FWD, double>(M, M->d_foff, sweep, in, out, rdot, part, sc, rr_part, rr_n);
 }
 
-template <int LPR, bool FWD>
-static cudaError_t sweep_cplx(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
-                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+template <int LPR, bool FWD, typename TV>
+static cudaError_t sweep_cplx_tv(dfm_ilu M, const TV* fo, int sweep, const double* in, double* out,
+                                 const double* rdot, double* part, KrylovScalars* sc, const double* rr_part,
+                                 int rr_n) {
   dfm_ctx c = M->ctx;
   const unsigned* order = FWD ? M->d_order_f : M->d_order_b;
   auto* fd = reinterpret_cast<const double2*>(M->d_fdiag);
-  auto* fo = reinterpret_cast<const double2*>(M->d_foff);
   auto* vi = reinterpret_cast<const double2*>(in);
   auto* vo = reinterpret_cast<double2*>(out);
   auto* rd = reinterpret_cast<const double2*>(rdot);
@@ -711,36 +713,46 @@ static cudaError_t sweep_cplx(dfm_ilu M, int sweep, const double* in, double* ou
     const unsigned* lvl = FWD ? M->d_lvl_f : M->d_lvl_b;
     const unsigned nlev = FWD ? M->nlev_f : M->nlev_b;
     if (part)
-      k_zsweep_cta<LPR, FWD, true><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr, M->A->d_colind,
-                                                              M->d_diaind, fd, fo, vi, vo, rd, part, sc, rr_part,
-                                                              rr_n);
+      k_zsweep_cta<LPR, FWD, true, TV><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr,
+                                                                  M->A->d_colind, M->d_diaind, fd, fo, vi, vo, rd,
+                                                                  part, sc, rr_part, rr_n);
     else
-      k_zsweep_cta<LPR, FWD, false><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr, M->A->d_colind,
-                                                               M->d_diaind, fd, fo, vi, vo, rd, nullptr, sc,
-                                                               rr_part, rr_n);
+      k_zsweep_cta<LPR, FWD, false, TV><<<1, 1024, 0, c->stream>>>(nlev, lvl, order, M->A->d_rowptr,
+                                                                   M->A->d_colind, M->d_diaind, fd, fo, vi, vo, rd,
+                                                                   nullptr, sc, rr_part, rr_n);
     return cudaGetLastError();
   }
   const int grid = sweep_grid(M, 1);
   if (part)
-    return launch_coop(k_zsweep_syncfree<LPR, FWD, true>, grid, 256, c->stream, M->N, order,
+    return launch_coop(k_zsweep_syncfree<LPR, FWD, true, TV>, grid, 256, c->stream, M->N, order,
                        (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind,
                        (const unsigned*)M->d_diaind, fd, fo, vi, vo, rd, part, sc, rr_part, rr_n, c->d_status,
                        (uint64_t)c->wait_ns);
-  return launch_coop(k_zsweep_syncfree<LPR, FWD, false>, grid, 256, c->stream, M->N, order,
+  return launch_coop(k_zsweep_syncfree<LPR, FWD, false, TV>, grid, 256, c->stream, M->N, order,
                      (const unsigned*)M->A->d_rowptr, (const unsigned*)M->A->d_colind, (const unsigned*)M->d_diaind,
                      fd, fo, vi, vo, rd, (double*)nullptr, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+}
+
+template <int LPR, bool FWD>
+static cudaError_t sweep_cplx(dfm_ilu M, int sweep, const double* in, double* out, const double* rdot,
+                              double* part, KrylovScalars* sc, const double* rr_part, int rr_n, bool f32) {
+  if (f32)
+    return sweep_cplx_tv<LPR, FWD, float2>(M, reinterpret_cast<const float2*>(M->d_foff32), sweep, in, out, rdot,
+                                           part, sc, rr_part, rr_n);
+  return sweep_cplx_tv<LPR, FWD, double2>(M, reinterpret_cast<const double2*>(M->d_foff), sweep, in, out, rdot,
+                                          part, sc, rr_part, rr_n);
 }
 
 static int sweep_dispatch(dfm_ilu M, bool fwd, int sweep, const double* in, double* out, const double* rdot,
                           double* part, KrylovScalars* sc, const double* rr_part, int rr_n, bool f32) {
   if (M->N == 0) return DFM_OK;
   if (sweep <= 0) sweep = M->sweep > 0 ? M->sweep : 1;
-  if (f32 && (M->vt != DFM_REAL || !M->d_foff32)) return DFM_ERR_INVALID;
+  if (f32 && !M->d_foff32) return DFM_ERR_INVALID;
   if (sweep == 3) return sweep_ranges_launch(M, fwd, in, out, rdot, part, sc, rr_part, rr_n, f32);
   cudaError_t e;
   if (M->vt == DFM_COMPLEX) {
-    e = fwd ? sweep_cplx<8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n)
-            : sweep_cplx<8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n);
+    e = fwd ? sweep_cplx<8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32)
+            : sweep_cplx<8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32);
   } else if (M->b == 1) {
     e = fwd ? sweep_real<1, 8, true>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32)
             : sweep_real<1, 8, false>(M, sweep, in, out, rdot, part, sc, rr_part, rr_n, f32);
@@ -772,12 +784,11 @@ int ilu_prepare(dfm_ilu M, bool f32) {
     if (M->plan_b.stale && (M->plan_b.valid) && sweep_plan_refresh(M, &M->plan_b)) return DFM_ERR_CUDA;
   }
   if (!f32) return DFM_OK;
-  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
   const size_t no = (size_t)M->ncrs * M->vw();
   if (!M->d_foff32) DFM_CUDA_TRY(cudaMalloc(&M->d_foff32, std::max<size_t>(no, 1) * sizeof(float)));
   int rc = to_f32(M->ctx, M->d_foff, M->d_foff32, no);
   if (rc) return rc;
-  if (M->sweep == 3) {
+  if (M->sweep == 3 && M->vt == DFM_REAL) {
     // FP32 plans with the FP64 plans' ranges and lanes
     for (int f = 0; f < 2; f++) {
       SweepPlan& P64 = f ? M->plan_b : M->plan_f;

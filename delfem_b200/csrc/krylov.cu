@@ -341,9 +341,16 @@ k_cocg_p(size_t N, KrylovScalars* sc, const double* part_rw, int np_rw, const do
 // (Z = Mp, Q = AMp).
 enum { kVecR, kVecX, kVecP, kVecZ, kVecY, kVecQ, kVecR2, kVecS, kVecMs, kVecAMs, kNumVec };
 
+static bool is_mixed(int method) { return method == DFM_PCG_MIXED || method == DFM_PCOCG_MIXED; }
+
 static int vectors_of(int method) {
-  return method == DFM_PBICGSTAB ? kNumVec : method == DFM_PCOCG ? kVecQ + 1 : method == DFM_PCG_MIXED ? kVecR2 + 1
-                                                                                                     : kVecY + 1;
+  switch (method) {
+    case DFM_PBICGSTAB: return kNumVec;
+    case DFM_PCOCG: return kVecQ + 1;
+    case DFM_PCG_MIXED:
+    case DFM_PCOCG_MIXED: return kVecR2 + 1;  // kVecR2 keeps b for the true residual
+    default: return kVecY + 1;
+  }
 }
 
 // Workspace of one (M, method) pair: vectors and the captured graph, with the
@@ -480,7 +487,12 @@ static int mixed_verify(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   // completes the iteration if the solve goes on (kernels skip when done)
   if ((rc = ilu_fwd_launch(M, P->v[kVecR], P->v[kVecY], sc, M->sweep, false, true))) return rc;
   if ((rc = ilu_bwd_launch(M, P->v[kVecY], P->v[kVecZ], P->v[kVecR], c->part(3), sc, M->sweep, true))) return rc;
-  k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(3), gs, P->v[kVecZ], P->v[kVecP]);
+  if (P->method == DFM_PCOCG_MIXED)
+    k_cocg_p<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(3), gs,
+                                               reinterpret_cast<const double2*>(P->v[kVecZ]),
+                                               reinterpret_cast<double2*>(P->v[kVecP]));
+  else
+    k_pcg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(3), gs, P->v[kVecZ], P->v[kVecP]);
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;
 }
@@ -514,12 +526,15 @@ static int enqueue_bicg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   return DFM_OK;
 }
 
-static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
+static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, bool f32 = false,
+                        bool replace = false) {
   dfm_ctx c = A->ctx;
   const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
   double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *w = P->v[kVecZ], *y = P->v[kVecY];
   double* Ap = P->v[kVecQ];
-  int rc = spmv_launch(A, 1.0, p, 0.0, Ap, c->part(0), gv, sc, A->lanes);  // (p, Ap) re/im in slots 0/1
+  SpmvOpts o;
+  o.f32 = f32;
+  int rc = spmv_launch(A, 1.0, p, 0.0, Ap, c->part(0), gv, sc, A->lanes, o);  // (p, Ap) re/im in slots 0/1
   if (rc) return rc;
   k_cocg_xr<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv,
                                               reinterpret_cast<const double2*>(p),
@@ -527,8 +542,9 @@ static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
                                               reinterpret_cast<double2*>(r), reinterpret_cast<double2*>(y),
                                               reinterpret_cast<double2*>(w));
   DFM_CUDA_TRY(cudaGetLastError());
-  if ((rc = ilu_fwd_launch(M, r, y, sc, M->sweep))) return rc;                 // stop test on slot 2
-  if ((rc = ilu_bwd_launch(M, y, w, r, c->part(3), sc, M->sweep))) return rc;  // (r, w) re/im in slots 3/4
+  if (replace && (rc = enqueue_true_residual(A, P, sc))) return rc;
+  if ((rc = ilu_fwd_launch(M, r, y, sc, M->sweep, true, f32))) return rc;                 // stop test on slot 2
+  if ((rc = ilu_bwd_launch(M, y, w, r, c->part(3), sc, M->sweep, f32))) return rc;  // (r, w) re/im in slots 3/4
   k_cocg_p<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(3), gs, reinterpret_cast<const double2*>(w),
                                              reinterpret_cast<double2*>(p));
   DFM_CUDA_TRY(cudaGetLastError());
@@ -541,6 +557,7 @@ static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* 
     case DFM_PBICGSTAB: return enqueue_bicg(A, M, P, sc);
     case DFM_PCOCG: return enqueue_cocg(A, M, P, sc);
     case DFM_PCG_MIXED: return enqueue_pcg_mixed(A, M, P, sc, k == kIterPerGraph - 1);
+    case DFM_PCOCG_MIXED: return enqueue_cocg(A, M, P, sc, true, k == kIterPerGraph - 1);
     default: return enqueue_pcg(A, M, P, sc);
   }
 }
@@ -559,12 +576,16 @@ static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
       k_bicg_start2<<<1, kVecThreads, 0, s>>>(sc, c->part(2), gv);
       break;
     case DFM_PCOCG:
+    case DFM_PCOCG_MIXED: {
+      const bool f32 = P->method == DFM_PCOCG_MIXED;
+      if (f32) DFM_CUDA_TRY(cudaMemcpyAsync(P->v[kVecR2], r, P->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
       k_cocg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, y, z, c->part(2));
       DFM_CUDA_TRY(cudaGetLastError());
-      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep))) return rc;
-      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep))) return rc;
+      if ((rc = ilu_fwd_launch(M, r, y, nullptr, M->sweep, true, f32))) return rc;
+      if ((rc = ilu_bwd_launch(M, y, z, r, c->part(3), nullptr, M->sweep, f32))) return rc;
       k_cocg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, z, p);
       break;
+    }
     default: {
       const bool f32 = P->method == DFM_PCG_MIXED;
       if (f32) DFM_CUDA_TRY(cudaMemcpyAsync(P->v[kVecR2], r, P->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -620,7 +641,7 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
   int rc = spmv_autotune(A);
   if (rc) return rc;
   if ((rc = ilu_autotune(M))) return rc;
-  const bool f32 = method == DFM_PCG_MIXED;
+  const bool f32 = is_mixed(method);
   if (f32 && (rc = mat_make_f32(A))) return rc;
   if ((rc = ilu_prepare(M, f32))) return rc;
   SolvePlan* P = nullptr;

@@ -77,13 +77,15 @@ k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restri
   if (NDOT == 2) block_partial<256>(dacc2, part2);
 }
 
-// Complex b = 1: values and vectors interleaved (re, im).
-template <int LPR, bool DOT>
+// Complex b = 1: values and vectors interleaved (re, im).  NDOT: 0 none,
+// 1 unconjugated x^T y (re / im partials), 3 |y|^2 (one partial).  TV is the
+// value type (double2, or float2 for the mixed-precision solve).
+template <int LPR, int NDOT, typename TV>
 __global__ void __launch_bounds__(256)
 k_zspmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
-        const double2* __restrict__ diag, const double2* __restrict__ off, double alpha,
+        const TV* __restrict__ diag, const TV* __restrict__ off, double alpha,
         const double2* __restrict__ x, double beta, double2* __restrict__ y, double* __restrict__ part,
-        const int* done) {
+        const int* done, const double2* __restrict__ y0) {
   if (done && block_flag(done)) return;
   const int lane = threadIdx.x % LPR;
   const unsigned g0 = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
@@ -94,10 +96,11 @@ k_zspmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restr
     const unsigned s0 = __ldg(rowptr + i), s1 = __ldg(rowptr + i + 1);
     double re = 0.0, im = 0.0;
     for (unsigned s = s0 + lane; s <= s1; s += LPR) {
-      double2 m;
+      TV mv;
       unsigned col;
-      if (s < s1) { m = __ldcs(off + s); col = __ldcs(colind + s); }
-      else { m = diag[i]; col = i; }
+      if (s < s1) { mv = __ldcs(off + s); col = __ldcs(colind + s); }
+      else { mv = diag[i]; col = i; }
+      const double2 m = make_double2((double)mv.x, (double)mv.y);
       const double2 xv = __ldg(x + col);
       re += m.x * xv.x - m.y * xv.y;
       im += m.x * xv.y + m.y * xv.x;
@@ -109,19 +112,19 @@ k_zspmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restr
     }
     if (lane == 0) {
       double2 v = make_double2(alpha * re, alpha * im);
-      if (beta != 0.0) { const double2 yo = y[i]; v.x += beta * yo.x; v.y += beta * yo.y; }
+      if (y0) { const double2 a = y0[i]; v.x += a.x; v.y += a.y; }
+      else if (beta != 0.0) { const double2 yo = y[i]; v.x += beta * yo.x; v.y += beta * yo.y; }
       y[i] = v;
-      if (DOT) {  // unconjugated x^T y (CZVector_Blk operator*, src/matvec/zvector_blk.cpp:39-59)
+      if (NDOT == 1) {  // unconjugated x^T y (CZVector_Blk operator*, src/matvec/zvector_blk.cpp:39-59)
         const double2 xi = x[i];
         dre += xi.x * v.x - xi.y * v.y;
         dim += xi.x * v.y + xi.y * v.x;
       }
+      if (NDOT == 3) dre += v.x * v.x + v.y * v.y;
     }
   }
-  if (DOT) {
-    block_partial<256>(dre, part);
-    block_partial<256>(dim, part + kMaxBlocks);
-  }
+  if (NDOT >= 1) block_partial<256>(dre, part);
+  if (NDOT == 1) block_partial<256>(dim, part + kMaxBlocks);
 }
 
 int spmv_grid(dfm_mat A) {
@@ -169,23 +172,40 @@ static void launch_real_lpr(int lanes, dfm_mat A, int grid, cudaStream_t s, doub
   }
 }
 
-template <int LPR>
-static void launch_cplx(dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x, double beta,
-                        double* y, double* part, const int* done) {
-  auto* d = reinterpret_cast<const double2*>(A->d_diag);
-  auto* o = reinterpret_cast<const double2*>(A->d_off);
+template <int LPR, typename TV>
+static void launch_cplx_tv(dfm_mat A, const TV* d, const TV* o, int grid, cudaStream_t s, double alpha,
+                           const double* x, double beta, double* y, double* part, const int* done,
+                           const SpmvOpts& op) {
   auto* xx = reinterpret_cast<const double2*>(x);
   auto* yy = reinterpret_cast<double2*>(y);
-  if (part)
-    k_zspmv<LPR, true><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, d, o, alpha, xx, beta, yy, part, done);
+  auto* y0 = reinterpret_cast<const double2*>(op.y0);
+  if (part && op.yy)
+    k_zspmv<LPR, 3, TV><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, d, o, alpha, xx, beta, yy, part, done,
+                                             y0);
+  else if (part)
+    k_zspmv<LPR, 1, TV><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, d, o, alpha, xx, beta, yy, part, done,
+                                             y0);
   else
-    k_zspmv<LPR, false><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, d, o, alpha, xx, beta, yy, nullptr,
-                                             done);
+    k_zspmv<LPR, 0, TV><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, d, o, alpha, xx, beta, yy, nullptr,
+                                             done, y0);
+}
+
+template <int LPR>
+static void launch_cplx(dfm_mat A, int grid, cudaStream_t s, double alpha, const double* x, double beta,
+                        double* y, double* part, const int* done, const SpmvOpts& op) {
+  if (op.f32)
+    launch_cplx_tv<LPR, float2>(A, reinterpret_cast<const float2*>(A->d_diag32),
+                                reinterpret_cast<const float2*>(A->d_off32), grid, s, alpha, x, beta, y, part, done,
+                                op);
+  else
+    launch_cplx_tv<LPR, double2>(A, reinterpret_cast<const double2*>(A->d_diag),
+                                 reinterpret_cast<const double2*>(A->d_off), grid, s, alpha, x, beta, y, part, done,
+                                 op);
 }
 
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
                 int grid, KrylovScalars* sc, int lanes, const SpmvOpts& o) {
-  if (A->vt == DFM_COMPLEX && (o.dot_w || o.dot_part2 || o.yy || o.y0 || o.f32)) return DFM_ERR_UNSUPPORTED;
+  if (A->vt == DFM_COMPLEX && (o.dot_w || o.dot_part2)) return DFM_ERR_UNSUPPORTED;
   if (o.f32 && !A->d_off32) return DFM_ERR_INVALID;
   if (A->N == 0) return DFM_OK;
   cudaStream_t s = A->ctx->stream;
@@ -194,10 +214,10 @@ int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y
   const int* done = sc ? &sc->done : nullptr;
   if (A->vt == DFM_COMPLEX) {
     switch (lanes) {
-      case 4: launch_cplx<4>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
-      case 8: launch_cplx<8>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
-      case 16: launch_cplx<16>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
-      default: launch_cplx<32>(A, grid, s, alpha, x, beta, y, dot_part, done); break;
+      case 4: launch_cplx<4>(A, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      case 8: launch_cplx<8>(A, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      case 16: launch_cplx<16>(A, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      default: launch_cplx<32>(A, grid, s, alpha, x, beta, y, dot_part, done, o); break;
     }
   } else if (A->b == 1) {
     launch_real_lpr<1>(lanes, A, grid, s, alpha, x, beta, y, dot_part, done, o);

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED = range(9)
 REAL, COMPLEX = 0, 1
 HOST, DEVICE = 0, 1
-PCG, PBICGSTAB, PCOCG, PCG_MIXED = 0, 1, 2, 3
+PCG, PBICGSTAB, PCOCG, PCG_MIXED, PCOCG_MIXED = 0, 1, 2, 3, 4
 
 _lib = None
 
@@ -74,6 +74,7 @@ PROTOS = {
     "dfm_solve_pbicgstab": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcocg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_mixed": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_pcocg_mixed": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_batch_create": (_i, [_vp, _u, _up, C.POINTER(_vp)]),
     "dfm_batch_destroy": (_i, [_vp]),
     "dfm_batch_set_tuning": (_i, [_vp, _i, _i]),
@@ -467,6 +468,15 @@ def solve_pcg_mixed(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, 
     _sync_torch()
     rc = lib().dfm_solve_pcg_mixed(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_pcg_mixed", allow)
+    return rc, it.value, conv.value
+
+
+def solve_pcocg_mixed(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """PCOCG with complex64 values inside complex128 residual replacement."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_pcocg_mixed(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_pcocg_mixed", allow)
     return rc, it.value, conv.value
 
 

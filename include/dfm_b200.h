@@ -51,7 +51,7 @@ typedef enum dfm_status {
 
 enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
 enum { DFM_HOST = 0, DFM_DEVICE = 1 };
-enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2, DFM_PCG_MIXED = 3 };
+enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2, DFM_PCG_MIXED = 3, DFM_PCOCG_MIXED = 4 };
 
 typedef struct dfm_ctx_s* dfm_ctx;
 typedef struct dfm_mat_s* dfm_mat;
@@ -227,6 +227,11 @@ DFM_API int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double t
  * cost iterations. */
 DFM_API int dfm_solve_pcg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                         unsigned* iters, double* conv);
+/* The same scheme for PCOCG on complex matrices: complex64 values in SpMV and
+ * ILU sweeps, complex128 vectors, dots, scalars and D^-1, complex128 residual
+ * replacement; conventions of dfm_solve_pcocg. */
+DFM_API int dfm_solve_pcocg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
+                          unsigned* iters, double* conv);
 /* ---- batched solves (no counterpart in the reference) -------------------- */
 /* A batch of independent systems stored as one block-diagonal matrix: instance
  * k owns block rows [row_off[k], row_off[k+1]) of M's matrix (row_off: host,
@@ -248,7 +253,7 @@ DFM_API int dfm_batch_solve_pcg(dfm_batch batch, const double* b, int b_where, d
                         double tol, unsigned maxit, unsigned* iters, double* conv, int* status);
 
 /* End-to-end variants with HOST buffers (b copied in, x copied out, inside the
- * call); method is DFM_PCG, DFM_PBICGSTAB, DFM_PCOCG or DFM_PCG_MIXED. */
+ * call); method is any DFM_PCG ... DFM_PCOCG_MIXED. */
 DFM_API int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv);
 DFM_API int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol,

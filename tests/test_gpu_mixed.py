@@ -83,3 +83,28 @@ def test_mixed_follows_value_updates(ctx):
     rc, it, conv = lib.solve_pcg_mixed(A, M, r, x2, tol=1e-9)
     assert rc == lib.OK
     assert np.allclose(x2.cpu().numpy() * 2.0, x.cpu().numpy(), rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("nring", [40])
+@pytest.mark.parametrize("sweep", [1, 2])
+def test_cocg_mixed_true_residual(ctx, nring, sweep):
+    """complex64 values inside complex128 residual replacement (Helmholtz)."""
+    from delfem_b200 import lib
+    m, S = cases.helmholtz(nring)
+    ns, fd, fo = S.ilu0()
+    tol = 1e-8
+    ref = S.solve(fd, fo, method="pcocg", tol=tol, maxit=5000)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, 1, lib.COMPLEX)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    M.sweep = sweep
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcocg_mixed(A, M, r, x, tol=tol, maxit=5000)
+    assert rc == lib.OK, (rc, it, conv)
+    xg = x.cpu().numpy()
+    res = S.rhs - S.spmv(1.0, xg, 0.0, np.zeros_like(S.rhs))
+    assert np.linalg.norm(res) < tol * np.linalg.norm(S.rhs)
+    err = np.linalg.norm(xg - ref["x"]) / np.linalg.norm(ref["x"])
+    assert err <= 1e-5, err
