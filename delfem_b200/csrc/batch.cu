@@ -19,6 +19,14 @@
 // The ILU sweeps run over the whole batch (the persistent sync-free or level
 // schedules).  One iteration = 10 launches, captured as a CUDA graph of
 // kBatchIterPerGraph iterations and replayed until every instance has stopped.
+//
+// A second schedule solves the batch in ONE persistent launch: every CTA
+// takes instances from a queue (largest first) and runs an instance's whole
+// PCG on its own - SpMV, level-by-level ILU sweeps over the instance's own
+// level sets (a __syncthreads per level), block reductions in fixed order -
+// so thousands of small solves proceed side by side with no grid-wide
+// synchronisation.  The autotuner times both schedules (and the CTA size and
+// lanes per row of the second) on the batch and keeps the faster.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -56,6 +64,18 @@ struct dfm_batch_s {
   unsigned key_gen = ~0u;
   unsigned long long key_wait = 0;
   int lanes = 0;  // SpMV lanes per row for the batch kernels (autotuned)
+  // persistent CTA-per-instance schedule
+  int schedule = 0;           // 0 untuned, 1 graph of phases, 2 persistent CTA per instance
+  int cta_threads = 0, cta_lanes = 0;
+  unsigned* d_bord_f = nullptr;   // per-instance rows by forward level (instance k at row_off[k])
+  unsigned* d_bord_b = nullptr;
+  unsigned* d_blv_f = nullptr;    // concatenated per-instance level pointers (absolute positions)
+  unsigned* d_blv_b = nullptr;
+  unsigned* d_blvo_f = nullptr;   // ninst + 1 offsets into d_blv_f
+  unsigned* d_blvo_b = nullptr;
+  unsigned* d_queue = nullptr;    // instances, largest first
+  unsigned* d_row_off = nullptr;  // ninst + 1
+  unsigned* d_next = nullptr;     // queue head
 };
 
 namespace dfm {
@@ -392,6 +412,343 @@ static int enqueue_iter_any(dfm_batch B, const BatchCtl* ctl) {
   }
 }
 
+// ------------------------------------------- persistent CTA-per-instance
+struct CtaArgs {
+  unsigned ninst;
+  const unsigned* queue;
+  unsigned* next;
+  const unsigned* row_off;
+  const unsigned *rowptr, *colind, *diaind;
+  const double *diag, *off, *fdiag, *foff;
+  const unsigned *ord_f, *ord_b, *lv_f, *lv_b, *lvo_f, *lvo_b;
+  double *r, *x, *p, *z, *q;
+  InstScal* sc;
+  unsigned* ndone;
+  const BatchCtl* ctl;
+};
+
+template <int NT>
+DFM_DEVINL double cta_sum(double v, double* s_w) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();  // s_w free
+  if (l == 0) s_w[w] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int k = 0; k < NT / 32; k++) t += s_w[k];  // every thread, same fixed order
+  return t;
+}
+
+// rows [ord[a], ...) of one level of one sweep; FWD: y_i = D^-1 (in_i - L y),
+// BWD: z_i = in_i - (D^-1 U) z
+template <int B, int LPR, bool FWD>
+DFM_DEVINL void cta_sweep(const CtaArgs& A, unsigned k, const double* in, double* out) {
+  constexpr int BB = B * B;
+  const int lane = threadIdx.x % LPR;
+  const unsigned g = threadIdx.x / LPR, ng = blockDim.x / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned* ord = FWD ? A.ord_f : A.ord_b;
+  const unsigned* lv = (FWD ? A.lv_f : A.lv_b) + (FWD ? A.lvo_f[k] : A.lvo_b[k]);
+  const unsigned nlev = (FWD ? A.lvo_f[k + 1] - A.lvo_f[k] : A.lvo_b[k + 1] - A.lvo_b[k]) - 1;
+  for (unsigned l = 0; l < nlev; l++) {
+    const unsigned p0 = lv[l], p1 = lv[l + 1];
+    for (unsigned pb = p0; pb < p1; pb += ng) {
+      const unsigned pp = pb + g;
+      const bool valid = pp < p1;  // uniform within a group
+      unsigned i = 0, s0 = 0, s1 = 0;
+      if (valid) {
+        i = __ldg(ord + pp);
+        if (FWD) { s0 = __ldg(A.rowptr + i); s1 = __ldg(A.diaind + i); }
+        else { s0 = __ldg(A.diaind + i); s1 = __ldg(A.rowptr + i + 1); }
+      }
+      double acc[B];
+#pragma unroll
+      for (int r = 0; r < B; r++) acc[r] = 0.0;
+      for (unsigned s = s0 + lane; s < s1; s += LPR) {
+        const unsigned col = __ldg(A.colind + s);
+        const double* m = A.foff + (size_t)s * BB;
+#pragma unroll
+        for (int r = 0; r < B; r++)
+#pragma unroll
+          for (int c = 0; c < B; c++) acc[r] += __ldg(m + r * B + c) * out[(size_t)col * B + c];
+      }
+      if (LPR > 1)
+#pragma unroll
+        for (int r = 0; r < B; r++)
+#pragma unroll
+          for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+      if (valid && lane == 0) {
+        double t[B];
+#pragma unroll
+        for (int r = 0; r < B; r++) t[r] = in[(size_t)i * B + r] - acc[r];
+        if (FWD) {
+          const double* d = A.fdiag + (size_t)i * BB;
+#pragma unroll
+          for (int r = 0; r < B; r++) {
+            double v = 0.0;
+#pragma unroll
+            for (int c = 0; c < B; c++) v += __ldg(d + r * B + c) * t[c];
+            out[(size_t)i * B + r] = v;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < B; r++) out[(size_t)i * B + r] = t[r];
+        }
+      }
+    }
+    __syncthreads();  // level done
+  }
+}
+
+template <int B, int LPR, int NT>
+__global__ void __launch_bounds__(NT)
+k_batch_cta(CtaArgs A) {
+  constexpr int BB = B * B;
+  __shared__ double s_w[NT / 32];
+  __shared__ unsigned s_k;
+  const int lane = threadIdx.x % LPR;
+  const unsigned g = threadIdx.x / LPR, ng = NT / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned maxit = A.ctl->maxit;
+  const double tol2 = A.ctl->tol2;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned t = atomicAdd(A.next, 1u);
+      s_k = t < A.ninst ? A.queue[t] : 0xffffffffu;
+    }
+    __syncthreads();
+    const unsigned k = s_k;
+    __syncthreads();
+    if (k == 0xffffffffu) break;
+    const unsigned r0 = A.row_off[k], r1 = A.row_off[k + 1];
+    const size_t e0 = (size_t)r0 * B, e1 = (size_t)r1 * B;
+    double* r = A.r;
+    double* x = A.x;
+    double* p = A.p;
+    double* z = A.z;
+    double* q = A.q;  // holds y = L^-1 r during the preconditioner
+    // x = 0, (r, r)
+    double acc = 0.0;
+    for (size_t e = e0 + threadIdx.x; e < e1; e += NT) {
+      x[e] = 0.0;
+      acc += r[e] * r[e];
+    }
+    const double rr0 = cta_sum<NT>(acc, s_w);
+    InstScal res = {};
+    if (rr0 < 1.0e-30) {
+      res.status = 100 + DFM_OK;
+    } else {
+      const double inv0 = 1.0 / rr0;
+      res.inv0 = inv0;
+      __syncthreads();
+      cta_sweep<B, LPR, true>(A, k, r, q);
+      cta_sweep<B, LPR, false>(A, k, q, z);
+      acc = 0.0;
+      for (size_t e = e0 + threadIdx.x; e < e1; e += NT) {
+        p[e] = z[e];
+        acc += r[e] * z[e];
+      }
+      double rz = cta_sum<NT>(acc, s_w);
+      double rr = rr0;
+      unsigned it = 0;
+      for (;; it++) {
+        if (it >= maxit) {
+          res.status = 100 + DFM_NOT_CONVERGED;
+          res.conv = sqrt(rr * inv0);
+          break;
+        }
+        // q = A p, (p, q)
+        acc = 0.0;
+        for (unsigned i = r0 + g; i < r1; i += ng) {
+          const unsigned s0 = __ldg(A.rowptr + i), s1 = __ldg(A.rowptr + i + 1);
+          double a[B];
+#pragma unroll
+          for (int rr_ = 0; rr_ < B; rr_++) a[rr_] = 0.0;
+          for (unsigned s = s0 + lane; s <= s1; s += LPR) {
+            const double* m = (s < s1) ? A.off + (size_t)s * BB : A.diag + (size_t)i * BB;
+            const unsigned col = (s < s1) ? __ldg(A.colind + s) : i;
+#pragma unroll
+            for (int rr_ = 0; rr_ < B; rr_++)
+#pragma unroll
+              for (int c = 0; c < B; c++) a[rr_] += __ldg(m + rr_ * B + c) * p[(size_t)col * B + c];
+          }
+          if (LPR > 1)
+#pragma unroll
+            for (int rr_ = 0; rr_ < B; rr_++)
+#pragma unroll
+              for (int o = LPR / 2; o > 0; o >>= 1) a[rr_] += __shfl_xor_sync(gmask, a[rr_], o);
+          if (lane == 0)
+#pragma unroll
+            for (int rr_ = 0; rr_ < B; rr_++) {
+              q[(size_t)i * B + rr_] = a[rr_];
+              acc += p[(size_t)i * B + rr_] * a[rr_];
+            }
+        }
+        const double pq = cta_sum<NT>(acc, s_w);
+        const double alpha = rz / pq;
+        if (!isfinite(alpha)) {
+          res.status = 100 + DFM_BREAKDOWN;
+          res.conv = NAN;
+          break;
+        }
+        acc = 0.0;
+        for (size_t e = e0 + threadIdx.x; e < e1; e += NT) {
+          x[e] += alpha * p[e];
+          const double rv = r[e] - alpha * q[e];
+          r[e] = rv;
+          acc += rv * rv;
+        }
+        rr = cta_sum<NT>(acc, s_w);
+        if (rr * inv0 < tol2) {
+          res.status = 100 + DFM_OK;
+          res.conv = sqrt(rr * inv0);
+          break;
+        }
+        cta_sweep<B, LPR, true>(A, k, r, q);
+        cta_sweep<B, LPR, false>(A, k, q, z);
+        acc = 0.0;
+        for (size_t e = e0 + threadIdx.x; e < e1; e += NT) acc += r[e] * z[e];
+        const double rz_new = cta_sum<NT>(acc, s_w);
+        const double beta = rz_new / rz;
+        rz = rz_new;
+        for (size_t e = e0 + threadIdx.x; e < e1; e += NT) p[e] = p[e] * beta + z[e];
+        __syncthreads();
+      }
+      res.it = it;
+      res.conv_it = it;
+      res.rz = rz;
+      res.rr = rr;
+    }
+    if (threadIdx.x == 0) {
+      A.sc[k] = res;
+      atomicAdd(A.ndone, 1u);
+    }
+    __syncthreads();
+  }
+}
+
+// Per-instance level-ordered rows and level pointers from the global level
+// sets (an instance's levels are its own: no entry leaves the instance).
+static int build_cta_tables(dfm_batch B) {
+  dfm_ilu M = B->M;
+  const unsigned N = M->N;
+  std::vector<unsigned> ord_f(N), ord_b(N), lv_f, lv_b, lvo_f(B->ninst + 1), lvo_b(B->ninst + 1);
+  std::vector<unsigned> cnt;
+  for (int f = 0; f < 2; f++) {
+    const std::vector<unsigned>& lev = f ? M->lev_b : M->lev_f;
+    std::vector<unsigned>& ord = f ? ord_b : ord_f;
+    std::vector<unsigned>& lv = f ? lv_b : lv_f;
+    std::vector<unsigned>& lvo = f ? lvo_b : lvo_f;
+    for (unsigned k = 0; k < B->ninst; k++) {
+      const unsigned r0 = B->h_row_off[k], r1 = B->h_row_off[k + 1];
+      unsigned nl = 0;
+      for (unsigned i = r0; i < r1; i++) nl = std::max(nl, lev[i] + 1);
+      cnt.assign(nl + 1, 0);
+      for (unsigned i = r0; i < r1; i++) cnt[lev[i] + 1]++;
+      for (unsigned l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+      lvo[k] = (unsigned)lv.size();
+      for (unsigned l = 0; l <= nl; l++) lv.push_back(r0 + cnt[l]);
+      for (unsigned i = r0; i < r1; i++) ord[r0 + cnt[lev[i]]++] = i;  // ascending row within a level
+    }
+    lvo[B->ninst] = (unsigned)lv.size();
+  }
+  std::vector<unsigned> queue(B->ninst);
+  for (unsigned k = 0; k < B->ninst; k++) queue[k] = k;
+  std::stable_sort(queue.begin(), queue.end(), [&](unsigned a, unsigned b) {
+    return B->h_row_off[a + 1] - B->h_row_off[a] > B->h_row_off[b + 1] - B->h_row_off[b];
+  });
+  cudaStream_t s = B->ctx->stream;
+  auto up = [&](unsigned** d, const std::vector<unsigned>& h) -> int {
+    DFM_CUDA_TRY(cudaMalloc(d, std::max<size_t>(h.size(), 1) * sizeof(unsigned)));
+    if (!h.empty())
+      DFM_CUDA_TRY(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+    return DFM_OK;
+  };
+  int rc = up(&B->d_bord_f, ord_f);
+  if (!rc) rc = up(&B->d_bord_b, ord_b);
+  if (!rc) rc = up(&B->d_blv_f, lv_f);
+  if (!rc) rc = up(&B->d_blv_b, lv_b);
+  if (!rc) rc = up(&B->d_blvo_f, lvo_f);
+  if (!rc) rc = up(&B->d_blvo_b, lvo_b);
+  if (!rc) rc = up(&B->d_queue, queue);
+  if (!rc) DFM_CUDA_TRY(cudaMalloc(&B->d_next, sizeof(unsigned)));
+  if (!rc) DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  return rc;
+}
+
+template <int BS, int LPR, int NT>
+static cudaError_t launch_cta_t(dfm_batch B, const CtaArgs& a) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cta<BS, LPR, NT>, NT, 0);
+  const int grid = std::max(1, std::min<int>((int)B->ninst, B->ctx->nsm * std::max(per_sm, 1)));
+  k_batch_cta<BS, LPR, NT><<<grid, NT, 0, B->ctx->stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int BS, int NT>
+static cudaError_t launch_cta_l(dfm_batch B, const CtaArgs& a, int lanes) {
+  switch (lanes) {
+    case 2: return launch_cta_t<BS, 2, NT>(B, a);
+    case 4: return launch_cta_t<BS, 4, NT>(B, a);
+    default: return launch_cta_t<BS, 8, NT>(B, a);
+  }
+}
+
+template <int BS>
+static cudaError_t launch_cta_n(dfm_batch B, const CtaArgs& a, int threads, int lanes) {
+  switch (threads) {
+    case 256: return launch_cta_l<BS, 256>(B, a, lanes);
+    case 512: return launch_cta_l<BS, 512>(B, a, lanes);
+    default: return launch_cta_l<BS, 1024>(B, a, lanes);
+  }
+}
+
+// One persistent launch solves the whole batch (b already in B->r).
+static int run_cta(dfm_batch B, const BatchCtl* d_ctl, int threads, int lanes) {
+  if (!B->d_bord_f) {
+    int rc = build_cta_tables(B);
+    if (rc) return rc;
+  }
+  cudaStream_t s = B->ctx->stream;
+  DFM_CUDA_TRY(cudaMemsetAsync(B->d_next, 0, sizeof(unsigned), s));
+  DFM_CUDA_TRY(cudaMemsetAsync(B->d_ndone, 0, sizeof(unsigned), s));
+  CtaArgs a;
+  a.ninst = B->ninst;
+  a.queue = B->d_queue;
+  a.next = B->d_next;
+  a.row_off = B->d_row_off;
+  a.rowptr = B->A->d_rowptr;
+  a.colind = B->A->d_colind;
+  a.diaind = B->M->d_diaind;
+  a.diag = B->A->d_diag;
+  a.off = B->A->d_off;
+  a.fdiag = B->M->d_fdiag;
+  a.foff = B->M->d_foff;
+  a.ord_f = B->d_bord_f;
+  a.ord_b = B->d_bord_b;
+  a.lv_f = B->d_blv_f;
+  a.lv_b = B->d_blv_b;
+  a.lvo_f = B->d_blvo_f;
+  a.lvo_b = B->d_blvo_b;
+  a.r = B->r;
+  a.x = B->x;
+  a.p = B->p;
+  a.z = B->z;
+  a.q = B->q;
+  a.sc = B->d_scal;
+  a.ndone = B->d_ndone;
+  a.ctl = d_ctl;
+  cudaError_t e;
+  switch (B->A->b) {
+    case 1: e = launch_cta_n<1>(B, a, threads, lanes); break;
+    case 2: e = launch_cta_n<2>(B, a, threads, lanes); break;
+    default: e = launch_cta_n<3>(B, a, threads, lanes); break;
+  }
+  DFM_CUDA_TRY(e);
+  return DFM_OK;
+}
+
 // Chunk table: each instance's rows cut into chunks of at most `rows` block rows.
 static int build_chunks(dfm_batch B, int rows) {
   std::vector<unsigned> ch_inst, ch_row, inst_ch(B->ninst + 1, 0);
@@ -518,6 +875,9 @@ int dfm_batch_create(dfm_ilu M, unsigned ninst, const unsigned* row_off, dfm_bat
   if (!rc && cudaMalloc(&B->d_ndone, kCtlOffset + sizeof(BatchCtl)) != cudaSuccess) rc = DFM_ERR_NOMEM;
   if (!rc && cudaMallocHost((void**)&B->h_scal, ninst * sizeof(InstScal)) != cudaSuccess) rc = DFM_ERR_NOMEM;
   if (!rc && cudaMallocHost((void**)&B->h_ndone, sizeof(unsigned)) != cudaSuccess) rc = DFM_ERR_NOMEM;
+  if (!rc && cudaMalloc(&B->d_row_off, (ninst + 1) * sizeof(unsigned)) != cudaSuccess) rc = DFM_ERR_NOMEM;
+  if (!rc && cudaMemcpy(B->d_row_off, row_off, (ninst + 1) * sizeof(unsigned), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = DFM_ERR_CUDA;
   if (rc) {
     cudaGetLastError();
     dfm_batch_destroy(B);
@@ -538,6 +898,9 @@ int dfm_batch_destroy(dfm_batch B) {
   cudaFree(B->d_part);
   cudaFree(B->d_scal);
   cudaFree(B->d_ndone);
+  for (unsigned* v : {B->d_bord_f, B->d_bord_b, B->d_blv_f, B->d_blv_b, B->d_blvo_f, B->d_blvo_b, B->d_queue,
+                      B->d_next, B->d_row_off})
+    cudaFree(v);
   if (B->h_scal) cudaFreeHost(B->h_scal);
   if (B->h_ndone) cudaFreeHost(B->h_ndone);
   delete B;
@@ -563,24 +926,12 @@ int dfm_batch_get_tuning(dfm_batch B, int* lanes, int* chunk_rows) {
   return DFM_OK;
 }
 
-int dfm_batch_solve_pcg(dfm_batch B, const double* b, int b_where, double* x, int x_where, double tol,
-                        unsigned maxit, unsigned* iters, double* conv, int* status) {
-  if (!B || !b || !x || !B->M->factored) return DFM_ERR_INVALID;
+// Runs the graph-of-phases schedule to the end (b already in B->r).
+static int run_phases(dfm_batch B, const BatchCtl* d_ctl) {
   dfm_ctx c = B->ctx;
   cudaStream_t s = c->stream;
-  const size_t n = (size_t)B->A->N * B->A->b;
-  int rc = ilu_autotune(B->M);
-  if (!rc) rc = ilu_prepare(B->M, false);
-  if (!rc) rc = batch_autotune(B);
+  int rc = enqueue_start_any(B);
   if (rc) return rc;
-  BatchCtl* d_ctl = reinterpret_cast<BatchCtl*>(reinterpret_cast<char*>(B->d_ndone) + kCtlOffset);
-  {
-    BatchCtl h = {maxit, tol * tol};
-    DFM_CUDA_TRY(cudaMemcpyAsync(d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  }
-  DFM_CUDA_TRY(cudaMemcpyAsync(B->r, b, n * sizeof(double),
-                               b_where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
-  if ((rc = enqueue_start_any(B))) return rc;
   const bool same = B->exec && B->key_sweep == B->M->sweep && B->key_lanes == B->lanes &&
                     B->key_chunk == B->chunk_rows && B->key_gen == B->M->plan_gen && B->key_wait == c->wait_ns;
   if (!same) {
@@ -618,6 +969,98 @@ int dfm_batch_solve_pcg(dfm_batch B, const double* b, int b_where, double* x, in
     if (code) return code;
     if (*B->h_ndone >= B->ninst) break;
   }
+  return DFM_OK;
+}
+
+static int run_schedule(dfm_batch B, const BatchCtl* d_ctl, int schedule, int threads, int lanes) {
+  if (schedule == 2) {
+    int rc = run_cta(B, d_ctl, threads, lanes);
+    if (rc) return rc;
+    DFM_CUDA_TRY(cudaStreamSynchronize(B->ctx->stream));
+    return take_code(B->ctx);
+  }
+  return run_phases(B, d_ctl);
+}
+
+static int set_ctl(dfm_batch B, BatchCtl* d_ctl, unsigned maxit, double tol) {
+  BatchCtl h = {maxit, tol * tol};
+  DFM_CUDA_TRY(cudaMemcpyAsync(d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, B->ctx->stream));
+  return DFM_OK;
+}
+
+// Schedule autotuner: the graph of phases and the persistent CTA-per-instance
+// kernel (CTA sizes 256 / 512 / 1024, 2 / 4 / 8 lanes per row) each run the
+// batch for a few iterations from b; the fastest is kept.
+static int schedule_autotune(dfm_batch B, BatchCtl* d_ctl, const double* b, int b_where, double tol) {
+  if (B->schedule) return DFM_OK;
+  cudaStream_t s = B->ctx->stream;
+  const size_t n = (size_t)B->A->N * B->A->b;
+  const unsigned trial_it = 12;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bs = 1, bt = 0, bl = 0;
+  struct Cand { int sched, threads, lanes; };
+  std::vector<Cand> cands = {{1, 0, 0}};
+  for (int t : {256, 512, 1024})
+    for (int l : {2, 4, 8}) cands.push_back({2, t, l});
+  int rc = DFM_OK;
+  for (const Cand& cd : cands) {
+    if ((rc = set_ctl(B, d_ctl, trial_it, tol))) break;
+    DFM_CUDA_TRY(cudaMemcpyAsync(B->r, b, n * sizeof(double),
+                                 b_where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+    cudaEventRecord(e0, s);
+    if ((rc = run_schedule(B, d_ctl, cd.sched, cd.threads, cd.lanes))) break;
+    cudaEventRecord(e1, s);
+    DFM_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) { best = ms; bs = cd.sched; bt = cd.threads; bl = cd.lanes; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  B->schedule = bs;
+  B->cta_threads = bt;
+  B->cta_lanes = bl;
+  return DFM_OK;
+}
+
+int dfm_batch_set_schedule(dfm_batch B, int schedule, int cta_threads, int cta_lanes) {
+  if (!B || schedule < 0 || schedule > 2) return DFM_ERR_INVALID;
+  if (schedule == 2 && (cta_threads != 256 && cta_threads != 512 && cta_threads != 1024)) return DFM_ERR_INVALID;
+  if (schedule == 2 && (cta_lanes != 2 && cta_lanes != 4 && cta_lanes != 8)) return DFM_ERR_INVALID;
+  B->schedule = schedule;
+  B->cta_threads = schedule == 2 ? cta_threads : 0;
+  B->cta_lanes = schedule == 2 ? cta_lanes : 0;
+  return DFM_OK;
+}
+
+int dfm_batch_get_schedule(dfm_batch B, int* schedule, int* cta_threads, int* cta_lanes) {
+  if (!B) return DFM_ERR_INVALID;
+  if (schedule) *schedule = B->schedule;
+  if (cta_threads) *cta_threads = B->cta_threads;
+  if (cta_lanes) *cta_lanes = B->cta_lanes;
+  return DFM_OK;
+}
+
+int dfm_batch_solve_pcg(dfm_batch B, const double* b, int b_where, double* x, int x_where, double tol,
+                        unsigned maxit, unsigned* iters, double* conv, int* status) {
+  if (!B || !b || !x || !B->M->factored) return DFM_ERR_INVALID;
+  dfm_ctx c = B->ctx;
+  cudaStream_t s = c->stream;
+  const size_t n = (size_t)B->A->N * B->A->b;
+  int rc = ilu_autotune(B->M);
+  if (!rc) rc = ilu_prepare(B->M, false);
+  if (!rc) rc = batch_autotune(B);
+  if (rc) return rc;
+  BatchCtl* d_ctl = reinterpret_cast<BatchCtl*>(reinterpret_cast<char*>(B->d_ndone) + kCtlOffset);
+  if ((rc = schedule_autotune(B, d_ctl, b, b_where, tol))) return rc;
+  if ((rc = set_ctl(B, d_ctl, maxit, tol))) return rc;
+  DFM_CUDA_TRY(cudaMemcpyAsync(B->r, b, n * sizeof(double),
+                               b_where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  if ((rc = run_schedule(B, d_ctl, B->schedule, B->cta_threads, B->cta_lanes))) return rc;
   DFM_CUDA_TRY(cudaMemcpyAsync(x, B->x, n * sizeof(double),
                                x_where == DFM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(B->h_scal, B->d_scal, B->ninst * sizeof(InstScal), cudaMemcpyDeviceToHost, s));

@@ -79,6 +79,8 @@ PROTOS = {
     "dfm_batch_destroy": (_i, [_vp]),
     "dfm_batch_set_tuning": (_i, [_vp, _i, _i]),
     "dfm_batch_get_tuning": (_i, [_vp, _ip, _ip]),
+    "dfm_batch_set_schedule": (_i, [_vp, _i, _i, _i]),
+    "dfm_batch_get_schedule": (_i, [_vp, _ip, _ip, _ip]),
     "dfm_batch_solve_pcg": (_i, [_vp, _vp, _i, _vp, _i, _d, _u, _up, _dp, _ip]),
     "dfm_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_host": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
@@ -415,6 +417,17 @@ class Batch:
     @tuning.setter
     def tuning(self, v):
         check(lib().dfm_batch_set_tuning(self.h, int(v[0]), int(v[1])), "dfm_batch_set_tuning")
+
+    @property
+    def schedule(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().dfm_batch_get_schedule(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    @schedule.setter
+    def schedule(self, v):
+        v = tuple(v) + (0, 0)
+        check(lib().dfm_batch_set_schedule(self.h, int(v[0]), int(v[1]), int(v[2])), "dfm_batch_set_schedule")
 
     def solve(self, b, x=None, tol=1e-8, maxit=10000, allow=(OK, NOT_CONVERGED)):
         """b, x: device tensors (x written) or host arrays (x returned).  Returns

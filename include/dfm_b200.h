@@ -243,6 +243,12 @@ DFM_API int dfm_batch_destroy(dfm_batch batch);
  * tile of the per-instance reductions); 0, 0 = autotuned on the next solve. */
 DFM_API int dfm_batch_set_tuning(dfm_batch batch, int lanes, int chunk_rows);
 DFM_API int dfm_batch_get_tuning(dfm_batch batch, int* lanes, int* chunk_rows);
+/* Schedule: 0 = autotuned on the next solve, 1 = every phase one launch over
+ * all instances with the iteration captured as a CUDA graph, 2 = one
+ * persistent launch in which each CTA (cta_threads 256/512/1024, cta_lanes
+ * 2/4/8 lanes per row) solves whole instances taken from a queue. */
+DFM_API int dfm_batch_set_schedule(dfm_batch batch, int schedule, int cta_threads, int cta_lanes);
+DFM_API int dfm_batch_get_schedule(dfm_batch batch, int* schedule, int* cta_threads, int* cta_lanes);
 /* Every instance runs Solve_PCG's algorithm with its own scalars, stop test
  * and iteration count, all instances advancing in the same launches; stopped
  * instances are masked.  b (N*b doubles) and x at DFM_HOST or DFM_DEVICE;

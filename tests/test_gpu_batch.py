@@ -44,13 +44,16 @@ def _gpu_batch(ctx, S, noff):
     return A, M, lib.Batch(M, noff)
 
 
-@pytest.mark.parametrize("sweep", [1, 2, 3])
-def test_batch_matches_per_instance_oracle(ctx, sweep):
+@pytest.mark.parametrize("sweep,schedule", [(1, (1,)), (2, (1,)), (3, (1,)), (1, (2, 256, 2)), (1, (2, 512, 4)),
+                                            (1, (2, 1024, 8)), (0, (0,))])
+def test_batch_matches_per_instance_oracle(ctx, sweep, schedule):
     from delfem_b200 import lib
     sizes = [3, 17, 8, 30, 1, 12, 24, 5]
     S, noff, inst = _batch_problem(sizes, seed=1)
     A, M, B = _gpu_batch(ctx, S, noff)
-    M.sweep = sweep
+    if sweep:
+        M.sweep = sweep
+    B.schedule = schedule
     rc, x, it, conv, st = B.solve(S.rhs, tol=1e-10, maxit=2000)
     assert rc == lib.OK and (st == lib.OK).all()
     for k, Si in enumerate(inst):
@@ -63,11 +66,13 @@ def test_batch_matches_per_instance_oracle(ctx, sweep):
         assert conv[k] < 1e-10
 
 
-def test_batch_masks_and_maxit(ctx):
+@pytest.mark.parametrize("schedule", [(1,), (2, 512, 4)])
+def test_batch_masks_and_maxit(ctx, schedule):
     from delfem_b200 import lib
     sizes = [20, 4, 16, 9]
     S, noff, inst = _batch_problem(sizes, seed=2, zero_rhs=(2,))
     A, M, B = _gpu_batch(ctx, S, noff)
+    B.schedule = schedule
     rc, x, it, conv, st = B.solve(S.rhs, tol=1e-10, maxit=12)
     assert rc == lib.NOT_CONVERGED
     assert st[2] == lib.OK and it[2] == 0 and np.all(x[noff[2]:noff[3]] == 0)  # zero rhs: stops at once
@@ -113,3 +118,21 @@ def test_batch_rejects_cross_instance_entries(ctx):
     bad[1] += 1  # cuts through instance 0's rows
     with pytest.raises(lib.DfmError):
         lib.Batch(M, bad)
+
+
+def test_batch_schedules_agree(ctx):
+    """Both schedules run the same per-instance algorithm: the same iteration
+    counts up to reduction-order effects and solutions to rounding."""
+    from delfem_b200 import lib
+    S, noff, inst = _batch_problem([40, 9, 25, 64, 2], seed=7)
+    A, M, B = _gpu_batch(ctx, S, noff)
+    B.schedule = (1,)
+    rc1, x1, it1, c1, st1 = B.solve(S.rhs, tol=1e-10)
+    B.schedule = (2, 256, 4)
+    rc2, x2, it2, c2, st2 = B.solve(S.rhs, tol=1e-10)
+    assert rc1 == rc2 == lib.OK
+    assert np.all(np.abs(it1.astype(int) - it2.astype(int)) <= 2)
+    assert np.allclose(x1, x2, rtol=1e-7, atol=1e-12)
+    B.schedule = (0,)
+    B.solve(S.rhs, tol=1e-10)
+    assert B.schedule[0] in (1, 2)  # autotuned
