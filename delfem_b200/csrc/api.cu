@@ -434,8 +434,14 @@ int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int whe
 }
 
 int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
-  if (!M || mode < 0 || mode > 3) return DFM_ERR_INVALID;
-  if (mode == 3) return ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm);
+  if (!M || mode < 0 || mode > 4) return DFM_ERR_INVALID;
+  if (mode >= 3) {
+    const int rc = ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm);
+    if (rc) return rc;
+    if (mode == 4 && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) return DFM_ERR_UNSUPPORTED;
+    M->plan_f.nb = M->plan_b.nb = mode == 4;
+    return DFM_OK;
+  }
   M->sweep = mode;
   M->plan_gen++;
   return DFM_OK;
@@ -450,7 +456,7 @@ int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) 
 
 int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {
   if (!M || !mode) return DFM_ERR_INVALID;
-  *mode = M->sweep;
+  *mode = (M->sweep == 3 && M->plan_f.nb) ? 4 : M->sweep;
   return DFM_OK;
 }
 

@@ -798,6 +798,7 @@ int ilu_prepare(dfm_ilu M, bool f32) {
         P32.lpr = P64.lpr;
         M->plan_gen++;  // captured graphs hold the old plan's buffers
       }
+      P32.nb = P64.nb && P32.nb_ok;
       if ((rc = sweep_plan_refresh(M, &P32))) return rc;
     }
   }
@@ -866,14 +867,19 @@ int ilu_autotune(dfm_ilu M) {
       std::swap(M->plan_b, pb);
       float ms = 1e30f;
       int rc = DFM_OK, best_lpr = 1;
-      for (int lpr : {1, 2, 4, 8}) {  // consumer lanes per row
-        M->plan_f.lpr = M->plan_b.lpr = lpr;
-        float t = 1e30f;
-        rc = time_mode(3, &t);
-        if (rc) break;
-        if (t < ms) { ms = t; best_lpr = lpr; }
-      }
+      bool best_nb = false;
+      for (int nbv = 0; nbv < 2 && !rc; nbv++)  // level-barrier and barrier-free kernels
+        for (int lpr : {1, 2, 4, 8}) {          // consumer lanes per row
+          if (nbv && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) break;
+          M->plan_f.lpr = M->plan_b.lpr = lpr;
+          M->plan_f.nb = M->plan_b.nb = nbv != 0;
+          float t = 1e30f;
+          rc = time_mode(3, &t);
+          if (rc) break;
+          if (t < ms) { ms = t; best_lpr = lpr; best_nb = nbv != 0; }
+        }
       M->plan_f.lpr = M->plan_b.lpr = best_lpr;
+      M->plan_f.nb = M->plan_b.nb = best_nb;
       std::swap(M->plan_f, pf);  // candidate back in pf/pb, M empty
       std::swap(M->plan_b, pb);
       if (rc == DFM_OK && ms < best) {

@@ -246,6 +246,233 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
   }
 }
 
+// ------------------------------------------------ barrier-free variant
+// The same plan, without the per-level CTA barrier: the CTA's rows (in chunk,
+// i.e. level, order) are dealt round-robin to the lane groups, and each row
+// waits only for its own operands - a local one until its shared-memory slot
+// (initialised to the sentinel) holds a value, a remote one in global memory as
+// before.  Rows of consecutive levels therefore overlap.  A stage is released
+// when its chunk's last row completes (a shared-memory counter): the thread
+// that completes it records which chunk the stage will hold next and issues
+// that chunk's bulk copy.  A group reading a chunk first waits until the stage
+// is assigned to that chunk, then for the copy's mbarrier phase.  Every wait is
+// bounded; after an expired wait the CTA stops and drains its copies.
+DFM_DEVINL double ld_volatile_s(const double* p) { return *reinterpret_cast<const volatile double*>(p); }
+DFM_DEVINL float ld_volatile_s(const float* p) { return *reinterpret_cast<const volatile float*>(p); }
+DFM_DEVINL void st_volatile_s(double* p, double v) { *reinterpret_cast<volatile double*>(p) = v; }
+DFM_DEVINL void st_volatile_s(float* p, float v) { *reinterpret_cast<volatile float*>(p) = v; }
+DFM_DEVINL void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+template <typename TX>
+DFM_DEVINL TX poll_local(const TX* p, volatile int* alive, DevStatus* st, uint64_t wait_ns) {
+  TX v = ld_volatile_s(p);
+  if (!Sent<TX>::is(v)) return v;
+  SpinGuard g(wait_ns);
+  for (;;) {
+    v = ld_volatile_s(p);
+    if (!Sent<TX>::is(v)) return v;
+    if (!*alive) return v;
+    if (g.expired()) {
+      raise_error(st, DFM_WAIT_TIMEOUT, 13);
+      *alive = 0;
+      return v;
+    }
+  }
+}
+
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
+__global__ void __launch_bounds__(kSweepThreads)
+k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
+                  const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
+                  int nstage, unsigned x_bytes, unsigned max_chunks, const TX* __restrict__ in, TX* out,
+                  const TX* __restrict__ rdot, double* part, KrylovScalars* sc, const double* rr_part,
+                  int rr_nparts, DevStatus* st, uint64_t wait_ns) {
+  constexpr int BB = B * B;
+  extern __shared__ __align__(128) char smem[];
+  __shared__ int s_alive;
+  __shared__ int s_issued[kMaxStages];      // chunk (CTA-local index) a stage holds or is loading
+  __shared__ unsigned s_done[kMaxStages];   // rows of that chunk completed
+  if (sc) {
+    if (block_flag(&sc->done)) return;
+    if (FWD && rr_part) {
+      const double rr = reduce_partials(rr_part, rr_nparts);
+      if (rr * sc->inv0 < sc->tol2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          sc->conv = sqrt(rr * sc->inv0);
+          sc->conv_it = sc->it;
+          sc->done = sc->conv_code;
+        }
+        return;
+      }
+    }
+  }
+  const unsigned a0 = range[blockIdx.x], a1 = range[blockIdx.x + 1];
+  const unsigned q0 = cta_chunk[blockIdx.x], q1 = cta_chunk[blockIdx.x + 1];
+  const unsigned K = q1 - q0, len = a1 - a0;
+  TX* X = reinterpret_cast<TX*>(smem);
+  char* stages = smem + x_bytes;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
+  unsigned* rowpre = reinterpret_cast<unsigned*>(bar + kMaxStages);  // K + 1 prefix row counts
+  volatile int* alive = &s_alive;
+
+  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = Sent<TX>::value();
+  if (threadIdx.x == 0) {  // prefix of rows per chunk (K is at most max_chunks)
+    unsigned acc = 0;
+    for (unsigned k = 0; k < K && k < max_chunks; k++) {
+      rowpre[k] = acc;
+      acc += chunks[q0 + k].nrows;
+    }
+    rowpre[K < max_chunks ? K : max_chunks] = acc;
+    s_alive = K <= max_chunks ? 1 : 0;
+    if (K > max_chunks) raise_error(st, DFM_ERR_INVALID, 14);
+    for (int s = 0; s < nstage; s++) {
+      mbar_init(&bar[s], 1);
+      s_issued[s] = -1;
+      s_done[s] = 0;
+    }
+    fence_mbar_init();
+    if (s_alive)
+      for (unsigned k = 0; k < K && k < (unsigned)nstage; k++) {
+        const ChunkDesc cd = chunks[q0 + k];
+        s_issued[k] = (int)k;
+        mbar_arrive_tx(&bar[k], cd.bytes);
+        bulk_g2s(stages + (size_t)k * stage_bytes, blob + cd.off, cd.bytes, &bar[k]);
+      }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x % LPR;
+  const unsigned g = threadIdx.x / LPR, ng = kSweepThreads / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  const unsigned R = s_alive ? rowpre[K] : 0u;
+  unsigned k = 0;
+  for (unsigned t = g; t < R; t += ng) {
+    while (rowpre[k + 1] <= t) k++;  // group-uniform
+    const int s = (int)(k % (unsigned)nstage);
+    // the stage must hold chunk k, and its copy must have landed
+    bool ok = true;
+    if (*reinterpret_cast<volatile int*>(&s_issued[s]) != (int)k) {
+      SpinGuard gd(wait_ns);
+      while (*reinterpret_cast<volatile int*>(&s_issued[s]) != (int)k) {
+        if (!*alive) { ok = false; break; }
+        if (gd.expired()) {
+          raise_error(st, DFM_WAIT_TIMEOUT, 15);
+          *alive = 0;
+          ok = false;
+          break;
+        }
+      }
+    }
+    if (ok && !mbar_try_wait(&bar[s], (k / (unsigned)nstage) & 1u)) {
+      SpinGuard gd(wait_ns);
+      while (!mbar_try_wait(&bar[s], (k / (unsigned)nstage) & 1u)) {
+        if (!*alive) { ok = false; break; }
+        if (gd.expired()) {
+          raise_error(st, DFM_WAIT_TIMEOUT, 16);
+          *alive = 0;
+          ok = false;
+          break;
+        }
+      }
+    }
+    ok = __all_sync(gmask, ok) != 0;  // group-uniform decision (only the group's lanes vote)
+    if (!ok) break;
+    const char* sb = stages + (size_t)s * stage_bytes;
+    const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+    const unsigned r = t - rowpre[k];
+    const uint4 rd = reinterpret_cast<const uint4*>(sb + 32)[r];
+    const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+    const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+    TX vin[B];
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < B; c++) vin[c] = in[((size_t)a0 + rd.x) * B + c];
+    double acc[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) acc[c] = 0.0;
+    for (unsigned kk = rd.y + lane; kk < rd.z; kk += LPR) {
+      const unsigned xo = xoff[kk];
+      TX xv[B];
+      if (xo & 0x80000000u) {
+        const unsigned col = xo & 0x7fffffffu;
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = ld_relaxed(out + (size_t)col * B + c);
+#pragma unroll
+        for (int c = 0; c < B; c++)
+          if (Sent<TX>::is(xv[c])) xv[c] = poll_remote(out + (size_t)col * B + c, st, wait_ns, FWD ? 11 : 12);
+      } else {
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = poll_local(X + xo + c, alive, st, wait_ns);
+      }
+      const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+      for (int rr = 0; rr < B; rr++)
+#pragma unroll
+        for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)xv[c];
+    }
+    if (LPR > 1) {
+#pragma unroll
+      for (int rr = 0; rr < B; rr++)
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
+    }
+    if (lane == 0) {
+      double tt[B];
+#pragma unroll
+      for (int rr = 0; rr < B; rr++) tt[rr] = (double)vin[rr] - acc[rr];
+      TX o[B];
+      if (FWD) {
+        const double* d = reinterpret_cast<const double*>(sb + hdr->dinv) + (size_t)r * BB;
+#pragma unroll
+        for (int rr = 0; rr < B; rr++) {
+          double v = 0.0;
+#pragma unroll
+          for (int c = 0; c < B; c++) v += d[rr * B + c] * tt[c];
+          o[rr] = (TX)v;
+        }
+      } else {
+#pragma unroll
+        for (int rr = 0; rr < B; rr++) o[rr] = (TX)tt[rr];
+      }
+#pragma unroll
+      for (int rr = 0; rr < B; rr++) {
+        st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+        st_volatile_s(X + rd.x * B + rr, o[rr]);
+      }
+      // release the stage after the chunk's last row (its reads are all done:
+      // every lane of this group passed the shuffles above)
+      __threadfence_block();
+      const unsigned old = atomicAdd(&s_done[s], 1u);
+      if (old + 1 == hdr->nrows) {
+        __threadfence_block();
+        s_done[s] = 0;
+        const unsigned nb = hdr->next_bytes;
+        if (nb && *alive) {
+          const unsigned long long noff = hdr->next_off;
+          const unsigned k2 = k + (unsigned)nstage;
+          fence_proxy_async_smem();
+          *reinterpret_cast<volatile int*>(&s_issued[s]) = (int)k2;
+          mbar_arrive_tx(&bar[s], nb);
+          bulk_g2s(stages + (size_t)s * stage_bytes, blob + noff, nb, &bar[s]);
+        }
+      }
+    }
+    __syncwarp(gmask);
+  }
+  __syncthreads();
+  if (DOT) {
+    double dacc = 0.0;
+    if (s_alive)
+      for (unsigned e = threadIdx.x; e < len * B; e += blockDim.x) dacc += (double)rdot[(size_t)a0 * B + e] * (double)X[e];
+    block_partial<kSweepThreads>(dacc, part);
+  }
+  // every stage's last issued copy must have landed before the CTA exits
+  if (threadIdx.x == 0)
+    for (int s2 = 0; s2 < nstage; s2++) {
+      const int kl = s_issued[s2];
+      if (kl >= 0) (void)wait_stage(&bar[s2], ((unsigned)kl / (unsigned)nstage) & 1u, st, wait_ns);
+    }
+}
+
 // Refreshes the blob's values from the factor after a numeric factorisation:
 // one CTA per chunk copies its blocks (and D^-1 rows for the forward sweep).
 template <typename TV>
@@ -408,6 +635,8 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   P->vec_bytes = vec_bytes;
   P->nstage = ns;
   P->smem = x_bytes + (size_t)ns * stage_bytes + bar_bytes;
+  for (int c = 0; c < G; c++) P->max_cta_chunks = std::max(P->max_cta_chunks, cta_chunk[c + 1] - cta_chunk[c]);
+  P->nb_ok = P->smem + ((size_t)P->max_cta_chunks + 1) * 4 + 16 + 1024 <= (size_t)227 * 1024;
   P->lpr = (b == 3) ? 4 : 1;
   cudaStream_t s = M->ctx->stream;
   DFM_CUDA_TRY(cudaMalloc(&P->d_chunks, sizeof(ChunkDesc) * std::max<size_t>(chunks.size(), 1)));
@@ -456,6 +685,18 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (P->nb) {  // barrier-free variant: the same plan plus the per-chunk row prefix
+    if (!P->nb_ok) return cudaErrorInvalidValue;
+    const size_t smem = P->smem + (((size_t)P->max_cta_chunks + 1) * 4 + 15) / 16 * 16;
+    cfg.dynamicSmemBytes = smem;
+    auto fn = part ? k_sweep_ranges_nb<B, LPR, TV, TX, FWD, true> : k_sweep_ranges_nb<B, LPR, TV, TX, FWD, false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
+                              (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
+                              P->x_bytes, P->max_cta_chunks, in, out, rdot, part, sc, rr_part, rr_n, c->d_status,
+                              (uint64_t)c->wait_ns);
+  }
   if (part) {
     auto fn = k_sweep_ranges<B, LPR, TV, TX, FWD, true>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);

@@ -64,6 +64,9 @@ struct SweepPlan {
   bool fwd = true;
   int G = 0;               // CTAs (contiguous row ranges)
   int lpr = 1;             // consumer lanes per row
+  bool nb = false;         // barrier-free kernel variant (rows wait on their own operands)
+  bool nb_ok = false;      // its extra shared memory (row prefix per chunk) fits
+  unsigned max_cta_chunks = 0;
   int nstage = 0;
   int val_bytes = 8;       // 8 = FP64 factor blocks, 4 = FP32
   int vec_bytes = 8;       // 8 = FP64 vectors, 4 = FP32

@@ -186,8 +186,10 @@ DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
 DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
 /* Sweep schedule: 0 = autotuned, 1 = sync-free across the GPU, 2 = one CTA with
  * level barriers, 3 = contiguous row ranges per CTA (shared-memory slice, TMA-
- * streamed level data; the CTA count is the max_blocks of
- * dfm_ilu_set_sweep_tuning, default one per SM).  Real matrices only for 3. */
+ * streamed level data, a CTA barrier per level; the CTA count is the max_blocks
+ * of dfm_ilu_set_sweep_tuning, default one per SM), 4 = the row ranges of 3
+ * without level barriers (each row waits on its own operands).  Real matrices
+ * only for 3 and 4. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all

@@ -69,11 +69,11 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
-    if sweep == 3 and S.cplx:
+    if sweep >= 3 and S.cplx:
         pytest.skip("range-partitioned sweep is real-only")
     A = make(ctx, S)
     M = lib.ILU(A)
@@ -90,7 +90,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -114,15 +114,17 @@ def test_pcg_matches_oracle(ctx, name, sweep):
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
-def test_range_sweep_cta_counts(ctx, name, ctas):
-    """Mode 3 with every CTA count: same result as the oracle's sweeps."""
+@pytest.mark.parametrize("mode", [3, 4])
+def test_range_sweep_cta_counts(ctx, name, ctas, mode):
+    """Modes 3 and 4 with every CTA count: same result as the oracle's sweeps."""
     from delfem_b200 import lib
     S = SYSTEMS[name]()
     A = make(ctx, S)
     M = lib.ILU(A)
     M.factor()
     lib.check(lib.lib().dfm_ilu_set_sweep_tuning(M.h, ctas, 64))
-    M.sweep = 3
+    M.sweep = mode
+    assert M.sweep == mode
     _, fd, fo = S.ilu0()
     r = np.random.default_rng(5).standard_normal(S.N * S.xw)
     ref = S.precond(fd, fo, r)
