@@ -300,6 +300,114 @@ def run_profile():
     log(f"[profile-run] sweep mode {M.sweep}, lanes {A.lanes}")
 
 
+# ------------------------------------------------------- c1 and c5 sections
+def build_c1(ctx, torch, dev):
+    from delfem_b200 import lib, meshes
+    m = meshes.unit_square_tri(256)
+    G = lib.Mesh(ctx, m.coord, m.elem)
+    rp, ci = G.pattern()
+    A = lib.Matrix(ctx, rp, ci, 1)
+    b = torch.empty(m.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+    G.assemble_poisson(A, 1.0, 1.0, b)
+    fl = np.zeros(m.nnode, np.int32)
+    fl[np.unique(m.bnd.ravel())] = 1
+    lib.apply_dirichlet(A, torch.from_numpy(fl).cuda(dev), b)
+    return A, b
+
+
+def run_c1(ctx, torch, dev, timed, with_reference):
+    """c1: 2-D Poisson 256^2 to rel.res 1e-10, plain FP64 and mixed, against the
+    reference's own CPU solve of the same (bit-identical) system."""
+    from delfem_b200 import lib
+    A, b = build_c1(ctx, torch, dev)
+    M = lib.ILU(A)
+    M.factor()
+    x = torch.zeros_like(b)
+    r = b.clone()
+
+    def plain():
+        r.copy_(b)
+        return lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=20000)
+
+    def mixed():
+        r.copy_(b)
+        return lib.solve_pcg_mixed(A, M, r, x, tol=1e-10, maxit=20000)
+
+    plain()
+    t_plain = timed(plain, 5)
+    rc, it, conv = plain()
+    x64 = x.cpu().numpy()
+    mixed()
+    t_mixed = timed(mixed, 5)
+    rc_m, it_m, conv_m = mixed()
+    xm = x.cpu().numpy()
+    out = {"workload": "c1 2-D Poisson 256x256 P1 (N = 66,049), ILU(0) + PCG to rel.res 1e-10",
+           "plain_s": t_plain, "iterations": it + 1, "mixed_s": t_mixed, "mixed_iterations": it_m + 1,
+           "mixed_speedup_vs_plain": t_plain / t_mixed,
+           "mixed_rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
+           "sweep_mode": M.sweep}
+    if with_reference:
+        try:
+            from oracle import refshim as R
+            d, o = A.get_values()
+            rc_r, x_ref, it_r, conv_r, t_ilu, t_sol = R.mat_solve(A.N, 1, A.rowptr, A.colind, d, o,
+                                                                  b.cpu().numpy(), R.PCG, 1e-10, 20000)
+            out.update({"reference_cpu_s": t_ilu + t_sol, "reference_iterations": it_r + 1,
+                        "rel_err_vs_reference": float(np.linalg.norm(x64 - x_ref) / np.linalg.norm(x_ref)),
+                        "speedup_vs_reference_cpu": (t_ilu + t_sol) / t_plain})
+        except Exception as e:  # the reference build may be absent
+            out["reference_cpu_s"] = f"unavailable: {e}"
+    for h in (M, A):
+        h.close()
+    return out
+
+
+def run_c5(ctx, torch, dev, timed):
+    """c5: Helmholtz k = 20 on the unit disk (~200k nodes), complex ILU(0)-COCG to
+    rel.res 1e-8 in complex128 and with complex64 values inside complex128
+    residual replacement."""
+    from delfem_b200 import lib, meshes
+    m = meshes.unit_disk_tri(258)
+    G = lib.Mesh(ctx, m.coord, m.elem, m.bnd)
+    rp, ci = G.pattern()
+    A = lib.Matrix(ctx, rp, ci, 1, lib.COMPLEX)
+    b = torch.empty(2 * m.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+    load = torch.from_numpy(meshes.gaussian_source_load(m).ravel()).cuda(dev)
+    G.assemble_helmholtz(A, 2 * 3.1416 / 20, b, load=load)
+    M = lib.ILU(A)
+    M.factor()
+    x = torch.zeros_like(b)
+    r = b.clone()
+
+    def plain():
+        r.copy_(b)
+        return lib.solve_pcocg(A, M, r, x, tol=1e-8, maxit=20000)
+
+    def mixed():
+        r.copy_(b)
+        return lib.solve_pcocg_mixed(A, M, r, x, tol=1e-8, maxit=20000)
+
+    plain()
+    t_plain = timed(plain, 2)
+    rc, it, conv = plain()
+    x128 = x.clone()
+    mixed()
+    t_mixed = timed(mixed, 2)
+    rc_m, it_m, conv_m = mixed()
+    y = torch.empty_like(b)
+    A.spmv(1.0, x, 0.0, y)
+    torch.cuda.synchronize()
+    res_m = float(torch.linalg.norm(b - y) / torch.linalg.norm(b))
+    out = {"workload": f"c5 Helmholtz k=20 unit disk, {m.nnode} nodes, complex ILU(0)-COCG to rel.res 1e-8",
+           "complex128_s": t_plain, "iterations": it, "status": rc,
+           "complex64_inner_s": t_mixed, "complex64_iterations": it_m, "complex64_status": rc_m,
+           "complex64_speedup": t_plain / t_mixed, "complex64_true_rel_residual": res_m,
+           "complex64_rel_err_vs_complex128": float(torch.linalg.norm(x - x128) / torch.linalg.norm(x128))}
+    for h in (M, A, G):
+        h.close()
+    return out
+
+
 # -------------------------------------------------------------------- our arm
 def run_ours(args, rank, world):
     import torch
@@ -438,6 +546,11 @@ def run_ours(args, rank, world):
     batched = {}
     if not args.skip_batched and world == 1:
         batched = run_c3(ctx, torch, dev, stream, timed, args.steps)
+    c1 = {}
+    c5 = {}
+    if not args.skip_extra and world == 1:
+        c1 = run_c1(ctx, torch, dev, timed, rank == 0 and not args.no_cpu_baseline)
+        c5 = run_c5(ctx, torch, dev, timed)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -471,6 +584,8 @@ def run_ours(args, rank, world):
             "kernels": kernels,
             "mixed": mixed,
             "batched": batched,
+            "c1": c1,
+            "c5": c5,
             "e2e": {"value": 1.0 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": t_e2e * 1e3},
             "cpu_baseline": cpu,
@@ -489,6 +604,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-mixed", action="store_true")
+    ap.add_argument("--skip-extra", action="store_true", help="skip the c1 and c5 sections")
     ap.add_argument("--profile-run", action="store_true")
     args = ap.parse_args()
     if args.profile_run:

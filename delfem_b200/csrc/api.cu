@@ -242,10 +242,11 @@ int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* ro
   A->h_rowptr.assign(rowptr, rowptr + N + 1);
   A->h_colind.assign(colind, colind + ncrs);
   for (unsigned i = 0; i < N; i++) A->max_row = std::max(A->max_row, rowptr[i + 1] - rowptr[i]);
-  int rc = dalloc(&A->d_rowptr, N + 1);
-  if (!rc) rc = dalloc(&A->d_colind, ncrs);
-  if (!rc) rc = dalloc(&A->d_diag, (size_t)N * A->vw());
-  if (!rc) rc = dalloc(&A->d_off, (size_t)ncrs * A->vw());
+  // kArrayPad spare elements: the TMA-staged SpMV rounds its bulk copies out to 16 bytes
+  int rc = dalloc(&A->d_rowptr, N + 1 + kArrayPad);
+  if (!rc) rc = dalloc(&A->d_colind, ncrs + kArrayPad);
+  if (!rc) rc = dalloc(&A->d_diag, (size_t)N * A->vw() + kArrayPad);
+  if (!rc) rc = dalloc(&A->d_off, (size_t)ncrs * A->vw() + kArrayPad);
   if (!rc) rc = copy_in(A->d_rowptr, rowptr, sizeof(unsigned) * (N + 1), DFM_HOST, c->stream);
   if (!rc) rc = copy_in(A->d_colind, colind, sizeof(unsigned) * ncrs, DFM_HOST, c->stream);
   if (!rc) rc = dfm_mat_set_zero(A);
@@ -263,6 +264,7 @@ int dfm_mat_destroy(dfm_mat A) {
   cudaFree(A->d_off);
   cudaFree(A->d_diag32);
   cudaFree(A->d_off32);
+  spmv_free_tiles(A);
   delete A;
   return DFM_OK;
 }
@@ -310,6 +312,19 @@ int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes) {
   if (!A) return DFM_ERR_INVALID;
   if (lanes != 0 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return DFM_ERR_INVALID;
   A->lanes = lanes;
+  return DFM_OK;
+}
+
+int dfm_mat_set_spmv_kernel(dfm_mat A, int kernel) {
+  if (!A || kernel < 0 || kernel > 2) return DFM_ERR_INVALID;
+  if (kernel >= 1 && A->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
+  A->spmv_kind = kernel;
+  return DFM_OK;
+}
+
+int dfm_mat_get_spmv_kernel(dfm_mat A, int* kernel) {
+  if (!A || !kernel) return DFM_ERR_INVALID;
+  *kernel = A->spmv_kind;
   return DFM_OK;
 }
 
@@ -434,12 +449,13 @@ int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int whe
 }
 
 int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
-  if (!M || mode < 0 || mode > 4) return DFM_ERR_INVALID;
+  if (!M || mode < 0 || mode > 6) return DFM_ERR_INVALID;
   if (mode >= 3) {
-    const int rc = ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm);
+    const bool merge = mode >= 5, nb = mode == 4 || mode == 6;
+    const int rc = ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm, merge);
     if (rc) return rc;
-    if (mode == 4 && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) return DFM_ERR_UNSUPPORTED;
-    M->plan_f.nb = M->plan_b.nb = mode == 4;
+    if (nb && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) return DFM_ERR_UNSUPPORTED;
+    M->plan_f.nb = M->plan_b.nb = nb;
     return DFM_OK;
   }
   M->sweep = mode;
@@ -456,7 +472,8 @@ int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) 
 
 int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {
   if (!M || !mode) return DFM_ERR_INVALID;
-  *mode = (M->sweep == 3 && M->plan_f.nb) ? 4 : M->sweep;
+  *mode = M->sweep;
+  if (M->sweep == 3) *mode = (M->plan_f.merged ? 5 : 3) + (M->plan_f.nb ? 1 : 0);
   return DFM_OK;
 }
 

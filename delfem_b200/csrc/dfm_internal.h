@@ -40,6 +40,17 @@ struct KrylovScalars {
 
 // Upper bound of blocks of the grid-stride kernels (partials arrays length).
 constexpr int kMaxBlocks = 148 * 16;
+// Spare elements at the end of every matrix array (bulk copies round to 16 B).
+constexpr size_t kArrayPad = 16;
+
+// Row tiles of the TMA-staged SpMV (spmv.cu) for one value width.
+struct SpmvTiles {
+  bool valid = false;
+  unsigned ntiles = 0, max_rows = 0, max_blocks = 0;
+  unsigned* d_tiles = nullptr;  // ntiles + 1 row bounds
+  unsigned stage_bytes = 0, vals_bytes = 0, col_bytes = 0, diag_bytes = 0, rp_bytes = 0;
+  int nstage = 0;
+};
 
 }  // namespace dfm
 
@@ -70,6 +81,8 @@ struct dfm_mat_s {
   std::vector<unsigned> h_rowptr, h_colind;
   unsigned max_row = 0;     // most off-diagonal blocks in one row
   int lanes = 0;            // SpMV lanes per block row (0 = not tuned yet)
+  int spmv_kind = 0;        // 0 lane per block, 1 TMA-staged tiles, 2 element-wise (autotuned)
+  dfm::SpmvTiles tiles[2];  // [0] FP64 values, [1] FP32 copies
   size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }   // doubles per block
   size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }               // doubles per vector block
 };
@@ -120,10 +133,12 @@ struct SpmvOpts {
   bool yy = false;
   const double* y0 = nullptr;
   bool f32 = false;
+  int kind = -1;  // -1: the matrix's tuned kernel; 0 lane per block; 1 TMA-staged tiles; 2 element-wise
 };
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
                 int nblocks_hint, KrylovScalars* sc, int lanes, const SpmvOpts& o = SpmvOpts());
 int mat_make_f32(dfm_mat A);
+void spmv_free_tiles(dfm_mat A);
 int to_f32(dfm_ctx c, const double* in, float* out, size_t n);
 int spmv_autotune(dfm_mat A);
 int spmv_grid(dfm_mat A);
@@ -145,11 +160,12 @@ int sweep_grid(dfm_ilu M, int sweep);
 int ilu_wait_selftest(dfm_ctx ctx, unsigned long long limit_ns);
 int set_poll_sleep(unsigned ns);
 // sweep.cu
-int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P,
-                     bool direct_remote = true);
+// merge: steps are pairs of levels (the second level's operands on the
+// first are substituted by products with the factor; see sweep.cu)
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge = false);
 void sweep_plan_free(SweepPlan* P);
 int sweep_plan_refresh(dfm_ilu M, SweepPlan* P);
-int ilu_set_ranges(dfm_ilu M, int G);
+int ilu_set_ranges(dfm_ilu M, int G, bool merge = false);
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
                         KrylovScalars* sc, const double* rr_part, int rr_n, bool f32 = false);
 // krylov.cu

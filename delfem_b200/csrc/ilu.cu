@@ -793,8 +793,8 @@ int ilu_prepare(dfm_ilu M, bool f32) {
     for (int f = 0; f < 2; f++) {
       SweepPlan& P64 = f ? M->plan_b : M->plan_f;
       SweepPlan& P32 = f ? M->plan32_b : M->plan32_f;
-      if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr) {
-        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32))) return rc;
+      if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr || P32.merged != P64.merged) {
+        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32, P64.merged))) return rc;
         P32.lpr = P64.lpr;
         M->plan_gen++;  // captured graphs hold the old plan's buffers
       }
@@ -845,32 +845,28 @@ int ilu_autotune(dfm_ilu M) {
     if (rc) return rc;
     if (ms < best) { best = ms; best_mode = mode; }
   }
-  // range-partitioned schedule: every CTA count whose slice fits in shared memory
+  // range-partitioned schedule: every CTA count whose slice fits in shared memory,
+  // then, at the best count, merged level pairs and the barrier-free kernel
   if (M->vt == DFM_REAL) {
     sweep_plan_free(&M->plan_f);
     sweep_plan_free(&M->plan_b);
     SweepPlan best_f, best_b;  // owned here until the end
     const int nsm = M->ctx->nsm;
     const int cand[] = {nsm, nsm / 2, nsm / 4, 16, 8, 4, 2, 1};
-    int last = -1;
-    for (int G : cand) {
-      if (G < 1 || G == last) continue;
-      last = G;
-      SweepPlan pf, pb;
-      if (sweep_plan_build(M, true, G, 8, 8, &pf) != DFM_OK || sweep_plan_build(M, false, G, 8, 8, &pb) != DFM_OK) {
-        sweep_plan_free(&pf);
-        sweep_plan_free(&pb);
-        cudaGetLastError();
-        continue;  // slice does not fit in shared memory at this CTA count
-      }
+    int last = -1, best_G = 0;
+    float best3 = 1e30f;
+    // times the candidate plans (pf, pb) over lanes per row and the kernel
+    // variants in `nbs`; keeps them in best_f/best_b if they beat `best`
+    auto try_plans = [&](SweepPlan& pf, SweepPlan& pb, std::initializer_list<int> nbs, float* tbest) -> int {
       std::swap(M->plan_f, pf);  // M holds the candidate
       std::swap(M->plan_b, pb);
       float ms = 1e30f;
       int rc = DFM_OK, best_lpr = 1;
       bool best_nb = false;
-      for (int nbv = 0; nbv < 2 && !rc; nbv++)  // level-barrier and barrier-free kernels
-        for (int lpr : {1, 2, 4, 8}) {          // consumer lanes per row
-          if (nbv && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) break;
+      for (int nbv : nbs) {
+        if (rc) break;
+        if (nbv && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) continue;
+        for (int lpr : {1, 2, 4, 8}) {  // consumer lanes per row
           M->plan_f.lpr = M->plan_b.lpr = lpr;
           M->plan_f.nb = M->plan_b.nb = nbv != 0;
           float t = 1e30f;
@@ -878,10 +874,12 @@ int ilu_autotune(dfm_ilu M) {
           if (rc) break;
           if (t < ms) { ms = t; best_lpr = lpr; best_nb = nbv != 0; }
         }
+      }
       M->plan_f.lpr = M->plan_b.lpr = best_lpr;
       M->plan_f.nb = M->plan_b.nb = best_nb;
       std::swap(M->plan_f, pf);  // candidate back in pf/pb, M empty
       std::swap(M->plan_b, pb);
+      if (tbest) *tbest = ms;
       if (rc == DFM_OK && ms < best) {
         best = ms;
         best_mode = 3;
@@ -892,6 +890,39 @@ int ilu_autotune(dfm_ilu M) {
       } else {
         sweep_plan_free(&pf);
         sweep_plan_free(&pb);
+      }
+      return rc;
+    };
+    for (int G : cand) {
+      if (G < 1 || G == last) continue;
+      last = G;
+      SweepPlan pf, pb;
+      if (sweep_plan_build(M, true, G, 8, 8, &pf) != DFM_OK || sweep_plan_build(M, false, G, 8, 8, &pb) != DFM_OK) {
+        sweep_plan_free(&pf);
+        sweep_plan_free(&pb);
+        cudaGetLastError();
+        continue;  // slice does not fit in shared memory at this CTA count
+      }
+      float t = 1e30f;
+      const int rc = try_plans(pf, pb, {0}, &t);
+      if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
+        sweep_plan_free(&best_f);
+        sweep_plan_free(&best_b);
+        return rc;
+      }
+      if (rc == DFM_OK && t < best3) { best3 = t; best_G = G; }
+    }
+    if (best_G > 0) {
+      for (int mg = 0; mg < 2; mg++) {  // barrier-free kernel unmerged, then merged pairs with both kernels
+        SweepPlan pf, pb;
+        if (sweep_plan_build(M, true, best_G, 8, 8, &pf, mg != 0) != DFM_OK ||
+            sweep_plan_build(M, false, best_G, 8, 8, &pb, mg != 0) != DFM_OK) {
+          sweep_plan_free(&pf);
+          sweep_plan_free(&pb);
+          cudaGetLastError();
+          continue;
+        }
+        const int rc = mg ? try_plans(pf, pb, {0, 1}, nullptr) : try_plans(pf, pb, {1}, nullptr);
         if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
           sweep_plan_free(&best_f);
           sweep_plan_free(&best_b);
@@ -913,11 +944,11 @@ int ilu_autotune(dfm_ilu M) {
   return DFM_OK;
 }
 
-int ilu_set_ranges(dfm_ilu M, int G) {
+int ilu_set_ranges(dfm_ilu M, int G, bool merge) {
   if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
   SweepPlan pf, pb;
-  int rc = sweep_plan_build(M, true, G, 8, 8, &pf);
-  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb);
+  int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge);
+  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge);
   if (rc) {
     sweep_plan_free(&pf);
     sweep_plan_free(&pb);

@@ -605,12 +605,13 @@ static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
 // Capture kIterPerGraph iterations once per plan and launch configuration.
 static void ensure_graph(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   dfm_ctx c = A->ctx;
-  const bool same = P->key_sweep == M->sweep && P->key_lanes == A->lanes && P->key_gen == M->plan_gen &&
+  const int lanes_key = A->lanes * 2 + A->spmv_kind;
+  const bool same = P->key_sweep == M->sweep && P->key_lanes == lanes_key && P->key_gen == M->plan_gen &&
                     P->key_wait == c->wait_ns;
   if (!same) {
     plan_drop_graph(P);
     P->key_sweep = M->sweep;
-    P->key_lanes = A->lanes;
+    P->key_lanes = lanes_key;
     P->key_gen = M->plan_gen;
     P->key_wait = c->wait_ns;
   }

@@ -16,6 +16,8 @@
 
 namespace dfm {
 
+static unsigned al16_host(unsigned x) { return (x + 15u) & ~15u; }
+
 template <int B, int LPR, typename TV, typename TX, int NDOT>
 __global__ void __launch_bounds__(256)
 k_spmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
@@ -127,6 +129,423 @@ k_zspmv(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restr
   if (NDOT == 1) block_partial<256>(dim, part + kMaxBlocks);
 }
 
+// --------------------------------------------- element-wise coalesced SpMV
+// A group of LPR lanes per block row walks the row's off-diagonal values as
+// one contiguous run of doubles (lane e takes elements e, e+LPR, ...), so every
+// load instruction of the group reads consecutive addresses; the diagonal
+// block follows as the run's last b*b elements.  Element e belongs to block
+// e / b^2, row (e % b^2) / b and column (e % b^2) % b of the block; the column
+// index of its block and the matching x entry come through L1.
+template <int B, int LPR, typename TV, int NDOT>
+__global__ void __launch_bounds__(256)
+k_spmv_elem(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+            const TV* __restrict__ diag, const TV* __restrict__ off, double alpha, const double* __restrict__ x,
+            double beta, double* __restrict__ y, double* __restrict__ part, const int* done,
+            const double* __restrict__ w, double* __restrict__ part2, const double* __restrict__ y0) {
+  if (done && block_flag(done)) return;
+  constexpr unsigned BB = B * B;
+  const int lane = threadIdx.x % LPR;
+  const unsigned g0 = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+  const unsigned ng = gridDim.x * blockDim.x / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  double dacc = 0.0, dacc2 = 0.0;
+  for (unsigned i = g0; i < N; i += ng) {
+    const unsigned s0 = __ldg(rowptr + i), s1 = __ldg(rowptr + i + 1);
+    const unsigned nbo = s1 - s0, ne = (nbo + 1) * BB;
+    const TV* vo = off + (size_t)s0 * BB;
+    double acc[B];
+#pragma unroll
+    for (int r = 0; r < B; r++) acc[r] = 0.0;
+#pragma unroll 2
+    for (unsigned e = lane; e < ne; e += LPR) {
+      const unsigned blk = e / BB, q = e - blk * BB;
+      const unsigned rr = q / B, c = q - rr * B;
+      double v;
+      unsigned col;
+      if (blk < nbo) {
+        v = (double)__ldcs(vo + e);
+        col = __ldg(colind + s0 + blk);
+      } else {
+        v = (double)__ldg(diag + (size_t)i * BB + q);
+        col = i;
+      }
+      const double xv = __ldg(x + (size_t)col * B + c);
+#pragma unroll
+      for (int r = 0; r < B; r++)
+        if (rr == (unsigned)r) acc[r] += v * xv;
+    }
+#pragma unroll
+    for (int r = 0; r < B; r++)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+    if (lane == 0) {
+#pragma unroll
+      for (int r = 0; r < B; r++) {
+        double v = alpha * acc[r];
+        if (y0) v += y0[(size_t)i * B + r];
+        else if (beta != 0.0) v += beta * y[(size_t)i * B + r];
+        y[(size_t)i * B + r] = v;
+        if (NDOT == 1 || NDOT == 2) dacc += w[(size_t)i * B + r] * v;
+        if (NDOT == 2) dacc2 += v * v;
+        if (NDOT == 3) dacc += v * v;
+      }
+    }
+  }
+  if (NDOT >= 1) block_partial<256>(dacc, part);
+  if (NDOT == 2) block_partial<256>(dacc2, part2);
+}
+
+template <int B, int LPR, typename TV>
+static void launch_elem_t(dfm_mat A, const TV* diag, const TV* off, int grid, cudaStream_t s, double alpha,
+                          const double* x, double beta, double* y, double* part, const int* done,
+                          const SpmvOpts& o) {
+  const double* w = o.dot_w ? o.dot_w : x;
+  if (part && o.yy)
+    k_spmv_elem<B, LPR, TV, 3><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                    part, done, nullptr, nullptr, o.y0);
+  else if (part && o.dot_part2)
+    k_spmv_elem<B, LPR, TV, 2><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                    part, done, w, o.dot_part2, o.y0);
+  else if (part)
+    k_spmv_elem<B, LPR, TV, 1><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                    part, done, w, nullptr, o.y0);
+  else
+    k_spmv_elem<B, LPR, TV, 0><<<grid, 256, 0, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y,
+                                                    nullptr, done, nullptr, nullptr, o.y0);
+}
+
+template <int B>
+static void launch_elem(dfm_mat A, int lanes, int grid, cudaStream_t s, double alpha, const double* x, double beta,
+                        double* y, double* part, const int* done, const SpmvOpts& o) {
+#define DFM_ELEM_L(L)                                                                                        \
+  if (o.f32) launch_elem_t<B, L, float>(A, A->d_diag32, A->d_off32, grid, s, alpha, x, beta, y, part, done, o); \
+  else launch_elem_t<B, L, double>(A, A->d_diag, A->d_off, grid, s, alpha, x, beta, y, part, done, o);          \
+  return
+  switch (lanes) {
+    case 4: DFM_ELEM_L(4);
+    case 8: DFM_ELEM_L(8);
+    case 16: DFM_ELEM_L(16);
+    default: DFM_ELEM_L(32);
+  }
+#undef DFM_ELEM_L
+}
+
+// ------------------------------------------------------ TMA-staged SpMV
+// Rows are cut into tiles (at most kTileRows rows and kTileValBytes of
+// off-diagonal values).  A persistent CTA walks its tiles (t = blockIdx.x +
+// k*gridDim.x); for each, thread 0 issues four 1-D bulk copies (values,
+// column indices, diagonal blocks, row pointers; no multicast) into a stage
+// of a shared-memory ring several tiles ahead, completing on the stage's
+// mbarrier.  Lane groups then read a row's blocks from shared memory element
+// by element (consecutive lanes, consecutive doubles) and gather x through
+// L1/L2, so the value stream never occupies the load/store units.  A copy
+// starts at the 16-byte boundary below its first byte and is rounded up to 16
+// bytes (the arrays carry kArrayPad spare elements); the offsets of the first
+// element are kept per stage.
+constexpr unsigned kTileRows = 128;
+constexpr unsigned kTileValBytes = 24 * 1024;
+constexpr int kTmaThreads = 256;
+
+DFM_DEVINL unsigned sp_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+DFM_DEVINL void sp_mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sp_smem(bar)), "r"(count) : "memory");
+}
+DFM_DEVINL void sp_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+DFM_DEVINL void sp_arrive_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(sp_smem(bar)), "r"(bytes)
+               : "memory");
+}
+DFM_DEVINL bool sp_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(sp_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+DFM_DEVINL void sp_bulk(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   sp_smem(dst)),
+               "l"(src), "r"(bytes), "r"(sp_smem(bar))
+               : "memory");
+}
+DFM_DEVINL void sp_fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+struct TileHdr {
+  unsigned r0, r1, s0, dv, dc, dd, dr, pad;  // rows, first block, byte offsets of the first elements
+};
+
+template <typename TV>
+struct TmaArgs {
+  unsigned N;
+  const unsigned* rowptr;
+  const unsigned* colind;
+  const TV* diag;
+  const TV* off;
+  const unsigned* tiles;
+  unsigned ntiles, stage_bytes, vals_bytes, col_bytes, diag_bytes;
+  int nstage;
+  double alpha, beta;
+  const double* x;
+  double* y;
+  const double* y0;
+  const double* w;
+  double* part;
+  double* part2;
+  int npart;
+  const int* done;
+  DevStatus* st;
+  uint64_t wait_ns;
+};
+
+DFM_DEVINL const char* al16_down(const void* p, unsigned* delta) {
+  const uintptr_t a = (uintptr_t)p;
+  *delta = (unsigned)(a & 15u);
+  return reinterpret_cast<const char*>(a & ~(uintptr_t)15);
+}
+DFM_DEVINL unsigned al16_up(unsigned x) { return (x + 15u) & ~15u; }
+
+// thread 0: stage s <- tile t
+template <int B, typename TV>
+DFM_DEVINL void tma_issue(const TmaArgs<TV>& a, char* stage, uint64_t* bar, TileHdr* hdr, unsigned t) {
+  constexpr unsigned BB = B * B;
+  const unsigned r0 = a.tiles[t], r1 = a.tiles[t + 1];
+  const unsigned s0 = a.rowptr[r0], s1 = a.rowptr[r1];
+  TileHdr h;
+  h.r0 = r0;
+  h.r1 = r1;
+  h.s0 = s0;
+  const char* pv = al16_down(a.off + (size_t)s0 * BB, &h.dv);
+  const char* pc = al16_down(a.colind + s0, &h.dc);
+  const char* pd = al16_down(a.diag + (size_t)r0 * BB, &h.dd);
+  const char* pr = al16_down(a.rowptr + r0, &h.dr);
+  const unsigned nv = al16_up((s1 - s0) * BB * (unsigned)sizeof(TV) + h.dv);
+  const unsigned nc = al16_up((s1 - s0) * 4u + h.dc);
+  const unsigned nd = al16_up((r1 - r0) * BB * (unsigned)sizeof(TV) + h.dd);
+  const unsigned nr = al16_up((r1 - r0 + 1) * 4u + h.dr);
+  *hdr = h;
+  sp_fence_proxy();
+  sp_arrive_tx(bar, nv + nc + nd + nr);
+  if (nv) sp_bulk(stage, pv, nv, bar);
+  if (nc) sp_bulk(stage + a.vals_bytes, pc, nc, bar);
+  if (nd) sp_bulk(stage + a.vals_bytes + a.col_bytes, pd, nd, bar);
+  sp_bulk(stage + a.vals_bytes + a.col_bytes + a.diag_bytes, pr, nr, bar);  // nr >= 16
+}
+
+template <int B, int LPR, typename TV, int NDOT>
+__global__ void __launch_bounds__(kTmaThreads)
+k_spmv_tma(TmaArgs<TV> a) {
+  constexpr unsigned BB = B * B;
+  extern __shared__ __align__(128) char smem[];
+  __shared__ uint64_t bar[8];
+  __shared__ TileHdr hdr[8];
+  __shared__ int s_alive;
+  if (a.done && block_flag(a.done)) return;
+  const int ns = a.nstage;
+  const unsigned my_tiles = a.ntiles > blockIdx.x ? (a.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+  if (threadIdx.x == 0) {
+    s_alive = 1;
+    for (int s = 0; s < ns; s++) sp_mbar_init(&bar[s], 1);
+    sp_fence_init();
+    for (unsigned k = 0; k < my_tiles && k < (unsigned)ns; k++)
+      tma_issue<B, TV>(a, smem + (size_t)k * a.stage_bytes, &bar[k], &hdr[k], blockIdx.x + k * gridDim.x);
+  }
+  if (blockIdx.x == 0)  // partial slots past this grid belong to nobody: zero for the consumer's fixed count
+    for (int k = gridDim.x + threadIdx.x; k < a.npart; k += blockDim.x) {
+      if (NDOT >= 1) a.part[k] = 0.0;
+      if (NDOT == 2) a.part2[k] = 0.0;
+    }
+  __syncthreads();
+  const int lane = threadIdx.x % LPR;
+  const unsigned g = threadIdx.x / LPR, ng = kTmaThreads / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  double dacc = 0.0, dacc2 = 0.0;
+  unsigned consumed = 0;
+  for (unsigned k = 0; k < my_tiles; k++) {
+    const int s = (int)(k % (unsigned)ns);
+    char* stage = smem + (size_t)s * a.stage_bytes;
+    if (threadIdx.x == 0 && s_alive) {
+      const unsigned par = (k / (unsigned)ns) & 1u;
+      if (!sp_try_wait(&bar[s], par)) {
+        SpinGuard gd(a.wait_ns);
+        while (!sp_try_wait(&bar[s], par))
+          if (gd.expired()) {
+            raise_error(a.st, DFM_WAIT_TIMEOUT, 20);
+            s_alive = 0;
+            break;
+          }
+      }
+    }
+    __syncthreads();
+    if (!s_alive) break;
+    const TileHdr h = hdr[s];
+    const TV* vals = reinterpret_cast<const TV*>(stage + h.dv);
+    const unsigned* cols = reinterpret_cast<const unsigned*>(stage + a.vals_bytes + h.dc);
+    const TV* dg = reinterpret_cast<const TV*>(stage + a.vals_bytes + a.col_bytes + h.dd);
+    const unsigned* rp = reinterpret_cast<const unsigned*>(stage + a.vals_bytes + a.col_bytes + a.diag_bytes + h.dr);
+    for (unsigned i = h.r0 + g; i < h.r1; i += ng) {  // group-uniform
+      const unsigned li = i - h.r0;
+      const unsigned b0 = rp[li] - h.s0, b1 = rp[li + 1] - h.s0;
+      const unsigned ne = (b1 - b0 + 1) * BB;  // off-diagonal blocks, then the diagonal block
+      double acc[B];
+#pragma unroll
+      for (int r = 0; r < B; r++) acc[r] = 0.0;
+      for (unsigned e = lane; e < ne; e += LPR) {
+        const unsigned blk = e / BB, q = e - blk * BB;
+        const unsigned rr = q / B, c = q - rr * B;
+        double v;
+        unsigned col;
+        if (blk < b1 - b0) {
+          v = (double)vals[(size_t)(b0 + blk) * BB + q];
+          col = cols[b0 + blk];
+        } else {
+          v = (double)dg[(size_t)li * BB + q];
+          col = i;
+        }
+        const double xv = __ldg(a.x + (size_t)col * B + c);
+#pragma unroll
+        for (int r = 0; r < B; r++)
+          if (rr == (unsigned)r) acc[r] += v * xv;
+      }
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+      if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < B; r++) {
+          double v = a.alpha * acc[r];
+          if (a.y0) v += a.y0[(size_t)i * B + r];
+          else if (a.beta != 0.0) v += a.beta * a.y[(size_t)i * B + r];
+          a.y[(size_t)i * B + r] = v;
+          if (NDOT == 1 || NDOT == 2) dacc += a.w[(size_t)i * B + r] * v;
+          if (NDOT == 2) dacc2 += v * v;
+          if (NDOT == 3) dacc += v * v;
+        }
+      }
+    }
+    __syncthreads();  // stage s free
+    consumed = k + 1;
+    if (threadIdx.x == 0 && k + ns < my_tiles && s_alive)
+      tma_issue<B, TV>(a, stage, &bar[s], &hdr[s], blockIdx.x + (k + ns) * gridDim.x);
+  }
+  if (NDOT >= 1) block_partial<kTmaThreads>(dacc, a.part);
+  if (NDOT == 2) block_partial<kTmaThreads>(dacc2, a.part2);
+  // copies issued but not consumed (after an expired wait) must land before the CTA exits
+  if (threadIdx.x == 0 && !s_alive) {
+    const unsigned issued = std::min(my_tiles, consumed + (unsigned)ns);
+    for (unsigned j = consumed; j < issued; j++) {
+      const unsigned par = (j / (unsigned)ns) & 1u;
+      SpinGuard gd(a.wait_ns);
+      while (!sp_try_wait(&bar[j % (unsigned)ns], par))
+        if (gd.expired()) break;
+    }
+  }
+}
+
+// Tiles for value width sv (bytes); stage sizes from the largest tile.
+static int build_tiles(dfm_mat A, int which) {
+  SpmvTiles& T = A->tiles[which];
+  if (T.valid) return DFM_OK;
+  const unsigned bb = A->b * A->b, sv = which ? 4u : 8u;
+  std::vector<unsigned> t(1, 0);
+  unsigned r = 0, mr = 0, mb = 0;
+  while (r < A->N) {
+    unsigned r1 = r, nb = 0;
+    while (r1 < A->N && r1 - r < kTileRows) {
+      const unsigned rb = A->h_rowptr[r1 + 1] - A->h_rowptr[r1];
+      if (r1 > r && (nb + rb) * bb * sv > kTileValBytes) break;
+      nb += rb;
+      r1++;
+    }
+    mr = std::max(mr, r1 - r);
+    mb = std::max(mb, nb);
+    t.push_back(r1);
+    r = r1;
+  }
+  T.ntiles = (unsigned)t.size() - 1;
+  T.max_rows = mr;
+  T.max_blocks = mb;
+  T.vals_bytes = al16_host(mb * bb * sv + 16);
+  T.col_bytes = al16_host(mb * 4 + 16);
+  T.diag_bytes = al16_host(mr * bb * sv + 16);
+  T.rp_bytes = al16_host((mr + 1) * 4 + 16);
+  T.stage_bytes = T.vals_bytes + T.col_bytes + T.diag_bytes + T.rp_bytes;
+  T.nstage = (int)std::min<size_t>(8, (size_t)(200 * 1024) / T.stage_bytes);
+  if (T.nstage < 2) return DFM_ERR_UNSUPPORTED;
+  DFM_CUDA_TRY(cudaMalloc(&T.d_tiles, t.size() * sizeof(unsigned)));
+  DFM_CUDA_TRY(cudaMemcpy(T.d_tiles, t.data(), t.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  T.valid = true;
+  return DFM_OK;
+}
+
+void spmv_free_tiles(dfm_mat A) {
+  for (SpmvTiles& T : A->tiles) {
+    cudaFree(T.d_tiles);
+    T = SpmvTiles();
+  }
+}
+
+template <int B, int LPR, typename TV>
+static cudaError_t launch_tma_t(dfm_mat A, const SpmvTiles& T, const TV* diag, const TV* off, int npart,
+                                cudaStream_t s, double alpha, const double* x, double beta, double* y,
+                                double* part, const int* done, const SpmvOpts& o) {
+  TmaArgs<TV> a;
+  a.N = A->N;
+  a.rowptr = A->d_rowptr;
+  a.colind = A->d_colind;
+  a.diag = diag;
+  a.off = off;
+  a.tiles = T.d_tiles;
+  a.ntiles = T.ntiles;
+  a.stage_bytes = T.stage_bytes;
+  a.vals_bytes = T.vals_bytes;
+  a.col_bytes = T.col_bytes;
+  a.diag_bytes = T.diag_bytes;
+  a.nstage = T.nstage;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.x = x;
+  a.y = y;
+  a.y0 = o.y0;
+  a.w = o.dot_w ? o.dot_w : x;
+  a.part = part;
+  a.part2 = o.dot_part2;
+  a.npart = npart;
+  a.done = done;
+  a.st = A->ctx->d_status;
+  a.wait_ns = A->ctx->wait_ns;
+  const size_t smem = (size_t)T.nstage * T.stage_bytes;
+  const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 2048)));
+  const int grid = std::max(1, std::min<int>((int)T.ntiles, std::min(A->ctx->nsm * per_sm, npart > 0 ? npart
+                                                                                                       : kMaxBlocks)));
+  auto fn = (part && o.yy) ? k_spmv_tma<B, LPR, TV, 3>
+            : (part && o.dot_part2) ? k_spmv_tma<B, LPR, TV, 2>
+            : part ? k_spmv_tma<B, LPR, TV, 1> : k_spmv_tma<B, LPR, TV, 0>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<grid, kTmaThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int B>
+static cudaError_t launch_tma(dfm_mat A, int lanes, int npart, cudaStream_t s, double alpha, const double* x,
+                              double beta, double* y, double* part, const int* done, const SpmvOpts& o) {
+  const SpmvTiles& T = A->tiles[o.f32 ? 1 : 0];
+#define DFM_TMA_L(L)                                                                                             \
+  return o.f32 ? launch_tma_t<B, L, float>(A, T, A->d_diag32, A->d_off32, npart, s, alpha, x, beta, y, part, done, \
+                                           o)                                                                    \
+               : launch_tma_t<B, L, double>(A, T, A->d_diag, A->d_off, npart, s, alpha, x, beta, y, part, done, o)
+  switch (lanes) {
+    case 4: DFM_TMA_L(4);
+    case 8: DFM_TMA_L(8);
+    case 16: DFM_TMA_L(16);
+    default: DFM_TMA_L(32);
+  }
+#undef DFM_TMA_L
+}
+
 int spmv_grid(dfm_mat A) {
   // grid-stride: 8 blocks of 256 threads per SM keep enough loads in flight
   const int want = A->ctx->nsm * 8;
@@ -212,6 +631,30 @@ int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y
   if (grid <= 0) grid = spmv_grid(A);
   if (lanes <= 0) lanes = A->lanes > 0 ? A->lanes : (A->b == 3 ? 16 : 8);
   const int* done = sc ? &sc->done : nullptr;
+  const int kind = o.kind >= 0 ? o.kind : A->spmv_kind;
+  if (kind == 2 && A->vt == DFM_REAL) {
+    switch (A->b) {
+      case 1: launch_elem<1>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      case 2: launch_elem<2>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      default: launch_elem<3>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+    }
+    DFM_CUDA_TRY(cudaGetLastError());
+    return DFM_OK;
+  }
+  if (kind == 1 && A->vt == DFM_REAL) {
+    if (!A->tiles[o.f32 ? 1 : 0].valid) {
+      const int rc = build_tiles(A, o.f32 ? 1 : 0);  // host set-up; normally done by the autotuner
+      if (rc) return rc;
+    }
+    cudaError_t e;
+    switch (A->b) {
+      case 1: e = launch_tma<1>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      case 2: e = launch_tma<2>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      default: e = launch_tma<3>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+    }
+    DFM_CUDA_TRY(e);
+    return DFM_OK;
+  }
   if (A->vt == DFM_COMPLEX) {
     switch (lanes) {
       case 4: launch_cplx<4>(A, grid, s, alpha, x, beta, y, dot_part, done, o); break;
@@ -247,11 +690,12 @@ int to_f32(dfm_ctx c, const double* in, float* out, size_t n) {
 int mat_make_f32(dfm_mat A) {
   const size_t nd = (size_t)A->N * A->vw(), no = (size_t)A->ncrs * A->vw();
   if (!A->d_diag32) {
-    DFM_CUDA_TRY(cudaMalloc(&A->d_diag32, std::max<size_t>(nd, 1) * sizeof(float)));
-    DFM_CUDA_TRY(cudaMalloc(&A->d_off32, std::max<size_t>(no, 1) * sizeof(float)));
+    DFM_CUDA_TRY(cudaMalloc(&A->d_diag32, (nd + kArrayPad) * sizeof(float)));
+    DFM_CUDA_TRY(cudaMalloc(&A->d_off32, (no + kArrayPad) * sizeof(float)));
   }
   int rc = to_f32(A->ctx, A->d_diag, A->d_diag32, nd);
   if (!rc) rc = to_f32(A->ctx, A->d_off, A->d_off32, no);
+  if (!rc && A->vt == DFM_REAL && A->spmv_kind == 1 && !A->tiles[1].valid) rc = build_tiles(A, 1);
   return rc;
 }
 
@@ -271,21 +715,33 @@ int spmv_autotune(dfm_mat A) {
   cudaEventCreate(&e1);
   const int cand[4] = {4, 8, 16, 32};
   float best = 1e30f;
-  int best_l = 8;
-  for (int c = 0; c < 4; c++) {
-    int rc = spmv_launch(A, 1.0, x, 0.0, y, nullptr, 0, nullptr, cand[c]);
-    if (rc) return rc;
-    float tmin = 1e30f;
-    for (int rep = 0; rep < 3; rep++) {
-      cudaEventRecord(e0, s);
-      spmv_launch(A, 1.0, x, 0.0, y, nullptr, 0, nullptr, cand[c]);
-      cudaEventRecord(e1, s);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      tmin = std::min(tmin, ms);
+  int best_l = 8, best_k = 0;
+  const bool tiles_ok = A->vt == DFM_REAL && build_tiles(A, 0) == DFM_OK;
+  cudaGetLastError();
+  for (int kind = 0; kind < 3; kind++)
+    for (int c = 0; c < 4; c++) {
+      if (kind > 0 && A->vt != DFM_REAL) break;
+      if (kind == 1 && !tiles_ok) break;
+      SpmvOpts o;
+      o.kind = kind;
+      int rc = spmv_launch(A, 1.0, x, 0.0, y, nullptr, 0, nullptr, cand[c], o);
+      if (rc) return rc;
+      float tmin = 1e30f;
+      for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(e0, s);
+        spmv_launch(A, 1.0, x, 0.0, y, nullptr, 0, nullptr, cand[c], o);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        tmin = std::min(tmin, ms);
+      }
+      if (tmin < best) { best = tmin; best_l = cand[c]; best_k = kind; }
     }
-    if (tmin < best) { best = tmin; best_l = cand[c]; }
+  A->spmv_kind = best_k;
+  if (best_k == 1 && A->d_off32 && !A->tiles[1].valid) {
+    const int rc = build_tiles(A, 1);
+    if (rc) return rc;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -32,6 +32,8 @@
 
 namespace dfm {
 
+constexpr int kOpBatch = 4;  // operands of one lane loaded together in the range sweeps
+
 // ------------------------------------------------------------ PTX helpers
 DFM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -163,25 +165,51 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; c++) acc[c] = 0.0;
-        for (unsigned kk = rd.y + lane; kk < rd.z; kk += LPR) {
-          const unsigned xo = xoff[kk];
-          TX xv[B];
-          if (xo & 0x80000000u) {  // another range's row: poll its published value
-            const unsigned col = xo & 0x7fffffffu;
+        // a lane's operands in batches of kOpBatch: every load of a batch is
+        // issued before any is waited on, so remote operands cost one round
+        // trip per batch instead of one each
+        for (unsigned kb = rd.y + lane; kb < rd.z; kb += kOpBatch * LPR) {
+          unsigned xo[kOpBatch];
+          TX xv[kOpBatch][B];
 #pragma unroll
-            for (int c = 0; c < B; c++) xv[c] = ld_relaxed(out + (size_t)col * B + c);
-#pragma unroll
-            for (int c = 0; c < B; c++)
-              if (Sent<TX>::is(xv[c])) xv[c] = poll_remote(out + (size_t)col * B + c, st, wait_ns, FWD ? 11 : 12);
-          } else {
-#pragma unroll
-            for (int c = 0; c < B; c++) xv[c] = X[xo + c];
+          for (int u = 0; u < kOpBatch; u++) {
+            const unsigned kk = kb + u * LPR;
+            xo[u] = kk < rd.z ? xoff[kk] : 0xffffffffu;
           }
-          const TV* m = vals + (size_t)kk * BB;
 #pragma unroll
-          for (int rr = 0; rr < B; rr++)
+          for (int u = 0; u < kOpBatch; u++) {
+            const unsigned o = xo[u];
+            if (o == 0xffffffffu) {
 #pragma unroll
-            for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)xv[c];
+              for (int c = 0; c < B; c++) xv[u][c] = (TX)0;
+            } else if (o & 0x40000000u) {  // an entry of the input vector (merged level pairs)
+#pragma unroll
+              for (int c = 0; c < B; c++) xv[u][c] = __ldg(in + (size_t)(o & 0x3fffffffu) * B + c);
+            } else if (o & 0x80000000u) {  // another range's row: its published value (may not be ready)
+#pragma unroll
+              for (int c = 0; c < B; c++) xv[u][c] = ld_relaxed(out + (size_t)(o & 0x7fffffffu) * B + c);
+            } else {
+#pragma unroll
+              for (int c = 0; c < B; c++) xv[u][c] = X[o + c];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kOpBatch; u++)
+            if (xo[u] != 0xffffffffu && (xo[u] & 0xc0000000u) == 0x80000000u)
+#pragma unroll
+              for (int c = 0; c < B; c++)
+                if (Sent<TX>::is(xv[u][c]))
+                  xv[u][c] = poll_remote(out + (size_t)(xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+#pragma unroll
+          for (int u = 0; u < kOpBatch; u++) {
+            const unsigned kk = kb + u * LPR;
+            if (kk >= rd.z) break;
+            const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+            for (int rr = 0; rr < B; rr++)
+#pragma unroll
+              for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)xv[u][c];
+          }
         }
         if (LPR > 1) {
 #pragma unroll
@@ -392,7 +420,11 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
     for (unsigned kk = rd.y + lane; kk < rd.z; kk += LPR) {
       const unsigned xo = xoff[kk];
       TX xv[B];
-      if (xo & 0x80000000u) {
+      if (xo & 0x40000000u) {  // an entry of the input vector (merged level pairs)
+        const unsigned col = xo & 0x3fffffffu;
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = __ldg(in + (size_t)col * B + c);
+      } else if (xo & 0x80000000u) {
         const unsigned col = xo & 0x7fffffffu;
 #pragma unroll
         for (int c = 0; c < B; c++) xv[c] = ld_relaxed(out + (size_t)col * B + c);
@@ -473,26 +505,77 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
     }
 }
 
-// Refreshes the blob's values from the factor after a numeric factorisation:
-// one CTA per chunk copies its blocks (and D^-1 rows for the forward sweep).
-template <typename TV>
-__global__ void k_gather_blob(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ blk_src,
-                              int bb, const double* __restrict__ fdiag, const double* __restrict__ foff,
-                              char* blob, int with_dinv) {
-  const ChunkDesc cd = chunks[blockIdx.x];
-  char* base = blob + cd.off;
-  TV* vals = reinterpret_cast<TV*>(base + cd.vals_off);
-  const unsigned* src = blk_src + cd.blk0;
-  for (unsigned e = threadIdx.x; e < cd.nblk_pad * (unsigned)bb; e += blockDim.x) {
-    const unsigned kk = e / bb, q = e % bb;
-    const unsigned sl = src[kk];
-    vals[e] = (sl == 0xffffffffu) ? (TV)0 : (TV)foff[(size_t)sl * bb + q];
-  }
-  if (with_dinv) {
-    const uint4* rd = reinterpret_cast<const uint4*>(base + 32);
-    double* dinv = reinterpret_cast<double*>(base + cd.dinv_off);
-    for (unsigned e = threadIdx.x; e < cd.nrows * (unsigned)bb; e += blockDim.x)
-      dinv[e] = fdiag[((size_t)cd.row0 + rd[e / bb].x) * bb + e % bb];
+// Refreshes the blob's values from the factor after a numeric factorisation.
+// Every packed block has a recipe {base, t0, t1, sign}:
+//   value = (base != NONE ? F[base] : 0) + sign * sum_{t0 <= t < t1} F[s1] (D_j^-1) (F[s2])
+// with a term {s1, j, s2} (j or s2 NONE = identity), F the factor's off-diagonal
+// blocks.  Plain operands are copies (no terms); the merged plans' operands of
+// the second level of a pair are the products L_ij D_j^-1 (forward input
+// terms), U'_ij (backward input terms) and the fill blocks
+// F_ik - sum_j F_ij (D_j^-1) F_jk.  One thread per packed block; D^-1 rows of the
+// forward sweep are copied alongside.
+template <int B, typename TV>
+__global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned nchunks,
+                                 const uint4* __restrict__ recipe, const uint4* __restrict__ terms,
+                                 const double* __restrict__ fdiag, const double* __restrict__ foff, char* blob,
+                                 int with_dinv) {
+  constexpr int BB = B * B;
+  constexpr unsigned NONE = 0xffffffffu;
+  for (unsigned q = blockIdx.x; q < nchunks; q += gridDim.x) {
+    const ChunkDesc cd = chunks[q];
+    char* base = blob + cd.off;
+    TV* vals = reinterpret_cast<TV*>(base + cd.vals_off);
+    for (unsigned k = threadIdx.x; k < cd.nblk_pad; k += blockDim.x) {
+      const uint4 rc = recipe[cd.blk0 + k];
+      double v[BB];
+#pragma unroll
+      for (int e = 0; e < BB; e++) v[e] = (rc.x != NONE) ? foff[(size_t)rc.x * BB + e] : 0.0;
+      const double sg = rc.w ? -1.0 : 1.0;
+      for (unsigned t = rc.y; t < rc.z; t++) {
+        const uint4 tm = terms[t];
+        double a[BB], m[BB];
+#pragma unroll
+        for (int e = 0; e < BB; e++) a[e] = foff[(size_t)tm.x * BB + e];
+        if (tm.y != NONE) {  // a = a * D_j^-1
+          const double* d = fdiag + (size_t)tm.y * BB;
+#pragma unroll
+          for (int r = 0; r < B; r++)
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              double acc = 0.0;
+#pragma unroll
+              for (int l = 0; l < B; l++) acc += a[r * B + l] * d[l * B + c];
+              m[r * B + c] = acc;
+            }
+#pragma unroll
+          for (int e = 0; e < BB; e++) a[e] = m[e];
+        }
+        if (tm.z != NONE) {  // a = a * F[s2]
+          const double* f = foff + (size_t)tm.z * BB;
+#pragma unroll
+          for (int r = 0; r < B; r++)
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              double acc = 0.0;
+#pragma unroll
+              for (int l = 0; l < B; l++) acc += a[r * B + l] * f[l * B + c];
+              m[r * B + c] = acc;
+            }
+#pragma unroll
+          for (int e = 0; e < BB; e++) a[e] = m[e];
+        }
+#pragma unroll
+        for (int e = 0; e < BB; e++) v[e] += sg * a[e];
+      }
+#pragma unroll
+      for (int e = 0; e < BB; e++) vals[(size_t)k * BB + e] = (TV)v[e];
+    }
+    if (with_dinv) {
+      const uint4* rd = reinterpret_cast<const uint4*>(base + 32);
+      double* dinv = reinterpret_cast<double*>(base + cd.dinv_off);
+      for (unsigned e = threadIdx.x; e < cd.nrows * (unsigned)BB; e += blockDim.x)
+        dinv[e] = fdiag[((size_t)cd.row0 + rd[e / BB].x) * BB + e % BB];
+    }
   }
 }
 
@@ -503,11 +586,12 @@ void sweep_plan_free(SweepPlan* P) {
   cudaFree(P->d_cta_chunk);
   cudaFree(P->d_range);
   cudaFree(P->d_blob);
-  cudaFree(P->d_blk_src);
+  cudaFree(P->d_recipe);
+  cudaFree(P->d_terms);
   *P = SweepPlan();
 }
 
-int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool) {
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge) {
   const unsigned N = M->N;
   const unsigned b = M->b;
   const unsigned bb = b * b;
@@ -519,7 +603,7 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   const std::vector<unsigned>& lev = fwd ? M->lev_f : M->lev_b;
   sweep_plan_free(P);
   if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
-  if (N >= 0x80000000u) return DFM_ERR_UNSUPPORTED;
+  if (N >= 0x40000000u) return DFM_ERR_UNSUPPORTED;  // operand encodings use the top two bits
   if (G < 1) G = 1;
   if ((unsigned)G > std::max(N, 1u)) G = std::max(N, 1u);
   // balanced contiguous ranges by (dependency blocks + 1) per row
@@ -547,32 +631,106 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   std::vector<ChunkDesc> chunks;
   std::vector<Pend> pend;
   std::vector<unsigned> cta_chunk(G + 1, 0);
-  std::vector<unsigned> blk_src;
+  std::vector<uint4> recipe, terms;
   size_t blob_size = 0;
   unsigned stage_max = 0;
+  constexpr unsigned NONE = 0xffffffffu;
+  // step of a row: its level, or with merged level pairs its level / 2
+  auto step = [&](unsigned i) { return merge ? lev[i] / 2 : lev[i]; };
+  // operands of row i: {encoded operand, recipe}.  Encoding: local slice
+  // offset, 0x80000000|row (an output of another range), 0x40000000|row (an
+  // entry of the input vector).
+  struct Op { unsigned xo; uint4 rc; };
+  std::vector<Op> ops;
+  std::vector<unsigned> kmap(N, NONE);  // scratch: column -> position in ops
+  auto slots = [&](unsigned i, unsigned& s0, unsigned& s1) {
+    s0 = fwd ? rp[i] : dia[i];
+    s1 = fwd ? dia[i] : rp[i + 1];
+  };
+  auto row_ops = [&](unsigned i, unsigned a0, unsigned a1) {
+    ops.clear();
+    unsigned s0, s1;
+    slots(i, s0, s1);
+    auto out_code = [&](unsigned col) { return (col >= a0 && col < a1) ? (col - a0) * b : (0x80000000u | col); };
+    const bool second = merge && (lev[i] & 1u);
+    if (!second) {
+      for (unsigned s = s0; s < s1; s++) ops.push_back({out_code(ci[s]), make_uint4(s, 0u, 0u, 0u)});
+      return;
+    }
+    // second level of a pair: operands on the first level are substituted
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned j = ci[s];
+      if (lev[j] + 1 != lev[i]) continue;
+      const unsigned t0 = (unsigned)terms.size();
+      terms.push_back(make_uint4(s, fwd ? j : NONE, NONE, 0u));  // L_ij D_j^-1  |  U'_ij
+      ops.push_back({0x40000000u | j, make_uint4(NONE, t0, t0 + 1, 0u)});
+    }
+    const size_t first_c = ops.size();
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned k = ci[s];
+      if (lev[k] + 1 == lev[i]) continue;
+      kmap[k] = (unsigned)ops.size();
+      ops.push_back({out_code(k), make_uint4(s, 0u, 0u, 1u)});
+    }
+    // fill terms, grouped per column
+    std::vector<std::vector<uint4>> tl(ops.size() - first_c);
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned j = ci[s];
+      if (lev[j] + 1 != lev[i]) continue;
+      unsigned t0, t1;
+      slots(j, t0, t1);
+      for (unsigned t = t0; t < t1; t++) {
+        const unsigned k = ci[t];
+        if (kmap[k] == NONE) {
+          kmap[k] = (unsigned)ops.size();
+          ops.push_back({out_code(k), make_uint4(NONE, 0u, 0u, 1u)});
+          tl.emplace_back();
+        }
+        tl[kmap[k] - first_c].push_back(make_uint4(s, fwd ? j : NONE, t, 0u));
+      }
+    }
+    for (size_t q = first_c; q < ops.size(); q++) {
+      const unsigned t0 = (unsigned)terms.size();
+      for (const uint4& t : tl[q - first_c]) terms.push_back(t);
+      ops[q].rc.y = t0;
+      ops[q].rc.z = (unsigned)terms.size();
+      // an operand with neither base nor terms cannot occur (each came from one)
+    }
+    for (size_t q = first_c; q < ops.size(); q++) {
+      unsigned col;
+      const unsigned code = ops[q].xo;
+      if (code & 0x80000000u) col = code & 0x3fffffffu;
+      else col = a0 + code / b;
+      kmap[col] = NONE;
+    }
+  };
   for (int c = 0; c < G; c++) {
     cta_chunk[c] = (unsigned)chunks.size();
     const unsigned a0 = range[c], a1 = range[c + 1];
     std::vector<unsigned> rows(a1 - a0);
     for (unsigned i = a0; i < a1; i++) rows[i - a0] = fwd ? i : (a1 - 1 - (i - a0));
-    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return lev[x] < lev[y]; });
+    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return step(x) < step(y); });
     size_t p = 0;
     while (p < rows.size()) {
-      const unsigned L = lev[rows[p]];
-      // one chunk: rows of level L, capped in rows and bytes
+      const unsigned L = step(rows[p]);
+      // one chunk: rows of one step, capped in rows and bytes
       Pend pd;
       unsigned nblk = 0;
-      while (p < rows.size() && lev[rows[p]] == L) {
+      const size_t rec0 = recipe.size();
+      while (p < rows.size() && step(rows[p]) == L) {
         const unsigned i = rows[p];
-        const unsigned s0 = fwd ? rp[i] : dia[i], s1 = fwd ? dia[i] : rp[i + 1];
-        const unsigned nb = s1 - s0;
+        const size_t tmark = terms.size();
+        row_ops(i, a0, a1);
+        const unsigned nb = (unsigned)ops.size();
         const ChunkLayout est = chunk_layout((unsigned)pd.rd.size() + 1, ((nblk + nb) + 3) & ~3u, 0u, vblk, drow);
-        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) break;
+        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) {
+          terms.resize(tmark);  // this row starts the next chunk
+          break;
+        }
         pd.rd.push_back(make_uint4(i - a0, nblk, nblk + nb, 0u));
-        for (unsigned s = s0; s < s1; s++) {
-          const unsigned col = ci[s];
-          pd.xo.push_back((col >= a0 && col < a1) ? (col - a0) * b : (0x80000000u | col));
-          blk_src.push_back(s);
+        for (const Op& o : ops) {
+          pd.xo.push_back(o.xo);
+          recipe.push_back(o.rc);
         }
         nblk += nb;
         p++;
@@ -580,12 +738,12 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
       const unsigned nblk_pad = (nblk + 3) & ~3u;
       for (unsigned k = nblk; k < nblk_pad; k++) {
         pd.xo.push_back(0);  // padding: never referenced (outside every row's block range)
-        blk_src.push_back(0xffffffffu);
+        recipe.push_back(make_uint4(NONE, 0u, 0u, 0u));
       }
       ChunkDesc cd = {};
       cd.nrows = (unsigned)pd.rd.size();
       cd.nblk_pad = nblk_pad;
-      cd.blk0 = (unsigned)(blk_src.size() - nblk_pad);
+      cd.blk0 = (unsigned)rec0;
       cd.row0 = a0;
       const ChunkLayout cl = chunk_layout(cd.nrows, nblk_pad, 0u, vblk, drow);
       cd.vals_off = cl.vals;
@@ -643,14 +801,18 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   DFM_CUDA_TRY(cudaMalloc(&P->d_cta_chunk, sizeof(unsigned) * (G + 1)));
   DFM_CUDA_TRY(cudaMalloc(&P->d_range, sizeof(unsigned) * (G + 1)));
   DFM_CUDA_TRY(cudaMalloc(&P->d_blob, hblob.size()));
-  DFM_CUDA_TRY(cudaMalloc(&P->d_blk_src, sizeof(unsigned) * std::max<size_t>(blk_src.size(), 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_recipe, sizeof(uint4) * std::max<size_t>(recipe.size(), 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_terms, sizeof(uint4) * std::max<size_t>(terms.size(), 1)));
   if (!chunks.empty())
     DFM_CUDA_TRY(cudaMemcpyAsync(P->d_chunks, chunks.data(), sizeof(ChunkDesc) * chunks.size(), cudaMemcpyHostToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_cta_chunk, cta_chunk.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_range, range.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blob, hblob.data(), hblob.size(), cudaMemcpyHostToDevice, s));
-  if (!blk_src.empty())
-    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blk_src, blk_src.data(), sizeof(unsigned) * blk_src.size(), cudaMemcpyHostToDevice, s));
+  if (!recipe.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_recipe, recipe.data(), sizeof(uint4) * recipe.size(), cudaMemcpyHostToDevice, s));
+  if (!terms.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_terms, terms.data(), sizeof(uint4) * terms.size(), cudaMemcpyHostToDevice, s));
+  P->merged = merge;
   DFM_CUDA_TRY(cudaStreamSynchronize(s));
   P->valid = true;
   P->stale = true;
@@ -659,13 +821,18 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
 
 int sweep_plan_refresh(dfm_ilu M, SweepPlan* P) {
   if (!P->valid || P->nchunks == 0) { P->stale = false; return DFM_OK; }
-  const int bb = (int)M->vw();
-  if (P->val_bytes == 8)
-    k_gather_blob<double><<<P->nchunks, 256, 0, M->ctx->stream>>>(P->d_chunks, P->d_blk_src, bb, M->d_fdiag,
-                                                                  M->d_foff, P->d_blob, P->fwd ? 1 : 0);
-  else
-    k_gather_blob<float><<<P->nchunks, 256, 0, M->ctx->stream>>>(P->d_chunks, P->d_blk_src, bb, M->d_fdiag,
-                                                                 M->d_foff, P->d_blob, P->fwd ? 1 : 0);
+  const int grid = (int)std::min<unsigned>(P->nchunks, (unsigned)M->ctx->nsm * 8);
+  const int wd = P->fwd ? 1 : 0;
+  cudaStream_t s = M->ctx->stream;
+#define DFM_GATHER(BV, TV)                                                                                    \
+  k_gather_recipes<BV, TV><<<grid, 128, 0, s>>>(P->d_chunks, P->nchunks, P->d_recipe, P->d_terms, M->d_fdiag,  \
+                                                M->d_foff, P->d_blob, wd)
+  if (P->val_bytes == 8) {
+    if (M->b == 1) DFM_GATHER(1, double); else if (M->b == 2) DFM_GATHER(2, double); else DFM_GATHER(3, double);
+  } else {
+    if (M->b == 1) DFM_GATHER(1, float); else if (M->b == 2) DFM_GATHER(2, float); else DFM_GATHER(3, float);
+  }
+#undef DFM_GATHER
   DFM_CUDA_TRY(cudaGetLastError());
   P->stale = false;
   return DFM_OK;

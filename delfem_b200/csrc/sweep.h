@@ -53,7 +53,7 @@ struct ChunkDesc {
   unsigned nrows;
   unsigned nblk_pad;       // packed blocks (multiple of 4)
   unsigned nhalo;
-  unsigned blk0;           // index of the first packed block in blk_src
+  unsigned blk0;           // index of the first packed block's recipe
   unsigned vals_off, dinv_off;
   unsigned row0;           // first row of the owning range
 };
@@ -78,7 +78,9 @@ struct SweepPlan {
   unsigned* d_cta_chunk = nullptr;  // G+1 chunk ranges
   unsigned* d_range = nullptr;      // G+1 row ranges
   char* d_blob = nullptr;
-  unsigned* d_blk_src = nullptr;    // factor slot of every packed block
+  uint4* d_recipe = nullptr;        // per packed block: {base slot, term range, sign}
+  uint4* d_terms = nullptr;         // {s1, j, s2, 0}: F[s1] (D_j^-1) (F[s2])
+  bool merged = false;              // steps are pairs of levels
 };
 
 }  // namespace dfm

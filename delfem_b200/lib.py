@@ -48,6 +48,8 @@ PROTOS = {
     "dfm_mat_values_device": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
     "dfm_mat_set_spmv_lanes": (_i, [_vp, _i]),
     "dfm_mat_get_spmv_lanes": (_i, [_vp, _ip]),
+    "dfm_mat_set_spmv_kernel": (_i, [_vp, _i]),
+    "dfm_mat_get_spmv_kernel": (_i, [_vp, _ip]),
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
@@ -237,6 +239,16 @@ class Matrix:
     @lanes.setter
     def lanes(self, v):
         check(lib().dfm_mat_set_spmv_lanes(self.h, int(v)))
+
+    @property
+    def spmv_kernel(self):
+        v = C.c_int()
+        check(lib().dfm_mat_get_spmv_kernel(self.h, C.byref(v)))
+        return v.value
+
+    @spmv_kernel.setter
+    def spmv_kernel(self, v):
+        check(lib().dfm_mat_set_spmv_kernel(self.h, int(v)), "dfm_mat_set_spmv_kernel")
 
 
 class Mesh:

@@ -101,6 +101,12 @@ DFM_API int dfm_mat_values_device(dfm_mat A, double** diag, double** off);
 /* Lanes per block row of the SpMV (4, 8, 16, 32); 0 = autotuned on first use. */
 DFM_API int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes);
 DFM_API int dfm_mat_get_spmv_lanes(dfm_mat A, int* lanes);
+/* SpMV kernel: 0 = a lane per block (direct loads), 1 = row tiles staged in
+ * shared memory by TMA bulk copies, 2 = element-wise coalesced loads of each
+ * row's contiguous values (1 and 2 real matrices only).  Autotuned together
+ * with the lanes. */
+DFM_API int dfm_mat_set_spmv_kernel(dfm_mat A, int kernel);
+DFM_API int dfm_mat_get_spmv_kernel(dfm_mat A, int* kernel);
 
 /* y = beta*y + alpha*A x  (CMatDia_BlkCrs::MatVec, src/matvec/matdia_blkcrs.cpp:921-1094;
  * complex: CZMatDia_BlkCrs::MatVec, src/matvec/zmatdia_blkcrs.cpp:737-801).
@@ -188,8 +194,11 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * level barriers, 3 = contiguous row ranges per CTA (shared-memory slice, TMA-
  * streamed level data, a CTA barrier per level; the CTA count is the max_blocks
  * of dfm_ilu_set_sweep_tuning, default one per SM), 4 = the row ranges of 3
- * without level barriers (each row waits on its own operands).  Real matrices
- * only for 3 and 4. */
+ * without level barriers (each row waits on its own operands), 5 and 6 = 3 and
+ * 4 with the levels taken in pairs (the second level's operands on the first
+ * substituted by products with the factor, recomputed after every
+ * factorization: half the sequential steps, results equal to rounding).  Real
+ * matrices only for 3-6. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all

@@ -35,10 +35,14 @@ SYSTEMS = {
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
 @pytest.mark.parametrize("lanes", [4, 8, 16, 32])
-def test_spmv_matches_oracle(ctx, name, lanes):
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_spmv_matches_oracle(ctx, name, lanes, kernel):
     S = SYSTEMS[name]()
+    if kernel >= 1 and S.cplx:
+        pytest.skip("kernels 1 and 2 are real-only")
     A = make(ctx, S)
     A.lanes = lanes
+    A.spmv_kernel = kernel
     rng = np.random.default_rng(7)
     x = rng.standard_normal(S.N * S.xw)
     y0 = rng.standard_normal(S.N * S.xw)
@@ -69,7 +73,7 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -90,7 +94,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -114,9 +118,9 @@ def test_pcg_matches_oracle(ctx, name, sweep):
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
-@pytest.mark.parametrize("mode", [3, 4])
+@pytest.mark.parametrize("mode", [3, 4, 5, 6])
 def test_range_sweep_cta_counts(ctx, name, ctas, mode):
-    """Modes 3 and 4 with every CTA count: same result as the oracle's sweeps."""
+    """Modes 3-6 with every CTA count: same result as the oracle's sweeps."""
     from delfem_b200 import lib
     S = SYSTEMS[name]()
     A = make(ctx, S)
@@ -189,3 +193,19 @@ def test_determinism(ctx):
         lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=2000)
         outs.append(x.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_spmv_large_rows_and_tiles(ctx, kernel):
+    """Rows of very different lengths and a system spanning many TMA tiles
+    (block rows with up to 60 neighbours; tiles cut by rows and by bytes)."""
+    from tests import cases as C
+    S = C.random_spd_like(5000, 3, seed=21, density=30)
+    A = make(ctx, S)
+    A.spmv_kernel = kernel
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(S.N * S.xw)
+    y = torch.zeros(S.N * S.xw, dtype=torch.float64, device="cuda")
+    A.spmv(1.0, dev(x), 0.0, y)
+    ref = S.spmv(1.0, x, 0.0, np.zeros_like(x))
+    assert np.allclose(y.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
