@@ -33,6 +33,7 @@
 namespace dfm {
 
 constexpr int kOpBatch = 4;  // operands of one lane loaded together in the range sweeps
+constexpr int kStageThread = kSweepThreads - 32;  // drives the stage ring of the range sweep
 
 // ------------------------------------------------------------ PTX helpers
 DFM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -131,8 +132,8 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
 
   // X slice <- in[a0:a1) (rows overwrite their entry with the output)
   for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[(size_t)a0 * B + k];
-  unsigned issued_end = q0;  // thread 0: chunks [q0, issued_end) requested
-  if (threadIdx.x == 0) {
+  unsigned issued_end = q0;  // stage thread: chunks [q0, issued_end) requested
+  if (threadIdx.x == kStageThread) {
     s_alive = 1;
     for (int s = 0; s < nstage; s++) mbar_init(&bar_data[s], 1);
     fence_mbar_init();
@@ -244,13 +245,14 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
         }
       }
     }
-    // thread 0: the next level's chunk must have landed before the barrier
-    if (threadIdx.x == 0 && s_alive && q + 1 < q1) {
+    // the stage thread (lane 0 of the last warp, which rarely has rows): the next
+    // level's chunk must have landed before the barrier
+    if (threadIdx.x == kStageThread && s_alive && q + 1 < q1) {
       const unsigned k1 = k + 1;
       if (!wait_stage(&bar_data[k1 % (unsigned)nstage], (k1 / (unsigned)nstage) & 1u, st, wait_ns)) s_alive = 0;
     }
     __syncthreads();  // level done: slice entries visible, stage s free
-    if (threadIdx.x == 0 && s_alive) {
+    if (threadIdx.x == kStageThread && s_alive) {
       const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
       if (hdr->next_bytes) {
         mbar_arrive_tx(&bar_data[s], hdr->next_bytes);
@@ -266,7 +268,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
     block_partial<kSweepThreads>(dacc, part);
   }
   // after an aborted wait, copies already requested must land before the CTA exits
-  if (threadIdx.x == 0 && !s_alive) {
+  if (threadIdx.x == kStageThread && !s_alive) {
     for (unsigned q = q0; q < issued_end; q++) {
       const unsigned k = q - q0;
       (void)wait_stage(&bar_data[k % (unsigned)nstage], (k / (unsigned)nstage) & 1u, st, wait_ns);
