@@ -799,6 +799,7 @@ int ilu_prepare(dfm_ilu M, bool f32) {
         M->plan_gen++;  // captured graphs hold the old plan's buffers
       }
       P32.nb = P64.nb && P32.nb_ok;
+      P32.pipe = P64.pipe;
       if ((rc = sweep_plan_refresh(M, &P32))) return rc;
     }
   }
@@ -856,27 +857,30 @@ int ilu_autotune(dfm_ilu M) {
     int last = -1, best_G = 0;
     float best3 = 1e30f;
     // times the candidate plans (pf, pb) over lanes per row and the kernel
-    // variants in `nbs`; keeps them in best_f/best_b if they beat `best`
-    auto try_plans = [&](SweepPlan& pf, SweepPlan& pb, std::initializer_list<int> nbs, float* tbest) -> int {
+    // variants in `kinds` (0 = level barrier, 1 = barrier-free, 2 = level
+    // barrier with the two-half row pipeline); keeps them in best_f/best_b if
+    // they beat `best`
+    auto try_plans = [&](SweepPlan& pf, SweepPlan& pb, std::initializer_list<int> kinds, float* tbest) -> int {
       std::swap(M->plan_f, pf);  // M holds the candidate
       std::swap(M->plan_b, pb);
       float ms = 1e30f;
-      int rc = DFM_OK, best_lpr = 1;
-      bool best_nb = false;
-      for (int nbv : nbs) {
+      int rc = DFM_OK, best_lpr = 1, best_kind = 0;
+      for (int kind : kinds) {
         if (rc) break;
-        if (nbv && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) continue;
+        if (kind == 1 && !(M->plan_f.nb_ok && M->plan_b.nb_ok)) continue;
         for (int lpr : {1, 2, 4, 8}) {  // consumer lanes per row
           M->plan_f.lpr = M->plan_b.lpr = lpr;
-          M->plan_f.nb = M->plan_b.nb = nbv != 0;
+          M->plan_f.nb = M->plan_b.nb = kind == 1;
+          M->plan_f.pipe = M->plan_b.pipe = kind == 2;
           float t = 1e30f;
           rc = time_mode(3, &t);
           if (rc) break;
-          if (t < ms) { ms = t; best_lpr = lpr; best_nb = nbv != 0; }
+          if (t < ms) { ms = t; best_lpr = lpr; best_kind = kind; }
         }
       }
       M->plan_f.lpr = M->plan_b.lpr = best_lpr;
-      M->plan_f.nb = M->plan_b.nb = best_nb;
+      M->plan_f.nb = M->plan_b.nb = best_kind == 1;
+      M->plan_f.pipe = M->plan_b.pipe = best_kind == 2;
       std::swap(M->plan_f, pf);  // candidate back in pf/pb, M empty
       std::swap(M->plan_b, pb);
       if (tbest) *tbest = ms;
@@ -904,7 +908,7 @@ int ilu_autotune(dfm_ilu M) {
         continue;  // slice does not fit in shared memory at this CTA count
       }
       float t = 1e30f;
-      const int rc = try_plans(pf, pb, {0}, &t);
+      const int rc = try_plans(pf, pb, {0, 2}, &t);
       if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
         sweep_plan_free(&best_f);
         sweep_plan_free(&best_b);
@@ -913,7 +917,7 @@ int ilu_autotune(dfm_ilu M) {
       if (rc == DFM_OK && t < best3) { best3 = t; best_G = G; }
     }
     if (best_G > 0) {
-      for (int mg = 0; mg < 2; mg++) {  // barrier-free kernel unmerged, then merged pairs with both kernels
+      for (int mg = 0; mg < 2; mg++) {  // barrier-free kernel unmerged, then merged pairs with every kernel
         SweepPlan pf, pb;
         if (sweep_plan_build(M, true, best_G, 8, 8, &pf, mg != 0) != DFM_OK ||
             sweep_plan_build(M, false, best_G, 8, 8, &pb, mg != 0) != DFM_OK) {
@@ -922,7 +926,7 @@ int ilu_autotune(dfm_ilu M) {
           cudaGetLastError();
           continue;
         }
-        const int rc = mg ? try_plans(pf, pb, {0, 1}, nullptr) : try_plans(pf, pb, {1}, nullptr);
+        const int rc = mg ? try_plans(pf, pb, {0, 1, 2}, nullptr) : try_plans(pf, pb, {1}, nullptr);
         if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
           sweep_plan_free(&best_f);
           sweep_plan_free(&best_b);

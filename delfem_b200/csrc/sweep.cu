@@ -97,15 +97,168 @@ DFM_DEVINL bool wait_stage(uint64_t* bar, unsigned parity, DevStatus* st, uint64
   }
 }
 
+// ------------------------------------------------- row helpers (mode 3)
+// A row's first batch of operands as issued ahead of time: codes and values
+// (remote and input-vector entries loaded, local ones filled in later).
+template <int B, typename TX>
+struct RowPF {
+  bool valid;
+  uint4 rd;
+  unsigned xo[kOpBatch];
+  TX xv[kOpBatch][B];
+};
+
+template <int B, int LPR, typename TX>
+DFM_DEVINL void row_prefetch(const char* sb, unsigned r, int lane, const TX* __restrict__ in, const TX* out,
+                             RowPF<B, TX>& pf) {
+  const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+  const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+  pf.rd = reinterpret_cast<const uint4*>(sb + 32)[r];
+  pf.valid = true;
+#pragma unroll
+  for (int u = 0; u < kOpBatch; u++) {
+    const unsigned kk = pf.rd.y + lane + u * LPR;
+    pf.xo[u] = kk < pf.rd.z ? xoff[kk] : 0xffffffffu;
+  }
+#pragma unroll
+  for (int u = 0; u < kOpBatch; u++) {
+    const unsigned o = pf.xo[u];
+    if (o != 0xffffffffu && (o & 0x40000000u)) {  // an entry of the input vector (merged level pairs)
+#pragma unroll
+      for (int c = 0; c < B; c++) pf.xv[u][c] = __ldg(in + (size_t)(o & 0x3fffffffu) * B + c);
+    } else if (o != 0xffffffffu && (o & 0x80000000u)) {  // another range's row (may not be published yet)
+#pragma unroll
+      for (int c = 0; c < B; c++) pf.xv[u][c] = ld_relaxed(out + (size_t)(o & 0x7fffffffu) * B + c);
+    } else {
+#pragma unroll
+      for (int c = 0; c < B; c++) pf.xv[u][c] = (TX)0;
+    }
+  }
+}
+
+// Finishes a prefetched row: local operands, re-polls, the remaining operand
+// batches, the group reduction and the row's output (slice and global).
+template <int B, int LPR, typename TV, typename TX, bool FWD>
+DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask, unsigned a0, TX* X,
+                           const TX* __restrict__ in, TX* out, RowPF<B, TX>& pf, DevStatus* st, uint64_t wait_ns) {
+  constexpr int BB = B * B;
+  const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+  const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+  const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+  const uint4 rd = pf.rd;
+  double acc[B];
+#pragma unroll
+  for (int c = 0; c < B; c++) acc[c] = 0.0;
+  // first batch: prefetched codes
+#pragma unroll
+  for (int u = 0; u < kOpBatch; u++) {
+    const unsigned o = pf.xo[u];
+    if (o != 0xffffffffu && (o & 0xc0000000u) == 0u)
+#pragma unroll
+      for (int c = 0; c < B; c++) pf.xv[u][c] = X[o + c];
+  }
+#pragma unroll
+  for (int u = 0; u < kOpBatch; u++)
+    if (pf.xo[u] != 0xffffffffu && (pf.xo[u] & 0xc0000000u) == 0x80000000u)
+#pragma unroll
+      for (int c = 0; c < B; c++)
+        if (Sent<TX>::is(pf.xv[u][c]))
+          pf.xv[u][c] = poll_remote(out + (size_t)(pf.xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+#pragma unroll
+  for (int u = 0; u < kOpBatch; u++) {
+    const unsigned kk = rd.y + lane + u * LPR;
+    if (kk >= rd.z) break;
+    const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+    for (int rr = 0; rr < B; rr++)
+#pragma unroll
+      for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)pf.xv[u][c];
+  }
+  // remaining batches (rows with more than kOpBatch * LPR operands)
+  for (unsigned kb = rd.y + lane + kOpBatch * LPR; kb < rd.z; kb += kOpBatch * LPR) {
+    unsigned xo[kOpBatch];
+    TX xv[kOpBatch][B];
+#pragma unroll
+    for (int u = 0; u < kOpBatch; u++) {
+      const unsigned kk = kb + u * LPR;
+      xo[u] = kk < rd.z ? xoff[kk] : 0xffffffffu;
+    }
+#pragma unroll
+    for (int u = 0; u < kOpBatch; u++) {
+      const unsigned o = xo[u];
+      if (o == 0xffffffffu) {
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[u][c] = (TX)0;
+      } else if (o & 0x40000000u) {
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[u][c] = __ldg(in + (size_t)(o & 0x3fffffffu) * B + c);
+      } else if (o & 0x80000000u) {
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[u][c] = ld_relaxed(out + (size_t)(o & 0x7fffffffu) * B + c);
+      } else {
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[u][c] = X[o + c];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kOpBatch; u++)
+      if (xo[u] != 0xffffffffu && (xo[u] & 0xc0000000u) == 0x80000000u)
+#pragma unroll
+        for (int c = 0; c < B; c++)
+          if (Sent<TX>::is(xv[u][c]))
+            xv[u][c] = poll_remote(out + (size_t)(xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+#pragma unroll
+    for (int u = 0; u < kOpBatch; u++) {
+      const unsigned kk = kb + u * LPR;
+      if (kk >= rd.z) break;
+      const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+      for (int rr = 0; rr < B; rr++)
+#pragma unroll
+        for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * (double)xv[u][c];
+    }
+  }
+  if (LPR > 1) {
+#pragma unroll
+    for (int rr = 0; rr < B; rr++)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
+  }
+  if (lane == 0) {
+    TX* xi = X + rd.x * B;
+    double t[B];
+#pragma unroll
+    for (int rr = 0; rr < B; rr++) t[rr] = (double)xi[rr] - acc[rr];
+    TX o[B];
+    if (FWD) {
+      const double* d = reinterpret_cast<const double*>(sb + hdr->dinv) + (size_t)r * BB;
+#pragma unroll
+      for (int rr = 0; rr < B; rr++) {
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < B; c++) v += d[rr * B + c] * t[c];
+        o[rr] = (TX)v;
+      }
+    } else {
+#pragma unroll
+      for (int rr = 0; rr < B; rr++) o[rr] = (TX)t[rr];
+    }
+#pragma unroll
+    for (int rr = 0; rr < B; rr++) {
+      xi[rr] = o[rr];
+      st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+    }
+  }
+}
+
 // --------------------------------------------------------------- kernel
-template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
-__global__ void __launch_bounds__(kSweepThreads)
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT, bool PIPE>
+__global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
                const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
                int nstage, unsigned x_bytes, const TX* __restrict__ in, TX* out, const TX* __restrict__ rdot,
                double* part, KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st,
                uint64_t wait_ns) {
-  constexpr int BB = B * B;
   extern __shared__ __align__(128) char smem[];
   __shared__ int s_alive;
   // guards (block-uniform)
@@ -150,6 +303,50 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
   const int lane = threadIdx.x % LPR;
   const unsigned g = threadIdx.x / LPR, ng = kSweepThreads / LPR;
   const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+  if constexpr (PIPE) {
+  // Software pipeline across levels: the lane groups form two halves that
+  // take alternate levels.  While one half computes level k, the other waits
+  // for level k+1's stage and, for its first row there, reads the descriptor
+  // and operand offsets and issues the remote and input-vector loads; after
+  // the barrier that ends level k it only loads its local operands, re-polls
+  // a remote value that was not yet published, and finishes the row.
+  const unsigned half = ng / 2, h = g >= half ? 1u : 0u, gl = g - h * half;
+  RowPF<B, TX> pf;
+  pf.valid = false;
+  if (s_alive && q0 < q1 && h == 0 && gl < reinterpret_cast<const ChunkHeader*>(stages)->nrows)
+    row_prefetch<B, LPR, TX>(stages, gl, lane, in, out, pf);
+  for (unsigned q = q0; q < q1; q++) {
+    const unsigned k = q - q0;
+    const int s = (int)(k % (unsigned)nstage);
+    const char* sb = stages + (size_t)s * stage_bytes;
+    if (s_alive && h == (k & 1u)) {  // this half computes level k
+      const unsigned nrows = reinterpret_cast<const ChunkHeader*>(sb)->nrows;
+      if (pf.valid) row_finish<B, LPR, TV, TX, FWD>(sb, gl, lane, gmask, a0, X, in, out, pf, st, wait_ns);
+      pf.valid = false;
+      for (unsigned r = gl + half; r < nrows; r += half) {  // more rows than the half has groups
+        RowPF<B, TX> ex;
+        row_prefetch<B, LPR, TX>(sb, r, lane, in, out, ex);
+        row_finish<B, LPR, TV, TX, FWD>(sb, r, lane, gmask, a0, X, in, out, ex, st, wait_ns);
+      }
+    } else if (s_alive && q + 1 < q1) {  // the other half prepares level k+1
+      const unsigned k1 = k + 1;
+      const int s1 = (int)(k1 % (unsigned)nstage);
+      if (!wait_stage(&bar_data[s1], (k1 / (unsigned)nstage) & 1u, st, wait_ns)) s_alive = 0;
+      const char* sb1 = stages + (size_t)s1 * stage_bytes;
+      if (s_alive && gl < reinterpret_cast<const ChunkHeader*>(sb1)->nrows)
+        row_prefetch<B, LPR, TX>(sb1, gl, lane, in, out, pf);
+    }
+    __syncthreads();  // level done: slice entries visible, stage s free
+    if (threadIdx.x == kStageThread && s_alive) {
+      const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(sb);
+      if (hdr->next_bytes) {
+        mbar_arrive_tx(&bar_data[s], hdr->next_bytes);
+        bulk_g2s(stages + (size_t)s * stage_bytes, blob + hdr->next_off, hdr->next_bytes, &bar_data[s]);
+        issued_end = q + nstage + 1;
+      }
+    }
+  }
+  } else {  // every group loads its rows after the level barrier
   for (unsigned q = q0; q < q1; q++) {
     const unsigned k = q - q0;
     const int s = (int)(k % (unsigned)nstage);
@@ -161,6 +358,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
       const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
       const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
       const double* dinv = reinterpret_cast<const double*>(sb + hdr->dinv);
+      constexpr int BB = B * B;
       for (unsigned r = g; r < nrows; r += ng) {  // uniform within a group (lanes share r)
         const uint4 rd = rdesc[r];
         double acc[B];
@@ -261,6 +459,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
       }
     }
   }
+  }
   if (DOT) {  // (rdot, out) over this CTA's range, from the finished slice
     double dacc = 0.0;
     for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
@@ -311,7 +510,7 @@ DFM_DEVINL TX poll_local(const TX* p, volatile int* alive, DevStatus* st, uint64
 }
 
 template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
-__global__ void __launch_bounds__(kSweepThreads)
+__global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
                   const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
                   int nstage, unsigned x_bytes, unsigned max_chunks, const TX* __restrict__ in, TX* out,
@@ -866,19 +1065,14 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
                               P->x_bytes, P->max_cta_chunks, in, out, rdot, part, sc, rr_part, rr_n, c->d_status,
                               (uint64_t)c->wait_ns);
   }
-  if (part) {
-    auto fn = k_sweep_ranges<B, LPR, TV, TX, FWD, true>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
-    return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
-                              (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
-                              P->x_bytes, in, out, rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
-  }
-  auto fn = k_sweep_ranges<B, LPR, TV, TX, FWD, false>;
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
+  auto fn = part ? (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, true, true> : k_sweep_ranges<B, LPR, TV, TX, FWD, true, false>)
+                 : (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, false, true>
+                            : k_sweep_ranges<B, LPR, TV, TX, FWD, false, false>);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
+  if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
                             (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
-                            P->x_bytes, in, out, rdot, (double*)nullptr, sc, rr_part, rr_n, c->d_status,
-                            (uint64_t)c->wait_ns);
+                            P->x_bytes, in, out, rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
 }
 
 template <int B, typename TV, typename TX, bool FWD>

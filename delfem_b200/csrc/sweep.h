@@ -66,6 +66,7 @@ struct SweepPlan {
   int lpr = 1;             // consumer lanes per row
   bool nb = false;         // barrier-free kernel variant (rows wait on their own operands)
   bool nb_ok = false;      // its extra shared memory (row prefix per chunk) fits
+  bool pipe = false;       // barrier kernel with the two-half row pipeline across levels
   unsigned max_cta_chunks = 0;
   int nstage = 0;
   int val_bytes = 8;       // 8 = FP64 factor blocks, 4 = FP32

@@ -197,8 +197,10 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * without level barriers (each row waits on its own operands), 5 and 6 = 3 and
  * 4 with the levels taken in pairs (the second level's operands on the first
  * substituted by products with the factor, recomputed after every
- * factorization: half the sequential steps, results equal to rounding).  Real
- * matrices only for 3-6. */
+ * factorization: half the sequential steps, results equal to rounding), 7 and
+ * 8 = 3 and 5 with the row groups in two halves taking alternate levels, the
+ * idle half fetching its next row's operands before the level barrier (same
+ * results as 3 and 5).  Real matrices only for 3-8. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all

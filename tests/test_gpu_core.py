@@ -73,7 +73,7 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -94,7 +94,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -118,9 +118,9 @@ def test_pcg_matches_oracle(ctx, name, sweep):
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
-@pytest.mark.parametrize("mode", [3, 4, 5, 6])
+@pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8])
 def test_range_sweep_cta_counts(ctx, name, ctas, mode):
-    """Modes 3-6 with every CTA count: same result as the oracle's sweeps."""
+    """Modes 3-8 with every CTA count: same result as the oracle's sweeps."""
     from delfem_b200 import lib
     S = SYSTEMS[name]()
     A = make(ctx, S)

@@ -24,7 +24,7 @@ SYSTEMS = {
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 5])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7])
 def test_mixed_true_residual_and_solution(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
