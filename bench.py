@@ -53,6 +53,7 @@ NU = 0.3
 LAM3 = NU / ((1 + NU) * (1 - 2 * NU))
 MYU3 = 1.0 / (2 * (1 + NU))
 C3_COUNT, C3_LO, C3_HI, C3_SEED = 512, 32, 512, 3
+C5_MAXIT = 5000  # the oracle's COCG needs 1794 iterations on this system
 
 
 def log(*a):
@@ -225,9 +226,13 @@ def run_c3(ctx, torch, dev, stream, timed, steps):
     sizes, ms, noff, eoff, kappa, A, M, B, rhs = build_c3(ctx, torch, dev)
     x = torch.zeros_like(rhs)
     res = {}
+    t0 = time.time()
     B.solve(rhs, x, tol=TOL)  # warm-up: autotunes the sweep schedule and the batch tiles
+    log(f"[bench] c3 warm-up (tuning) {time.time() - t0:.1f}s: sweep {M.sweep}, schedule {B.schedule}")
     t_batch = timed(lambda: B.solve(rhs, x, tol=TOL), max(2, min(steps, 3)))
     rc, _, it, conv, st = B.solve(rhs, x, tol=TOL)
+    log(f"[bench] c3 batched solve {t_batch:.2f}s, max iterations {int(it.max())}")
+    t0 = time.time()
     xb = x.cpu().numpy()
     # looped plain solves on a size-stratified sample (every k-th instance by size)
     order = np.argsort(sizes, kind="stable")
@@ -263,13 +268,15 @@ def run_c3(ctx, torch, dev, stream, timed, steps):
         for h in (Mk, Ak, Gk):
             h.close()
     t_loop = t_loop_sample * (len(sizes) / len(sample))
+    log(f"[bench] c3 looped sample {t_loop_sample:.2f}s ({time.time() - t0:.1f}s with set-up and tuning)")
     res.update({
         "instances": int(len(sizes)), "nodes": int(noff[-1]), "grid_sides": [int(sizes.min()), int(sizes.max())],
         "batched_s": t_batch, "looped_s_estimated": t_loop, "speedup_vs_looped": t_loop / t_batch,
         "looped_sample": f"{len(sample)} instances (every {stride}th by size) timed one by one with dfm_solve_pcg, "
                          f"scaled by {len(sizes) / len(sample):.0f}",
         "max_iterations": int(it.max()), "all_converged": bool((st == lib.OK).all()),
-        "max_rel_diff_vs_single_solves": err, "tuning": list(B.tuning), "sweep": M.sweep,
+        "max_rel_diff_vs_single_solves": err, "tuning": list(B.tuning), "schedule": list(B.schedule),
+        "sweep": M.sweep,
     })
     for h in (B, M, A):
         h.close()
@@ -365,9 +372,12 @@ def run_c1(ctx, torch, dev, timed, with_reference):
 def run_c5(ctx, torch, dev, timed):
     """c5: Helmholtz k = 20 on the unit disk (~200k nodes), complex ILU(0)-COCG to
     rel.res 1e-8 in complex128 and with complex64 values inside complex128
-    residual replacement."""
+    residual replacement.  The disk's nodes are numbered in horizontal bands
+    (ILU level depth ~1200); numbered ring by ring, every row of the lower
+    triangle would depend on the previous one and the sweeps would be a
+    200k-step chain."""
     from delfem_b200 import lib, meshes
-    m = meshes.unit_disk_tri(258)
+    m = meshes.unit_disk_tri(258, numbering="bands")
     G = lib.Mesh(ctx, m.coord, m.elem, m.bnd)
     rp, ci = G.pattern()
     A = lib.Matrix(ctx, rp, ci, 1, lib.COMPLEX)
@@ -381,11 +391,11 @@ def run_c5(ctx, torch, dev, timed):
 
     def plain():
         r.copy_(b)
-        return lib.solve_pcocg(A, M, r, x, tol=1e-8, maxit=20000)
+        return lib.solve_pcocg(A, M, r, x, tol=1e-8, maxit=C5_MAXIT)
 
     def mixed():
         r.copy_(b)
-        return lib.solve_pcocg_mixed(A, M, r, x, tol=1e-8, maxit=20000)
+        return lib.solve_pcocg_mixed(A, M, r, x, tol=1e-8, maxit=C5_MAXIT)
 
     plain()
     t_plain = timed(plain, 2)
@@ -398,7 +408,8 @@ def run_c5(ctx, torch, dev, timed):
     A.spmv(1.0, x, 0.0, y)
     torch.cuda.synchronize()
     res_m = float(torch.linalg.norm(b - y) / torch.linalg.norm(b))
-    out = {"workload": f"c5 Helmholtz k=20 unit disk, {m.nnode} nodes, complex ILU(0)-COCG to rel.res 1e-8",
+    out = {"workload": f"c5 Helmholtz k=20 unit disk, {m.nnode} nodes (band numbering), complex ILU(0)-COCG to "
+                       f"rel.res 1e-8", "sweep_mode": M.sweep,
            "complex128_s": t_plain, "iterations": it, "status": rc,
            "complex64_inner_s": t_mixed, "complex64_iterations": it_m, "complex64_status": rc_m,
            "complex64_speedup": t_plain / t_mixed, "complex64_true_rel_residual": res_m,

@@ -154,6 +154,18 @@ int dfm_ctx_set_wait_limit(dfm_ctx c, unsigned long long ns) {
   return DFM_OK;
 }
 
+int dfm_ctx_set_mixed_operator(dfm_ctx c, int fp32) {
+  if (!c || (fp32 != 0 && fp32 != 1)) return DFM_ERR_INVALID;
+  c->mixed_op32 = fp32;
+  return DFM_OK;
+}
+
+int dfm_ctx_get_mixed_operator(dfm_ctx c, int* fp32) {
+  if (!c || !fp32) return DFM_ERR_INVALID;
+  *fp32 = c->mixed_op32;
+  return DFM_OK;
+}
+
 int dfm_ctx_take_error(dfm_ctx c, int* code, int* where) {
   if (!c) return DFM_ERR_INVALID;
   DevStatus h = {};

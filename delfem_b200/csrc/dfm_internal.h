@@ -62,6 +62,7 @@ struct dfm_ctx_s {
   cudaStream_t stream = nullptr;
   DevStatus* d_status = nullptr;
   unsigned long long wait_ns = 2000000000ull;
+  int mixed_op32 = 0;                       // mixed-precision solves: FP32 operator values
   double* d_part = nullptr;                 // 8 partial arrays of kMaxBlocks doubles
   dfm::KrylovScalars* d_scal = nullptr;
   dfm::KrylovScalars* h_scal = nullptr;     // pinned mirror

@@ -788,7 +788,7 @@ int ilu_prepare(dfm_ilu M, bool f32) {
   if (!M->d_foff32) DFM_CUDA_TRY(cudaMalloc(&M->d_foff32, std::max<size_t>(no, 1) * sizeof(float)));
   int rc = to_f32(M->ctx, M->d_foff, M->d_foff32, no);
   if (rc) return rc;
-  if (M->sweep == 3 && M->vt == DFM_REAL) {
+  if (M->sweep == 3) {
     // FP32 plans with the FP64 plans' ranges and lanes
     for (int f = 0; f < 2; f++) {
       SweepPlan& P64 = f ? M->plan_b : M->plan_f;
@@ -848,7 +848,8 @@ int ilu_autotune(dfm_ilu M) {
   }
   // range-partitioned schedule: every CTA count whose slice fits in shared memory,
   // then, at the best count, merged level pairs and the barrier-free kernel
-  if (M->vt == DFM_REAL) {
+  // (complex matrices run as real 2x2 blocks)
+  {
     sweep_plan_free(&M->plan_f);
     sweep_plan_free(&M->plan_b);
     SweepPlan best_f, best_b;  // owned here until the end
@@ -949,7 +950,6 @@ int ilu_autotune(dfm_ilu M) {
 }
 
 int ilu_set_ranges(dfm_ilu M, int G, bool merge) {
-  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
   SweepPlan pf, pb;
   int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge);
   if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge);

@@ -16,14 +16,18 @@
 // later kernel needs is written by block 0 of the producer and read by the
 // consumer kernel only, never within the kernel that writes it.
 //
-// Mixed precision (dfm_solve_pcg_mixed): the PCG recurrences run with the FP32
-// copies of A's values and of L / D^-1 U (D^-1 and every vector, dot and
-// scalar stay FP64), inside FP64 iterative refinement done as residual
-// replacement: every kIterPerGraph-th iteration, and whenever the recursive
-// residual meets the tolerance, r is replaced by the true b - A x computed
-// with the FP64 values.  Only a true residual below the tolerance ends the
-// solve.  Unlike restarting an inner solve per refinement step, this keeps
-// the Krylov space across refinements.
+// Mixed precision (dfm_solve_pcg_mixed): the preconditioner runs with the FP32
+// copies of L / D^-1 U (D^-1 and every vector, dot and scalar stay FP64), and
+// the recurrences' SpMV with A's FP64 values or, when the context asks for it
+// (mixed_op32), with FP32 copies, inside FP64 iterative refinement done as
+// residual replacement: every kIterPerGraph-th iteration, and whenever the
+// recursive residual meets the tolerance, r is replaced by the true b - A x
+// computed with the FP64 values.  Only a true residual below the tolerance
+// ends the solve.  Unlike restarting an inner solve per refinement step, this
+// keeps the Krylov space across refinements.  An FP32 operator perturbs A by
+// ~2^-24 |A|, so its search directions lose A-conjugacy on systems with
+// cond(A) 2^-24 not << 1 (3-D elasticity: ~9x the iterations), hence the
+// FP64 default.
 //
 // Partial slots: 0,1 SpMV dots; 2 (r, r); 3,4 preconditioned dots.
 #include <algorithm>
@@ -363,7 +367,7 @@ struct SolvePlan {
   cudaGraphExec_t exec = nullptr;
   bool graph_failed = false;
   // capture key: everything the captured kernel arguments depend on
-  int key_sweep = -1, key_lanes = -1;
+  int key_sweep = -1, key_lanes = -1, key_op32 = -1;
   unsigned key_gen = ~0u;
   unsigned long long key_wait = 0;
 };
@@ -448,7 +452,7 @@ static int enqueue_pcg_mixed(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* 
   const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
   double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *z = P->v[kVecZ], *y = P->v[kVecY];
   SpmvOpts o;
-  o.f32 = true;
+  o.f32 = c->mixed_op32 != 0;
   int rc = spmv_launch(A, 1.0, p, 0.0, z, c->part(0), gv, sc, A->lanes, o);
   if (rc) return rc;
   k_pcg_update_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv, z, p,
@@ -533,7 +537,7 @@ static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, b
   double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *w = P->v[kVecZ], *y = P->v[kVecY];
   double* Ap = P->v[kVecQ];
   SpmvOpts o;
-  o.f32 = f32;
+  o.f32 = f32 && c->mixed_op32 != 0;
   int rc = spmv_launch(A, 1.0, p, 0.0, Ap, c->part(0), gv, sc, A->lanes, o);  // (p, Ap) re/im in slots 0/1
   if (rc) return rc;
   k_cocg_xr<<<gv, kVecThreads, 0, c->stream>>>(A->N, sc, c->part(0), gv, c->part(3), gs, c->part(2), gv,
@@ -607,9 +611,10 @@ static void ensure_graph(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
   dfm_ctx c = A->ctx;
   const int lanes_key = A->lanes * 2 + A->spmv_kind;
   const bool same = P->key_sweep == M->sweep && P->key_lanes == lanes_key && P->key_gen == M->plan_gen &&
-                    P->key_wait == c->wait_ns;
+                    P->key_wait == c->wait_ns && P->key_op32 == c->mixed_op32;
   if (!same) {
     plan_drop_graph(P);
+    P->key_op32 = c->mixed_op32;
     P->key_sweep = M->sweep;
     P->key_lanes = lanes_key;
     P->key_gen = M->plan_gen;
@@ -643,7 +648,7 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
   if (rc) return rc;
   if ((rc = ilu_autotune(M))) return rc;
   const bool f32 = is_mixed(method);
-  if (f32 && (rc = mat_make_f32(A))) return rc;
+  if (f32 && c->mixed_op32 && (rc = mat_make_f32(A))) return rc;
   if ((rc = ilu_prepare(M, f32))) return rc;
   SolvePlan* P = nullptr;
   if ((rc = plan_of(M, method, &P))) return rc;

@@ -236,15 +236,19 @@ static void launch_elem(dfm_mat A, int lanes, int grid, cudaStream_t s, double a
 // k*gridDim.x); for each, thread 0 issues four 1-D bulk copies (values,
 // column indices, diagonal blocks, row pointers; no multicast) into a stage
 // of a shared-memory ring several tiles ahead, completing on the stage's
-// mbarrier.  Lane groups then read a row's blocks from shared memory element
-// by element (consecutive lanes, consecutive doubles) and gather x through
-// L1/L2, so the value stream never occupies the load/store units.  A copy
+// mbarrier.  The value stream thus reaches shared memory as whole contiguous
+// lines, instead of as the scattered per-lane 8-byte pieces of the
+// lane-per-block kernel (whose every load instruction touches ~32 sectors).
+// Lane groups then take a row each, lane j the row's blocks j, j+LPR, ... (the
+// diagonal block last), reading b*b values from shared memory and gathering b
+// entries of x through L1/L2; with 1024 threads a tile's rows are covered in
+// about one pass, so a tile costs one round of x-gather latency.  A copy
 // starts at the 16-byte boundary below its first byte and is rounded up to 16
 // bytes (the arrays carry kArrayPad spare elements); the offsets of the first
 // element are kept per stage.
-constexpr unsigned kTileRows = 128;
-constexpr unsigned kTileValBytes = 24 * 1024;
-constexpr int kTmaThreads = 256;
+constexpr unsigned kTileRows = 256;
+constexpr unsigned kTileValBytes = 48 * 1024;
+constexpr int kTmaThreads = 1024;
 
 DFM_DEVINL unsigned sp_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 DFM_DEVINL void sp_mbar_init(uint64_t* bar, unsigned count) {
@@ -387,26 +391,27 @@ k_spmv_tma(TmaArgs<TV> a) {
     for (unsigned i = h.r0 + g; i < h.r1; i += ng) {  // group-uniform
       const unsigned li = i - h.r0;
       const unsigned b0 = rp[li] - h.s0, b1 = rp[li + 1] - h.s0;
-      const unsigned ne = (b1 - b0 + 1) * BB;  // off-diagonal blocks, then the diagonal block
+      const unsigned nb = b1 - b0;  // off-diagonal blocks; index nb is the diagonal block
       double acc[B];
 #pragma unroll
       for (int r = 0; r < B; r++) acc[r] = 0.0;
-      for (unsigned e = lane; e < ne; e += LPR) {
-        const unsigned blk = e / BB, q = e - blk * BB;
-        const unsigned rr = q / B, c = q - rr * B;
-        double v;
+      for (unsigned k = lane; k <= nb; k += LPR) {
+        const TV* m;
         unsigned col;
-        if (blk < b1 - b0) {
-          v = (double)vals[(size_t)(b0 + blk) * BB + q];
-          col = cols[b0 + blk];
+        if (k < nb) {
+          m = vals + (size_t)(b0 + k) * BB;
+          col = cols[b0 + k];
         } else {
-          v = (double)dg[(size_t)li * BB + q];
+          m = dg + (size_t)li * BB;
           col = i;
         }
-        const double xv = __ldg(a.x + (size_t)col * B + c);
+        double xv[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = __ldg(a.x + (size_t)col * B + c);
 #pragma unroll
         for (int r = 0; r < B; r++)
-          if (rr == (unsigned)r) acc[r] += v * xv;
+#pragma unroll
+          for (int c = 0; c < B; c++) acc[r] += (double)m[r * B + c] * xv[c];
       }
 #pragma unroll
       for (int r = 0; r < B; r++)

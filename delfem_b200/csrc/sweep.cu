@@ -252,7 +252,34 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
 }
 
 // --------------------------------------------------------------- kernel
-template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT, bool PIPE>
+// Block partial of the CTA's share of (rdot, out) from its finished slice X.
+// DOT 1: real dot over len*B entries; DOT 2: complex matrices run as real 2x2
+// blocks (re, im per row), the unconjugated sum of rdot_i out_i with the real
+// and imaginary parts in part[] and part[kMaxBlocks + ...].
+template <int B, int DOT, typename TX>
+DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0, unsigned len, bool alive,
+                          double* part) {
+  if constexpr (DOT == 2) {
+    static_assert(B == 2, "complex rows are 2x2 real blocks");
+    double re = 0.0, im = 0.0;
+    if (alive)
+      for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
+        const double rr = (double)rdot[(size_t)(a0 + k) * 2], ri = (double)rdot[(size_t)(a0 + k) * 2 + 1];
+        const double xr = (double)X[2 * k], xi = (double)X[2 * k + 1];
+        re += rr * xr - ri * xi;
+        im += rr * xi + ri * xr;
+      }
+    block_partial<kSweepThreads>(re, part);
+    block_partial<kSweepThreads>(im, part + kMaxBlocks);
+  } else {
+    double dacc = 0.0;
+    if (alive)
+      for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) dacc += (double)rdot[(size_t)a0 * B + k] * (double)X[k];
+    block_partial<kSweepThreads>(dacc, part);
+  }
+}
+
+template <int B, int LPR, typename TV, typename TX, bool FWD, int DOT, bool PIPE>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
                const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
@@ -460,12 +487,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
     }
   }
   }
-  if (DOT) {  // (rdot, out) over this CTA's range, from the finished slice
-    double dacc = 0.0;
-    for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
-      dacc += (double)rdot[(size_t)a0 * B + k] * (double)X[k];
-    block_partial<kSweepThreads>(dacc, part);
-  }
+  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, true, part);  // (rdot, out) over this CTA's range
   // after an aborted wait, copies already requested must land before the CTA exits
   if (threadIdx.x == kStageThread && !s_alive) {
     for (unsigned q = q0; q < issued_end; q++) {
@@ -509,7 +531,7 @@ DFM_DEVINL TX poll_local(const TX* p, volatile int* alive, DevStatus* st, uint64
   }
 }
 
-template <int B, int LPR, typename TV, typename TX, bool FWD, bool DOT>
+template <int B, int LPR, typename TV, typename TX, bool FWD, int DOT>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
                   const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
@@ -692,12 +714,7 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
     __syncwarp(gmask);
   }
   __syncthreads();
-  if (DOT) {
-    double dacc = 0.0;
-    if (s_alive)
-      for (unsigned e = threadIdx.x; e < len * B; e += blockDim.x) dacc += (double)rdot[(size_t)a0 * B + e] * (double)X[e];
-    block_partial<kSweepThreads>(dacc, part);
-  }
+  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, s_alive != 0, part);
   // every stage's last issued copy must have landed before the CTA exits
   if (threadIdx.x == 0)
     for (int s2 = 0; s2 < nstage; s2++) {
@@ -714,12 +731,29 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
 // the second level of a pair are the products L_ij D_j^-1 (forward input
 // terms), U'_ij (backward input terms) and the fill blocks
 // F_ik - sum_j F_ij (D_j^-1) F_jk.  One thread per packed block; D^-1 rows of the
-// forward sweep are copied alongside.
-template <int B, typename TV>
+// forward sweep are copied alongside.  CPLX: the factor holds complex scalars
+// (re, im), packed as the real 2x2 blocks [re -im; im re] (B = 2), whose
+// products are the complex products.
+template <int B, bool CPLX>
+DFM_DEVINL void load_factor_blk(const double* __restrict__ src, size_t k, double* v) {
+  if constexpr (CPLX) {
+    const double re = src[2 * k], im = src[2 * k + 1];
+    v[0] = re;
+    v[1] = -im;
+    v[2] = im;
+    v[3] = re;
+  } else {
+#pragma unroll
+    for (int e = 0; e < B * B; e++) v[e] = src[k * (B * B) + e];
+  }
+}
+
+template <int B, typename TV, bool CPLX>
 __global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned nchunks,
                                  const uint4* __restrict__ recipe, const uint4* __restrict__ terms,
                                  const double* __restrict__ fdiag, const double* __restrict__ foff, char* blob,
                                  int with_dinv) {
+  static_assert(!CPLX || B == 2, "complex scalars pack as 2x2 blocks");
   constexpr int BB = B * B;
   constexpr unsigned NONE = 0xffffffffu;
   for (unsigned q = blockIdx.x; q < nchunks; q += gridDim.x) {
@@ -729,16 +763,19 @@ __global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned 
     for (unsigned k = threadIdx.x; k < cd.nblk_pad; k += blockDim.x) {
       const uint4 rc = recipe[cd.blk0 + k];
       double v[BB];
+      if (rc.x != NONE) {
+        load_factor_blk<B, CPLX>(foff, rc.x, v);
+      } else {
 #pragma unroll
-      for (int e = 0; e < BB; e++) v[e] = (rc.x != NONE) ? foff[(size_t)rc.x * BB + e] : 0.0;
+        for (int e = 0; e < BB; e++) v[e] = 0.0;
+      }
       const double sg = rc.w ? -1.0 : 1.0;
       for (unsigned t = rc.y; t < rc.z; t++) {
         const uint4 tm = terms[t];
-        double a[BB], m[BB];
-#pragma unroll
-        for (int e = 0; e < BB; e++) a[e] = foff[(size_t)tm.x * BB + e];
+        double a[BB], m[BB], d[BB];
+        load_factor_blk<B, CPLX>(foff, tm.x, a);
         if (tm.y != NONE) {  // a = a * D_j^-1
-          const double* d = fdiag + (size_t)tm.y * BB;
+          load_factor_blk<B, CPLX>(fdiag, tm.y, d);
 #pragma unroll
           for (int r = 0; r < B; r++)
 #pragma unroll
@@ -752,7 +789,8 @@ __global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned 
           for (int e = 0; e < BB; e++) a[e] = m[e];
         }
         if (tm.z != NONE) {  // a = a * F[s2]
-          const double* f = foff + (size_t)tm.z * BB;
+          double f[BB];
+          load_factor_blk<B, CPLX>(foff, tm.z, f);
 #pragma unroll
           for (int r = 0; r < B; r++)
 #pragma unroll
@@ -774,8 +812,12 @@ __global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned 
     if (with_dinv) {
       const uint4* rd = reinterpret_cast<const uint4*>(base + 32);
       double* dinv = reinterpret_cast<double*>(base + cd.dinv_off);
-      for (unsigned e = threadIdx.x; e < cd.nrows * (unsigned)BB; e += blockDim.x)
-        dinv[e] = fdiag[((size_t)cd.row0 + rd[e / BB].x) * BB + e % BB];
+      for (unsigned r = threadIdx.x; r < cd.nrows; r += blockDim.x) {
+        double v[BB];
+        load_factor_blk<B, CPLX>(fdiag, (size_t)cd.row0 + rd[r].x, v);
+#pragma unroll
+        for (int e = 0; e < BB; e++) dinv[(size_t)r * BB + e] = v[e];
+      }
     }
   }
 }
@@ -794,7 +836,7 @@ void sweep_plan_free(SweepPlan* P) {
 
 int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge) {
   const unsigned N = M->N;
-  const unsigned b = M->b;
+  const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks
   const unsigned bb = b * b;
   const unsigned vblk = (unsigned)val_bytes * bb;     // bytes per packed block
   const unsigned drow = fwd ? 8u * bb : 0u;           // D^-1 bytes per row (FP64)
@@ -803,7 +845,6 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   const std::vector<unsigned>& dia = M->h_diaind;
   const std::vector<unsigned>& lev = fwd ? M->lev_f : M->lev_b;
   sweep_plan_free(P);
-  if (M->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
   if (N >= 0x40000000u) return DFM_ERR_UNSUPPORTED;  // operand encodings use the top two bits
   if (G < 1) G = 1;
   if ((unsigned)G > std::max(N, 1u)) G = std::max(N, 1u);
@@ -1025,13 +1066,17 @@ int sweep_plan_refresh(dfm_ilu M, SweepPlan* P) {
   const int grid = (int)std::min<unsigned>(P->nchunks, (unsigned)M->ctx->nsm * 8);
   const int wd = P->fwd ? 1 : 0;
   cudaStream_t s = M->ctx->stream;
-#define DFM_GATHER(BV, TV)                                                                                    \
-  k_gather_recipes<BV, TV><<<grid, 128, 0, s>>>(P->d_chunks, P->nchunks, P->d_recipe, P->d_terms, M->d_fdiag,  \
-                                                M->d_foff, P->d_blob, wd)
-  if (P->val_bytes == 8) {
-    if (M->b == 1) DFM_GATHER(1, double); else if (M->b == 2) DFM_GATHER(2, double); else DFM_GATHER(3, double);
+#define DFM_GATHER(BV, TV, CX)                                                                                 \
+  k_gather_recipes<BV, TV, CX><<<grid, 128, 0, s>>>(P->d_chunks, P->nchunks, P->d_recipe, P->d_terms, M->d_fdiag, \
+                                                    M->d_foff, P->d_blob, wd)
+  if (M->vt == DFM_COMPLEX) {
+    if (P->val_bytes == 8) DFM_GATHER(2, double, true); else DFM_GATHER(2, float, true);
+  } else if (P->val_bytes == 8) {
+    if (M->b == 1) DFM_GATHER(1, double, false); else if (M->b == 2) DFM_GATHER(2, double, false);
+    else DFM_GATHER(3, double, false);
   } else {
-    if (M->b == 1) DFM_GATHER(1, float); else if (M->b == 2) DFM_GATHER(2, float); else DFM_GATHER(3, float);
+    if (M->b == 1) DFM_GATHER(1, float, false); else if (M->b == 2) DFM_GATHER(2, float, false);
+    else DFM_GATHER(3, float, false);
   }
 #undef DFM_GATHER
   DFM_CUDA_TRY(cudaGetLastError());
@@ -1039,9 +1084,10 @@ int sweep_plan_refresh(dfm_ilu M, SweepPlan* P) {
   return DFM_OK;
 }
 
-template <int B, int LPR, typename TV, typename TX, bool FWD>
+template <int B, int LPR, typename TV, typename TX, bool FWD, bool CPLX>
 static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX* out, const TX* rdot,
                                  double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  constexpr int DK = CPLX ? 2 : 1;  // fused dot kind
   dfm_ctx c = M->ctx;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P->G);
@@ -1057,7 +1103,7 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
     if (!P->nb_ok) return cudaErrorInvalidValue;
     const size_t smem = P->smem + (((size_t)P->max_cta_chunks + 1) * 4 + 15) / 16 * 16;
     cfg.dynamicSmemBytes = smem;
-    auto fn = part ? k_sweep_ranges_nb<B, LPR, TV, TX, FWD, true> : k_sweep_ranges_nb<B, LPR, TV, TX, FWD, false>;
+    auto fn = part ? k_sweep_ranges_nb<B, LPR, TV, TX, FWD, DK> : k_sweep_ranges_nb<B, LPR, TV, TX, FWD, 0>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
@@ -1065,9 +1111,8 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
                               P->x_bytes, P->max_cta_chunks, in, out, rdot, part, sc, rr_part, rr_n, c->d_status,
                               (uint64_t)c->wait_ns);
   }
-  auto fn = part ? (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, true, true> : k_sweep_ranges<B, LPR, TV, TX, FWD, true, false>)
-                 : (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, false, true>
-                            : k_sweep_ranges<B, LPR, TV, TX, FWD, false, false>);
+  auto fn = part ? (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, DK, true> : k_sweep_ranges<B, LPR, TV, TX, FWD, DK, false>)
+                 : (P->pipe ? k_sweep_ranges<B, LPR, TV, TX, FWD, 0, true> : k_sweep_ranges<B, LPR, TV, TX, FWD, 0, false>);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
   if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
@@ -1075,14 +1120,31 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
                             P->x_bytes, in, out, rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
 }
 
-template <int B, typename TV, typename TX, bool FWD>
+template <int B, typename TV, typename TX, bool FWD, bool CPLX = false>
 static cudaError_t launch_ranges_lpr(dfm_ilu M, const SweepPlan* P, const TX* in, TX* out, const TX* rdot,
                                      double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
   switch (P->lpr) {
-    case 1: return launch_ranges<B, 1, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-    case 2: return launch_ranges<B, 2, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-    case 4: return launch_ranges<B, 4, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-    default: return launch_ranges<B, 8, TV, TX, FWD>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 1: return launch_ranges<B, 1, TV, TX, FWD, CPLX>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 2: return launch_ranges<B, 2, TV, TX, FWD, CPLX>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 4: return launch_ranges<B, 4, TV, TX, FWD, CPLX>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    default: return launch_ranges<B, 8, TV, TX, FWD, CPLX>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  }
+}
+
+template <typename TV>
+static cudaError_t launch_ranges_b(dfm_ilu M, bool fwd, const SweepPlan* P, const double* in, double* out,
+                                   const double* rdot, double* part, KrylovScalars* sc, const double* rr_part,
+                                   int rr_n) {
+  if (M->vt == DFM_COMPLEX)  // complex scalars run as real 2x2 blocks [re -im; im re]
+    return fwd ? launch_ranges_lpr<2, TV, double, true, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+               : launch_ranges_lpr<2, TV, double, false, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  switch (M->b) {
+    case 1: return fwd ? launch_ranges_lpr<1, TV, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                       : launch_ranges_lpr<1, TV, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 2: return fwd ? launch_ranges_lpr<2, TV, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                       : launch_ranges_lpr<2, TV, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    default: return fwd ? launch_ranges_lpr<3, TV, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+                        : launch_ranges_lpr<3, TV, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
   }
 }
 
@@ -1094,32 +1156,8 @@ int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, cons
     int rc = sweep_plan_refresh(M, P);
     if (rc) return rc;
   }
-  if (M->vt == DFM_COMPLEX) return DFM_ERR_UNSUPPORTED;
-  cudaError_t e;
-  if (f32) {
-    switch (M->b) {
-      case 1: e = fwd ? launch_ranges_lpr<1, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                      : launch_ranges_lpr<1, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-        break;
-      case 2: e = fwd ? launch_ranges_lpr<2, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                      : launch_ranges_lpr<2, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-        break;
-      default: e = fwd ? launch_ranges_lpr<3, float, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                       : launch_ranges_lpr<3, float, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
-        break;
-    }
-    DFM_CUDA_TRY(e);
-    return DFM_OK;
-  }
-  switch (M->b) {
-    case 1: e = fwd ? launch_ranges_lpr<1, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                    : launch_ranges_lpr<1, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
-    case 2: e = fwd ? launch_ranges_lpr<2, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                    : launch_ranges_lpr<2, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
-    default: e = fwd ? launch_ranges_lpr<3, double, double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
-                     : launch_ranges_lpr<3, double, double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n); break;
-  }
-  DFM_CUDA_TRY(e);
+  DFM_CUDA_TRY(f32 ? launch_ranges_b<float>(M, fwd, P, in, out, rdot, part, sc, rr_part, rr_n)
+                   : launch_ranges_b<double>(M, fwd, P, in, out, rdot, part, sc, rr_part, rr_n));
   return DFM_OK;
 }
 

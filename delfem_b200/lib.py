@@ -33,6 +33,8 @@ PROTOS = {
     "dfm_ctx_set_stream": (_i, [_vp, _vp]),
     "dfm_ctx_sync": (_i, [_vp]),
     "dfm_ctx_set_wait_limit": (_i, [_vp, C.c_ulonglong]),
+    "dfm_ctx_set_mixed_operator": (_i, [_vp, _i]),
+    "dfm_ctx_get_mixed_operator": (_i, [_vp, _ip]),
     "dfm_ctx_take_error": (_i, [_vp, _ip, _ip]),
     "dfm_ctx_wait_selftest": (_i, [_vp, C.c_ulonglong]),
     "dfm_buf_alloc": (_i, [_vp, C.c_size_t, C.POINTER(_vp)]),
@@ -180,6 +182,17 @@ class Context:
 
     def wait_selftest(self, ns: int) -> int:
         return lib().dfm_ctx_wait_selftest(self.h, ns)
+
+    @property
+    def mixed_operator(self) -> int:
+        """Operator values of the mixed-precision solves: 0 FP64, 1 FP32."""
+        v = C.c_int()
+        check(lib().dfm_ctx_get_mixed_operator(self.h, C.byref(v)))
+        return v.value
+
+    @mixed_operator.setter
+    def mixed_operator(self, fp32: int):
+        check(lib().dfm_ctx_set_mixed_operator(self.h, int(fp32)), "dfm_ctx_set_mixed_operator")
 
 
 class Matrix:

@@ -113,9 +113,17 @@ def box_tet(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 0.2, lz: flo
     return Mesh(coord, elem, bnd)
 
 
-def unit_disk_tri(nring: int) -> Mesh:
+def unit_disk_tri(nring: int, numbering: str = "rings") -> Mesh:
     """Unit disk: centre node plus rings k = 1..nring of 6k nodes at radius
-    k/nring; 6 nring^2 triangles; the outer circle as 6 nring bars."""
+    k/nring; 6 nring^2 triangles; the outer circle as 6 nring bars.
+
+    numbering "rings": centre, then ring by ring in angle order.  Every node of
+    a ring is adjacent to the one before it and a ring's first node to the
+    previous ring's last, so the lower triangle of the natural ordering is one
+    chain: ILU(0) level depth = nnode (fully sequential sweeps).
+    numbering "bands": the same nodes and triangles renumbered row-major in
+    horizontal bands one ring spacing high (by band, then x), like a
+    structured grid: level depth O(nring)."""
     starts = [0, 1]
     for k in range(1, nring + 1):
         starts.append(starts[-1] + 6 * k)
@@ -155,6 +163,14 @@ def unit_disk_tri(nring: int) -> Mesh:
     o = starts[nring]
     m = 6 * nring
     bnd = np.stack([o + np.arange(m), o + (np.arange(m) + 1) % m], axis=1).astype(np.int32)
+    if numbering == "bands":
+        band = np.floor((coord[:, 1] + 1.0) * nring + 0.5).astype(np.int64)
+        old = np.lexsort((coord[:, 0], band))  # new -> old
+        new = np.empty(nnode, np.int64)
+        new[old] = np.arange(nnode)
+        coord, elem, bnd = coord[old], new[elem].astype(np.int32), new[bnd].astype(np.int32)
+    elif numbering != "rings":
+        raise ValueError(f"unknown numbering {numbering!r}")
     return Mesh(coord, elem, bnd)
 
 

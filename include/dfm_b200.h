@@ -70,6 +70,10 @@ DFM_API int dfm_ctx_set_stream(dfm_ctx ctx, void* stream);
 DFM_API int dfm_ctx_sync(dfm_ctx ctx);
 /* Time limit of every device-side spin-wait (default 2 s). */
 DFM_API int dfm_ctx_set_wait_limit(dfm_ctx ctx, unsigned long long ns);
+/* Operator values of the mixed-precision solves (dfm_solve_pcg_mixed,
+ * dfm_solve_pcocg_mixed): 0 = FP64 (default), 1 = FP32 copies. */
+DFM_API int dfm_ctx_set_mixed_operator(dfm_ctx ctx, int fp32);
+DFM_API int dfm_ctx_get_mixed_operator(dfm_ctx ctx, int* fp32);
 /* First device-side error since the last call (code, kernel id); clears it. */
 DFM_API int dfm_ctx_take_error(dfm_ctx ctx, int* code, int* where);
 /* Failure-detection self test: one kernel waits on a flag nothing sets, under
@@ -200,7 +204,8 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * factorization: half the sequential steps, results equal to rounding), 7 and
  * 8 = 3 and 5 with the row groups in two halves taking alternate levels, the
  * idle half fetching its next row's operands before the level barrier (same
- * results as 3 and 5).  Real matrices only for 3-8. */
+ * results as 3 and 5).  Complex matrices run 3-8 as real 2x2 blocks
+ * [re -im; im re]. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all
@@ -228,20 +233,21 @@ DFM_API int dfm_solve_pbicgstab(dfm_mat A, dfm_ilu M, double* r, double* x, doub
  * r and x are interleaved (re, im). */
 DFM_API int dfm_solve_pcocg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                     unsigned* iters, double* conv);
-/* No counterpart in the reference: PCG whose recurrences use FP32 copies of
- * A's values and of the ILU(0) L / D^-1 U blocks (D^-1 pivots, vectors, dots
- * and scalars stay FP64), inside FP64 iterative refinement done as residual
- * replacement - the true residual b - A x with the FP64 values replaces the
- * recursive one every 16 iterations and whenever the latter meets tol, and
- * only a true residual below tol ends the solve.  Same arguments and
- * conventions as dfm_solve_pcg (x = 0 start, *iters 0-based); real matrices.
- * It pays where the FP32 copies keep the preconditioned operator's accuracy
- * (scalar Poisson-type systems); on stiff elasticity systems the FP32 values
- * cost iterations. */
+/* No counterpart in the reference: PCG whose ILU(0) sweeps read FP32 copies of
+ * the L / D^-1 U blocks (D^-1 pivots, vectors, dots and scalars stay FP64),
+ * inside FP64 iterative refinement done as residual replacement - the true
+ * residual b - A x with the FP64 values replaces the recursive one every 16
+ * iterations and whenever the latter meets tol, and only a true residual
+ * below tol ends the solve.  The SpMV of the recurrences uses A's FP64 values
+ * unless dfm_ctx_set_mixed_operator(ctx, 1) selects FP32 copies of them too
+ * (which pays only where cond(A) * 2^-24 << 1: on stiff systems the FP32
+ * operator loses conjugacy and costs iterations).  Same arguments and
+ * conventions as dfm_solve_pcg (x = 0 start, *iters 0-based); real matrices. */
 DFM_API int dfm_solve_pcg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                         unsigned* iters, double* conv);
-/* The same scheme for PCOCG on complex matrices: complex64 values in SpMV and
- * ILU sweeps, complex128 vectors, dots, scalars and D^-1, complex128 residual
+/* The same scheme for PCOCG on complex matrices: complex64 factor values in
+ * the ILU sweeps (and in the SpMV under dfm_ctx_set_mixed_operator(ctx, 1)),
+ * complex128 vectors, dots, scalars and D^-1, complex128 residual
  * replacement; conventions of dfm_solve_pcocg. */
 DFM_API int dfm_solve_pcocg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                           unsigned* iters, double* conv);

@@ -44,8 +44,8 @@ def solid3d(nx, ny, nz):
     return m, S
 
 
-def helmholtz(nring):
-    m = meshes.unit_disk_tri(nring)
+def helmholtz(nring, numbering="rings"):
+    m = meshes.unit_disk_tri(nring, numbering=numbering)
     rp, ci = P.pattern(m.nnode, m.elem)
     S = P.System(rp, ci, 1, cplx=True)
     S.asm_helmholtz(m, WAVE_LENGTH)

@@ -30,6 +30,7 @@ SYSTEMS = {
     "random_b2": lambda: cases.random_spd_like(200, 2, 2),
     "random_b3": lambda: cases.random_spd_like(150, 3, 3),
     "helmholtz": lambda: cases.helmholtz(10)[1],
+    "helmholtz_bands": lambda: cases.helmholtz(14, "bands")[1],
 }
 
 
@@ -77,8 +78,6 @@ def test_ilu_factor_bit_exact(ctx, name):
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
-    if sweep >= 3 and S.cplx:
-        pytest.skip("range-partitioned sweep is real-only")
     A = make(ctx, S)
     M = lib.ILU(A)
     M.factor()
@@ -116,7 +115,7 @@ def test_pcg_matches_oracle(ctx, name, sweep):
     assert conv < 1e-10
 
 
-@pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1"])
+@pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1", "helmholtz_bands"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
 @pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8])
 def test_range_sweep_cta_counts(ctx, name, ctas, mode):

@@ -23,9 +23,17 @@ SYSTEMS = {
 }
 
 
+@pytest.fixture(params=[0, 1], ids=["fp64_operator", "fp32_operator"])
+def op32(ctx, request):
+    ctx.mixed_operator = request.param
+    assert ctx.mixed_operator == request.param
+    yield request.param
+    ctx.mixed_operator = 0
+
+
 @pytest.mark.parametrize("name", list(SYSTEMS))
 @pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7])
-def test_mixed_true_residual_and_solution(ctx, name, sweep):
+def test_mixed_true_residual_and_solution(ctx, op32, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
     ns, fd, fo = S.ilu0()
@@ -46,8 +54,14 @@ def test_mixed_true_residual_and_solution(ctx, name, sweep):
     assert conv < tol
     err = np.linalg.norm(xg - ref["x"]) / np.linalg.norm(ref["x"])
     assert err <= 1e-7, err
-    # returned r is the final (true) residual
-    assert np.allclose(r.cpu().numpy(), res, rtol=0, atol=1e-12 * np.linalg.norm(S.rhs))
+    if not op32:  # FP64 operator: no loss of conjugacy in A; the FP32 factor alone costs
+        # up to ~50% more iterations (L and D^-1 U round separately, so the preconditioner
+        # is not exactly symmetric; elasticity's ill-conditioned factors amplify that)
+        assert it <= 2 * ref["iters"] + 5, (it, ref["iters"])
+    # returned r is the final (true) residual, up to the rounding of b - A x in
+    # another summation order: |dr| <= c eps (|b| + |A| |x|)
+    absAx = S.spmv(1.0, np.abs(xg), 0.0, np.zeros_like(S.rhs), diag=np.abs(S.diag), off=np.abs(S.off))
+    assert (np.abs(r.cpu().numpy() - res) <= 1e-13 * (np.abs(S.rhs) + absAx)).all()
 
 
 def test_mixed_deterministic_and_host_entry(ctx):
@@ -63,6 +77,33 @@ def test_mixed_deterministic_and_host_entry(ctx):
         assert rc == lib.OK
         out.append((x, it, conv))
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1:] == out[1][1:]
+
+
+def test_mixed_operator_switch_recaptures(ctx):
+    """Switching the operator precision between solves re-captures the graph:
+    both settings give the FP64 true residual, and the FP64 operator keeps the
+    FP64 solve's iteration count."""
+    from delfem_b200 import lib
+    S = SYSTEMS["solid3d"]()
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcg", tol=1e-10, maxit=5000)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A)
+    M.factor()
+    for op in (0, 1, 0):
+        ctx.mixed_operator = op
+        r = _dev(S.rhs)
+        x = torch.zeros_like(r)
+        rc, it, conv = lib.solve_pcg_mixed(A, M, r, x, tol=1e-10, maxit=5000)
+        assert rc == lib.OK
+        res = S.rhs - S.spmv(1.0, x.cpu().numpy(), 0.0, np.zeros_like(S.rhs))
+        assert np.linalg.norm(res) < 1e-10 * np.linalg.norm(S.rhs)
+        if op == 0:
+            assert it <= 2 * ref["iters"] + 5, (it, ref["iters"])
+    ctx.mixed_operator = 0
+    with pytest.raises(lib.DfmError):
+        ctx.mixed_operator = 2
 
 
 def test_mixed_follows_value_updates(ctx):
@@ -86,11 +127,11 @@ def test_mixed_follows_value_updates(ctx):
 
 
 @pytest.mark.parametrize("nring", [40])
-@pytest.mark.parametrize("sweep", [1, 2])
-def test_cocg_mixed_true_residual(ctx, nring, sweep):
+@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7])
+def test_cocg_mixed_true_residual(ctx, op32, nring, sweep):
     """complex64 values inside complex128 residual replacement (Helmholtz)."""
     from delfem_b200 import lib
-    m, S = cases.helmholtz(nring)
+    m, S = cases.helmholtz(nring, "bands")
     ns, fd, fo = S.ilu0()
     tol = 1e-8
     ref = S.solve(fd, fo, method="pcocg", tol=tol, maxit=5000)

@@ -96,11 +96,14 @@ def test_pbicgstab_host_entry(ctx):
     assert rc == lib.OK and _rel(x, ref["x"]) <= X_TOL
 
 
-@pytest.mark.parametrize("nring", [40, 60])
-@pytest.mark.parametrize("sweep", [1, 2])
-def test_pcocg_matches_oracle(ctx, nring, sweep):
+PCOCG_CASES = [(40, "rings", sw) for sw in (1, 2, 3)] + [(60, "rings", sw) for sw in (1, 2)] + \
+    [(60, "bands", sw) for sw in range(1, 9)]
+
+
+@pytest.mark.parametrize("nring,numbering,sweep", PCOCG_CASES)
+def test_pcocg_matches_oracle(ctx, nring, numbering, sweep):
     from delfem_b200 import lib
-    m, S = cases.helmholtz(nring)
+    m, S = cases.helmholtz(nring, numbering)
     ns, fd, fo = S.ilu0()
     ref = S.solve(fd, fo, method="pcocg", tol=1e-10, maxit=5000)
     assert ref["ok"] and ref["iters"] < 5000
