@@ -18,10 +18,11 @@ Beside it, in the same JSON line:
            [32, 512], per-element kappa ~ lognormal(0, 1)) in one batched solve
            against a loop of plain single-instance solves (timed on a
            size-stratified sample of the instances and scaled)
+  ilu1     the same c2 solve with ILU(1) (CPreconditioner_ILU::SetFillInLevel(1))
   spmv     SpMV HBM throughput against the measured peak
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--skip-batched] [--skip-mixed] [--no-cpu-baseline]
+                    [--skip-batched] [--skip-mixed] [--skip-iluk] [--no-cpu-baseline]
     python bench.py --profile-run      # short c2 workload for ncu captures
 
 
@@ -490,8 +491,8 @@ def run_ours(args, rank, world):
 
     # ---- kernel breakdown (CUDA events on the library stream) ----
     y = torch.empty_like(b_dev)
-    t_spmv = timed(lambda: A.spmv(1.0, x, 0.0, y), 20)
-    t_apply = timed(lambda: M.apply(r, y), 10)
+    t_spmv = A.time_spmv(x, y, 50)
+    t_apply = M.time_apply(r, y, 20)
     t_factor = timed(lambda: M.factor(), 3)
     B_spmv, B_ilu, B_it = alg_bytes(N, ncrs, b)
     peaks_p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -538,6 +539,33 @@ def run_ours(args, rank, world):
                  "iterations": it_m + 1, "plain_iterations": n_it, "status": rc_m,
                  "true_rel_residual": true_rel_residual(xm),
                  "rel_err_vs_fp64_solution": float(torch.linalg.norm(xm - x64) / torch.linalg.norm(x64))}
+
+    # ---- ILU(1) on the same system (SetFillInLevel(1), the reference's default for solids) ----
+    iluk = {}
+    if not args.skip_iluk and world == 1:
+        t0 = time.perf_counter()
+        M1 = lib.ILU(A, fill_level=1)
+        t_sym = time.perf_counter() - t0
+        x1 = torch.zeros_like(b_dev)
+
+        def k1step():
+            M1.factor()
+            r.copy_(b_dev)
+            torch.cuda.synchronize()
+            return lib.solve_pcg(A, M1, r, x1, tol=TOL, maxit=20000)
+
+        k1step()
+        t_k1 = timed(k1step, max(2, min(args.steps, 3)))
+        rc_k, it_k, conv_k = k1step()
+        t_k1_apply = M1.time_apply(r, y, 10)
+        iluk = {"fill_level": 1, "factor_ncrs": M1.ncrs, "matrix_ncrs": ncrs, "symbolic_s": t_sym,
+                "solve_s": t_k1, "iterations": it_k + 1, "status": rc_k, "apply_ms": t_k1_apply * 1e3,
+                "sweep_mode": M1.sweep, "ilu0_solve_s": t_step, "ilu0_iterations": n_it,
+                "speedup_vs_ilu0": t_step / t_k1, "true_rel_residual": true_rel_residual(x1),
+                "rel_err_vs_ilu0_solution": float(torch.linalg.norm(x1 - x64) / torch.linalg.norm(x64))}
+        M1.close()
+        log(f"[bench] c2 ILU(1): factor ncrs {M1.ncrs} (A {ncrs}), {it_k + 1} iterations, {t_k1:.3f}s "
+            f"(ILU(0): {n_it}, {t_step:.3f}s)")
 
     # ---- end-to-end through the C ABI with host buffers ----
     diag_d, off_d = A.get_values()
@@ -600,6 +628,7 @@ def run_ours(args, rank, world):
                               "frac": kernels["spmv_bcrs_b3"]["frac"]},
             "kernels": kernels,
             "mixed": mixed,
+            "ilu1": iluk,
             "batched": batched,
             "c1": c1,
             "c5": c5,
@@ -621,6 +650,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-mixed", action="store_true")
+    ap.add_argument("--skip-iluk", action="store_true", help="skip the c2 ILU(1) section")
     ap.add_argument("--skip-extra", action="store_true", help="skip the c1 and c5 sections")
     ap.add_argument("--profile-run", action="store_true")
     args = ap.parse_args()

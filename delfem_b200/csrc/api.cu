@@ -16,15 +16,7 @@ int cuda_fail(cudaError_t e, const char* what) {
   return DFM_ERR_CUDA;
 }
 
-template <typename T>
-static int dalloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  DFM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
-  return DFM_OK;
-}
-
-static int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t s) {
+int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t s) {
   if (bytes == 0) return DFM_OK;
   if (!src || !dst) return DFM_ERR_INVALID;
   DFM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, where == DFM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
@@ -76,6 +68,31 @@ static unsigned make_levels(unsigned N, const std::vector<unsigned>& rowptr, con
   std::vector<unsigned> fill(lvlptr.begin(), lvlptr.end() - (nl ? 1 : 0));
   for (unsigned i = 0; i < N; i++) order[fill[lev[i]]++] = i;
   return nl;
+}
+
+// Average duration of `reps` launches of `launch` on stream s (CUDA events).
+template <typename F>
+static int time_launches(cudaStream_t s, int reps, float* ms, F launch) {
+  int rc = launch();  // untimed first launch
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  DFM_CUDA_TRY(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return DFM_ERR_CUDA;
+  }
+  cudaEventRecord(e0, s);
+  for (int k = 0; k < reps && !rc; k++) rc = launch();
+  cudaEventRecord(e1, s);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "time_launches");
+  *ms = t / (float)reps;
+  return DFM_OK;
 }
 
 }  // namespace dfm
@@ -328,7 +345,7 @@ int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes) {
 }
 
 int dfm_mat_set_spmv_kernel(dfm_mat A, int kernel) {
-  if (!A || kernel < 0 || kernel > 2) return DFM_ERR_INVALID;
+  if (!A || kernel < 0 || kernel > 3) return DFM_ERR_INVALID;
   if (kernel >= 1 && A->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
   A->spmv_kind = kernel;
   return DFM_OK;
@@ -356,6 +373,14 @@ int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, double* y) {
   return DFM_OK;
 }
 
+int dfm_time_spmv(dfm_mat A, const double* x, double* y, int reps, float* ms) {
+  if (!A || !ms || reps <= 0 || (A->N && (!x || !y))) return DFM_ERR_INVALID;
+  int rc = spmv_autotune(A);
+  if (rc) return rc;
+  return time_launches(A->ctx->stream, reps, ms,
+                       [&] { return spmv_launch(A, 1.0, x, 0.0, y, nullptr, 0, nullptr, A->lanes); });
+}
+
 // -------------------------------------------------------------------- ILU
 int dfm_ilu_create(dfm_mat A, dfm_ilu* out) {
   if (!A || !out) return DFM_ERR_INVALID;
@@ -364,6 +389,7 @@ int dfm_ilu_create(dfm_mat A, dfm_ilu* out) {
   if (!M) return DFM_ERR_NOMEM;
   M->ctx = A->ctx;
   M->A = A;
+  M->user = A;
   M->N = A->N;
   M->b = A->b;
   M->ncrs = A->ncrs;
@@ -417,6 +443,8 @@ int dfm_ilu_destroy(dfm_ilu M) {
   cudaFree(M->d_foff);
   cudaFree(M->d_flags);
   cudaFree(M->d_tmp);
+  cudaFree(M->d_fillmap);
+  if (M->fillpat) dfm_mat_destroy(M->fillpat);
   delete M;
   return DFM_OK;
 }
@@ -431,7 +459,9 @@ int dfm_ilu_levels(dfm_ilu M, unsigned* nf, unsigned* nb, unsigned* lev_f, unsig
 }
 
 int dfm_ilu_factor(dfm_ilu M, dfm_mat A, unsigned* n_singular) {
-  if (!M || !A || A->N != M->N || A->ncrs != M->ncrs || A->b != M->b || A->vt != M->vt) return DFM_ERR_INVALID;
+  if (!M || !A || A->N != M->N || A->b != M->b || A->vt != M->vt) return DFM_ERR_INVALID;
+  // the values must come in the pattern the preconditioner was made for (its size is checked)
+  if (A->ncrs != M->user->ncrs) return DFM_ERR_INVALID;
   int rc = ilu_factor_launch(M, A);
   if (rc) return rc;
   DevStatus h = {};
@@ -503,9 +533,25 @@ int dfm_ilu_apply(dfm_ilu M, const double* r, double* z) {
   return take_code(M->ctx);
 }
 
+int dfm_time_ilu_apply(dfm_ilu M, const double* r, double* z, int reps, float* ms) {
+  if (!M || !ms || reps <= 0 || (M->N && (!r || !z)) || r == z) return DFM_ERR_INVALID;
+  int rc = ilu_autotune(M);
+  if (rc) return rc;
+  const size_t n = (size_t)M->N * M->xw();
+  rc = time_launches(M->ctx->stream, reps, ms, [&] {
+    int q = ilu_fill_sentinel(M, M->d_tmp, n);
+    if (!q) q = ilu_fill_sentinel(M, z, n);
+    if (!q) q = ilu_fwd_launch(M, r, M->d_tmp, nullptr, M->sweep);
+    if (!q) q = ilu_bwd_launch(M, M->d_tmp, z, nullptr, nullptr, nullptr, M->sweep);
+    return q;
+  });
+  if (rc) return rc;
+  return take_code(M->ctx);
+}
+
 // ---------------------------------------------------------------- solvers
 static int solve_args(dfm_mat A, dfm_ilu M, int method, const void* b, const void* x) {
-  if (!A || !M || M->A != A || (A->N && (!b || !x))) return DFM_ERR_INVALID;
+  if (!A || !M || M->user != A || (A->N && (!b || !x))) return DFM_ERR_INVALID;
   const bool cplx = method == DFM_PCOCG || method == DFM_PCOCG_MIXED;
   if (cplx ? A->vt != DFM_COMPLEX : A->vt != DFM_REAL) return DFM_ERR_INVALID;
   if (!M->factored) return DFM_ERR_INVALID;

@@ -851,7 +851,7 @@ int dfm_batch_create(dfm_ilu M, unsigned ninst, const unsigned* row_off, dfm_bat
   if (!M || !out || !row_off || ninst == 0) return DFM_ERR_INVALID;
   *out = nullptr;
   dfm_mat A = M->A;
-  if (A->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;
+  if (A->vt != DFM_REAL || M->fillpat) return DFM_ERR_UNSUPPORTED;  // batches use ILU(0)
   if (row_off[0] != 0 || row_off[ninst] != A->N) return DFM_ERR_INVALID;
   for (unsigned k = 0; k < ninst; k++) {
     if (row_off[k + 1] < row_off[k]) return DFM_ERR_INVALID;

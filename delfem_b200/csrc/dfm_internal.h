@@ -20,6 +20,16 @@ namespace dfm {
 
 int cuda_fail(cudaError_t e, const char* what);
 int take_code(dfm_ctx c);
+// Host (DFM_HOST, then synchronises) or device source -> device memory.
+int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t s);
+
+template <typename T>
+inline int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  DFM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+  return DFM_OK;
+}
 
 // Scalars of one Krylov solve, in device memory so a captured CUDA graph can
 // run many iterations without the host.
@@ -82,7 +92,7 @@ struct dfm_mat_s {
   std::vector<unsigned> h_rowptr, h_colind;
   unsigned max_row = 0;     // most off-diagonal blocks in one row
   int lanes = 0;            // SpMV lanes per block row (0 = not tuned yet)
-  int spmv_kind = 0;        // 0 lane per block, 1 TMA-staged tiles, 2 element-wise (autotuned)
+  int spmv_kind = 0;        // 0 lane per block, 1 TMA-staged tiles, 2 element-wise, 3 warp-staged (autotuned)
   dfm::SpmvTiles tiles[2];  // [0] FP64 values, [1] FP32 copies
   size_t vw() const { return vt == DFM_COMPLEX ? 2 : (size_t)b * b; }   // doubles per block
   size_t xw() const { return vt == DFM_COMPLEX ? 2 : b; }               // doubles per vector block
@@ -90,7 +100,11 @@ struct dfm_mat_s {
 
 struct dfm_ilu_s {
   dfm_ctx ctx = nullptr;
-  dfm_mat A = nullptr;      // pattern owner (rowptr/colind shared)
+  dfm_mat A = nullptr;      // pattern owner (rowptr/colind shared): the system matrix, or fillpat
+  dfm_mat user = nullptr;   // the system matrix the preconditioner was made for
+  dfm_mat fillpat = nullptr;   // ILU(k), k != 0: owned pattern-only matrix of the filled pattern
+  unsigned* d_fillmap = nullptr;  // ILU(k): factor slot of each of user's off-diagonal slots
+  int fill_level = 0;
   unsigned N = 0, b = 1, ncrs = 0;
   int vt = DFM_REAL;
   unsigned* d_diaind = nullptr;
@@ -134,7 +148,8 @@ struct SpmvOpts {
   bool yy = false;
   const double* y0 = nullptr;
   bool f32 = false;
-  int kind = -1;  // -1: the matrix's tuned kernel; 0 lane per block; 1 TMA-staged tiles; 2 element-wise
+  int kind = -1;  // -1: the matrix's tuned kernel; 0 lane per block; 1 TMA-staged tiles; 2 element-wise;
+                  // 3 warp-staged
 };
 int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y, double* dot_part,
                 int nblocks_hint, KrylovScalars* sc, int lanes, const SpmvOpts& o = SpmvOpts());
@@ -145,6 +160,10 @@ int spmv_autotune(dfm_mat A);
 int spmv_grid(dfm_mat A);
 // ilu.cu
 int ilu_factor_launch(dfm_ilu M, dfm_mat A);
+// fill.cu
+int ilu_fill_pattern(unsigned N, const std::vector<unsigned>& rp, const std::vector<unsigned>& ci, int lev,
+                     std::vector<unsigned>& frp, std::vector<unsigned>& fci);
+int ilu_fill_values(dfm_ilu M, dfm_mat A);
 // With sc, a forward sweep first stops the solve when |r|^2/|r0|^2 < tol^2
 // (partials in part(2)) unless rr_check is false.
 // f32: the sweeps read the FP32 copy of L / D^-1 U (D^-1 itself stays FP64).

@@ -587,8 +587,12 @@ int ilu_factor_launch(dfm_ilu M, dfm_mat A) {
   cudaStream_t s = c->stream;
   const size_t vw = M->vw();
   DFM_CUDA_TRY(cudaMemcpyAsync(M->d_fdiag, A->d_diag, sizeof(double) * vw * M->N, cudaMemcpyDeviceToDevice, s));
-  if (M->ncrs)
+  if (M->d_fillmap) {  // ILU(k): A's blocks into the filled pattern, zero elsewhere (SetValue_Initialize)
+    const int rc = ilu_fill_values(M, A);
+    if (rc) return rc;
+  } else if (M->ncrs) {
     DFM_CUDA_TRY(cudaMemcpyAsync(M->d_foff, A->d_off, sizeof(double) * vw * M->ncrs, cudaMemcpyDeviceToDevice, s));
+  }
   DFM_CUDA_TRY(cudaMemsetAsync(&c->d_status->nsing, 0, sizeof(unsigned), s));
   M->plan_f.stale = true;  // packed sweep values are re-gathered on next use
   M->plan_b.stale = true;

@@ -195,6 +195,187 @@ k_spmv_elem(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __r
   if (NDOT == 2) block_partial<256>(dacc2, part2);
 }
 
+// ------------------------------------------------------ warp-staged SpMV
+// A warp takes R = 32/LPR consecutive block rows per pass.  Their off-diagonal
+// blocks form one contiguous run of the value array and their diagonal blocks
+// another; the warp copies both runs into its own slice of shared memory with
+// 16-byte cp.async copies (each instruction covers 512 contiguous bytes and
+// holds no registers), then every group of LPR lanes multiplies its row as the
+// lane-per-block kernel does, reading the b*b values of a block from shared
+// memory.  The lane-per-block kernel reads a block with b*b 8-byte loads at a
+// b*b*8-byte lane stride, so each of its load instructions touches ~20 cache
+// lines and the L1 (one line per cycle), not DRAM, sets its speed; here a span
+// of 32 3x3 blocks costs 5 coalesced copies and 9 shared loads per lane.
+// Blocks past the slice (rows longer than it holds) are read
+// from global memory directly.  The copy starts at the 16-byte boundary below
+// the run and ends at the one above it (the arrays carry kArrayPad spare
+// elements).
+constexpr int kWsChunks = 8;  // 16-byte chunks per lane and pass: a 4,096-byte slice of off-diagonal values
+
+template <int B, int LPR, typename TV>
+struct WsShape {
+  static constexpr unsigned R = 32 / LPR;
+  static constexpr unsigned VB = B * B * sizeof(TV);
+  static constexpr unsigned OFF = 32u * kWsChunks * 16u;
+  static constexpr unsigned DIAG = (R * VB + 16u + 15u) & ~15u;
+  static constexpr int DCH = (int)((DIAG / 16 + 31) / 32);
+  static constexpr unsigned WARP = OFF + DIAG;
+};
+
+// 16-byte global -> shared copy that bypasses L1 and registers (cp.async.cg)
+DFM_DEVINL void ws_cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+DFM_DEVINL void ws_cp_wait() { asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory"); }
+
+template <int B, typename TV>
+DFM_DEVINL void ws_mac(double* acc, const TV* m, const double* xv) {
+#pragma unroll
+  for (int r = 0; r < B; r++)
+#pragma unroll
+    for (int c = 0; c < B; c++) acc[r] += (double)m[r * B + c] * xv[c];
+}
+
+template <int B, int LPR, typename TV, int NDOT>
+__global__ void __launch_bounds__(256)
+k_spmv_ws(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __restrict__ colind,
+          const TV* __restrict__ diag, const TV* __restrict__ off, double alpha, const double* __restrict__ x,
+          double beta, double* __restrict__ y, double* __restrict__ part, const int* done,
+          const double* __restrict__ w, double* __restrict__ part2, const double* __restrict__ y0, int npart) {
+  using S = WsShape<B, LPR, TV>;
+  constexpr unsigned BB = B * B;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) char ws_smem[];
+  if (done && block_flag(done)) return;
+  if (blockIdx.x == 0)  // partial slots past this grid belong to nobody: zero for the consumer's fixed count
+    for (int k = gridDim.x + threadIdx.x; k < npart; k += blockDim.x) {
+      if (NDOT >= 1) part[k] = 0.0;
+      if (NDOT == 2) part2[k] = 0.0;
+    }
+  const unsigned l = threadIdx.x & 31u, wi = threadIdx.x >> 5;
+  char* wb = ws_smem + wi * S::WARP;
+  int4* wv = reinterpret_cast<int4*>(wb);
+  int4* wd = reinterpret_cast<int4*>(wb + S::OFF);
+  const unsigned g = l / LPR, lane = l % LPR;
+  const unsigned gmask = (LPR == 32) ? FULL : (((1u << LPR) - 1u) << (g * LPR));
+  const unsigned wpb = blockDim.x >> 5;
+  const unsigned step = gridDim.x * wpb * S::R;
+  double dacc = 0.0, dacc2 = 0.0;
+  for (unsigned r0 = (blockIdx.x * wpb + wi) * S::R; r0 < N; r0 += step) {
+    const unsigned rend = min(r0 + S::R, N);
+    const unsigned rp = __ldg(rowptr + min(r0 + l, rend));
+    const unsigned sb = __shfl_sync(FULL, rp, 0);
+    const unsigned se = __shfl_sync(FULL, rp, S::R);
+    const uintptr_t va = reinterpret_cast<uintptr_t>(off + (size_t)sb * BB);
+    const unsigned dv = (unsigned)(va & 15u);
+    const int4* vsrc = reinterpret_cast<const int4*>(va - dv);
+    const size_t want = (size_t)(se - sb) * S::VB + dv;
+    const unsigned nch = (unsigned)((min(want, (size_t)S::OFF) + 15u) / 16u);
+    const uintptr_t da = reinterpret_cast<uintptr_t>(diag + (size_t)r0 * BB);
+    const unsigned dd = (unsigned)(da & 15u);
+    const int4* dsrc = reinterpret_cast<const int4*>(da - dd);
+    const unsigned nchd = ((rend - r0) * S::VB + dd + 15u) / 16u;
+    __syncwarp();  // the previous pass's reads of the slice are done
+#pragma unroll
+    for (int c = 0; c < kWsChunks; c++)
+      if (l + 32u * c < nch) ws_cp16(wv + l + 32u * c, vsrc + l + 32u * c);
+#pragma unroll
+    for (int c = 0; c < S::DCH; c++)
+      if (l + 32u * c < nchd) ws_cp16(wd + l + 32u * c, dsrc + l + 32u * c);
+    ws_cp_wait();
+    __syncwarp();  // every lane's copies visible to the warp
+    const unsigned i = r0 + g;
+    const unsigned s0 = __shfl_sync(FULL, rp, g), s1 = __shfl_sync(FULL, rp, g + 1);
+    if (i < rend) {  // group-uniform
+      double acc[B];
+#pragma unroll
+      for (int r = 0; r < B; r++) acc[r] = 0.0;
+      for (unsigned s = s0 + lane; s <= s1; s += LPR) {
+        const unsigned col = s < s1 ? __ldcs(colind + s) : i;
+        double xv[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) xv[c] = __ldg(x + (size_t)col * B + c);
+        if (s < s1) {
+          const size_t boff = (size_t)(s - sb) * S::VB + dv;
+          if (boff + S::VB <= S::OFF) ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + boff), xv);
+          else ws_mac<B>(acc, off + (size_t)s * BB, xv);
+        } else {
+          ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + S::OFF + dd + g * S::VB), xv);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(gmask, acc[r], o);
+      if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < B; r++) {
+          double val = alpha * acc[r];
+          if (y0) val += y0[(size_t)i * B + r];
+          else if (beta != 0.0) val += beta * y[(size_t)i * B + r];
+          y[(size_t)i * B + r] = val;
+          if (NDOT == 1 || NDOT == 2) dacc += w[(size_t)i * B + r] * val;
+          if (NDOT == 2) dacc2 += val * val;
+          if (NDOT == 3) dacc += val * val;
+        }
+      }
+    }
+  }
+  if (NDOT >= 1) block_partial<256>(dacc, part);
+  if (NDOT == 2) block_partial<256>(dacc2, part2);
+}
+
+template <int B, int LPR, typename TV, int NDOT>
+static cudaError_t launch_ws_n(dfm_mat A, const TV* diag, const TV* off, int npart, cudaStream_t s, double alpha,
+                               const double* x, double beta, double* y, double* part, const int* done,
+                               const double* w, double* part2, const double* y0) {
+  using S = WsShape<B, LPR, TV>;
+  auto fn = k_spmv_ws<B, LPR, TV, NDOT>;
+  const int smem = (int)(8 * S::WARP);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, smem);
+  if (e != cudaSuccess) return e;
+  // one resident wave: a second partial wave would leave most SMs idle at the end
+  const int cap = npart > 0 ? npart : kMaxBlocks;
+  const int grid = std::max(1, std::min(A->ctx->nsm * std::max(occ, 1), cap));
+  fn<<<grid, 256, smem, s>>>(A->N, A->d_rowptr, A->d_colind, diag, off, alpha, x, beta, y, part, done, w, part2, y0,
+                             part ? npart : 0);
+  return cudaGetLastError();
+}
+
+template <int B, int LPR, typename TV>
+static cudaError_t launch_ws_t(dfm_mat A, const TV* diag, const TV* off, int npart, cudaStream_t s, double alpha,
+                               const double* x, double beta, double* y, double* part, const int* done,
+                               const SpmvOpts& o) {
+  const double* w = o.dot_w ? o.dot_w : x;
+  if (part && o.yy)
+    return launch_ws_n<B, LPR, TV, 3>(A, diag, off, npart, s, alpha, x, beta, y, part, done, nullptr, nullptr, o.y0);
+  if (part && o.dot_part2)
+    return launch_ws_n<B, LPR, TV, 2>(A, diag, off, npart, s, alpha, x, beta, y, part, done, w, o.dot_part2, o.y0);
+  if (part)
+    return launch_ws_n<B, LPR, TV, 1>(A, diag, off, npart, s, alpha, x, beta, y, part, done, w, nullptr, o.y0);
+  return launch_ws_n<B, LPR, TV, 0>(A, diag, off, npart, s, alpha, x, beta, y, nullptr, done, nullptr, nullptr,
+                                    o.y0);
+}
+
+template <int B>
+static cudaError_t launch_ws(dfm_mat A, int lanes, int npart, cudaStream_t s, double alpha, const double* x,
+                             double beta, double* y, double* part, const int* done, const SpmvOpts& o) {
+#define DFM_WS_L(L)                                                                                              \
+  return o.f32 ? launch_ws_t<B, L, float>(A, A->d_diag32, A->d_off32, npart, s, alpha, x, beta, y, part, done, o) \
+               : launch_ws_t<B, L, double>(A, A->d_diag, A->d_off, npart, s, alpha, x, beta, y, part, done, o)
+  switch (lanes) {
+    case 4: DFM_WS_L(4);
+    case 8: DFM_WS_L(8);
+    case 16: DFM_WS_L(16);
+    default: DFM_WS_L(32);
+  }
+#undef DFM_WS_L
+}
+
 template <int B, int LPR, typename TV>
 static void launch_elem_t(dfm_mat A, const TV* diag, const TV* off, int grid, cudaStream_t s, double alpha,
                           const double* x, double beta, double* y, double* part, const int* done,
@@ -646,6 +827,16 @@ int spmv_launch(dfm_mat A, double alpha, const double* x, double beta, double* y
     DFM_CUDA_TRY(cudaGetLastError());
     return DFM_OK;
   }
+  if (kind == 3 && A->vt == DFM_REAL) {
+    cudaError_t e;
+    switch (A->b) {
+      case 1: e = launch_ws<1>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      case 2: e = launch_ws<2>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+      default: e = launch_ws<3>(A, lanes, grid, s, alpha, x, beta, y, dot_part, done, o); break;
+    }
+    DFM_CUDA_TRY(e);
+    return DFM_OK;
+  }
   if (kind == 1 && A->vt == DFM_REAL) {
     if (!A->tiles[o.f32 ? 1 : 0].valid) {
       const int rc = build_tiles(A, o.f32 ? 1 : 0);  // host set-up; normally done by the autotuner
@@ -723,7 +914,7 @@ int spmv_autotune(dfm_mat A) {
   int best_l = 8, best_k = 0;
   const bool tiles_ok = A->vt == DFM_REAL && build_tiles(A, 0) == DFM_OK;
   cudaGetLastError();
-  for (int kind = 0; kind < 3; kind++)
+  for (int kind = 0; kind < 4; kind++)
     for (int c = 0; c < 4; c++) {
       if (kind > 0 && A->vt != DFM_REAL) break;
       if (kind == 1 && !tiles_ok) break;

@@ -53,6 +53,7 @@ PROTOS = {
     "dfm_mat_set_spmv_kernel": (_i, [_vp, _i]),
     "dfm_mat_get_spmv_kernel": (_i, [_vp, _ip]),
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
+    "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
     "dfm_mesh_pattern": (_i, [_vp, _up, _up, C.POINTER(C.c_size_t)]),
@@ -64,12 +65,15 @@ PROTOS = {
     "dfm_coef_grad_poisson2d": (_i, [_vp, _d, _vp, _vp, _vp]),
     "dfm_coef_grad_solid2d": (_i, [_vp, _d, _d, _vp, _vp, _vp]),
     "dfm_ilu_create": (_i, [_vp, C.POINTER(_vp)]),
+    "dfm_ilu_create_fill": (_i, [_vp, _i, C.POINTER(_vp)]),
+    "dfm_ilu_pattern": (_i, [_vp, _up, _up, _up]),
     "dfm_ilu_destroy": (_i, [_vp]),
     "dfm_ilu_levels": (_i, [_vp, _up, _up, _up, _up]),
     "dfm_ilu_factor": (_i, [_vp, _vp, _up]),
     "dfm_ilu_get_values": (_i, [_vp, _vp, _vp, _i]),
     "dfm_ilu_set_values": (_i, [_vp, _vp, _vp, _i]),
     "dfm_ilu_apply": (_i, [_vp, _vp, _vp]),
+    "dfm_time_ilu_apply": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_ilu_apply_static": (_i, [_vp, _vp, _vp]),
     "dfm_ilu_set_sweep": (_i, [_vp, _i]),
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
@@ -243,6 +247,13 @@ class Matrix:
         check(lib().dfm_spmv(self.h, alpha, _ptr(x), beta, _ptr(y)), "dfm_spmv")
         return y
 
+    def time_spmv(self, x, y, reps=50):
+        """Average seconds per launch of y = A x over `reps` back-to-back launches."""
+        _sync_torch()
+        ms = C.c_float()
+        check(lib().dfm_time_spmv(self.h, _ptr(x), _ptr(y), int(reps), C.byref(ms)), "dfm_time_spmv")
+        return ms.value / 1e3
+
     @property
     def lanes(self):
         v = C.c_int()
@@ -350,13 +361,29 @@ def apply_dirichlet(A: Matrix, flags, rhs=None):
 
 
 class ILU:
-    """LsSol::CPreconditioner_ILU(0) on the device."""
+    """LsSol::CPreconditioner_ILU on the device: ILU(0), or ILU(fill_level)
+    (SetFillInLevel; -1 = no limit) with the factor in its own fill pattern."""
 
-    def __init__(self, A: Matrix):
+    def __init__(self, A: Matrix, fill_level: int = 0):
         self.A = A
+        self.fill_level = int(fill_level)
         h = C.c_void_p()
-        check(lib().dfm_ilu_create(A.h, C.byref(h)), "dfm_ilu_create")
+        if self.fill_level == 0:
+            check(lib().dfm_ilu_create(A.h, C.byref(h)), "dfm_ilu_create")
+        else:
+            check(lib().dfm_ilu_create_fill(A.h, self.fill_level, C.byref(h)), "dfm_ilu_create_fill")
         self.h = h
+        n = C.c_uint()
+        check(lib().dfm_ilu_pattern(h, None, None, C.byref(n)), "dfm_ilu_pattern")
+        self.ncrs = n.value
+
+    def pattern(self):
+        """The factor's pattern (rowptr, colind)."""
+        rp = np.zeros(self.A.N + 1, np.uint32)
+        ci = np.zeros(max(self.ncrs, 1), np.uint32)
+        check(lib().dfm_ilu_pattern(self.h, rp.ctypes.data_as(_up), ci.ctypes.data_as(_up), None),
+              "dfm_ilu_pattern")
+        return rp, ci[: self.ncrs]
 
     def close(self):
         if getattr(self, "h", None):
@@ -385,9 +412,9 @@ class ILU:
 
     def get_values(self):
         d = np.zeros(self.A.N * self.A.vw)
-        o = np.zeros(max(self.A.ncrs, 1) * self.A.vw)
+        o = np.zeros(max(self.ncrs, 1) * self.A.vw)
         check(lib().dfm_ilu_get_values(self.h, _ptr(d), _ptr(o), HOST), "dfm_ilu_get_values")
-        return d, o[: self.A.ncrs * self.A.vw]
+        return d, o[: self.ncrs * self.A.vw]
 
     def set_values(self, diag, off):
         diag = np.ascontiguousarray(diag, np.float64)
@@ -398,6 +425,13 @@ class ILU:
         _sync_torch()
         check(lib().dfm_ilu_apply(self.h, _ptr(r), _ptr(z)), "dfm_ilu_apply")
         return z
+
+    def time_apply(self, r, z, reps=20):
+        """Average seconds per z = U^-1 L^-1 r over `reps` back-to-back applications."""
+        _sync_torch()
+        ms = C.c_float()
+        check(lib().dfm_time_ilu_apply(self.h, _ptr(r), _ptr(z), int(reps), C.byref(ms)), "dfm_time_ilu_apply")
+        return ms.value / 1e3
 
     @property
     def sweep(self):

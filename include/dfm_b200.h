@@ -107,8 +107,9 @@ DFM_API int dfm_mat_set_spmv_lanes(dfm_mat A, int lanes);
 DFM_API int dfm_mat_get_spmv_lanes(dfm_mat A, int* lanes);
 /* SpMV kernel: 0 = a lane per block (direct loads), 1 = row tiles staged in
  * shared memory by TMA bulk copies, 2 = element-wise coalesced loads of each
- * row's contiguous values (1 and 2 real matrices only).  Autotuned together
- * with the lanes. */
+ * row's contiguous values, 3 = each warp stages its rows' contiguous value run
+ * in shared memory with coalesced 16-byte loads (1, 2 and 3 real matrices
+ * only).  Autotuned together with the lanes. */
 DFM_API int dfm_mat_set_spmv_kernel(dfm_mat A, int kernel);
 DFM_API int dfm_mat_get_spmv_kernel(dfm_mat A, int* kernel);
 
@@ -116,6 +117,10 @@ DFM_API int dfm_mat_get_spmv_kernel(dfm_mat A, int* kernel);
  * complex: CZMatDia_BlkCrs::MatVec, src/matvec/zmatdia_blkcrs.cpp:737-801).
  * beta == 0 writes y without reading it. */
 DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, double* y);
+/* Measurement hook, no counterpart in the reference: `reps` back-to-back
+ * launches of y = A x (the tuned kernel) on the context's stream between one
+ * pair of CUDA events, after one untimed launch; *ms = average per launch. */
+DFM_API int dfm_time_spmv(dfm_mat A, const double* x, double* y, int reps, float* ms);
 
 /* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
 /* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]
@@ -172,6 +177,17 @@ DFM_API int dfm_coef_grad_solid2d(dfm_mesh mesh, double lambda, double myu, cons
 /* Symbolic ILU(0) (CMatDiaFrac_BlkCrs(0, A), src/matvec/matdiafrac_blkcrs.cpp:227-287)
  * plus the level sets of both sweeps in the natural order. */
 DFM_API int dfm_ilu_create(dfm_mat A, dfm_ilu* out);
+/* ILU(k) (CPreconditioner_ILU::SetFillInLevel(lev) + SetLinearSystem,
+ * src/ls/preconditioner.cpp:57-212): the factor's pattern is A's plus the fill
+ * entries of CMatDiaFrac_BlkCrs::AddFracPtn (src/matvec/matdiafrac_blkcrs.cpp:
+ * 1249-1377) up to level lev (-1: no limit), identical to the reference's;
+ * dfm_ilu_factor then starts from A's values in it (SetValue_Initialize) and
+ * factors over it.  lev = 0 is dfm_ilu_create.  Real matrices only; batches
+ * (dfm_batch_create) take ILU(0) objects only. */
+DFM_API int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out);
+/* The factor's pattern (host arrays, nullable): rowptr[N+1], colind[*ncrs];
+ * the off-diagonal values of dfm_ilu_get_values/set_values follow it. */
+DFM_API int dfm_ilu_pattern(dfm_ilu M, unsigned* rowptr, unsigned* colind, unsigned* ncrs);
 DFM_API int dfm_ilu_destroy(dfm_ilu M);
 /* Level counts; lev_fwd / lev_bwd (host, N entries each, nullable) get the level of every row. */
 DFM_API int dfm_ilu_levels(dfm_ilu M, unsigned* nlev_fwd, unsigned* nlev_bwd, unsigned* lev_fwd,
@@ -183,6 +199,10 @@ DFM_API int dfm_ilu_get_values(dfm_ilu M, double* diag, double* off, int where);
 DFM_API int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int where);
 /* z = U^-1 L^-1 r (ForwardSubstitution + BackwardSubstitution, :332-663).  r != z. */
 DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
+/* Measurement hook, no counterpart in the reference: `reps` back-to-back
+ * dfm_ilu_apply launch sequences (forward + backward sweep) timed as
+ * dfm_time_spmv does; *ms = average per application. */
+DFM_API int dfm_time_ilu_apply(dfm_ilu M, const double* r, double* z, int reps, float* ms);
 /* No counterpart in the reference.  The same z = U^-1 L^-1 r as dfm_ilu_apply,
  * for callers that cannot allocate device memory at the point of use (code
  * inside a stream-ordered region that must not synchronise, a host framework

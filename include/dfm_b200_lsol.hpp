@@ -5,8 +5,8 @@
 //   MatVec::CMatDia_BlkCrs                 -> dfm_lsol::CMatDia_BlkCrs
 //       (include/delfem/matvec/matdia_blkcrs.h:44-118)
 //   LsSol::CPreconditioner_ILU             -> dfm_lsol::CPreconditioner_ILU
-//       (include/delfem/ls/preconditioner.h:54-108: SetLinearSystem,
-//        SetValue, SolvePrecond; ILU(0) only, no fill-in levels, no ordering)
+//       (include/delfem/ls/preconditioner.h:54-108: SetFillInLevel,
+//        SetLinearSystem, SetValue, SolvePrecond; one segment, no ordering)
 //   LsSol::Solve_PCG / Solve_PBiCGSTAB     -> dfm_lsol::Solve_PCG / Solve_PBiCGSTAB
 //       (include/delfem/ls/solver_ls_iter.h:35-45)
 //   Fem::Ls::Solve_PCOCG                   -> dfm_lsol::Solve_PCOCG
@@ -169,7 +169,8 @@ class CMatDia_BlkCrs {
   bool cplx_ = false;
 };
 
-// LsSol::CPreconditioner_ILU with fill-in level 0 and the natural ordering.
+// LsSol::CPreconditioner_ILU with the natural ordering: ILU(0), or ILU(k)
+// after SetFillInLevel(k).
 class CPreconditioner_ILU {
  public:
   CPreconditioner_ILU() = default;
@@ -181,10 +182,17 @@ class CPreconditioner_ILU {
     if (h_) dfm_ilu_destroy(h_);
     h_ = nullptr;
   }
-  // ILU(0) pattern and level sets of the sweeps
+  // SetFillInLevel(lev, ilss): ILU(lev) from the next SetLinearSystem on
+  // (-1: no limit).  A single-segment system: ilss must be -1 or 0.
+  void SetFillInLevel(int lev, int ilss = -1) {
+    if (ilss != -1 && ilss != 0) throw Error(DFM_ERR_UNSUPPORTED, "SetFillInLevel");
+    if (lev < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
+    lev_ = lev;
+  }
+  // fill pattern (ILU(lev)) and level sets of the sweeps
   void SetLinearSystem(const CMatDia_BlkCrs& A) {
     Clear();
-    check(dfm_ilu_create(A.get(), &h_), "SetLinearSystem");
+    check(dfm_ilu_create_fill(A.get(), lev_, &h_), "SetLinearSystem");
   }
   // numeric factorization; false when more than 10 pivots were singular
   bool SetValue(const CMatDia_BlkCrs& A) {
@@ -200,6 +208,7 @@ class CPreconditioner_ILU {
 
  private:
   dfm_ilu h_ = nullptr;
+  int lev_ = 0;
 };
 
 namespace detail {

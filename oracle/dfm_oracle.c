@@ -68,6 +68,105 @@ void dfo_diaind(unsigned N, const unsigned* rowptr, const unsigned* colind, unsi
   }
 }
 
+/* ILU(k) symbolic fill, CMatDiaFrac_BlkCrs::AddFracPtn(lev_fill)
+ * (src/matvec/matdiafrac_blkcrs.cpp:1249-1377) with its sorted row list
+ * CListRLN (include/delfem/matvec/matdiafrac_blkcrs.h:185-300).  Row i starts
+ * from A's entries at level 0.  Its pivots k < i are visited in ascending
+ * order, fill entries included as they appear; a pivot is used only when
+ * lev(i,k) + 1 <= lev_fill, and then every j of row k's upper part (of the
+ * already finished fill pattern) with lev(k,j) + 1 <= lev_fill and j != i is
+ * added with level max(lev(i,k), lev(k,j)) + 1 - unless row i holds j
+ * already, whose level is then left as it is (CListRLN::Insert returns
+ * without touching it).  lev_fill = -1 means no limit.  Here the sorted list
+ * is a linked list over column numbers (next[]) with a per-column level
+ * (ABSENT when not in the row); the resulting pattern is the same. */
+#define DFO_ABSENT 0xffffffffu
+int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
+                     unsigned* frowptr, unsigned** fcolind_out, unsigned** flev_out) {
+  const unsigned ncrs0 = rowptr[N];
+  size_t cap = (size_t)ncrs0 * 4 + 16, nf = 0;
+  unsigned* fcol = (unsigned*)malloc(cap * sizeof(unsigned));
+  unsigned* flev = (unsigned*)malloc(cap * sizeof(unsigned));
+  unsigned* fdia = (unsigned*)malloc((N ? N : 1) * sizeof(unsigned));
+  unsigned* lv = (unsigned*)malloc((N ? N : 1) * sizeof(unsigned));
+  unsigned* nx = (unsigned*)malloc((N ? N : 1) * sizeof(unsigned));
+  const unsigned END = DFO_ABSENT;
+  const int no_fill = lev_fill == 0 || ncrs0 == 0 || (size_t)ncrs0 == (size_t)N * (N ? N - 1 : 0);
+  for (unsigned j = 0; j < N; j++) lv[j] = DFO_ABSENT;
+  frowptr[0] = 0;
+  for (unsigned i = 0; i < N; i++) {
+    /* the row's list: A's entries, ascending, level 0 */
+    unsigned head = END, tail = END;
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) {
+      const unsigned c = colind[s];
+      lv[c] = 0;
+      nx[c] = END;
+      if (tail == END) head = c; else nx[tail] = c;
+      tail = c;
+    }
+    if (!no_fill) {
+      for (unsigned k = head; k != END; k = nx[k]) {
+        const unsigned lik = lv[k];
+        if (lev_fill != -1 && lik + 1 > (unsigned)lev_fill) continue;
+        if (k >= i) break;
+        unsigned hint = k; /* every new j lies after k */
+        for (unsigned s = fdia[k]; s < frowptr[k + 1]; s++) {
+          const unsigned lkj = flev[s];
+          if (lev_fill != -1 && lkj + 1 > (unsigned)lev_fill) continue;
+          const unsigned j = fcol[s];
+          if (j == i || lv[j] != DFO_ABSENT) continue;
+          while (nx[hint] != END && nx[hint] < j) hint = nx[hint];
+          nx[j] = nx[hint];
+          nx[hint] = j;
+          lv[j] = (lik > lkj ? lik : lkj) + 1;
+          hint = j;
+        }
+      }
+    }
+    /* finish the row (CListRLN::Finalize): entries in order, m_DiaInd */
+    fdia[i] = END;
+    for (unsigned c = head; c != END; c = nx[c]) {
+      if (nf == cap) {
+        cap *= 2;
+        fcol = (unsigned*)realloc(fcol, cap * sizeof(unsigned));
+        flev = (unsigned*)realloc(flev, cap * sizeof(unsigned));
+      }
+      if (fdia[i] == END && c > i) fdia[i] = (unsigned)nf;
+      fcol[nf] = c;
+      flev[nf] = lv[c];
+      nf++;
+    }
+    frowptr[i + 1] = (unsigned)nf;
+    if (fdia[i] == END) fdia[i] = (unsigned)nf;
+    for (unsigned c = head; c != END; c = nx[c]) lv[c] = DFO_ABSENT;
+  }
+  free(fdia);
+  free(lv);
+  free(nx);
+  *fcolind_out = fcol;
+  if (flev_out) *flev_out = flev; else free(flev);
+  return 0;
+}
+
+void dfo_free(void* p) { free(p); }
+
+/* CMatDiaFrac_BlkCrs::SetValue_Initialize (include/delfem/matvec/matdiafrac_blkcrs.h:90-117):
+ * the factor's values are zero except where A has an entry, which is copied. */
+void dfo_iluk_init(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                   const double* diag, const double* off, const unsigned* frowptr,
+                   const unsigned* fcolind, double* fdiag, double* foff) {
+  const size_t bb = (size_t)b * b;
+  memcpy(fdiag, diag, sizeof(double) * bb * N);
+  memset(foff, 0, sizeof(double) * bb * frowptr[N]);
+  for (unsigned i = 0; i < N; i++) {
+    unsigned t = frowptr[i];
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) {
+      while (fcolind[t] != colind[s]) t++; /* A's row is a sorted subset of the factor's */
+      memcpy(foff + t * bb, off + s * bb, sizeof(double) * bb);
+    }
+  }
+}
+
 unsigned dfo_levels_fwd(unsigned N, const unsigned* rowptr, const unsigned* colind,
                         const unsigned* diaind, unsigned* lev) {
   unsigned nl = 0;
@@ -610,6 +709,14 @@ int dfo_pcg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* coli
             const unsigned* diaind, const double* diag, const double* off, const double* fdiag,
             const double* foff, double* r, double* x, double tol, unsigned maxit,
             unsigned* iters, double* conv, double* hist) {
+  return dfo_pcg_fill(N, b, rowptr, colind, diag, off, rowptr, colind, diaind, fdiag, foff, r, x, tol, maxit,
+                      iters, conv, hist);
+}
+
+int dfo_pcg_fill(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                 const double* off, const unsigned* frowptr, const unsigned* fcolind, const unsigned* fdiaind,
+                 const double* fdiag, const double* foff, double* r, double* x, double tol, unsigned maxit,
+                 unsigned* iters, double* conv, double* hist) {
   const size_t n = (size_t)N * b;
   double* p = (double*)calloc(n ? n : 1, sizeof(double));
   double* z = (double*)calloc(n ? n : 1, sizeof(double));
@@ -622,7 +729,7 @@ int dfo_pcg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* coli
   }
   const double inv0 = 1.0 / sq0;
   memcpy(z, r, n * sizeof(double));
-  precond(N, b, rowptr, colind, diaind, fdiag, foff, z);
+  precond(N, b, frowptr, fcolind, fdiaind, fdiag, foff, z);
   memcpy(p, z, n * sizeof(double));
   double rz = vdot(n, r, z);
   for (unsigned it = 0; it < maxit; it++) {
@@ -640,7 +747,7 @@ int dfo_pcg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* coli
       return 1;
     }
     memcpy(z, r, n * sizeof(double));
-    precond(N, b, rowptr, colind, diaind, fdiag, foff, z);
+    precond(N, b, frowptr, fcolind, fdiaind, fdiag, foff, z);
     const double rz_new = vdot(n, r, z);
     const double beta = rz_new / rz;
     rz = rz_new;

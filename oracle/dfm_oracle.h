@@ -24,6 +24,18 @@ int dfo_pattern(int nnode, int nnoel, int nelem, const int* elem, unsigned* rowp
                 unsigned* colind, unsigned* ncrs);
 /* m_DiaInd of CMatDiaFrac_BlkCrs (src/matvec/matdiafrac_blkcrs.cpp:263-278). */
 void dfo_diaind(unsigned N, const unsigned* rowptr, const unsigned* colind, unsigned* diaind);
+/* ILU(k) symbolic fill: CMatDiaFrac_BlkCrs::AddFracPtn(lev_fill)
+ * (src/matvec/matdiafrac_blkcrs.cpp:1249-1377).  frowptr[N+1] is filled; the
+ * column and level arrays are allocated here (free with dfo_free).
+ * lev_fill = -1: no limit. */
+int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
+                     unsigned* frowptr, unsigned** fcolind, unsigned** flev);
+void dfo_free(void* p);
+/* SetValue_Initialize (include/delfem/matvec/matdiafrac_blkcrs.h:90-117): A's
+ * values into the fill pattern, zero elsewhere. */
+void dfo_iluk_init(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                   const double* diag, const double* off, const unsigned* frowptr,
+                   const unsigned* fcolind, double* fdiag, double* foff);
 /* Level sets of the forward (L) and backward (U) sweeps in the natural order:
  * lev_f(i) = 1 + max lev_f(j) over j in L(i) (0 when L(i) is empty),
  * lev_b(i) = 1 + max lev_b(j) over j in U(i).  Returns the number of levels. */
@@ -84,6 +96,11 @@ int dfo_pcg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* coli
             const unsigned* diaind, const double* diag, const double* off, const double* fdiag,
             const double* foff, double* r, double* x, double tol, unsigned maxit,
             unsigned* iters, double* conv, double* hist);
+/* dfo_pcg with a factor in its own (filled) pattern frowptr / fcolind / fdiaind. */
+int dfo_pcg_fill(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                 const double* off, const unsigned* frowptr, const unsigned* fcolind, const unsigned* fdiaind,
+                 const double* fdiag, const double* foff, double* r, double* x, double tol, unsigned maxit,
+                 unsigned* iters, double* conv, double* hist);
 /* LsSol::Solve_PBiCGSTAB (src/ls/solver_ls_iter.cpp:291-408); *iters is the
  * 1-based iitr at convergence, as in the reference. */
 int dfo_pbicgstab(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,

@@ -49,6 +49,10 @@ def lib():
         L.dfo_fwd.argtypes = [U, U, up, up, up, dp, dp, dp]
         L.dfo_bwd.argtypes = [U, U, up, up, up, dp, dp]
         L.dfo_pcg.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp, dp]
+        L.dfo_iluk_pattern.argtypes = [U, up, up, C.c_int, up, C.POINTER(up), C.POINTER(up)]
+        L.dfo_free.argtypes = [C.c_void_p]
+        L.dfo_iluk_init.argtypes = [U, U, up, up, dp, dp, up, up, dp, dp]
+        L.dfo_pcg_fill.argtypes = [U, U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp, dp]
         L.dfo_pbicgstab.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_zspmv.argtypes = [U, up, up, dp, dp, D, dp, D, dp]
         L.dfo_zilu0.argtypes = [U, up, up, up, dp, dp]
@@ -97,6 +101,23 @@ def diaind(rowptr, colind):
     ci = colind if colind.size else np.zeros(1, np.uint32)
     lib().dfo_diaind(N, _u(rowptr), _u(ci), _u(d))
     return d[:N]
+
+
+def iluk_pattern(rowptr, colind, lev_fill):
+    """ILU(k) fill pattern (CMatDiaFrac_BlkCrs::AddFracPtn): (frowptr, fcolind, flev)."""
+    rowptr = np.ascontiguousarray(rowptr, np.uint32)
+    colind = np.ascontiguousarray(colind, np.uint32)
+    N = rowptr.size - 1
+    fr = np.zeros(N + 1, np.uint32)
+    pc, pl = C.POINTER(C.c_uint)(), C.POINTER(C.c_uint)()
+    lib().dfo_iluk_pattern(N, _u(rowptr), _u(colind if colind.size else np.zeros(1, np.uint32)), int(lev_fill),
+                           _u(fr), C.byref(pc), C.byref(pl))
+    n = int(fr[-1])
+    fc = np.ctypeslib.as_array(pc, shape=(max(n, 1),))[:n].copy()
+    fl = np.ctypeslib.as_array(pl, shape=(max(n, 1),))[:n].copy()
+    lib().dfo_free(C.cast(pc, C.c_void_p))
+    lib().dfo_free(C.cast(pl, C.c_void_p))
+    return fr, fc, fl
 
 
 def levels(rowptr, colind, dia):
@@ -186,6 +207,32 @@ class System:
         else:
             ns = lib().dfo_ilu0(self.N, self.b, _u(self.rowptr), _u(self._ci), _u(self.dia), _d(fd), _dz(fo))
         return int(ns), fd, fo
+
+    def iluk(self, lev_fill):
+        """ILU(lev_fill): fill pattern, SetValue_Initialize, DoILUDecomp on it.
+        Returns (ns, fpat, fd, fo) with fpat = (frowptr, fcolind, fdiaind)."""
+        assert not self.cplx
+        fr, fc, _ = iluk_pattern(self.rowptr, self.colind, lev_fill)
+        fdia = diaind(fr, fc)
+        fd = np.zeros_like(self.diag)
+        fo = np.zeros(max(fc.size, 1) * self.b * self.b)
+        fcz = fc if fc.size else np.zeros(1, np.uint32)
+        lib().dfo_iluk_init(self.N, self.b, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off), _u(fr),
+                            _u(fcz), _d(fd), _d(fo))
+        ns = lib().dfo_ilu0(self.N, self.b, _u(fr), _u(fcz), _u(fdia), _d(fd), _d(fo))
+        return int(ns), (fr, fc, fdia), fd, fo[: fc.size * self.b * self.b]
+
+    def solve_fill(self, fpat, fd, fo, rhs=None, tol=1e-10, maxit=10000):
+        """Solve_PCG with a factor in its own pattern fpat = (frowptr, fcolind, fdiaind)."""
+        fr, fc, fdia = fpat
+        r = np.array(self.rhs if rhs is None else rhs, dtype=np.float64, copy=True)
+        x = np.zeros_like(r)
+        it, conv = C.c_uint(), C.c_double()
+        fcz = fc if fc.size else np.zeros(1, np.uint32)
+        ok = lib().dfo_pcg_fill(self.N, self.b, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off),
+                                _u(fr), _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(r), _d(x), tol, maxit,
+                                C.byref(it), C.byref(conv), None)
+        return dict(ok=bool(ok), x=x, iters=it.value, conv=conv.value, r=r)
 
     def fwd(self, fd, fo, v):
         v = np.array(v, dtype=np.float64, copy=True)

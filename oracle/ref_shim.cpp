@@ -525,10 +525,43 @@ int dfm_ref_mat_precond(unsigned N, unsigned b, const unsigned* rowptr, const un
   return 0;
 }
 
+int dfm_ref_mat_iluk(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                     const double* diag, const double* off, int lev, unsigned cap, unsigned* frowptr,
+                     unsigned* fcolind, double* fdiag, double* foff, unsigned* fncrs) {
+  Quiet q;
+  MatVec::CMatDia_BlkCrs* m = make_mat(N, b, rowptr, colind, diag, off);
+  MatVec::CMatDiaFrac_BlkCrs f(lev, *m);
+  *fncrs = f.NCrs();
+  if (!frowptr || f.NCrs() > cap) {
+    delete m;
+    return 2;
+  }
+  frowptr[0] = 0;
+  for (unsigned i = 0; i < N; i++) {
+    unsigned n = 0;
+    const unsigned* c = f.GetPtrIndPSuP(i, n);
+    if (n) std::memcpy(fcolind + frowptr[i], c, sizeof(unsigned) * n);
+    frowptr[i + 1] = frowptr[i] + n;
+  }
+  f.SetValue_Initialize(*m);
+  const bool ok = f.DoILUDecomp();
+  read_mat(f, b, fdiag, foff);
+  delete m;
+  return ok ? 0 : 1;
+}
+
 int dfm_ref_mat_solve(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, const double* rhs, int method,
                       double tol, unsigned maxit, unsigned* iters, double* conv, double* x,
                       double* t_ilu, double* t_solve) {
+  return dfm_ref_mat_solve_lev(N, b, rowptr, colind, diag, off, rhs, method, tol, maxit, 0, iters, conv, x,
+                               t_ilu, t_solve);
+}
+
+int dfm_ref_mat_solve_lev(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                          const double* diag, const double* off, const double* rhs, int method,
+                          double tol, unsigned maxit, int lev, unsigned* iters, double* conv, double* x,
+                          double* t_ilu, double* t_solve) {
   Quiet q;
   LsSol::CLinearSystem ls;
   ls.AddLinSysSeg(N, b);
@@ -549,7 +582,7 @@ int dfm_ref_mat_solve(unsigned N, unsigned b, const unsigned* rowptr, const unsi
   for (unsigned i = 0; i < N; i++)
     for (unsigned d = 0; d < b; d++) r.SetValue(i, d, rhs[(size_t)i * b + d]);
   LsSol::CPreconditioner_ILU prec;
-  prec.SetFillInLevel(0);
+  prec.SetFillInLevel(lev);
   prec.SetLinearSystem(ls);
   double t0 = now_s();
   const bool ilu_ok = prec.SetValue(ls);

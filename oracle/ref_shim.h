@@ -69,12 +69,24 @@ int dfm_ref_mat_ilu0(unsigned N, unsigned b, const unsigned* rowptr, const unsig
                      const double* diag, const double* off, double* fdiag, double* foff);
 int dfm_ref_mat_precond(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                         const double* fdiag, const double* foff, double* vec);
+/* CMatDiaFrac_BlkCrs(lev, A): the ILU(lev) fill pattern (AddFracPtn) and,
+ * after SetValue_Initialize + DoILUDecomp, the factor in it.  *fncrs gets the
+ * pattern's size; with frowptr == NULL or cap < *fncrs nothing else is written
+ * and 2 is returned.  Otherwise 0 (1 when DoILUDecomp gave up). */
+int dfm_ref_mat_iluk(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                     const double* diag, const double* off, int lev, unsigned cap, unsigned* frowptr,
+                     unsigned* fcolind, double* fdiag, double* foff, unsigned* fncrs);
 /* LsSol::CLinearSystem + CPreconditioner_ILU(0) + Solve_PCG / Solve_PBiCGSTAB.
  * Returns 0 when the solver reported convergence, 3 when it did not, 1 on ILU failure. */
 int dfm_ref_mat_solve(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, const double* rhs, int method,
                       double tol, unsigned maxit, unsigned* iters, double* conv, double* x,
                       double* t_ilu, double* t_solve);
+/* The same with CPreconditioner_ILU::SetFillInLevel(lev). */
+int dfm_ref_mat_solve_lev(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                          const double* diag, const double* off, const double* rhs, int method,
+                          double tol, unsigned maxit, int lev, unsigned* iters, double* conv, double* x,
+                          double* t_ilu, double* t_solve);
 
 /* ---- matrix level (complex, b = 1) ---- */
 int dfm_ref_zmat_spmv(unsigned N, const unsigned* rowptr, const unsigned* colind,

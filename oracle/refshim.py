@@ -59,6 +59,9 @@ def lib():
         L.dfm_ref_mat_precond.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp]
         L.dfm_ref_mat_solve.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                         C.c_uint, up, dp, dp, dp, dp]
+        L.dfm_ref_mat_iluk.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
+        L.dfm_ref_mat_solve_lev.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
+                                            C.c_uint, C.c_int, up, dp, dp, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
         _lib = L
@@ -169,12 +172,29 @@ def mat_precond(N, b, rowptr, colind, fdiag, foff, vec):
     return v
 
 
-def mat_solve(N, b, rowptr, colind, diag, off, rhs, method=PCG, tol=1e-10, maxit=10000):
+def mat_solve(N, b, rowptr, colind, diag, off, rhs, method=PCG, tol=1e-10, maxit=10000, lev=0):
     x = np.zeros(N * b)
     it, conv, ti, ts = C.c_uint(), C.c_double(), C.c_double(), C.c_double()
-    rc = lib().dfm_ref_mat_solve(N, b, _u(rowptr), _u(colind), _d(diag), _d(off), _d(np.ascontiguousarray(rhs)),
-                                 method, tol, maxit, C.byref(it), C.byref(conv), _d(x), C.byref(ti), C.byref(ts))
+    rc = lib().dfm_ref_mat_solve_lev(N, b, _u(rowptr), _u(colind), _d(diag), _d(off),
+                                     _d(np.ascontiguousarray(rhs)), method, tol, maxit, lev, C.byref(it),
+                                     C.byref(conv), _d(x), C.byref(ti), C.byref(ts))
     return rc, x, it.value, conv.value, ti.value, ts.value
+
+
+def mat_iluk(N, b, rowptr, colind, diag, off, lev):
+    """CMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp:
+    (rc, frowptr, fcolind, fdiag, foff)."""
+    n = C.c_uint()
+    o = off if off.size else np.zeros(1)
+    lib().dfm_ref_mat_iluk(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, 0, None, None, None, None,
+                           C.byref(n))
+    fr = np.zeros(N + 1, np.uint32)
+    fc = np.zeros(max(n.value, 1), np.uint32)
+    fd = np.zeros(N * b * b)
+    fo = np.zeros(max(n.value, 1) * b * b)
+    rc = lib().dfm_ref_mat_iluk(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, n.value, _u(fr), _u(fc),
+                                _d(fd), _d(fo), C.byref(n))
+    return rc, fr, fc[: n.value], fd, fo[: n.value * b * b]
 
 
 def zmat_ilu0(N, rowptr, colind, diag, off):

@@ -59,10 +59,24 @@ int main(int argc, char** argv) {
     dfm_lsol::DeviceVector x2(ctx, A.VectorSize());
     r.copy_from(f);
     const bool ok2 = dfm_lsol::Solve_PBiCGSTAB(conv2, it2, A, M, r, x2);
+    // ILU(1): CPreconditioner_ILU::SetFillInLevel before SetLinearSystem
+    dfm_lsol::CPreconditioner_ILU M1;
+    M1.SetFillInLevel(1);
+    M1.SetLinearSystem(A);
+    if (!M1.SetValue(A)) return 2;
+    double conv3 = 1e-10;
+    unsigned it3 = 1000;
+    dfm_lsol::DeviceVector x3(ctx, A.VectorSize());
+    r.copy_from(f);
+    const bool ok3 = dfm_lsol::Solve_PCG(conv3, it3, A, M1, r, x3);
+    std::vector<double> xh3(A.VectorSize());
+    x3.download(xh3.data());
     std::printf("{\"pcg_ok\": %s, \"pcg_iters\": %u, \"pcg_conv\": %.17g, \"bicg_ok\": %s, \"bicg_iters\": %u, "
-                "\"bicg_conv\": %.17g, \"x\": [",
-                ok ? "true" : "false", it, conv, ok2 ? "true" : "false", it2, conv2);
+                "\"bicg_conv\": %.17g, \"ilu1_ok\": %s, \"ilu1_iters\": %u, \"x\": [",
+                ok ? "true" : "false", it, conv, ok2 ? "true" : "false", it2, conv2, ok3 ? "true" : "false", it3);
     for (size_t k = 0; k < xh.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh[k]);
+    std::printf("], \"x_ilu1\": [");
+    for (size_t k = 0; k < xh3.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh3[k]);
     std::printf("]}\n");
     dfm_buf_free(ctx.get(), flags);
     dfm_mesh_destroy(mesh);

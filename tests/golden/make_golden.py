@@ -85,5 +85,25 @@ def generate(path=HERE):
         print(f"{name}: N={S.N} b={S.b} ncrs={S.ncrs} iters={it} conv={conv:.3e}")
 
 
+def generate_iluk(path=HERE):
+    """ILU(k) fixtures: a seeded system, the reference's fill pattern and
+    factor (CMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp)
+    and its Solve_PCG with CPreconditioner_ILU::SetFillInLevel(lev)."""
+    for name, S, lev in [("iluk1_solid3d_4x2x2", cases.solid3d(4, 2, 2)[1], 1),
+                         ("iluk2_poisson_n8", cases.poisson(8)[1], 2),
+                         ("iluk3_solid2d_n5", cases.solid2d(5, np.random.default_rng(5).lognormal(0, 0.5, 50))[1],
+                          3)]:
+        rc, fr, fc, fd, fo = R.mat_iluk(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, lev)
+        assert rc == 0
+        rc, x, it, conv, _, _ = R.mat_solve(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, S.rhs, tol=1e-10,
+                                            maxit=2000, lev=lev)
+        assert rc == 0
+        np.savez_compressed(os.path.join(path, f"{name}.npz"), lev=lev, b=S.b, rowptr=S.rowptr, colind=S.colind,
+                            diag=S.diag, off=S.off, rhs=S.rhs, frowptr=fr, fcolind=fc, ilu_diag=fd, ilu_off=fo, x=x,
+                            iters=it, conv=conv, tol=1e-10)
+        print(f"{name}: N={S.N} b={S.b} ncrs={S.colind.size} -> {fc.size} iters={it} conv={conv:.3e}")
+
+
 if __name__ == "__main__":
     generate()
+    generate_iluk()

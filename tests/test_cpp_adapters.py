@@ -51,3 +51,8 @@ def test_adapter_program_matches_oracle(demo):
     assert out["pcg_ok"] and abs(out["pcg_iters"] - ref["iters"]) <= 1
     assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
     assert out["bicg_ok"] and abs(out["bicg_iters"] - refb["iters"]) <= 2
+    ns1, fpat, fd1, fo1 = S.iluk(1)  # SetFillInLevel(1)
+    ref1 = S.solve_fill(fpat, fd1, fo1, tol=1e-10, maxit=1000)
+    x1 = np.array(out["x_ilu1"])
+    assert out["ilu1_ok"] and abs(out["ilu1_iters"] - ref1["iters"]) <= 1 and ref1["iters"] < ref["iters"]
+    assert np.linalg.norm(x1 - ref1["x"]) <= 1e-8 * np.linalg.norm(ref1["x"])

@@ -36,11 +36,11 @@ SYSTEMS = {
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
 @pytest.mark.parametrize("lanes", [4, 8, 16, 32])
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
 def test_spmv_matches_oracle(ctx, name, lanes, kernel):
     S = SYSTEMS[name]()
     if kernel >= 1 and S.cplx:
-        pytest.skip("kernels 1 and 2 are real-only")
+        pytest.skip("kernels 1, 2 and 3 are real-only")
     A = make(ctx, S)
     A.lanes = lanes
     A.spmv_kernel = kernel
@@ -194,7 +194,7 @@ def test_determinism(ctx):
     assert np.array_equal(outs[0], outs[1])
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
 def test_spmv_large_rows_and_tiles(ctx, kernel):
     """Rows of very different lengths and a system spanning many TMA tiles
     (block rows with up to 60 neighbours; tiles cut by rows and by bytes)."""

@@ -157,3 +157,38 @@ def test_switching_sweep_recaptures(ctx):
         x = torch.zeros_like(r)
         rc, it, conv = lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=2000)
         assert rc == lib.OK and _rel(x.cpu().numpy(), ref["x"]) <= X_TOL, mode
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("method", ["pcg", "pbicgstab", "pcg_mixed_op32"])
+def test_solvers_with_each_spmv_kernel(ctx, kernel, method):
+    """Every SpMV kernel inside the solvers: the fused (p, Ap) dot of PCG, the
+    two fused dots of PBiCGSTAB, and the FP32 values plus the true residual
+    b - A x (y0 form, |r|^2) of the mixed solve with the FP32 operator."""
+    from delfem_b200 import lib
+    S = cases.solid3d(6, 3, 3)[1]
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pbicgstab" if method == "pbicgstab" else "pcg", tol=1e-10, maxit=2000)
+    A, M = _gpu(ctx, S)
+    A.spmv_kernel = kernel
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    old = ctx.mixed_operator
+    try:
+        if method == "pcg":
+            rc, it, conv = lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=2000)
+        elif method == "pbicgstab":
+            rc, it, conv = lib.solve_pbicgstab(A, M, r, x, tol=1e-10, maxit=2000)
+        else:
+            ctx.mixed_operator = 1
+            rc, it, conv = lib.solve_pcg_mixed(A, M, r, x, tol=1e-10, maxit=4000)
+    finally:
+        ctx.mixed_operator = old
+    assert rc == lib.OK, (rc, it, conv)
+    xg = x.cpu().numpy()
+    if method == "pcg_mixed_op32":  # stops on the FP64 true residual
+        res = S.rhs - S.spmv(1.0, xg, 0.0, np.zeros_like(S.rhs))
+        assert np.linalg.norm(res) < 1e-10 * np.linalg.norm(S.rhs)
+        assert _rel(xg, ref["x"]) <= 1e-7
+    else:
+        assert _rel(xg, ref["x"]) <= X_TOL

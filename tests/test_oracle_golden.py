@@ -11,7 +11,9 @@ import pytest
 from delfem_b200.meshes import Mesh
 from oracle import port as P
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+_ALL = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+ILUK = [p for p in _ALL if os.path.basename(p).startswith("iluk")]
+GOLDEN = [p for p in _ALL if p not in ILUK]
 METHOD = {0: "pcg", 1: "pbicgstab", 2: "pcocg"}
 POISSON2D, SOLID2D, SOLID3D, HELMHOLTZ2D = 1, 2, 3, 4
 
@@ -79,3 +81,22 @@ def test_fixture_edge_case_maxit_is_recorded():
     max_iter, conv_ratio = its input tolerance)."""
     g = np.load([p for p in GOLDEN if p.endswith("maxit.npz")][0])
     assert bool(g["ok"]) and int(g["iters"]) == int(g["maxit"]) and float(g["conv"]) == float(g["tol"])
+
+
+@pytest.mark.parametrize("path", ILUK, ids=[os.path.basename(p)[:-4] for p in ILUK])
+def test_oracle_iluk_matches_reference_fixture(path):
+    """ILU(k): the fill pattern (AddFracPtn), the factor on it and the
+    ILU(k)-preconditioned Solve_PCG, bit-identical to the reference's."""
+    g = np.load(path)
+    S = P.System(g["rowptr"], g["colind"], int(g["b"]))
+    S.diag[:] = g["diag"]
+    S.off[:] = g["off"]
+    S.rhs[:] = g["rhs"]
+    ns, fpat, fd, fo = S.iluk(int(g["lev"]))
+    _same(fpat[0], g["frowptr"], "fill rowptr")
+    _same(fpat[1], g["fcolind"], "fill colind")
+    _same(fd, g["ilu_diag"], "ILU(k) diagonal")
+    _same(fo, g["ilu_off"], "ILU(k) off-diagonal")
+    o = S.solve_fill(fpat, fd, fo, tol=float(g["tol"]), maxit=2000)
+    _same(o["x"], g["x"], "x")
+    assert o["iters"] == int(g["iters"]) and o["conv"] == float(g["conv"])

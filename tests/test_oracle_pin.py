@@ -68,3 +68,42 @@ def test_oracle_pinned_to_reference(case):
     out = S.solve(pfd, pfo, method=method, tol=1e-10, maxit=3000)
     assert out["iters"] == it and out["conv"] == conv and _eq(out["x"], x)
     assert out["ok"] == (rc == 0)
+
+
+ILUK_SYSTEMS = {
+    "poisson14": lambda: cases.poisson(14)[1],
+    "poisson_coef": lambda: cases.poisson(10, np.random.default_rng(8).lognormal(0, 1, 2 * 10 * 10))[1],
+    "solid2d": lambda: cases.solid2d(7, np.random.default_rng(9).lognormal(0, 0.5, 2 * 7 * 7))[1],
+    "solid3d": lambda: cases.solid3d(5, 2, 2)[1],
+    "random_b1": lambda: cases.random_spd_like(120, 1, seed=11),
+    "random_b3": lambda: cases.random_spd_like(70, 3, seed=12),
+}
+
+
+@pytest.mark.parametrize("name", list(ILUK_SYSTEMS))
+@pytest.mark.parametrize("lev", [1, 2, 3, -1])
+def test_iluk_pinned_to_reference(name, lev):
+    """ILU(k) symbolic fill (AddFracPtn, including its keep-the-first-level
+    rule that makes ILU(3) smaller than ILU(2) on some meshes), the values'
+    initialisation and the numeric factor on the fill pattern: bit-identical
+    to CMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp."""
+    S = ILUK_SYSTEMS[name]()
+    ns, (fr, fc, fdia), fd, fo = S.iluk(lev)
+    rc, rfr, rfc, rfd, rfo = R.mat_iluk(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, lev)
+    assert rc == 0 and ns == 0
+    assert np.array_equal(fr, rfr) and np.array_equal(fc, rfc)
+    assert _eq(fd, rfd) and _eq(fo, rfo)
+    assert fc.size >= S.colind.size
+
+
+@pytest.mark.parametrize("lev", [0, 1, 2])
+def test_iluk_pcg_pinned_to_reference(lev):
+    """Solve_PCG with CPreconditioner_ILU::SetFillInLevel(lev): the same x,
+    iteration count and convergence ratio."""
+    S = cases.solid3d(6, 3, 3)[1]
+    ns, fpat, fd, fo = S.iluk(lev)
+    o = S.solve_fill(fpat, fd, fo, tol=1e-10, maxit=2000)
+    rc, x, it, conv, _, _ = R.mat_solve(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, S.rhs, tol=1e-10, maxit=2000,
+                                        lev=lev)
+    assert rc == 0 and o["ok"]
+    assert o["iters"] == it and _eq(o["x"], x) and o["conv"] == conv
