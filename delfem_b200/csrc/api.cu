@@ -106,6 +106,7 @@ const char* dfm_status_string(int s) {
     case DFM_OK: return "ok";
     case DFM_ERR_INVALID: return "invalid argument";
     case DFM_ERR_CUDA: return "CUDA error";
+    case DFM_ERR_IO: return "file could not be opened or read";
     case DFM_ERR_NOMEM: return "out of device memory";
     case DFM_NOT_CONVERGED: return "not converged";
     case DFM_BREAKDOWN: return "breakdown";

@@ -14,7 +14,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
 
-OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED = range(9)
+(OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, NOT_CONVERGED, BREAKDOWN, SINGULAR_PIVOT, WAIT_TIMEOUT, ERR_UNSUPPORTED,
+ ERR_IO) = range(10)
 REAL, COMPLEX = 0, 1
 HOST, DEVICE = 0, 1
 PCG, PBICGSTAB, PCOCG, PCG_MIXED, PCOCG_MIXED = 0, 1, 2, 3, 4
@@ -54,6 +55,7 @@ PROTOS = {
     "dfm_mat_get_spmv_kernel": (_i, [_vp, _ip]),
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
+    "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
     "dfm_mesh_pattern": (_i, [_vp, _up, _up, C.POINTER(C.c_size_t)]),
@@ -352,6 +354,22 @@ def coef_grad_poisson2d(G: Mesh, alpha, lam, u, grad):
     _sync_torch()
     check(lib().dfm_coef_grad_poisson2d(G.h, alpha, _ptr(lam), _ptr(u), _ptr(grad)), "dfm_coef_grad_poisson2d")
     return grad
+
+
+def read_complex_matrix_text(path):
+    """The reference's complex matrix text format (CZMatDia_BlkCrs(file_path)):
+    (N, rowptr, colind, diag, off) on the host, values interleaved (re, im)."""
+    L = lib()
+    n, m = C.c_uint(), C.c_uint()
+    p = os.fsencode(path)
+    check(L.dfm_zmat_read_text(p, C.byref(n), C.byref(m), None, None, None, None), "dfm_zmat_read_text")
+    rp = np.zeros(n.value + 1, np.uint32)
+    ci = np.zeros(max(m.value, 1), np.uint32)
+    d = np.zeros(max(2 * n.value, 1))
+    o = np.zeros(max(2 * m.value, 1))
+    check(L.dfm_zmat_read_text(p, C.byref(n), C.byref(m), rp.ctypes.data_as(_up), ci.ctypes.data_as(_up),
+                               d.ctypes.data_as(_dp), o.ctypes.data_as(_dp)), "dfm_zmat_read_text")
+    return n.value, rp, ci[: m.value], d[: 2 * n.value], o[: 2 * m.value]
 
 
 def apply_dirichlet(A: Matrix, flags, rhs=None):

@@ -46,7 +46,8 @@ typedef enum dfm_status {
   DFM_BREAKDOWN = 5,         /* p.Ap <= 0, rho == 0 or a non-finite scalar */
   DFM_SINGULAR_PIVOT = 6,    /* more than 10 singular ILU pivots (reference nmax_sing) */
   DFM_WAIT_TIMEOUT = 7,      /* a bounded device-side wait ran out */
-  DFM_ERR_UNSUPPORTED = 8    /* block size / value type not supported by this entry */
+  DFM_ERR_UNSUPPORTED = 8,   /* block size / value type not supported by this entry */
+  DFM_ERR_IO = 9             /* a file could not be opened or read */
 } dfm_status;
 
 enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
@@ -121,6 +122,19 @@ DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, doub
  * launches of y = A x (the tuned kernel) on the context's stream between one
  * pair of CUDA events, after one untimed launch; *ms = average per launch. */
 DFM_API int dfm_time_spmv(dfm_mat A, const double* x, double* y, int reps, float* ms);
+
+/* Reads a complex matrix with scalar blocks from the reference's text format
+ * (CZMatDia_BlkCrs(const std::string& file_path), src/matvec/zmatdia_blkcrs.cpp:
+ * 108-173): "nblk nnz", then nnz lines "icol irow re im", icol = row.  Host
+ * only.  With rowptr == NULL it reports *N and *ncrs (off-diagonal entries);
+ * then rowptr[N+1], colind[ncrs], diag[2N] and off[2 ncrs] (re, im
+ * interleaved; each nullable) receive the matrix, ready for dfm_mat_create
+ * (DFM_COMPLEX) and dfm_mat_set_values.  Rows without entries are empty with
+ * a zero diagonal and each row's columns come out ascending; a repeated
+ * off-diagonal column, an index out of range or a decreasing row is
+ * DFM_ERR_INVALID, an unreadable file DFM_ERR_IO. */
+DFM_API int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowptr, unsigned* colind,
+                               double* diag, double* off);
 
 /* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
 /* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]

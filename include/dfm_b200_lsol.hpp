@@ -121,6 +121,18 @@ class CMatDia_BlkCrs {
     A.SetValueFromReference(m);
     return A;
   }
+  // MatVec::CZMatDia_BlkCrs(const std::string& file_path): a complex matrix
+  // from the reference's text format (dfm_zmat_read_text).
+  static CMatDia_BlkCrs FromTextFile(Context& c, const std::string& path) {
+    unsigned n = 0, ncrs = 0;
+    check(dfm_zmat_read_text(path.c_str(), &n, &ncrs, nullptr, nullptr, nullptr, nullptr), "FromTextFile");
+    std::vector<unsigned> rp(n + 1), ci(ncrs);
+    std::vector<double> d(2 * (size_t)n), o(2 * (size_t)ncrs);
+    check(dfm_zmat_read_text(path.c_str(), &n, &ncrs, rp.data(), ci.data(), d.data(), o.data()), "FromTextFile");
+    CMatDia_BlkCrs A(c, n, 1, rp.data(), ci.data(), true);
+    A.SetValue(d.data(), o.data());
+    return A;
+  }
   template <class RefMat>
   void SetValueFromReference(const RefMat& m) {
     const size_t bb = (size_t)len_ * len_;

@@ -636,4 +636,22 @@ int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind
   return 0;
 }
 
+int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncrs, unsigned* rowptr,
+                      unsigned* colind, double* diag, double* off) {
+  Quiet q;
+  MatVec::CZMatDia_BlkCrs m{std::string(path)};
+  *N = m.NBlkMatCol();
+  *ncrs = m.NCrs();
+  if (!rowptr || m.NCrs() > cap) return 2;
+  rowptr[0] = 0;
+  for (unsigned i = 0; i < *N; i++) {
+    unsigned n = 0;
+    const unsigned* c = m.GetPtrIndPSuP(i, n);
+    if (n) std::memcpy(colind + rowptr[i], c, sizeof(unsigned) * n);
+    rowptr[i + 1] = rowptr[i] + n;
+  }
+  read_zmat(m, diag, off);
+  return 0;
+}
+
 }  // extern "C"

@@ -92,6 +92,10 @@ int dfm_ref_mat_solve_lev(unsigned N, unsigned b, const unsigned* rowptr, const 
 int dfm_ref_zmat_spmv(unsigned N, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, double alpha, const double* x,
                       double beta, double* y);
+/* CZMatDia_BlkCrs(file_path): pattern and values as read by the reference
+ * (*N, *ncrs always; the arrays when rowptr != NULL and cap >= *ncrs, else 2). */
+int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncrs, unsigned* rowptr,
+                      unsigned* colind, double* diag, double* off);
 int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, double* fdiag, double* foff);
 

@@ -62,6 +62,7 @@ def lib():
         L.dfm_ref_mat_iluk.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
         L.dfm_ref_mat_solve_lev.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                             C.c_uint, C.c_int, up, dp, dp, dp, dp]
+        L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
         _lib = L
@@ -208,3 +209,16 @@ def zmat_spmv(N, rowptr, colind, diag, off, alpha, x, beta, y):
     y = np.array(y, dtype=np.float64, copy=True)
     lib().dfm_ref_zmat_spmv(N, _u(rowptr), _u(colind), _d(diag), _d(off), alpha, _d(np.ascontiguousarray(x)), beta, _d(y))
     return y
+
+
+def zmat_read(path):
+    """The reference's CZMatDia_BlkCrs(file_path): (N, rowptr, colind, diag, off)."""
+    n, m = C.c_uint(), C.c_uint()
+    p = os.fsencode(path)
+    lib().dfm_ref_zmat_read(p, 0, C.byref(n), C.byref(m), None, None, None, None)
+    rp = np.zeros(n.value + 1, np.uint32)
+    ci = np.zeros(max(m.value, 1), np.uint32)
+    d = np.zeros(max(2 * n.value, 1))
+    o = np.zeros(max(2 * m.value, 1))
+    lib().dfm_ref_zmat_read(p, m.value, C.byref(n), C.byref(m), _u(rp), _u(ci), _d(d), _d(o))
+    return n.value, rp, ci[: m.value], d[: 2 * n.value], o[: 2 * m.value]

@@ -90,3 +90,23 @@ def adjoint_case(n, seed=0, nobs=256):
     fixed = np.unique(m.bnd.ravel())
     load = meshes.right_edge_traction(m, n)
     return m, theta, theta_t, obs, fixed, load
+
+
+def write_zmat_text(path, rowptr, colind, diag, off, shuffle_rows=None, skip_diag=()):
+    """Writes a complex matrix in the reference's text format (read by
+    CZMatDia_BlkCrs(file_path)): "nblk nnz", then "icol irow re im" per entry,
+    rows ascending, the diagonal among the row's entries in column order.
+    shuffle_rows: a numpy Generator to shuffle the columns inside each row;
+    skip_diag: rows written without a diagonal entry."""
+    N = rowptr.size - 1
+    lines = []
+    for i in range(N):
+        ent = [(int(colind[s]), off[2 * s], off[2 * s + 1]) for s in range(rowptr[i], rowptr[i + 1])]
+        if i not in skip_diag:
+            ent.append((i, diag[2 * i], diag[2 * i + 1]))
+        ent.sort()
+        if shuffle_rows is not None:
+            shuffle_rows.shuffle(ent)
+        lines += [f"{i} {j} {float(re)!r} {float(im)!r}" for j, re, im in ent]
+    with open(path, "w") as f:
+        f.write(f"{N} {len(lines)}\n" + "\n".join(lines) + "\n")

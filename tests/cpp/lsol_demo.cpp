@@ -77,7 +77,31 @@ int main(int argc, char** argv) {
     for (size_t k = 0; k < xh.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh[k]);
     std::printf("], \"x_ilu1\": [");
     for (size_t k = 0; k < xh3.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh3[k]);
-    std::printf("]}\n");
+    std::printf("]");
+    // optional: a complex matrix in the reference's text format (argv[2]) and
+    // its right-hand side (argv[3], one "re im" pair per row), solved by PCOCG
+    if (argc > 3) {
+      dfm_lsol::CMatDia_BlkCrs Z = dfm_lsol::CMatDia_BlkCrs::FromTextFile(ctx, argv[2]);
+      std::vector<double> bh(Z.VectorSize());
+      FILE* fb = std::fopen(argv[3], "r");
+      if (!fb) return 3;
+      for (double& v : bh)
+        if (std::fscanf(fb, "%lf", &v) != 1) { std::fclose(fb); return 3; }
+      std::fclose(fb);
+      dfm_lsol::CPreconditioner_ILU MZ(Z);
+      if (!MZ.SetValue(Z)) return 2;
+      dfm_lsol::DeviceVector rz(ctx, Z.VectorSize()), xz(ctx, Z.VectorSize());
+      rz.upload(bh.data());
+      double convz = 1e-10;
+      unsigned itz = 3000;
+      const bool okz = dfm_lsol::Solve_PCOCG(convz, itz, Z, MZ, rz, xz);
+      std::vector<double> xzh(Z.VectorSize());
+      xz.download(xzh.data());
+      std::printf(", \"pcocg_ok\": %s, \"pcocg_iters\": %u, \"x_file\": [", okz ? "true" : "false", itz);
+      for (size_t k = 0; k < xzh.size(); k++) std::printf("%s%.17g", k ? ", " : "", xzh[k]);
+      std::printf("]");
+    }
+    std::printf("}\n");
     dfm_buf_free(ctx.get(), flags);
     dfm_mesh_destroy(mesh);
   } catch (const dfm_lsol::Error& e) {

@@ -104,6 +104,20 @@ def generate_iluk(path=HERE):
         print(f"{name}: N={S.N} b={S.b} ncrs={S.colind.size} -> {fc.size} iters={it} conv={conv:.3e}")
 
 
+def generate_zmat_text(path=HERE):
+    """A complex matrix in the reference's text format (a Helmholtz disk
+    system with two rows lacking their diagonal entry and shuffled columns) and
+    the pattern and values the reference's CZMatDia_BlkCrs(file_path) reads
+    from it."""
+    m, S = cases.helmholtz(4)
+    txt = os.path.join(path, "zmat_helmholtz_r4.txt")
+    cases.write_zmat_text(txt, S.rowptr, S.colind, S.diag, S.off, shuffle_rows=None, skip_diag=(2, 5))
+    N, rp, ci, d, o = R.zmat_read(txt)
+    np.savez_compressed(os.path.join(path, "zmatref_helmholtz_r4.npz"), N=N, rowptr=rp, colind=ci, diag=d, off=o)
+    print(f"zmat_helmholtz_r4: N={N} ncrs={ci.size}")
+
+
 if __name__ == "__main__":
     generate()
     generate_iluk()
+    generate_zmat_text()

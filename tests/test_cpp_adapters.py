@@ -34,6 +34,25 @@ def test_adapter_program_compiles_and_links(demo):
 
 
 @pytest.mark.gpu
+def test_adapter_reads_complex_matrix_text(demo, tmp_path):
+    """CMatDia_BlkCrs::FromTextFile (CZMatDia_BlkCrs(file_path)) + PCOCG from a
+    C++ program, against the oracle's COCG on the same system."""
+    from tests import cases
+    m, S = cases.helmholtz(8)
+    mp, bp = tmp_path / "z.txt", tmp_path / "b.txt"
+    cases.write_zmat_text(str(mp), S.rowptr, S.colind, S.diag, S.off)
+    bp.write_text("\n".join(repr(float(v)) for v in S.rhs) + "\n")
+    r = subprocess.run([demo, "8", str(mp), str(bp)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    ns, fd, fo = S.ilu0()
+    ref = S.solve(fd, fo, method="pcocg", tol=1e-10, maxit=3000)
+    x = np.array(out["x_file"])
+    assert out["pcocg_ok"] and abs(out["pcocg_iters"] - ref["iters"]) <= 2
+    assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
+
+
+@pytest.mark.gpu
 def test_adapter_program_matches_oracle(demo):
     from delfem_b200 import meshes
     from oracle import port as P
