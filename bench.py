@@ -437,6 +437,10 @@ def run_ours(args, rank, world):
     m, G, A, b_dev, t_asm = build_c2(ctx, torch, dev)
     N, b, ncrs = A.N, A.b, A.ncrs
     M = lib.ILU(A)
+    # range-sweep CTAs as patches across the beam's long axis (the autotuner
+    # times this partition beside balanced ranges of the natural order)
+    part, nparts = lib.sweep_partition_patches(m.coord, torch.cuda.get_device_properties(dev).multi_processor_count)
+    M.set_sweep_partition(part, nparts)
     r = torch.empty_like(b_dev)
     x = torch.empty_like(b_dev)
     torch.cuda.synchronize()
@@ -493,6 +497,11 @@ def run_ours(args, rank, world):
     y = torch.empty_like(b_dev)
     t_spmv = A.time_spmv(x, y, 50)
     t_apply = M.time_apply(r, y, 20)
+    M0 = lib.ILU(A)  # the same preconditioner with balanced ranges of the natural order only
+    M0.factor()
+    t_apply_nat = M0.time_apply(r, y, 20)
+    sweep_nat = M0.sweep
+    M0.close()
     t_factor = timed(lambda: M.factor(), 3)
     B_spmv, B_ilu, B_it = alg_bytes(N, ncrs, b)
     peaks_p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -509,7 +518,8 @@ def run_ours(args, rank, world):
                          "kernel": A.spmv_kernel, "lanes": A.lanes},
         "ilu0_fwd_bwd": {"ms": t_apply * 1e3, "alg_bytes": B_ilu, "gbs": B_ilu / t_apply / 1e9,
                          "frac": B_ilu / t_apply / 1e9 / hbm, "share_of_step": share_sweep,
-                         "sweep_mode": M.sweep},
+                         "sweep_mode": M.sweep, "partition_parts": nparts,
+                         "ms_without_partition": t_apply_nat * 1e3, "sweep_mode_without_partition": sweep_nat},
         "ilu0_factor": {"ms": t_factor * 1e3},
         "pcg_iteration": {"ms": t_iter * 1e3, "alg_bytes": B_it, "gbs": B_it / t_iter / 1e9},
         "assembly_c2": {"ms": t_asm * 1e3},

@@ -514,6 +514,31 @@ int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) 
   return set_poll_sleep(poll_sleep_ns);
 }
 
+int dfm_ilu_set_sweep_partition(dfm_ilu M, const unsigned* part, unsigned nparts) {
+  if (!M) return DFM_ERR_INVALID;
+  if (part) {
+    if (nparts == 0 || nparts > (unsigned)M->ctx->nsm) return DFM_ERR_INVALID;  // one co-resident CTA per part
+    for (unsigned i = 0; i < M->N; i++)
+      if (part[i] >= nparts) return DFM_ERR_INVALID;
+  }
+  DFM_CUDA_TRY(cudaStreamSynchronize(M->ctx->stream));
+  solve_release(M);  // captured solves hold the old plans
+  sweep_plan_free(&M->plan_f);
+  sweep_plan_free(&M->plan_b);
+  sweep_plan_free(&M->plan32_f);
+  sweep_plan_free(&M->plan32_b);
+  if (part) {
+    M->part_of.assign(part, part + M->N);
+    M->nparts = nparts;
+  } else {
+    M->part_of.clear();
+    M->nparts = 0;
+  }
+  M->sweep = 0;  // autotuned again on next use
+  M->plan_gen++;
+  return DFM_OK;
+}
+
 int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {
   if (!M || !mode) return DFM_ERR_INVALID;
   *mode = M->sweep;

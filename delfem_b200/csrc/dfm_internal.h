@@ -105,6 +105,8 @@ struct dfm_ilu_s {
   dfm_mat fillpat = nullptr;   // ILU(k), k != 0: owned pattern-only matrix of the filled pattern
   unsigned* d_fillmap = nullptr;  // ILU(k): factor slot of each of user's off-diagonal slots
   int fill_level = 0;
+  std::vector<unsigned> part_of;  // optional row partition for the range sweeps: part of every row
+  unsigned nparts = 0;
   unsigned N = 0, b = 1, ncrs = 0;
   int vt = DFM_REAL;
   unsigned* d_diaind = nullptr;
@@ -182,7 +184,10 @@ int set_poll_sleep(unsigned ns);
 // sweep.cu
 // merge: steps are pairs of levels (the second level's operands on the
 // first are substituted by products with the factor; see sweep.cu)
-int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge = false);
+// part: the CTAs are the parts of the ILU's row partition (G must be its
+// part count) instead of balanced ranges of the natural row order
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge = false,
+                     bool part = false);
 void sweep_plan_free(SweepPlan* P);
 int sweep_plan_refresh(dfm_ilu M, SweepPlan* P);
 int ilu_set_ranges(dfm_ilu M, int G, bool merge = false);

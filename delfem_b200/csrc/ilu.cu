@@ -55,6 +55,35 @@ DFM_DEVINL T poll_value(const T* p, DevStatus* st, uint64_t wait_ns, int where) 
   }
 }
 
+// The K consecutive values of one row (a b x b block's operand, or re/im):
+// all K are read before any is checked and the missing ones are re-read
+// together, so a row costs one L2 round trip per pass, not one per value.
+template <int K, typename T>
+DFM_DEVINL void poll_values(const T* p, T* v, DevStatus* st, uint64_t wait_ns, int where) {
+#pragma unroll
+  for (int c = 0; c < K; c++) v[c] = ld_relaxed(p + c);
+  auto missing = [&]() {
+    bool m = false;
+#pragma unroll
+    for (int c = 0; c < K; c++) m |= Sent<T>::is(v[c]);
+    return m;
+  };
+  if (!missing()) return;
+  SpinGuard g(wait_ns);
+  const unsigned nap = c_poll_sleep_ns;
+  for (;;) {
+    if (nap) __nanosleep(nap);
+#pragma unroll
+    for (int c = 0; c < K; c++)
+      if (Sent<T>::is(v[c])) v[c] = ld_relaxed(p + c);
+    if (!missing()) return;
+    if (g.expired() || ((g.n & 1023u) == 0 && ld_status(st) != 0)) {
+      raise_error(st, DFM_WAIT_TIMEOUT, where);
+      return;
+    }
+  }
+}
+
 DFM_DEVINL void wait_epoch(const unsigned* flag, unsigned epoch, DevStatus* st, uint64_t wait_ns, int where) {
   if (ld_acquire_u32(flag) == epoch) return;
   SpinGuard g(wait_ns);
@@ -316,8 +345,7 @@ k_sweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned*
 #pragma unroll
       for (int e = 0; e < BB; e++) mv[e] = __ldcs(foff + (size_t)s * BB + e);
       TX xv[B];
-#pragma unroll
-      for (int c = 0; c < B; c++) xv[c] = poll_value(out + (size_t)col * B + c, st, wait_ns, FWD ? 3 : 4);
+      poll_values<B>(out + (size_t)col * B, xv, st, wait_ns, FWD ? 3 : 4);
       block_mv<B>(acc, mv, xv);
     }
 #pragma unroll
@@ -381,8 +409,9 @@ k_zsweep_syncfree(unsigned N, const unsigned* __restrict__ order, const unsigned
       const unsigned col = __ldg(colind + s);
       const TV mv = __ldcs(foff + s);
       const double2 m = make_double2((double)mv.x, (double)mv.y);
-      const double xr = poll_value(o64 + 2 * (size_t)col, st, wait_ns, FWD ? 5 : 6);
-      const double xi = poll_value(o64 + 2 * (size_t)col + 1, st, wait_ns, FWD ? 5 : 6);
+      double xz[2];
+      poll_values<2>(o64 + 2 * (size_t)col, xz, st, wait_ns, FWD ? 5 : 6);
+      const double xr = xz[0], xi = xz[1];
       re += m.x * xr - m.y * xi;
       im += m.x * xi + m.y * xr;
     }
@@ -798,7 +827,7 @@ int ilu_prepare(dfm_ilu M, bool f32) {
       SweepPlan& P64 = f ? M->plan_b : M->plan_f;
       SweepPlan& P32 = f ? M->plan32_b : M->plan32_f;
       if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr || P32.merged != P64.merged) {
-        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32, P64.merged))) return rc;
+        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32, P64.merged, P64.part))) return rc;
         P32.lpr = P64.lpr;
         M->plan_gen++;  // captured graphs hold the old plan's buffers
       }
@@ -902,30 +931,47 @@ int ilu_autotune(dfm_ilu M) {
       }
       return rc;
     };
-    for (int G : cand) {
-      if (G < 1 || G == last) continue;
-      last = G;
+    // the caller's row partition (one CTA per part) first, then balanced
+    // ranges of the natural order at every CTA count
+    bool best_part = false;
+    auto try_G = [&](int G, bool part) -> int {
       SweepPlan pf, pb;
-      if (sweep_plan_build(M, true, G, 8, 8, &pf) != DFM_OK || sweep_plan_build(M, false, G, 8, 8, &pb) != DFM_OK) {
+      if (sweep_plan_build(M, true, G, 8, 8, &pf, false, part) != DFM_OK ||
+          sweep_plan_build(M, false, G, 8, 8, &pb, false, part) != DFM_OK) {
         sweep_plan_free(&pf);
         sweep_plan_free(&pb);
         cudaGetLastError();
-        continue;  // slice does not fit in shared memory at this CTA count
+        return DFM_OK;  // slice does not fit in shared memory at this CTA count
       }
       float t = 1e30f;
       const int rc = try_plans(pf, pb, {0, 2}, &t);
-      if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) {
+      if (rc != DFM_OK && rc != DFM_ERR_UNSUPPORTED) return rc;
+      if (rc == DFM_OK && t < best3) { best3 = t; best_G = G; best_part = part; }
+      return DFM_OK;
+    };
+    if (M->nparts > 0 && M->nparts <= (unsigned)nsm) {
+      const int rc = try_G((int)M->nparts, true);
+      if (rc) {
         sweep_plan_free(&best_f);
         sweep_plan_free(&best_b);
         return rc;
       }
-      if (rc == DFM_OK && t < best3) { best3 = t; best_G = G; }
+    }
+    for (int G : cand) {
+      if (G < 1 || G == last) continue;
+      last = G;
+      const int rc = try_G(G, false);
+      if (rc) {
+        sweep_plan_free(&best_f);
+        sweep_plan_free(&best_b);
+        return rc;
+      }
     }
     if (best_G > 0) {
       for (int mg = 0; mg < 2; mg++) {  // barrier-free kernel unmerged, then merged pairs with every kernel
         SweepPlan pf, pb;
-        if (sweep_plan_build(M, true, best_G, 8, 8, &pf, mg != 0) != DFM_OK ||
-            sweep_plan_build(M, false, best_G, 8, 8, &pb, mg != 0) != DFM_OK) {
+        if (sweep_plan_build(M, true, best_G, 8, 8, &pf, mg != 0, best_part) != DFM_OK ||
+            sweep_plan_build(M, false, best_G, 8, 8, &pb, mg != 0, best_part) != DFM_OK) {
           sweep_plan_free(&pf);
           sweep_plan_free(&pb);
           cudaGetLastError();
@@ -955,8 +1001,10 @@ int ilu_autotune(dfm_ilu M) {
 
 int ilu_set_ranges(dfm_ilu M, int G, bool merge) {
   SweepPlan pf, pb;
-  int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge);
-  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge);
+  const bool part = M->nparts > 0;  // a row partition, when set, fixes the CTAs
+  if (part) G = (int)M->nparts;
+  int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge, part);
+  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge, part);
   if (rc) {
     sweep_plan_free(&pf);
     sweep_plan_free(&pb);

@@ -25,6 +25,7 @@
 // increasing level order and all CTAs are co-resident, so every wait ends
 // (induction on the level); all waits are also bounded.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "dfm_internal.h"
@@ -69,17 +70,38 @@ DFM_DEVINL int ld_status2(const DevStatus* st) {
   return v;
 }
 
-template <typename T>
-DFM_DEVINL T poll_remote(const T* p, DevStatus* st, uint64_t wait_ns, int where) {
-  T v = ld_relaxed(p);
-  if (!Sent<T>::is(v)) return v;
+// Re-reads the remote operands of a batch that still hold the sentinel: every
+// missing value is re-read in each pass, so a batch whose producers are just
+// publishing costs one L2 round trip per pass instead of one per value (a
+// b x b row of B values would otherwise wait for B round trips in a row).
+// xo[u]: operand codes (remote = 0x80000000 | row); xv[u][c]: values read so
+// far.  The wait is bounded: past wait_ns (or once another wait has failed)
+// it records DFM_WAIT_TIMEOUT and returns.
+template <int B, int NB, typename TX>
+DFM_DEVINL void repoll_batch(const unsigned* xo, TX (*xv)[B], const TX* out, DevStatus* st, uint64_t wait_ns,
+                             int where) {
+  auto missing = [&]() {
+    bool m = false;
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+      if ((xo[u] & 0xc0000000u) == 0x80000000u)
+#pragma unroll
+        for (int c = 0; c < B; c++) m |= Sent<TX>::is(xv[u][c]);
+    return m;
+  };
+  if (!missing()) return;
   SpinGuard g(wait_ns);
   for (;;) {
-    v = ld_relaxed(p);
-    if (!Sent<T>::is(v)) return v;
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+      if ((xo[u] & 0xc0000000u) == 0x80000000u)
+#pragma unroll
+        for (int c = 0; c < B; c++)
+          if (Sent<TX>::is(xv[u][c])) xv[u][c] = ld_relaxed(out + (size_t)(xo[u] & 0x7fffffffu) * B + c);
+    if (!missing()) return;
     if (g.expired() || ((g.n & 1023u) == 0 && ld_status2(st) != 0)) {
       raise_error(st, DFM_WAIT_TIMEOUT, where);
-      return v;
+      return;
     }
   }
 }
@@ -157,13 +179,7 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
 #pragma unroll
       for (int c = 0; c < B; c++) pf.xv[u][c] = X[o + c];
   }
-#pragma unroll
-  for (int u = 0; u < kOpBatch; u++)
-    if (pf.xo[u] != 0xffffffffu && (pf.xo[u] & 0xc0000000u) == 0x80000000u)
-#pragma unroll
-      for (int c = 0; c < B; c++)
-        if (Sent<TX>::is(pf.xv[u][c]))
-          pf.xv[u][c] = poll_remote(out + (size_t)(pf.xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+  repoll_batch<B, kOpBatch, TX>(pf.xo, pf.xv, out, st, wait_ns, FWD ? 11 : 12);
 #pragma unroll
   for (int u = 0; u < kOpBatch; u++) {
     const unsigned kk = rd.y + lane + u * LPR;
@@ -200,13 +216,7 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
         for (int c = 0; c < B; c++) xv[u][c] = X[o + c];
       }
     }
-#pragma unroll
-    for (int u = 0; u < kOpBatch; u++)
-      if (xo[u] != 0xffffffffu && (xo[u] & 0xc0000000u) == 0x80000000u)
-#pragma unroll
-        for (int c = 0; c < B; c++)
-          if (Sent<TX>::is(xv[u][c]))
-            xv[u][c] = poll_remote(out + (size_t)(xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+    repoll_batch<B, kOpBatch, TX>(xo, xv, out, st, wait_ns, FWD ? 11 : 12);
 #pragma unroll
     for (int u = 0; u < kOpBatch; u++) {
       const unsigned kk = kb + u * LPR;
@@ -246,7 +256,7 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
 #pragma unroll
     for (int rr = 0; rr < B; rr++) {
       xi[rr] = o[rr];
-      st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+      st_relaxed(out + (size_t)rd.w * B + rr, o[rr]);
     }
   }
 }
@@ -256,15 +266,20 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
 // DOT 1: real dot over len*B entries; DOT 2: complex matrices run as real 2x2
 // blocks (re, im per row), the unconjugated sum of rdot_i out_i with the real
 // and imaginary parts in part[] and part[kMaxBlocks + ...].
+// rows: the plan's row order (slot k of the slice is row rows[a0 + k]), or
+// nullptr for the natural order (row a0 + k).
+DFM_DEVINL size_t slot_row(const unsigned* rows, unsigned p) { return rows ? (size_t)rows[p] : (size_t)p; }
+
 template <int B, int DOT, typename TX>
 DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0, unsigned len, bool alive,
-                          double* part) {
+                          double* part, const unsigned* rows) {
   if constexpr (DOT == 2) {
     static_assert(B == 2, "complex rows are 2x2 real blocks");
     double re = 0.0, im = 0.0;
     if (alive)
       for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
-        const double rr = (double)rdot[(size_t)(a0 + k) * 2], ri = (double)rdot[(size_t)(a0 + k) * 2 + 1];
+        const size_t gi = slot_row(rows, a0 + k);
+        const double rr = (double)rdot[gi * 2], ri = (double)rdot[gi * 2 + 1];
         const double xr = (double)X[2 * k], xi = (double)X[2 * k + 1];
         re += rr * xr - ri * xi;
         im += rr * xi + ri * xr;
@@ -274,7 +289,8 @@ DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0,
   } else {
     double dacc = 0.0;
     if (alive)
-      for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) dacc += (double)rdot[(size_t)a0 * B + k] * (double)X[k];
+      for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
+        dacc += (double)rdot[slot_row(rows, a0 + k / B) * B + k % B] * (double)X[k];
     block_partial<kSweepThreads>(dacc, part);
   }
 }
@@ -282,7 +298,8 @@ DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0,
 template <int B, int LPR, typename TV, typename TX, bool FWD, int DOT, bool PIPE>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
-               const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
+               const unsigned* __restrict__ range, const unsigned* __restrict__ rows,
+               const char* __restrict__ blob, unsigned stage_bytes,
                int nstage, unsigned x_bytes, const TX* __restrict__ in, TX* out, const TX* __restrict__ rdot,
                double* part, KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st,
                uint64_t wait_ns) {
@@ -311,7 +328,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
   uint64_t* bar_data = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
 
   // X slice <- in[a0:a1) (rows overwrite their entry with the output)
-  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[(size_t)a0 * B + k];
+  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[slot_row(rows, a0 + k / B) * B + k % B];
   unsigned issued_end = q0;  // stage thread: chunks [q0, issued_end) requested
   if (threadIdx.x == kStageThread) {
     s_alive = 1;
@@ -419,13 +436,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
               for (int c = 0; c < B; c++) xv[u][c] = X[o + c];
             }
           }
-#pragma unroll
-          for (int u = 0; u < kOpBatch; u++)
-            if (xo[u] != 0xffffffffu && (xo[u] & 0xc0000000u) == 0x80000000u)
-#pragma unroll
-              for (int c = 0; c < B; c++)
-                if (Sent<TX>::is(xv[u][c]))
-                  xv[u][c] = poll_remote(out + (size_t)(xo[u] & 0x7fffffffu) * B + c, st, wait_ns, FWD ? 11 : 12);
+          repoll_batch<B, kOpBatch, TX>(xo, xv, out, st, wait_ns, FWD ? 11 : 12);
 #pragma unroll
           for (int u = 0; u < kOpBatch; u++) {
             const unsigned kk = kb + u * LPR;
@@ -465,7 +476,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
 #pragma unroll
           for (int rr = 0; rr < B; rr++) {
             xi[rr] = o[rr];
-            st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+            st_relaxed(out + (size_t)rd.w * B + rr, o[rr]);
           }
         }
       }
@@ -487,7 +498,7 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
     }
   }
   }
-  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, true, part);  // (rdot, out) over this CTA's range
+  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, true, part, rows);  // (rdot, out) over this CTA's range
   // after an aborted wait, copies already requested must land before the CTA exits
   if (threadIdx.x == kStageThread && !s_alive) {
     for (unsigned q = q0; q < issued_end; q++) {
@@ -534,7 +545,8 @@ DFM_DEVINL TX poll_local(const TX* p, volatile int* alive, DevStatus* st, uint64
 template <int B, int LPR, typename TV, typename TX, bool FWD, int DOT>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
-                  const unsigned* __restrict__ range, const char* __restrict__ blob, unsigned stage_bytes,
+                  const unsigned* __restrict__ range, const unsigned* __restrict__ rows,
+                  const char* __restrict__ blob, unsigned stage_bytes,
                   int nstage, unsigned x_bytes, unsigned max_chunks, const TX* __restrict__ in, TX* out,
                   const TX* __restrict__ rdot, double* part, KrylovScalars* sc, const double* rr_part,
                   int rr_nparts, DevStatus* st, uint64_t wait_ns) {
@@ -636,7 +648,7 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
     TX vin[B];
     if (lane == 0)
 #pragma unroll
-      for (int c = 0; c < B; c++) vin[c] = in[((size_t)a0 + rd.x) * B + c];
+      for (int c = 0; c < B; c++) vin[c] = in[(size_t)rd.w * B + c];
     double acc[B];
 #pragma unroll
     for (int c = 0; c < B; c++) acc[c] = 0.0;
@@ -651,9 +663,7 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
         const unsigned col = xo & 0x7fffffffu;
 #pragma unroll
         for (int c = 0; c < B; c++) xv[c] = ld_relaxed(out + (size_t)col * B + c);
-#pragma unroll
-        for (int c = 0; c < B; c++)
-          if (Sent<TX>::is(xv[c])) xv[c] = poll_remote(out + (size_t)col * B + c, st, wait_ns, FWD ? 11 : 12);
+        repoll_batch<B, 1, TX>(&xo, reinterpret_cast<TX(*)[B]>(xv), out, st, wait_ns, FWD ? 11 : 12);
       } else {
 #pragma unroll
         for (int c = 0; c < B; c++) xv[c] = poll_local(X + xo + c, alive, st, wait_ns);
@@ -690,7 +700,7 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
       }
 #pragma unroll
       for (int rr = 0; rr < B; rr++) {
-        st_relaxed(out + ((size_t)a0 + rd.x) * B + rr, o[rr]);
+        st_relaxed(out + (size_t)rd.w * B + rr, o[rr]);
         st_volatile_s(X + rd.x * B + rr, o[rr]);
       }
       // release the stage after the chunk's last row (its reads are all done:
@@ -714,7 +724,7 @@ k_sweep_ranges_nb(const ChunkDesc* __restrict__ chunks, const unsigned* __restri
     __syncwarp(gmask);
   }
   __syncthreads();
-  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, s_alive != 0, part);
+  if (DOT) range_dot<B, DOT, TX>(rdot, X, a0, len, s_alive != 0, part, rows);
   // every stage's last issued copy must have landed before the CTA exits
   if (threadIdx.x == 0)
     for (int s2 = 0; s2 < nstage; s2++) {
@@ -814,7 +824,7 @@ __global__ void k_gather_recipes(const ChunkDesc* __restrict__ chunks, unsigned 
       double* dinv = reinterpret_cast<double*>(base + cd.dinv_off);
       for (unsigned r = threadIdx.x; r < cd.nrows; r += blockDim.x) {
         double v[BB];
-        load_factor_blk<B, CPLX>(fdiag, (size_t)cd.row0 + rd[r].x, v);
+        load_factor_blk<B, CPLX>(fdiag, (size_t)rd[r].w, v);  // w: the row's global index
 #pragma unroll
         for (int e = 0; e < BB; e++) dinv[(size_t)r * BB + e] = v[e];
       }
@@ -828,13 +838,15 @@ void sweep_plan_free(SweepPlan* P) {
   cudaFree(P->d_chunks);
   cudaFree(P->d_cta_chunk);
   cudaFree(P->d_range);
+  cudaFree(P->d_rows);
   cudaFree(P->d_blob);
   cudaFree(P->d_recipe);
   cudaFree(P->d_terms);
   *P = SweepPlan();
 }
 
-int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge) {
+int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge,
+                     bool part) {
   const unsigned N = M->N;
   const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks
   const unsigned bb = b * b;
@@ -846,21 +858,43 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
   const std::vector<unsigned>& lev = fwd ? M->lev_f : M->lev_b;
   sweep_plan_free(P);
   if (N >= 0x40000000u) return DFM_ERR_UNSUPPORTED;  // operand encodings use the top two bits
-  if (G < 1) G = 1;
-  if ((unsigned)G > std::max(N, 1u)) G = std::max(N, 1u);
-  // balanced contiguous ranges by (dependency blocks + 1) per row
-  std::vector<unsigned long long> wpre(N + 1, 0);
-  for (unsigned i = 0; i < N; i++) {
-    const unsigned nb = fwd ? dia[i] - rp[i] : rp[i + 1] - dia[i];
-    wpre[i + 1] = wpre[i] + nb + 1;
+  // Rows are laid out in an order of positions; CTA c owns the positions
+  // [range[c], range[c+1]) and keeps their vector entries in its slice in that
+  // order.  Natural order: positions are rows, ranges balanced by (dependency
+  // blocks + 1) per row.  With the ILU's row partition: the rows of part c,
+  // ascending, are CTA c's positions.
+  std::vector<unsigned> order, pos;  // position -> row, row -> position (empty: the identity)
+  std::vector<unsigned> range;
+  if (part) {
+    if ((unsigned)G != M->nparts || M->part_of.size() != N) return DFM_ERR_INVALID;
+    range.assign(G + 1, 0);
+    for (unsigned i = 0; i < N; i++) range[M->part_of[i] + 1]++;
+    for (int c = 0; c < G; c++) range[c + 1] += range[c];
+    order.assign(N, 0);
+    pos.assign(N, 0);
+    std::vector<unsigned> fill(range.begin(), range.end() - 1);
+    for (unsigned i = 0; i < N; i++) {
+      pos[i] = fill[M->part_of[i]]++;
+      order[pos[i]] = i;
+    }
+  } else {
+    if (G < 1) G = 1;
+    if ((unsigned)G > std::max(N, 1u)) G = std::max(N, 1u);
+    std::vector<unsigned long long> wpre(N + 1, 0);
+    for (unsigned i = 0; i < N; i++) {
+      const unsigned nb = fwd ? dia[i] - rp[i] : rp[i + 1] - dia[i];
+      wpre[i + 1] = wpre[i] + nb + 1;
+    }
+    range.assign(G + 1, N);
+    range[0] = 0;
+    for (int c = 1; c < G; c++) {
+      const unsigned long long target = wpre[N] * (unsigned long long)c / (unsigned)G;
+      range[c] = (unsigned)(std::lower_bound(wpre.begin(), wpre.end(), target) - wpre.begin());
+      range[c] = std::max(range[c], range[c - 1]);
+    }
   }
-  std::vector<unsigned> range(G + 1, N);
-  range[0] = 0;
-  for (int c = 1; c < G; c++) {
-    const unsigned long long target = wpre[N] * (unsigned long long)c / (unsigned)G;
-    range[c] = (unsigned)(std::lower_bound(wpre.begin(), wpre.end(), target) - wpre.begin());
-    range[c] = std::max(range[c], range[c - 1]);
-  }
+  const auto pos_of = [&](unsigned row) { return pos.empty() ? row : pos[row]; };
+  const auto row_at = [&](unsigned p) { return order.empty() ? p : order[p]; };
   unsigned maxlen = 0;
   for (int c = 0; c < G; c++) maxlen = std::max(maxlen, range[c + 1] - range[c]);
   const size_t x_bytes = ((size_t)maxlen * b * vec_bytes + 127) & ~(size_t)127;
@@ -893,7 +927,10 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
     ops.clear();
     unsigned s0, s1;
     slots(i, s0, s1);
-    auto out_code = [&](unsigned col) { return (col >= a0 && col < a1) ? (col - a0) * b : (0x80000000u | col); };
+    auto out_code = [&](unsigned col) {
+      const unsigned p = pos_of(col);
+      return (p >= a0 && p < a1) ? (p - a0) * b : (0x80000000u | col);
+    };
     const bool second = merge && (lev[i] & 1u);
     if (!second) {
       for (unsigned s = s0; s < s1; s++) ops.push_back({out_code(ci[s]), make_uint4(s, 0u, 0u, 0u)});
@@ -942,7 +979,7 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
       unsigned col;
       const unsigned code = ops[q].xo;
       if (code & 0x80000000u) col = code & 0x3fffffffu;
-      else col = a0 + code / b;
+      else col = row_at(a0 + code / b);
       kmap[col] = NONE;
     }
   };
@@ -950,7 +987,7 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
     cta_chunk[c] = (unsigned)chunks.size();
     const unsigned a0 = range[c], a1 = range[c + 1];
     std::vector<unsigned> rows(a1 - a0);
-    for (unsigned i = a0; i < a1; i++) rows[i - a0] = fwd ? i : (a1 - 1 - (i - a0));
+    for (unsigned q = a0; q < a1; q++) rows[q - a0] = row_at(fwd ? q : (a1 - 1 - (q - a0)));
     std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return step(x) < step(y); });
     size_t p = 0;
     while (p < rows.size()) {
@@ -969,7 +1006,7 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
           terms.resize(tmark);  // this row starts the next chunk
           break;
         }
-        pd.rd.push_back(make_uint4(i - a0, nblk, nblk + nb, 0u));
+        pd.rd.push_back(make_uint4(pos_of(i) - a0, nblk, nblk + nb, i));  // {slot, blocks, global row}
         for (const Op& o : ops) {
           pd.xo.push_back(o.xo);
           recipe.push_back(o.rc);
@@ -1049,6 +1086,11 @@ int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, S
     DFM_CUDA_TRY(cudaMemcpyAsync(P->d_chunks, chunks.data(), sizeof(ChunkDesc) * chunks.size(), cudaMemcpyHostToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_cta_chunk, cta_chunk.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_range, range.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
+  if (!order.empty()) {
+    DFM_CUDA_TRY(cudaMalloc(&P->d_rows, sizeof(unsigned) * order.size()));
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_rows, order.data(), sizeof(unsigned) * order.size(), cudaMemcpyHostToDevice, s));
+  }
+  P->part = part;
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blob, hblob.data(), hblob.size(), cudaMemcpyHostToDevice, s));
   if (!recipe.empty())
     DFM_CUDA_TRY(cudaMemcpyAsync(P->d_recipe, recipe.data(), sizeof(uint4) * recipe.size(), cudaMemcpyHostToDevice, s));
@@ -1107,7 +1149,8 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
-                              (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
+                              (const unsigned*)P->d_range, (const unsigned*)P->d_rows, (const char*)P->d_blob,
+                              P->stage_bytes, P->nstage,
                               P->x_bytes, P->max_cta_chunks, in, out, rdot, part, sc, rr_part, rr_n, c->d_status,
                               (uint64_t)c->wait_ns);
   }
@@ -1116,7 +1159,8 @@ static cudaError_t launch_ranges(dfm_ilu M, const SweepPlan* P, const TX* in, TX
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
   if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
-                            (const unsigned*)P->d_range, (const char*)P->d_blob, P->stage_bytes, P->nstage,
+                            (const unsigned*)P->d_range, (const unsigned*)P->d_rows, (const char*)P->d_blob,
+                            P->stage_bytes, P->nstage,
                             P->x_bytes, in, out, rdot, part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
 }
 
@@ -1162,3 +1206,54 @@ int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, cons
 }
 
 }  // namespace dfm
+
+extern "C" {
+
+// Patches across the mesh's longest bounding-box axis (the direction the
+// level sets of a lexicographically numbered structured mesh advance along
+// farthest): the other axes' extent is cut into a grid of nj x nk cells (a row
+// of nj cells in 2-D) with nj * nk <= max_parts, the cells as close to square
+// as the extents allow, and a node's part is the cell its coordinates fall in.
+// Every line of nodes along the long axis then lies in one part, and a chain
+// of dependencies crosses at most about nj + nk parts.
+int dfm_sweep_partition_patches(unsigned nnode, int ndim, const double* coord, unsigned max_parts, unsigned* part,
+                                unsigned* nparts) {
+  if ((ndim != 2 && ndim != 3) || max_parts == 0 || !nparts || (nnode && (!coord || !part))) return DFM_ERR_INVALID;
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  for (int d = 0; d < ndim; d++) {
+    lo[d] = hi[d] = nnode ? coord[d] : 0.0;
+    for (unsigned i = 1; i < nnode; i++) {
+      lo[d] = std::min(lo[d], coord[(size_t)i * ndim + d]);
+      hi[d] = std::max(hi[d], coord[(size_t)i * ndim + d]);
+    }
+  }
+  int axis = 0;
+  for (int d = 1; d < ndim; d++)
+    if (hi[d] - lo[d] > hi[axis] - lo[axis]) axis = d;
+  int a = -1, bax = -1;  // the cross-section axes
+  for (int d = 0; d < ndim; d++) {
+    if (d == axis) continue;
+    if (a < 0) a = d; else bax = d;
+  }
+  unsigned nj = max_parts, nk = 1;
+  if (bax >= 0) {
+    const double ea = hi[a] - lo[a], eb = hi[bax] - lo[bax];
+    const double ratio = (ea > 0 && eb > 0) ? ea / eb : 1.0;
+    nj = (unsigned)std::max(1.0, std::min((double)max_parts, std::floor(std::sqrt((double)max_parts * ratio) + 0.5)));
+    nk = std::max(1u, max_parts / nj);
+  }
+  auto cell = [](double v, double l, double h, unsigned n) -> unsigned {
+    if (!(h > l) || n <= 1) return 0u;
+    const double t = (v - l) / (h - l) * (double)n;
+    return (unsigned)std::min<double>((double)(n - 1), std::max(0.0, std::floor(t)));
+  };
+  for (unsigned i = 0; i < nnode; i++) {
+    const unsigned qa = cell(coord[(size_t)i * ndim + a], lo[a], hi[a], nj);
+    const unsigned qb = bax >= 0 ? cell(coord[(size_t)i * ndim + bax], lo[bax], hi[bax], nk) : 0u;
+    part[i] = qa * nk + qb;
+  }
+  *nparts = nj * nk;
+  return DFM_OK;
+}
+
+}  // extern "C"

@@ -77,7 +77,9 @@ struct SweepPlan {
   size_t smem = 0;
   ChunkDesc* d_chunks = nullptr;
   unsigned* d_cta_chunk = nullptr;  // G+1 chunk ranges
-  unsigned* d_range = nullptr;      // G+1 row ranges
+  unsigned* d_range = nullptr;      // G+1 ranges of row positions
+  unsigned* d_rows = nullptr;       // with a row partition: the row at each position (else positions are rows)
+  bool part = false;                // ranges are the parts of the ILU's row partition
   char* d_blob = nullptr;
   uint4* d_recipe = nullptr;        // per packed block: {base slot, term range, sign}
   uint4* d_terms = nullptr;         // {s1, j, s2, 0}: F[s1] (D_j^-1) (F[s2])

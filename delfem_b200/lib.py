@@ -80,6 +80,8 @@ PROTOS = {
     "dfm_ilu_set_sweep": (_i, [_vp, _i]),
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
     "dfm_ilu_set_sweep_tuning": (_i, [_vp, _i, _u]),
+    "dfm_ilu_set_sweep_partition": (_i, [_vp, _up, _u]),
+    "dfm_sweep_partition_patches": (_i, [_u, _i, _dp, _u, _up, _up]),
     "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pbicgstab": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcocg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
@@ -372,6 +374,18 @@ def read_complex_matrix_text(path):
     return n.value, rp, ci[: m.value], d[: 2 * n.value], o[: 2 * m.value]
 
 
+def sweep_partition_patches(coord, max_parts):
+    """(part, nparts): patches across the longest axis of the node coordinates
+    (dfm_sweep_partition_patches), for ILU.set_sweep_partition."""
+    coord = np.ascontiguousarray(coord, np.float64)
+    n, ndim = coord.shape
+    part = np.zeros(max(n, 1), np.uint32)
+    k = C.c_uint()
+    check(lib().dfm_sweep_partition_patches(n, ndim, coord.ctypes.data_as(_dp), int(max_parts),
+                                            part.ctypes.data_as(_up), C.byref(k)), "dfm_sweep_partition_patches")
+    return part[:n], k.value
+
+
 def apply_dirichlet(A: Matrix, flags, rhs=None):
     """Dirichlet elimination with device int32 flags[N*b] (nonzero = fixed)."""
     _sync_torch()
@@ -443,6 +457,15 @@ class ILU:
         _sync_torch()
         check(lib().dfm_ilu_apply(self.h, _ptr(r), _ptr(z)), "dfm_ilu_apply")
         return z
+
+    def set_sweep_partition(self, part=None, nparts=0):
+        """Row partition of the range sweeps (part[i] = CTA of row i), or None."""
+        if part is None:
+            check(lib().dfm_ilu_set_sweep_partition(self.h, None, 0), "dfm_ilu_set_sweep_partition")
+            return
+        part = np.ascontiguousarray(part, np.uint32)
+        check(lib().dfm_ilu_set_sweep_partition(self.h, part.ctypes.data_as(_up), int(nparts)),
+              "dfm_ilu_set_sweep_partition")
 
     def time_apply(self, r, z, reps=20):
         """Average seconds per z = U^-1 L^-1 r over `reps` back-to-back applications."""

@@ -241,6 +241,22 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * results as 3 and 5).  Complex matrices run 3-8 as real 2x2 blocks
  * [re -im; im re]. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
+/* No counterpart in the reference (its sweeps are sequential).  A row
+ * partition for the range-partitioned sweep schedules: CTA c takes the rows
+ * with part[i] == c (part has N entries, nparts <= the GPU's SM count: one
+ * co-resident CTA per part).  The sweeps' results do not depend on it.  A
+ * caller that knows the geometry can shorten the chains of dependencies that
+ * cross CTAs, e.g. with compact patches across the direction the levels
+ * advance in.  The autotuner times the partition beside balanced ranges of the
+ * natural order and keeps the faster; explicit range modes (dfm_ilu_set_sweep
+ * 3-8) use it.  part == NULL clears it.  Resets the schedule to autotuned. */
+DFM_API int dfm_ilu_set_sweep_partition(dfm_ilu M, const unsigned* part, unsigned nparts);
+/* No counterpart in the reference.  A partition for dfm_ilu_set_sweep_partition
+ * from node coordinates (host, coord[nnode*ndim]): a grid of at most max_parts
+ * patches across the longest bounding-box axis, so that every line of nodes
+ * along that axis lies in one part.  *nparts gets the grid's cell count. */
+DFM_API int dfm_sweep_partition_patches(unsigned nnode, int ndim, const double* coord, unsigned max_parts,
+                                        unsigned* part, unsigned* nparts);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all
  * that fit) and the back-off between polls of a waiting lane in ns (global). */

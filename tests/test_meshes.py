@@ -47,3 +47,19 @@ def test_disk_level_depth():
     assert _depth(b) < 6 * 30
     with pytest.raises(ValueError):
         meshes.unit_disk_tri(3, numbering="spiral")
+
+
+def test_sweep_partition_patches():
+    """dfm_sweep_partition_patches (host only): every line of nodes along the
+    box's long axis lies in one part; a square grid of patches across it."""
+    from delfem_b200 import lib, meshes
+    m = meshes.box_tet(20, 6, 6)
+    part, nparts = lib.sweep_partition_patches(m.coord, 148)
+    assert nparts == 144 or nparts <= 148
+    p = part.reshape(7, 7, 21)  # nodes are x fastest: [k][j][i]
+    assert (p == p[:, :, :1]).all()  # constant along x
+    assert part.max() < nparts
+    part2, n2 = lib.sweep_partition_patches(m.coord, 4)
+    assert n2 == 4 and len(np.unique(part2)) == 4
+    with pytest.raises(lib.DfmError):
+        lib.sweep_partition_patches(m.coord, 0)
