@@ -295,6 +295,8 @@ def run_profile():
     ctx = lib.Context(0)
     m, G, A, b_dev, _ = build_c2(ctx, torch, 0)
     M = lib.ILU(A)
+    part, nparts = lib.sweep_partition_patches(m.coord, torch.cuda.get_device_properties(0).multi_processor_count)
+    M.set_sweep_partition(part, nparts)  # as the bench's c2 solve
     M.factor()
     x = torch.zeros_like(b_dev)
     y = torch.empty_like(b_dev)

@@ -86,3 +86,25 @@ def test_partition_rejected(ctx):
         M.set_sweep_partition(np.full(S.N, 3, np.uint32), 3)  # part index out of range
     with pytest.raises(lib.DfmError):
         M.set_sweep_partition(np.zeros(S.N, np.uint32), 100000)  # more parts than co-resident CTAs
+
+
+@pytest.mark.parametrize("sweep", [0, 3, 7])
+def test_partition_with_fill(ctx, sweep):
+    """ILU(1) under the patch partition: the partition applies to the rows of
+    the filled factor's pattern the same way; PCG to the oracle's x."""
+    from delfem_b200 import lib
+    m, S = cases.solid3d(12, 4, 4)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A, fill_level=1)
+    M.factor()
+    M.set_sweep_partition(*lib.sweep_partition_patches(m.coord, 16))
+    if sweep:
+        M.sweep = sweep
+    ns, fpat, fd, fo = S.iluk(1)
+    ref = S.solve_fill(fpat, fd, fo, tol=1e-10, maxit=2000)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcg(A, M, r, x, tol=1e-10, maxit=2000)
+    assert rc == lib.OK and abs(it - ref["iters"]) <= 2
+    assert np.linalg.norm(x.cpu().numpy() - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
