@@ -23,7 +23,10 @@
 #include <algorithm>
 #include <cerrno>
 #include <cstdio>
+#include <cmath>
 #include <cstdlib>
+#include <cstring>
+#include <string>
 #include <numeric>
 #include <vector>
 
@@ -139,6 +142,147 @@ int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* 
   if (colind) std::copy(cols.begin(), cols.end(), colind);
   if (diag) std::copy(dg.begin(), dg.end(), diag);
   if (off) std::copy(vals.begin(), vals.end(), off);
+  return DFM_OK;
+}
+
+// GiD ASCII mesh, as Msh::CMesh3D::ReadFromFile_GiDMsh (src/msh/mesh3d.cpp:
+// 601-800) and Msh::CMesher2D::ReadFromFile_GiDMsh (src/msh/mesher2d.cpp:
+// 2464-2640) read it: a header line
+//   MESH dimension <ndim> ElemType <Tetrahedra|Hexahedra|Triangle|Quadrilateral> Nnode <n>
+// then "Coordinates", lines "<id> x y z" (ids 1, 2, ... in order), "end
+// coordinates", one line, "Elements", lines "<id> v1 .. vn [material]"
+// (1-based nodes), "end elements".  Tetrahedra and hexahedra come out with 3-D
+// coordinates.  Triangles and quadrilaterals come out as the 2-D mesher makes
+// them: with ndim 3, the node cloud must be planar (the smallest of the three
+// coordinate variances at most 1e-4 of their sum, the reference's test) and
+// the axis of that smallest variance is dropped, the other two kept in cyclic
+// order (y,z / z,x / x,y); with ndim 2 the lines carry x y.  The volume
+// elements and coordinates are what the pattern and the assembly need; the
+// boundary facets the reference derives (outer bars / colour-coded
+// triangles) are not produced.
+namespace dfm {
+namespace {
+struct Lines {
+  std::vector<char> buf;
+  size_t pos = 0;
+  // next line (without the newline) or false at the end
+  bool next(const char** b, const char** e) {
+    if (pos >= buf.size() || buf[pos] == '\0') return false;
+    const char* p = buf.data() + pos;
+    size_t q = pos;
+    while (q < buf.size() && buf[q] != '\n' && buf[q] != '\0') q++;
+    *b = p;
+    *e = buf.data() + q;
+    pos = q < buf.size() && buf[q] == '\n' ? q + 1 : q;
+    return true;
+  }
+};
+bool starts(const char* b, const char* e, const char* w) {
+  size_t n = std::strlen(w);
+  return (size_t)(e - b) >= n && std::strncmp(b, w, n) == 0;
+}
+// whitespace-separated numbers of [b, e): integers or doubles
+int parse_numbers(const char* b, const char* e, double* out, int max) {
+  std::string line(b, e);
+  const char* p = line.c_str();
+  int n = 0;
+  while (n < max) {
+    char* q = nullptr;
+    const double v = std::strtod(p, &q);
+    if (q == p) break;
+    out[n++] = v;
+    p = q;
+  }
+  return n;
+}
+}  // namespace
+}  // namespace dfm
+
+int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel, unsigned* nelem,
+                      int* elem) {
+  if (!path || !ndim || !nnode || !nnoel || !nelem) return DFM_ERR_INVALID;
+  Lines L;
+  int rc = read_file(path, L.buf);
+  if (rc) return rc;
+  const char *b, *e;
+  if (!L.next(&b, &e)) return DFM_ERR_INVALID;
+  char w1[64], w2[64], w3[64], type[64], w4[64];
+  int nd = 0, nn = 0;
+  {
+    std::string h(b, e);
+    if (std::sscanf(h.c_str(), "%63s %63s %d %63s %63s %63s %d", w1, w2, &nd, w3, type, w4, &nn) != 7)
+      return DFM_ERR_INVALID;
+  }
+  const std::string t(type);
+  int want = 0;
+  bool surface = false;
+  if (t == "Tetrahedra") want = 4;
+  else if (t == "Hexahedra") want = 8;
+  else if (t == "Triangle") { want = 3; surface = true; }
+  else if (t == "Quadrilateral") { want = 4; surface = true; }
+  if (!want || nn != want) return DFM_ERR_INVALID;
+  if ((!surface && nd != 3) || (surface && nd != 2 && nd != 3)) return DFM_ERR_INVALID;
+  if (!L.next(&b, &e)) return DFM_ERR_INVALID;  // "Coordinates"
+  std::vector<double> xyz;
+  unsigned count = 0;
+  for (;;) {
+    if (!L.next(&b, &e)) return DFM_ERR_INVALID;
+    if (starts(b, e, "end coordinates")) break;
+    double v[4];
+    const int k = parse_numbers(b, e, v, 1 + nd);
+    if (k != 1 + nd || v[0] != (double)(count + 1)) return DFM_ERR_INVALID;
+    for (int d = 0; d < nd; d++) xyz.push_back(v[1 + d]);
+    count++;
+  }
+  if (count == 0) return DFM_ERR_INVALID;
+  int nd_out = nd, keep0 = 0, keep1 = 1;
+  if (surface && nd == 3) {  // planar cloud -> the 2-D mesher's coordinates
+    double ax = 0, ay = 0, az = 0, vx = 0, vy = 0, vz = 0;
+    for (unsigned i = 0; i < count; i++) {
+      const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+      ax += x; ay += y; az += z;
+      vx += x * x; vy += y * y; vz += z * z;
+    }
+    vx /= count; vy /= count; vz /= count;
+    ax /= count; ay /= count; az /= count;
+    vx -= ax * ax; vy -= ay * ay; vz -= az * az;
+    double vmin = vx;
+    int dmin = 0;
+    if (vy < vmin) { vmin = vy; dmin = 1; }
+    if (vz < vmin) { vmin = vz; dmin = 2; }
+    if (vmin > (vx + vy + vz) * 0.0001) return DFM_ERR_INVALID;  // not planar
+    keep0 = dmin == 0 ? 1 : (dmin == 1 ? 2 : 0);
+    keep1 = dmin == 0 ? 2 : (dmin == 1 ? 0 : 1);
+    nd_out = 2;
+  }
+  if (!L.next(&b, &e)) return DFM_ERR_INVALID;  // the line after "end coordinates"
+  if (!L.next(&b, &e)) return DFM_ERR_INVALID;  // "Elements"
+  std::vector<int> conn;
+  unsigned ne = 0;
+  for (;;) {
+    if (!L.next(&b, &e)) return DFM_ERR_INVALID;
+    if (starts(b, e, "end elements")) break;
+    double v[10];
+    const int k = parse_numbers(b, e, v, 1 + want);
+    if (k != 1 + want || v[0] != (double)(ne + 1)) return DFM_ERR_INVALID;
+    for (int j = 0; j < want; j++) {
+      if (!(v[1 + j] >= 1 && v[1 + j] <= (double)count) || v[1 + j] != std::floor(v[1 + j])) return DFM_ERR_INVALID;
+      conn.push_back((int)v[1 + j] - 1);
+    }
+    ne++;
+  }
+  *ndim = nd_out;
+  *nnode = count;
+  *nnoel = want;
+  *nelem = ne;
+  if (coord) {
+    for (unsigned i = 0; i < count; i++) {
+      if (nd_out == 3) for (int d = 0; d < 3; d++) coord[3 * (size_t)i + d] = xyz[3 * (size_t)i + d];
+      else if (nd == 3) { coord[2 * (size_t)i] = xyz[3 * (size_t)i + keep0]; coord[2 * (size_t)i + 1] = xyz[3 * (size_t)i + keep1]; }
+      else { coord[2 * (size_t)i] = xyz[2 * (size_t)i]; coord[2 * (size_t)i + 1] = xyz[2 * (size_t)i + 1]; }
+    }
+  }
+  if (elem) std::copy(conn.begin(), conn.end(), elem);
   return DFM_OK;
 }
 

@@ -56,6 +56,7 @@ PROTOS = {
     "dfm_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
+    "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
     "dfm_mesh_pattern": (_i, [_vp, _up, _up, C.POINTER(C.c_size_t)]),
@@ -384,6 +385,20 @@ def sweep_partition_patches(coord, max_parts):
     check(lib().dfm_sweep_partition_patches(n, ndim, coord.ctypes.data_as(_dp), int(max_parts),
                                             part.ctypes.data_as(_up), C.byref(k)), "dfm_sweep_partition_patches")
     return part[:n], k.value
+
+
+def read_gid_mesh(path):
+    """A GiD ASCII mesh as the reference reads it (dfm_gid_read_mesh):
+    (coord[nnode, ndim], elem[nelem, nnoel]) on the host, elem 0-based."""
+    L = lib()
+    p = os.fsencode(path)
+    nd, nn, ne, no = C.c_int(), C.c_uint(), C.c_uint(), C.c_int()
+    check(L.dfm_gid_read_mesh(p, C.byref(nd), C.byref(nn), None, C.byref(no), C.byref(ne), None), "dfm_gid_read_mesh")
+    coord = np.zeros((nn.value, nd.value))
+    elem = np.zeros((ne.value, no.value), np.int32)
+    check(L.dfm_gid_read_mesh(p, C.byref(nd), C.byref(nn), coord.ctypes.data_as(_dp), C.byref(no), C.byref(ne),
+                              elem.ctypes.data_as(_ip)), "dfm_gid_read_mesh")
+    return coord, elem
 
 
 def apply_dirichlet(A: Matrix, flags, rhs=None):

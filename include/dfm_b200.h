@@ -136,6 +136,20 @@ DFM_API int dfm_time_spmv(dfm_mat A, const double* x, double* y, int reps, float
 DFM_API int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowptr, unsigned* colind,
                                double* diag, double* off);
 
+/* Reads a GiD ASCII mesh as the reference's readers do
+ * (Msh::CMesh3D::ReadFromFile_GiDMsh, src/msh/mesh3d.cpp:601-800;
+ * Msh::CMesher2D::ReadFromFile_GiDMsh, src/msh/mesher2d.cpp:2464-2640).  Host
+ * only.  Tetrahedra / hexahedra: 3-D coordinates.  Triangles /
+ * quadrilaterals: 2-D coordinates, a planar 3-D node cloud projected by
+ * dropping its axis of least variance as the 2-D mesher does (a non-planar
+ * one is DFM_ERR_INVALID).  With coord == NULL it reports *ndim, *nnode,
+ * *nnoel and *nelem; then coord[nnode*ndim] and elem[nelem*nnoel] (0-based,
+ * nullable) receive the mesh, ready for dfm_mesh_create.  Boundary facets are
+ * not derived.  Malformed input is DFM_ERR_INVALID, an unreadable file
+ * DFM_ERR_IO. */
+DFM_API int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel,
+                              unsigned* nelem, int* elem);
+
 /* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
 /* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]
  * (triangles nnoel = 3 in 2D, tetrahedra 4 in 3D) and optional boundary bars

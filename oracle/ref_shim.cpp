@@ -20,7 +20,9 @@
 
 #include "delfem/field.h"
 #include "delfem/field_world.h"
+#include "delfem/mesh3d.h"
 #include "delfem/mesh_interface.h"
+#include "delfem/mesher2d.h"
 #include "delfem/femeqn/eqn_helmholtz.h"
 #include "delfem/femeqn/eqn_linear_solid2d.h"
 #include "delfem/femeqn/eqn_linear_solid3d.h"
@@ -651,6 +653,41 @@ int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncr
     rowptr[i + 1] = rowptr[i] + n;
   }
   read_zmat(m, diag, off);
+  return 0;
+}
+
+// The reference's GiD readers, read back through their public accessors.
+int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned cap_elem, unsigned* nnode,
+                     unsigned* nelem, int* nnoel, double* coord, int* elem) {
+  Quiet q;
+  if (want2d) {
+    Msh::CMesher2D m;
+    if (!m.ReadFromFile_GiDMsh(path)) return 1;
+    const std::vector<Com::CVector2D>& v = m.GetVectorAry();
+    const std::vector<Msh::CTriAry2D>& ta = m.GetTriArySet();
+    *nnode = (unsigned)v.size();
+    *nnoel = 3;
+    *nelem = ta.empty() ? 0u : (unsigned)ta[0].m_aTri.size();
+    if (!coord || *nnode > cap_node || *nelem > cap_elem) return 2;
+    for (unsigned i = 0; i < *nnode; i++) { coord[2 * i] = v[i].x; coord[2 * i + 1] = v[i].y; }
+    for (unsigned e = 0; e < *nelem; e++)
+      for (int k = 0; k < 3; k++) elem[3 * e + k] = (int)ta[0].m_aTri[e].v[k];
+    return 0;
+  }
+  Msh::CMesh3D m;
+  if (!m.ReadFromFile_GiDMsh(path)) return 1;
+  const auto& v = m.GetVectorAry();
+  *nnode = (unsigned)v.size();
+  const bool hex = !m.GetHexArySet().empty();
+  *nnoel = hex ? 8 : 4;
+  *nelem = hex ? (unsigned)m.GetHexArySet()[0].m_aHex.size()
+               : (m.GetTetArySet().empty() ? 0u : (unsigned)m.GetTetArySet()[0].m_aTet.size());
+  if (!coord || *nnode > cap_node || *nelem > cap_elem) return 2;
+  for (unsigned i = 0; i < *nnode; i++) { coord[3 * i] = v[i].x; coord[3 * i + 1] = v[i].y; coord[3 * i + 2] = v[i].z; }
+  for (unsigned e = 0; e < *nelem; e++)
+    for (int k = 0; k < *nnoel; k++)
+      elem[(size_t)*nnoel * e + k] =
+          hex ? (int)m.GetHexArySet()[0].m_aHex[e].v[k] : (int)m.GetTetArySet()[0].m_aTet[e].v[k];
   return 0;
 }
 

@@ -96,6 +96,12 @@ int dfm_ref_zmat_spmv(unsigned N, const unsigned* rowptr, const unsigned* colind
  * (*N, *ncrs always; the arrays when rowptr != NULL and cap >= *ncrs, else 2). */
 int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncrs, unsigned* rowptr,
                       unsigned* colind, double* diag, double* off);
+/* Msh::CMesher2D (want2d) or Msh::CMesh3D ReadFromFile_GiDMsh: node
+ * coordinates (2 or 3 per node) and the element array, 0-based.  Sizes always;
+ * the arrays when coord != NULL and they fit the caps (else 2); 1 when the
+ * reference's reader returned false. */
+int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned cap_elem, unsigned* nnode,
+                     unsigned* nelem, int* nnoel, double* coord, int* elem);
 int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, double* fdiag, double* foff);
 

@@ -62,6 +62,7 @@ def lib():
         L.dfm_ref_mat_iluk.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
         L.dfm_ref_mat_solve_lev.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                             C.c_uint, C.c_int, up, dp, dp, dp, dp]
+        L.dfm_ref_gid_read.argtypes = [C.c_char_p, C.c_int, C.c_uint, C.c_uint, up, up, ip, dp, ip]
         L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
@@ -222,3 +223,18 @@ def zmat_read(path):
     o = np.zeros(max(2 * m.value, 1))
     lib().dfm_ref_zmat_read(p, m.value, C.byref(n), C.byref(m), _u(rp), _u(ci), _d(d), _d(o))
     return n.value, rp, ci[: m.value], d[: 2 * n.value], o[: 2 * m.value]
+
+
+def gid_read(path, want2d):
+    """The reference's GiD reader (2-D mesher or 3-D mesh): (rc, coord, elem)."""
+    nn, ne, no = C.c_uint(), C.c_uint(), C.c_int()
+    p = os.fsencode(path)
+    rc = lib().dfm_ref_gid_read(p, int(want2d), 0, 0, C.byref(nn), C.byref(ne), C.byref(no), None, None)
+    if rc == 1:
+        return 1, None, None
+    nd = 2 if want2d else 3
+    coord = np.zeros((nn.value, nd))
+    elem = np.zeros((ne.value, no.value), np.int32)
+    rc = lib().dfm_ref_gid_read(p, int(want2d), nn.value, ne.value, C.byref(nn), C.byref(ne), C.byref(no),
+                                _d(coord.reshape(-1)), _i(elem.reshape(-1)))
+    return rc, coord, elem

@@ -110,3 +110,20 @@ def write_zmat_text(path, rowptr, colind, diag, off, shuffle_rows=None, skip_dia
         lines += [f"{i} {j} {float(re)!r} {float(im)!r}" for j, re, im in ent]
     with open(path, "w") as f:
         f.write(f"{N} {len(lines)}\n" + "\n".join(lines) + "\n")
+
+
+def write_gid_mesh(path, coord, elem, elem_type, ndim=3):
+    """Writes a GiD ASCII mesh (the format Msh::CMesh3D / CMesher2D
+    ReadFromFile_GiDMsh read): coordinates padded to `ndim` columns, 1-based
+    nodes, a material column on every element line."""
+    coord = np.asarray(coord, np.float64)
+    elem = np.asarray(elem)
+    if coord.shape[1] < ndim:
+        coord = np.hstack([coord, np.zeros((coord.shape[0], ndim - coord.shape[1]))])
+    lines = [f"MESH dimension {ndim} ElemType {elem_type} Nnode {elem.shape[1]}", "Coordinates"]
+    lines += [f"{i + 1} " + " ".join(repr(float(v)) for v in c[:ndim]) for i, c in enumerate(coord)]
+    lines += ["end coordinates", "", "Elements"]
+    lines += [f"{e + 1} " + " ".join(str(int(v) + 1) for v in row) + " 1" for e, row in enumerate(elem)]
+    lines += ["end elements"]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
