@@ -117,7 +117,30 @@ def generate_zmat_text(path=HERE):
     print(f"zmat_helmholtz_r4: N={N} ncrs={ci.size}")
 
 
+def generate_gid(path=HERE):
+    """Two GiD ASCII meshes (a tetrahedral box, scaled by pi so that the
+    coordinates use every digit; a triangulated square on the plane x = 0.25
+    in 3-D) and what the reference's readers (Msh::CMesh3D and
+    Msh::CMesher2D ReadFromFile_GiDMsh) build from them."""
+    m = meshes.box_tet(3, 2, 2)
+    f3 = os.path.join(path, "gid_box_tet.msh")
+    cases.write_gid_mesh(f3, m.coord * np.pi, m.elem, "Tetrahedra")
+    rc, c3, e3 = R.gid_read(f3, want2d=False)
+    assert rc == 0
+    t = meshes.unit_square_tri(3)
+    p3 = np.zeros((t.nnode, 3))
+    p3[:, 0], p3[:, 1], p3[:, 2] = 0.25, t.coord[:, 0] * 1.3, t.coord[:, 1] * 0.7
+    f2 = os.path.join(path, "gid_square_tri.msh")
+    cases.write_gid_mesh(f2, p3, t.elem, "Triangle")
+    rc, c2, e2 = R.gid_read(f2, want2d=True)
+    assert rc == 0
+    np.savez_compressed(os.path.join(path, "gidref_meshes.npz"), tet_coord=c3, tet_elem=e3, tri_coord=c2,
+                        tri_elem=e2)
+    print(f"gid: {c3.shape[0]} nodes / {e3.shape[0]} tets, {c2.shape[0]} nodes / {e2.shape[0]} triangles")
+
+
 if __name__ == "__main__":
     generate()
     generate_iluk()
     generate_zmat_text()
+    generate_gid()

@@ -74,6 +74,19 @@ def test_planar_triangles_match_reference_2d_mesher(tmp_path, plane):
     assert np.array_equal(elem, m.elem)
 
 
+def test_reader_matches_reference_fixture():
+    """tests/golden/gid_*.msh as the reference's readers built them
+    (tests/golden/make_golden.py)."""
+    import os
+    from delfem_b200 import lib
+    g = os.path.join(os.path.dirname(__file__), "golden")
+    ref = np.load(os.path.join(g, "gidref_meshes.npz"))
+    coord, elem = lib.read_gid_mesh(os.path.join(g, "gid_box_tet.msh"))
+    assert np.array_equal(coord, ref["tet_coord"]) and np.array_equal(elem, ref["tet_elem"])
+    coord, elem = lib.read_gid_mesh(os.path.join(g, "gid_square_tri.msh"))
+    assert np.array_equal(coord, ref["tri_coord"]) and np.array_equal(elem, ref["tri_elem"])
+
+
 def test_two_d_file_and_rejections(tmp_path):
     from delfem_b200 import lib
     m = meshes.unit_square_tri(3)
