@@ -558,6 +558,7 @@ def run_ours(args, rank, world):
         t0 = time.perf_counter()
         M1 = lib.ILU(A, fill_level=1)
         t_sym = time.perf_counter() - t0
+        M1.set_sweep_partition(part, nparts)  # the same patches as the ILU(0) solve
         x1 = torch.zeros_like(b_dev)
 
         def k1step():
