@@ -57,6 +57,7 @@ PROTOS = {
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
+    "dfm_boundary_matrix": (_i, [_u, _u, _up, _up, _dp, _dp, _ip, _up, _up, _dp, _dp, _up]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
     "dfm_mesh_pattern": (_i, [_vp, _up, _up, C.POINTER(C.c_size_t)]),
@@ -399,6 +400,30 @@ def read_gid_mesh(path):
     check(L.dfm_gid_read_mesh(p, C.byref(nd), C.byref(nn), coord.ctypes.data_as(_dp), C.byref(no), C.byref(ne),
                               elem.ctypes.data_as(_ip)), "dfm_gid_read_mesh")
     return coord, elem
+
+
+def boundary_matrix(rowptr, colind, diag, off, flags, b):
+    """CLinearSystem_Save's boundary matrix B from K's values before the
+    Dirichlet elimination (dfm_boundary_matrix): (brow, bcol, bdiag, boff);
+    MakeResidual is then r = Force - B u (Matrix.spmv(-1, u, 1, r))."""
+    rowptr = np.ascontiguousarray(rowptr, np.uint32)
+    colind = np.ascontiguousarray(colind if np.size(colind) else np.zeros(1), np.uint32)
+    diag = np.ascontiguousarray(diag, np.float64)
+    off = np.ascontiguousarray(off if np.size(off) else np.zeros(1), np.float64)
+    flags = np.ascontiguousarray(flags, np.int32)
+    N = rowptr.size - 1
+    n = C.c_uint()
+    args = (N, b, rowptr.ctypes.data_as(_up), colind.ctypes.data_as(_up), diag.ctypes.data_as(_dp),
+            off.ctypes.data_as(_dp), flags.ctypes.data_as(_ip))
+    L = lib()
+    check(L.dfm_boundary_matrix(*args, None, None, None, None, C.byref(n)), "dfm_boundary_matrix")
+    brow = np.zeros(N + 1, np.uint32)
+    bcol = np.zeros(max(n.value, 1), np.uint32)
+    bdiag = np.zeros(max(N * b * b, 1))
+    boff = np.zeros(max(n.value * b * b, 1))
+    check(L.dfm_boundary_matrix(*args, brow.ctypes.data_as(_up), bcol.ctypes.data_as(_up), bdiag.ctypes.data_as(_dp),
+                                boff.ctypes.data_as(_dp), C.byref(n)), "dfm_boundary_matrix")
+    return brow, bcol[: n.value], bdiag[: N * b * b], boff[: n.value * b * b]
 
 
 def apply_dirichlet(A: Matrix, flags, rhs=None):

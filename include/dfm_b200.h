@@ -150,6 +150,21 @@ DFM_API int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, un
 DFM_API int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel,
                               unsigned* nelem, int* elem);
 
+/* The stored boundary matrix B of Fem::Ls::CLinearSystem_Save
+ * (src/femls/linearsystem_fieldsave.cpp:64-260; pattern CMat_BlkCrs::
+ * SetPatternBoundary, src/matvec/mat_blkcrs.cpp:1177-1265; masks
+ * SetBoundaryConditionInverse_Colum / SetBoundaryCondition_Row, :876-951),
+ * host only: from K's values BEFORE dfm_apply_dirichlet (rowptr, colind, diag,
+ * off in the library's layout) and the flags (N*b, nonzero = fixed), B keeps
+ * the entries of free rows and fixed columns.  With brow == NULL it reports
+ * *bncrs; then brow[N+1], bcol[*bncrs], bdiag[N*b*b], boff[*bncrs*b*b]
+ * (each but brow nullable) receive B for dfm_mat_create + dfm_mat_set_values.
+ * CLinearSystem_Save::MakeResidual (:206-246), r = Force - B u, is then
+ * dfm_spmv(B, -1, u, 1, r) with r holding Force. */
+DFM_API int dfm_boundary_matrix(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                                const double* diag, const double* off, const int* flags, unsigned* brow,
+                                unsigned* bcol, double* bdiag, double* boff, unsigned* bncrs);
+
 /* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
 /* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]
  * (triangles nnoel = 3 in 2D, tetrahedra 4 in 3D) and optional boundary bars

@@ -27,6 +27,7 @@
 #ifndef DFM_B200_LSOL_HPP
 #define DFM_B200_LSOL_HPP
 
+#include <cmath>
 #include <cstddef>
 #include <stdexcept>
 #include <string>
@@ -222,6 +223,19 @@ class CPreconditioner_ILU {
   dfm_ilu h_ = nullptr;
   int lev_ = 0;
 };
+
+// Fem::Ls::CLinearSystem_Save::MakeResidual: {r} := {force} - [B]{u} with B
+// the stored boundary matrix (dfm_boundary_matrix); returns |r|.
+inline double MakeResidual(const CMatDia_BlkCrs& B, const DeviceVector& force, const DeviceVector& u,
+                           DeviceVector& r) {
+  r.copy_from(force);
+  B.MatVec(-1.0, u, 1.0, r);
+  std::vector<double> h(B.VectorSize());
+  r.download(h.data());
+  double s = 0.0;
+  for (double v : h) s += v * v;
+  return std::sqrt(s);
+}
 
 namespace detail {
 template <class Fn>

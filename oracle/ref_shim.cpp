@@ -36,6 +36,7 @@
 #include "delfem/ls/preconditioner.h"
 #include "delfem/ls/solver_ls_iter.h"
 #include "delfem/matvec/bcflag_blk.h"
+#include "delfem/matvec/mat_blkcrs.h"
 #include "delfem/matvec/matdia_blkcrs.h"
 #include "delfem/matvec/matdiafrac_blkcrs.h"
 #include "delfem/matvec/vector_blk.h"
@@ -653,6 +654,72 @@ int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncr
     rowptr[i + 1] = rowptr[i] + n;
   }
   read_zmat(m, diag, off);
+  return 0;
+}
+
+// CLinearSystem_Save's boundary matrix built the reference's way: the pattern
+// of CMat_BlkCrs::SetPatternBoundary over K, the entries filled with K's
+// values (what the element routines merge into both), the two masks of
+// FinalizeMarge, then MakeResidual's product r = force - B u.  B is returned
+// row by row in the reference's own entry order (the diagonal block first).
+int dfm_ref_boundary_residual(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                              const double* diag, const double* off, const int* flags, const double* force,
+                              const double* u, unsigned cap, unsigned* brow, unsigned* bcol, double* bval,
+                              unsigned* bncrs, double* r) {
+  Quiet q;
+  MatVec::CMatDia_BlkCrs* K = make_mat(N, b, rowptr, colind, diag, off);
+  MatVec::CBCFlag bc(N, b);
+  for (unsigned i = 0; i < N; i++)
+    for (unsigned d = 0; d < b; d++)
+      if (flags[(size_t)i * b + d]) bc.SetBC(i, d);
+  MatVec::CMat_BlkCrs B(N, b, N, b);
+  B.SetPatternBoundary(*K, bc, bc);
+  B.SetZero();  // allocates the values (CLinearSystem_Save::InitializeMarge does the same)
+  *bncrs = B.NCrs();
+  const unsigned bb = b * b;
+  for (unsigned i = 0; i < N; i++) {
+    unsigned n = 0;
+    const unsigned* cols = B.GetPtrIndPSuP(i, n);
+    double* vals = B.GetPtrValPSuP(i, n);
+    for (unsigned k = 0; k < n; k++) {
+      const unsigned j = cols[k];
+      const double* src = nullptr;
+      if (j == i) src = K->GetPtrValDia(i);
+      else {
+        unsigned nk = 0;
+        const unsigned* kc = K->GetPtrIndPSuP(i, nk);
+        const double* kv = K->GetPtrValPSuP(i, nk);
+        for (unsigned t = 0; t < nk; t++)
+          if (kc[t] == j) src = kv + (size_t)t * bb;
+      }
+      std::memcpy(vals + (size_t)k * bb, src, sizeof(double) * bb);
+    }
+  }
+  B.SetBoundaryConditionInverse_Colum(bc);
+  B.SetBoundaryCondition_Row(bc);
+  MatVec::CVector_Blk vu(N, b), vr(N, b);
+  for (unsigned i = 0; i < N; i++)
+    for (unsigned d = 0; d < b; d++) {
+      vu.SetValue(i, d, u[(size_t)i * b + d]);
+      vr.SetValue(i, d, force[(size_t)i * b + d]);
+    }
+  B.MatVec(-1.0, vu, 1.0, vr, true);
+  for (unsigned i = 0; i < N; i++)
+    for (unsigned d = 0; d < b; d++) r[(size_t)i * b + d] = vr.GetValue(i, d);
+  if (brow && B.NCrs() <= cap) {
+    brow[0] = 0;
+    for (unsigned i = 0; i < N; i++) {
+      unsigned n = 0;
+      const unsigned* cols = B.GetPtrIndPSuP(i, n);
+      const double* vals = B.GetPtrValPSuP(i, n);
+      for (unsigned k = 0; k < n; k++) {
+        bcol[brow[i] + k] = cols[k];
+        std::memcpy(bval + (size_t)(brow[i] + k) * bb, vals + (size_t)k * bb, sizeof(double) * bb);
+      }
+      brow[i + 1] = brow[i] + n;
+    }
+  }
+  delete K;
   return 0;
 }
 

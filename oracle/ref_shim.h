@@ -96,6 +96,15 @@ int dfm_ref_zmat_spmv(unsigned N, const unsigned* rowptr, const unsigned* colind
  * (*N, *ncrs always; the arrays when rowptr != NULL and cap >= *ncrs, else 2). */
 int dfm_ref_zmat_read(const char* path, unsigned cap, unsigned* N, unsigned* ncrs, unsigned* rowptr,
                       unsigned* colind, double* diag, double* off);
+/* CLinearSystem_Save's boundary matrix over K (values before elimination)
+ * and MakeResidual's r = force - B u, computed by the reference's CMat_BlkCrs
+ * (SetPatternBoundary, the two BC masks, MatVec).  *bncrs always; B row by row
+ * (brow[N+1], bcol, bval, diagonal block first as the reference stores it) when
+ * brow != NULL and cap >= *bncrs. */
+int dfm_ref_boundary_residual(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                              const double* diag, const double* off, const int* flags, const double* force,
+                              const double* u, unsigned cap, unsigned* brow, unsigned* bcol, double* bval,
+                              unsigned* bncrs, double* r);
 /* Msh::CMesher2D (want2d) or Msh::CMesh3D ReadFromFile_GiDMsh: node
  * coordinates (2 or 3 per node) and the element array, 0-based.  Sizes always;
  * the arrays when coord != NULL and they fit the caps (else 2); 1 when the

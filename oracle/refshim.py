@@ -62,6 +62,8 @@ def lib():
         L.dfm_ref_mat_iluk.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
         L.dfm_ref_mat_solve_lev.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                             C.c_uint, C.c_int, up, dp, dp, dp, dp]
+        L.dfm_ref_boundary_residual.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, ip, dp, dp, C.c_uint, up, up,
+                                                dp, up, dp]
         L.dfm_ref_gid_read.argtypes = [C.c_char_p, C.c_int, C.c_uint, C.c_uint, up, up, ip, dp, ip]
         L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
@@ -238,3 +240,21 @@ def gid_read(path, want2d):
     rc = lib().dfm_ref_gid_read(p, int(want2d), nn.value, ne.value, C.byref(nn), C.byref(ne), C.byref(no),
                                 _d(coord.reshape(-1)), _i(elem.reshape(-1)))
     return rc, coord, elem
+
+
+def boundary_residual(N, b, rowptr, colind, diag, off, flags, force, u):
+    """The reference's CLinearSystem_Save boundary matrix (row by row, diagonal
+    first) and MakeResidual's r = force - B u: (brow, bcol, bval, r)."""
+    n = C.c_uint()
+    r = np.zeros(N * b)
+    fl = np.ascontiguousarray(flags, np.int32)
+    o = off if off.size else np.zeros(1)
+    ci = colind if colind.size else np.zeros(1, np.uint32)
+    args = (N, b, _u(rowptr), _u(ci), _d(diag), _d(o), _i(fl), _d(np.ascontiguousarray(force)),
+            _d(np.ascontiguousarray(u)))
+    lib().dfm_ref_boundary_residual(*args, 0, None, None, None, C.byref(n), _d(r))
+    brow = np.zeros(N + 1, np.uint32)
+    bcol = np.zeros(max(n.value, 1), np.uint32)
+    bval = np.zeros(max(n.value, 1) * b * b)
+    lib().dfm_ref_boundary_residual(*args, n.value, _u(brow), _u(bcol), _d(bval), C.byref(n), _d(r))
+    return brow, bcol[: n.value], bval[: n.value * b * b], r

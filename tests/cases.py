@@ -127,3 +127,27 @@ def write_gid_mesh(path, coord, elem, elem_type, ndim=3):
     lines += ["end elements"]
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+def poisson_raw(n):
+    """As poisson(), before the Dirichlet elimination."""
+    m = meshes.unit_square_tri(n)
+    S = P.System(*P.pattern(m.nnode, m.elem), 1)
+    S.asm_poisson(m, 1.0, 1.0)
+    return m, S
+
+
+def solid2d_raw(n):
+    """As solid2d() with unit modulus, before the Dirichlet elimination."""
+    m = meshes.unit_square_tri(n, bnd="left")
+    S = P.System(*P.pattern(m.nnode, m.elem), 2)
+    S.asm_solid2d(m, LAM2_PS, MYU2, 0.0, 0.0, 0.0)
+    return m, S
+
+
+def solid3d_raw(nx, ny, nz):
+    """As solid3d(), before the Dirichlet elimination."""
+    m = meshes.box_tet(nx, ny, nz)
+    S = P.System(*P.pattern(m.nnode, m.elem), 3)
+    S.asm_solid3d(m, LAM3, MYU3, 1.0, 0.0, 0.0, -1.0)
+    return m, S
