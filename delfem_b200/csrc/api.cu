@@ -288,6 +288,7 @@ int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* ro
 int dfm_mat_destroy(dfm_mat A) {
   if (!A) return DFM_OK;
   cudaStreamSynchronize(A->ctx->stream);
+  solve_release_mat(A);
   cudaFree(A->d_rowptr);
   cudaFree(A->d_colind);
   cudaFree(A->d_diag);
@@ -619,8 +620,17 @@ int dfm_solve_pcocg_mixed(dfm_mat A, dfm_ilu M, double* r, double* x, double tol
   return krylov_solve(A, M, DFM_PCOCG_MIXED, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
 }
 
+int dfm_solve_cg(dfm_mat A, double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv) {
+  if (!A || A->vt != DFM_REAL || (A->N && (!r || !x))) return DFM_ERR_INVALID;
+  return krylov_solve(A, nullptr, DFM_CG, r, DFM_DEVICE, x, DFM_DEVICE, r, tol, maxit, iters, conv);
+}
+
 int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv) {
+  if (method == DFM_CG) {
+    if (!A || A->vt != DFM_REAL || (A->N && (!b_host || !x_host))) return DFM_ERR_INVALID;
+    return krylov_solve(A, nullptr, DFM_CG, b_host, DFM_HOST, x_host, DFM_HOST, nullptr, tol, maxit, iters, conv);
+  }
   if (method < DFM_PCG || method > DFM_PCOCG_MIXED) return DFM_ERR_INVALID;
   const int rc = solve_args(A, M, method, b_host, x_host);
   if (rc) return rc;

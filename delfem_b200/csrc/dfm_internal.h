@@ -76,6 +76,7 @@ struct dfm_ctx_s {
   double* d_part = nullptr;                 // 8 partial arrays of kMaxBlocks doubles
   dfm::KrylovScalars* d_scal = nullptr;
   dfm::KrylovScalars* h_scal = nullptr;     // pinned mirror
+  double* noalloc_scratch = nullptr;        // device address of noalloc.cu's static array (set on first use)
   double* part(int k) { return d_part + (size_t)k * dfm::kMaxBlocks; }
 };
 
@@ -194,8 +195,10 @@ int ilu_set_ranges(dfm_ilu M, int G, bool merge = false);
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
                         KrylovScalars* sc, const double* rr_part, int rr_n, bool f32 = false);
 // krylov.cu
-// method: DFM_PCG / DFM_PBICGSTAB / DFM_PCOCG; b and x at DFM_HOST or DFM_DEVICE.
+// method: DFM_PCG / DFM_PBICGSTAB / DFM_PCOCG / the mixed forms, or DFM_CG
+// with M == nullptr; b and x at DFM_HOST or DFM_DEVICE.
 int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where, double* x, int x_where,
                  double* r_out, double tol, unsigned maxit, unsigned* iters, double* conv);
 void solve_release(dfm_ilu M);
+void solve_release_mat(dfm_mat A);  // unpreconditioned (CG) plans of A
 }  // namespace dfm

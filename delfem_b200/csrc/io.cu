@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <new>
 #include <numeric>
 #include <vector>
 
@@ -82,16 +83,20 @@ int read_file(const char* path, std::vector<char>& buf) {
 
 using namespace dfm;
 
-extern "C" {
+namespace dfm {
+namespace {
 
-int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowptr, unsigned* colind,
-                       double* diag, double* off) {
+int zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowptr, unsigned* colind, double* diag,
+                   double* off) {
   if (!path || !N || !ncrs) return DFM_ERR_INVALID;
   Tokens t;
   int rc = read_file(path, t.buf);
   if (rc) return rc;
   long long nblk = 0, nnz = 0;
   if (!t.integer(&nblk) || !t.integer(&nnz) || nblk < 0 || nnz < 0 || nblk > 0x7fffffffLL) return DFM_ERR_INVALID;
+  // every entry line holds four numbers, at least 8 bytes with separators: a
+  // count the file cannot hold is malformed (and must not size an allocation)
+  if ((unsigned long long)nnz > t.buf.size() / 8 + 1) return DFM_ERR_INVALID;
   const unsigned n = (unsigned)nblk;
   std::vector<unsigned> rp(n + 1, 0), cols;
   std::vector<double> dg(2 * (size_t)n, 0.0), vals;
@@ -144,6 +149,9 @@ int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* 
   if (off) std::copy(vals.begin(), vals.end(), off);
   return DFM_OK;
 }
+
+}  // namespace
+}  // namespace dfm
 
 // GiD ASCII mesh, as Msh::CMesh3D::ReadFromFile_GiDMsh (src/msh/mesh3d.cpp:
 // 601-800) and Msh::CMesher2D::ReadFromFile_GiDMsh (src/msh/mesher2d.cpp:
@@ -198,8 +206,11 @@ int parse_numbers(const char* b, const char* e, double* out, int max) {
 }  // namespace
 }  // namespace dfm
 
-int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel, unsigned* nelem,
-                      int* elem) {
+namespace dfm {
+namespace {
+
+int gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel, unsigned* nelem,
+                  int* elem) {
   if (!path || !ndim || !nnode || !nnoel || !nelem) return DFM_ERR_INVALID;
   Lines L;
   int rc = read_file(path, L.buf);
@@ -284,6 +295,35 @@ int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coor
   }
   if (elem) std::copy(conn.begin(), conn.end(), elem);
   return DFM_OK;
+}
+
+}  // namespace
+}  // namespace dfm
+
+// The readers build host containers sized by the file: a failed allocation
+// (or any other exception) must not cross the C ABI.
+extern "C" {
+
+int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowptr, unsigned* colind,
+                       double* diag, double* off) {
+  try {
+    return dfm::zmat_read_text(path, N, ncrs, rowptr, colind, diag, off);
+  } catch (const std::bad_alloc&) {
+    return DFM_ERR_NOMEM;
+  } catch (...) {
+    return DFM_ERR_INVALID;
+  }
+}
+
+int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel, unsigned* nelem,
+                      int* elem) {
+  try {
+    return dfm::gid_read_mesh(path, ndim, nnode, coord, nnoel, nelem, elem);
+  } catch (const std::bad_alloc&) {
+    return DFM_ERR_NOMEM;
+  } catch (...) {
+    return DFM_ERR_INVALID;
+  }
 }
 
 }  // extern "C"

@@ -7,6 +7,10 @@
 //              is still `true` in the reference, DFM_NOT_CONVERGED here)
 //   PCOCG      Fem::Ls::Solve_PCOCG    src/femls/zsolver_ls_iter.cpp:171-267
 //              (complex symmetric, unconjugated products; 1-based iterations)
+//   CG         LsSol::Solve_CG         src/ls/solver_ls_iter.cpp:31-97
+//              (no preconditioner; x = 0; |r0|^2 < 1e-60 returns at once;
+//              *iters = 0-based index; max_iter reached is `true` in the
+//              reference with conv_ratio left at the tolerance)
 //
 // Every scalar lives in device memory (KrylovScalars); every reduction is a
 // fixed-order sum of per-block partials (ctx part(k) arrays), so a solve is
@@ -128,6 +132,89 @@ k_pcg_update_p(size_t n, KrylovScalars* sc, const double* part_rz, int np_rz, co
   GRID_LOOP(k, n) p[k] = p[k] * beta + z[k];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     sc->beta = beta;
+    sc->it = sc->it + 1;
+  }
+}
+
+// ======================================================= CG (real, no preconditioner)
+// start: x = 0, partials of (r, r) into slot 2
+__global__ void __launch_bounds__(kVecThreads)
+k_cg_start(size_t n, const double* __restrict__ r, double* __restrict__ x, double* part_rr) {
+  double acc = 0.0;
+  GRID_LOOP(k, n) {
+    const double rv = r[k];
+    acc += rv * rv;
+    x[k] = 0.0;
+  }
+  block_partial<kVecThreads>(acc, part_rr);
+}
+
+// |r0|^2 < 1e-60: the reference returns with num_iter = 0 and conv_ratio = |r0|
+__global__ void __launch_bounds__(kVecThreads)
+k_cg_start2(size_t n, KrylovScalars* sc, const double* part_rr, int np_rr, const double* __restrict__ r,
+            double* __restrict__ p) {
+  const double rr0 = reduce_partials(part_rr, np_rr);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->it = 0;
+    if (rr0 < 1.0e-60) {
+      sc->conv = sqrt(rr0);
+      sc->conv_it = 0;
+      sc->done = 100 + DFM_OK;
+    } else {
+      sc->inv0 = 1.0 / rr0;
+      sc->rz = rr0;
+      sc->done = 0;
+    }
+  }
+  GRID_LOOP(k, n) p[k] = r[k];
+}
+
+// alpha = (r, r) / (p, Ap); x += alpha p; r -= alpha Ap; partials of the new (r, r).
+// sc->rz holds (r, r); block 0 keeps it in sc->rho for k_cg_update_p, which
+// writes the new one into sc->rz (no kernel writes a scalar it also reads).
+__global__ void __launch_bounds__(kVecThreads)
+k_cg_update_xr(size_t n, KrylovScalars* sc, const double* part_pq, int np_pq, const double* __restrict__ q,
+               const double* __restrict__ p, double* __restrict__ r, double* __restrict__ x, double* part_rr) {
+  if (block_flag(&sc->done)) return;
+  if (sc->it >= sc->maxit) {
+    finish(sc, DFM_NOT_CONVERGED, sqrt(sc->rz * sc->inv0));
+    return;
+  }
+  const double rr = sc->rz;
+  const double alpha = rr / reduce_partials(part_pq, np_pq);
+  if (!isfinite(alpha)) {
+    finish(sc, DFM_BREAKDOWN, NAN);
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->rho = rr;
+    sc->alpha = alpha;
+  }
+  double acc = 0.0;
+  GRID_LOOP(k, n) {
+    x[k] += alpha * p[k];
+    const double rv = r[k] - alpha * q[k];
+    r[k] = rv;
+    acc += rv * rv;
+  }
+  block_partial<kVecThreads>(acc, part_rr);
+}
+
+// stop test on the new (r, r); else beta = (r, r)_new / (r, r) and p = beta p + r
+__global__ void __launch_bounds__(kVecThreads)
+k_cg_update_p(size_t n, KrylovScalars* sc, const double* part_rr, int np_rr, const double* __restrict__ r,
+              double* __restrict__ p) {
+  if (block_flag(&sc->done)) return;
+  const double rr_new = reduce_partials(part_rr, np_rr);
+  if (rr_new * sc->inv0 < sc->tol2) {
+    finish(sc, DFM_OK, sqrt(rr_new * sc->inv0));
+    return;
+  }
+  const double beta = rr_new / sc->rho;
+  GRID_LOOP(k, n) p[k] = beta * p[k] + r[k];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->beta = beta;
+    sc->rz = rr_new;
     sc->it = sc->it + 1;
   }
 }
@@ -349,6 +436,7 @@ static bool is_mixed(int method) { return method == DFM_PCG_MIXED || method == D
 
 static int vectors_of(int method) {
   switch (method) {
+    case DFM_CG: return kVecZ + 1;  // Z holds Ap
     case DFM_PBICGSTAB: return kNumVec;
     case DFM_PCOCG: return kVecQ + 1;
     case DFM_PCG_MIXED:
@@ -361,6 +449,7 @@ static int vectors_of(int method) {
 // launch configuration the graph was captured with.
 struct SolvePlan {
   dfm_ilu M = nullptr;
+  dfm_mat A = nullptr;  // the owner of an unpreconditioned (CG) plan, which has no M
   int method = 0;
   size_t n = 0;  // doubles per vector
   double* v[kNumVec] = {};
@@ -384,18 +473,20 @@ static void plan_drop_graph(SolvePlan* P) {
   P->graph_failed = false;
 }
 
-static int plan_of(dfm_ilu M, int method, SolvePlan** out) {
+static int plan_of(dfm_mat A, dfm_ilu M, int method, SolvePlan** out) {
   std::lock_guard<std::mutex> lock(g_plan_mu);
+  dfm_mat owner = M ? nullptr : A;
   for (auto* e : registry())
-    if (e->M == M && e->method == method) {
+    if (e->M == M && e->A == owner && e->method == method) {
       *out = e;
       return DFM_OK;
     }
   auto* P = new (std::nothrow) SolvePlan();
   if (!P) return DFM_ERR_NOMEM;
   P->M = M;
+  P->A = owner;
   P->method = method;
-  P->n = (size_t)M->N * M->xw();
+  P->n = (size_t)A->N * A->xw();
   const size_t bytes = std::max<size_t>(P->n, 1) * sizeof(double);
   for (int k = 0; k < vectors_of(method); k++)
     if (cudaMalloc(&P->v[k], bytes) != cudaSuccess) {
@@ -409,17 +500,27 @@ static int plan_of(dfm_ilu M, int method, SolvePlan** out) {
   return DFM_OK;
 }
 
-void solve_release(dfm_ilu M) {
+static void release_if(bool (*match)(const SolvePlan*, const void*), const void* key) {
   std::lock_guard<std::mutex> lock(g_plan_mu);
   auto& r = registry();
   for (size_t k = 0; k < r.size();) {
-    if (r[k]->M != M) { k++; continue; }
+    if (!match(r[k], key)) { k++; continue; }
     SolvePlan* P = r[k];
     plan_drop_graph(P);
     for (double* v : P->v) cudaFree(v);
     delete P;
     r.erase(r.begin() + k);
   }
+}
+
+void solve_release(dfm_ilu M) {
+  release_if([](const SolvePlan* P, const void* key) { return P->M == static_cast<dfm_ilu>(const_cast<void*>(key)); },
+             M);
+}
+
+void solve_release_mat(dfm_mat A) {
+  release_if([](const SolvePlan* P, const void* key) { return P->A == static_cast<dfm_mat>(const_cast<void*>(key)); },
+             A);
 }
 
 // -------------------------------------------------- one iteration per method
@@ -555,9 +656,23 @@ static int enqueue_cocg(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, b
   return DFM_OK;
 }
 
+static int enqueue_cg(dfm_mat A, SolvePlan* P, KrylovScalars* sc) {
+  dfm_ctx c = A->ctx;
+  const int gv = vec_grid(A);
+  double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *q = P->v[kVecZ];
+  int rc = spmv_launch(A, 1.0, p, 0.0, q, c->part(0), gv, sc, A->lanes);  // q = A p with (p, q)
+  if (rc) return rc;
+  k_cg_update_xr<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(0), gv, q, p, r, x, c->part(2));
+  DFM_CUDA_TRY(cudaGetLastError());
+  k_cg_update_p<<<gv, kVecThreads, 0, c->stream>>>(P->n, sc, c->part(2), gv, r, p);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
 // k: index of the iteration inside one graph of kIterPerGraph
 static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc, int k) {
   switch (P->method) {
+    case DFM_CG: return enqueue_cg(A, P, sc);
     case DFM_PBICGSTAB: return enqueue_bicg(A, M, P, sc);
     case DFM_PCOCG: return enqueue_cocg(A, M, P, sc);
     case DFM_PCG_MIXED: return enqueue_pcg_mixed(A, M, P, sc, k == kIterPerGraph - 1);
@@ -570,10 +685,15 @@ static int enqueue_iteration(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* 
 static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   dfm_ctx c = A->ctx;
   cudaStream_t s = c->stream;
-  const int gv = vec_grid(A), gs = sweep_grid(M, M->sweep);
+  const int gv = vec_grid(A);
   double *r = P->v[kVecR], *x = P->v[kVecX], *p = P->v[kVecP], *z = P->v[kVecZ], *y = P->v[kVecY];
   int rc;
   switch (P->method) {
+    case DFM_CG:
+      k_cg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, c->part(2));
+      DFM_CUDA_TRY(cudaGetLastError());
+      k_cg_start2<<<gv, kVecThreads, 0, s>>>(P->n, sc, c->part(2), gv, r, p);
+      break;
     case DFM_PBICGSTAB:
       k_bicg_start<<<gv, kVecThreads, 0, s>>>(P->n, r, x, P->v[kVecR2], p, y, z, c->part(2), c->part(3));
       DFM_CUDA_TRY(cudaGetLastError());
@@ -601,7 +721,6 @@ static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
       break;
     }
   }
-  (void)gs;
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;
 }
@@ -610,14 +729,16 @@ static int enqueue_start(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) 
 static void ensure_graph(dfm_mat A, dfm_ilu M, SolvePlan* P, KrylovScalars* sc) {
   dfm_ctx c = A->ctx;
   const int lanes_key = A->lanes * 2 + A->spmv_kind;
-  const bool same = P->key_sweep == M->sweep && P->key_lanes == lanes_key && P->key_gen == M->plan_gen &&
+  const int sweep_key = M ? M->sweep : 0;
+  const unsigned gen_key = M ? M->plan_gen : 0u;
+  const bool same = P->key_sweep == sweep_key && P->key_lanes == lanes_key && P->key_gen == gen_key &&
                     P->key_wait == c->wait_ns && P->key_op32 == c->mixed_op32;
   if (!same) {
     plan_drop_graph(P);
     P->key_op32 = c->mixed_op32;
-    P->key_sweep = M->sweep;
+    P->key_sweep = sweep_key;
     P->key_lanes = lanes_key;
-    P->key_gen = M->plan_gen;
+    P->key_gen = gen_key;
     P->key_wait = c->wait_ns;
   }
   if (P->exec || P->graph_failed) return;
@@ -644,14 +765,15 @@ int krylov_solve(dfm_mat A, dfm_ilu M, int method, const double* b, int b_where,
                  double* r_out, double tol, unsigned maxit, unsigned* iters, double* conv) {
   dfm_ctx c = A->ctx;
   cudaStream_t s = c->stream;
+  if (!M && method != DFM_CG) return DFM_ERR_INVALID;
   int rc = spmv_autotune(A);
   if (rc) return rc;
-  if ((rc = ilu_autotune(M))) return rc;
+  if (M && (rc = ilu_autotune(M))) return rc;
   const bool f32 = is_mixed(method);
   if (f32 && c->mixed_op32 && (rc = mat_make_f32(A))) return rc;
-  if ((rc = ilu_prepare(M, f32))) return rc;
+  if (M && (rc = ilu_prepare(M, f32))) return rc;
   SolvePlan* P = nullptr;
-  if ((rc = plan_of(M, method, &P))) return rc;
+  if ((rc = plan_of(A, M, method, &P))) return rc;
   const size_t n = P->n;
   KrylovScalars* sc = c->d_scal;
   {

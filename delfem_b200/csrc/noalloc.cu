@@ -2,14 +2,14 @@
 // z = U^-1 L^-1 r without any device allocation.
 //
 // Some callers cannot allocate device memory when they need the
-// preconditioner: code running inside a stream-ordered region that must not
-// synchronise (cudaMalloc/cudaFree implicitly synchronise the device), code
-// holding a fixed memory budget handed out by a host framework that owns all
-// allocations, and callbacks that run while an allocator lock is held.  For
-// them this entry point keeps its only scratch buffer - the intermediate
-// vector y = L^-1 r between the two sweeps - in a file-scope static device
-// array of kNoAllocMaxDoubles doubles (4 MiB).  Every GPU that loads the
-// library holds that array until the process exits.
+// preconditioner: code that enqueues work on a stream and must not stall it
+// (cudaMalloc and cudaFree can synchronise the device), code holding a fixed
+// memory budget handed out by a host framework that owns all allocations, and
+// callbacks that run while an allocator lock is held.  For them this entry
+// point keeps its only scratch buffer - the intermediate vector y = L^-1 r
+// between the two sweeps - in a file-scope static device array of
+// kNoAllocMaxDoubles doubles (4 MiB).  Every GPU that loads the library holds
+// that array until the process exits.
 //
 // Limits and sharing:
 //  * N * (doubles per block row) must not exceed kNoAllocMaxDoubles
@@ -19,40 +19,39 @@
 //    The sweeps write every entry they later read, so nothing needs clearing,
 //    but calls whose kernels overlap on the GPU (different streams, or
 //    different contexts on one device without ordering) race on it.
-//  * The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//  * The first call on a context looks up the array's device address
+//    (cudaGetSymbolAddress) with the context's device current and keeps it in
+//    the context; make that first call before any stream capture.
+//  * The call only enqueues the two sweeps on the context's stream and
+//    returns; it does not wait for them.  z is ready once the stream reaches
+//    that point.  Launch errors come back as DFM_ERR_CUDA; a device-side error
+//    of the sweeps is picked up later by dfm_ctx_take_error.
 // It runs the one-CTA level-barrier schedule, which needs no sentinel buffers
 // and no autotuning (both of which allocate on first use).
-#include <mutex>
-
 #include "dfm_internal.h"
 
 namespace dfm {
 
 constexpr size_t kNoAllocMaxDoubles = (size_t)1 << 19;  // 4 MiB
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxDoubles];
 
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch array on `device` (looked up once per device).
-static int noalloc_scratch(int device, double** out) {
-  if (device < 0 || device >= kNoAllocMaxDevices) return DFM_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
+// Device address of the scratch array for the context's device.  In host code
+// g_noalloc_scratch names a host-side stand-in, not device memory, so the
+// kernels get the address cudaGetSymbolAddress reports, looked up with the
+// context's device current (once per context).
+static int noalloc_scratch(dfm_ctx c, double** out) {
+  if (!c->noalloc_scratch) {
     int cur = 0;
     DFM_CUDA_TRY(cudaGetDevice(&cur));
-    if (cur != device) DFM_CUDA_TRY(cudaSetDevice(device));
+    if (cur != c->device) DFM_CUDA_TRY(cudaSetDevice(c->device));
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (cur != device) cudaSetDevice(cur);
+    if (cur != c->device) cudaSetDevice(cur);
     if (e != cudaSuccess || !p) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress");
-    g_noalloc_ptr[device] = static_cast<double*>(p);
+    c->noalloc_scratch = static_cast<double*>(p);
   }
-  *out = g_noalloc_ptr[device];
+  *out = c->noalloc_scratch;
   return DFM_OK;
 }
 
@@ -67,10 +66,8 @@ extern "C" int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z) {
   if ((M->N && (!r || !z)) || r == z || !M->factored) return DFM_ERR_INVALID;
   if (n == 0) return DFM_OK;
   double* y = nullptr;
-  int rc = noalloc_scratch(M->ctx->device, &y);
+  int rc = noalloc_scratch(M->ctx, &y);
   if (rc) return rc;
   if ((rc = ilu_fwd_launch(M, r, y, nullptr, 2))) return rc;
-  if ((rc = ilu_bwd_launch(M, y, z, nullptr, nullptr, nullptr, 2))) return rc;
-  DFM_CUDA_TRY(cudaStreamSynchronize(M->ctx->stream));
-  return take_code(M->ctx);
+  return ilu_bwd_launch(M, y, z, nullptr, nullptr, nullptr, 2);
 }

@@ -30,94 +30,11 @@
 
 #include "dfm_internal.h"
 #include "sweep.h"
+#include "sweep_dev.cuh"
 
 namespace dfm {
 
-constexpr int kOpBatch = 4;  // operands of one lane loaded together in the range sweeps
 constexpr int kStageThread = kSweepThreads - 32;  // drives the stage ring of the range sweep
-
-// ------------------------------------------------------------ PTX helpers
-DFM_DEVINL unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-DFM_DEVINL void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-DFM_DEVINL void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-DFM_DEVINL void mbar_arrive_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-DFM_DEVINL bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// 1-D bulk copy global -> this CTA's shared memory (addresses and size 16-byte multiples).
-DFM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
-DFM_DEVINL int ld_status2(const DevStatus* st) {
-  int v;
-  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(&st->code) : "memory");
-  return v;
-}
-
-// Re-reads the remote operands of a batch that still hold the sentinel: every
-// missing value is re-read in each pass, so a batch whose producers are just
-// publishing costs one L2 round trip per pass instead of one per value (a
-// b x b row of B values would otherwise wait for B round trips in a row).
-// xo[u]: operand codes (remote = 0x80000000 | row); xv[u][c]: values read so
-// far.  The wait is bounded: past wait_ns (or once another wait has failed)
-// it records DFM_WAIT_TIMEOUT and returns.
-template <int B, int NB, typename TX>
-DFM_DEVINL void repoll_batch(const unsigned* xo, TX (*xv)[B], const TX* out, DevStatus* st, uint64_t wait_ns,
-                             int where) {
-  auto missing = [&]() {
-    bool m = false;
-#pragma unroll
-    for (int u = 0; u < NB; u++)
-      if ((xo[u] & 0xc0000000u) == 0x80000000u)
-#pragma unroll
-        for (int c = 0; c < B; c++) m |= Sent<TX>::is(xv[u][c]);
-    return m;
-  };
-  if (!missing()) return;
-  SpinGuard g(wait_ns);
-  for (;;) {
-#pragma unroll
-    for (int u = 0; u < NB; u++)
-      if ((xo[u] & 0xc0000000u) == 0x80000000u)
-#pragma unroll
-        for (int c = 0; c < B; c++)
-          if (Sent<TX>::is(xv[u][c])) xv[u][c] = ld_relaxed(out + (size_t)(xo[u] & 0x7fffffffu) * B + c);
-    if (!missing()) return;
-    if (g.expired() || ((g.n & 1023u) == 0 && ld_status2(st) != 0)) {
-      raise_error(st, DFM_WAIT_TIMEOUT, where);
-      return;
-    }
-  }
-}
-
-// Waits for a stage phase; false (after recording the error) if it never completes.
-DFM_DEVINL bool wait_stage(uint64_t* bar, unsigned parity, DevStatus* st, uint64_t wait_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
-  SpinGuard g(wait_ns);
-  for (;;) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (g.expired()) {
-      raise_error(st, DFM_WAIT_TIMEOUT, 10);
-      return false;
-    }
-  }
-}
 
 // ------------------------------------------------- row helpers (mode 3)
 // A row's first batch of operands as issued ahead of time: codes and values
@@ -262,39 +179,6 @@ DFM_DEVINL void row_finish(const char* sb, unsigned r, int lane, unsigned gmask,
 }
 
 // --------------------------------------------------------------- kernel
-// Block partial of the CTA's share of (rdot, out) from its finished slice X.
-// DOT 1: real dot over len*B entries; DOT 2: complex matrices run as real 2x2
-// blocks (re, im per row), the unconjugated sum of rdot_i out_i with the real
-// and imaginary parts in part[] and part[kMaxBlocks + ...].
-// rows: the plan's row order (slot k of the slice is row rows[a0 + k]), or
-// nullptr for the natural order (row a0 + k).
-DFM_DEVINL size_t slot_row(const unsigned* rows, unsigned p) { return rows ? (size_t)rows[p] : (size_t)p; }
-
-template <int B, int DOT, typename TX>
-DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0, unsigned len, bool alive,
-                          double* part, const unsigned* rows) {
-  if constexpr (DOT == 2) {
-    static_assert(B == 2, "complex rows are 2x2 real blocks");
-    double re = 0.0, im = 0.0;
-    if (alive)
-      for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
-        const size_t gi = slot_row(rows, a0 + k);
-        const double rr = (double)rdot[gi * 2], ri = (double)rdot[gi * 2 + 1];
-        const double xr = (double)X[2 * k], xi = (double)X[2 * k + 1];
-        re += rr * xr - ri * xi;
-        im += rr * xi + ri * xr;
-      }
-    block_partial<kSweepThreads>(re, part);
-    block_partial<kSweepThreads>(im, part + kMaxBlocks);
-  } else {
-    double dacc = 0.0;
-    if (alive)
-      for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
-        dacc += (double)rdot[slot_row(rows, a0 + k / B) * B + k % B] * (double)X[k];
-    block_partial<kSweepThreads>(dacc, part);
-  }
-}
-
 template <int B, int LPR, typename TV, typename TX, bool FWD, int DOT, bool PIPE>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
@@ -519,12 +403,6 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
 // that chunk's bulk copy.  A group reading a chunk first waits until the stage
 // is assigned to that chunk, then for the copy's mbarrier phase.  Every wait is
 // bounded; after an expired wait the CTA stops and drains its copies.
-DFM_DEVINL double ld_volatile_s(const double* p) { return *reinterpret_cast<const volatile double*>(p); }
-DFM_DEVINL float ld_volatile_s(const float* p) { return *reinterpret_cast<const volatile float*>(p); }
-DFM_DEVINL void st_volatile_s(double* p, double v) { *reinterpret_cast<volatile double*>(p) = v; }
-DFM_DEVINL void st_volatile_s(float* p, float v) { *reinterpret_cast<volatile float*>(p) = v; }
-DFM_DEVINL void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 template <typename TX>
 DFM_DEVINL TX poll_local(const TX* p, volatile int* alive, DevStatus* st, uint64_t wait_ns) {
   TX v = ld_volatile_s(p);

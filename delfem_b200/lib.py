@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdfm_b200.so")
  ERR_IO) = range(10)
 REAL, COMPLEX = 0, 1
 HOST, DEVICE = 0, 1
-PCG, PBICGSTAB, PCOCG, PCG_MIXED, PCOCG_MIXED = 0, 1, 2, 3, 4
+PCG, PBICGSTAB, PCOCG, PCG_MIXED, PCOCG_MIXED, CG = 0, 1, 2, 3, 4, 5
 
 _lib = None
 
@@ -42,6 +42,10 @@ PROTOS = {
     "dfm_buf_free": (_i, [_vp, _vp]),
     "dfm_buf_copy": (_i, [_vp, _vp, _vp, C.c_size_t, _i]),
     "dfm_buf_zero": (_i, [_vp, _vp, C.c_size_t]),
+    "dfm_vec_dot": (_i, [_vp, C.c_size_t, _vp, _vp, _dp]),
+    "dfm_vec_copy": (_i, [_vp, C.c_size_t, _vp, _vp]),
+    "dfm_vec_scal": (_i, [_vp, C.c_size_t, _d, _vp]),
+    "dfm_vec_axpy": (_i, [_vp, C.c_size_t, _d, _vp, _vp]),
     "dfm_mat_create": (_i, [_vp, _u, _u, _i, _up, _up, C.POINTER(_vp)]),
     "dfm_mat_destroy": (_i, [_vp]),
     "dfm_mat_info": (_i, [_vp, _up, _up, _up, _ip]),
@@ -85,6 +89,7 @@ PROTOS = {
     "dfm_ilu_set_sweep_partition": (_i, [_vp, _up, _u]),
     "dfm_sweep_partition_patches": (_i, [_u, _i, _dp, _u, _up, _up]),
     "dfm_solve_pcg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
+    "dfm_solve_cg": (_i, [_vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pbicgstab": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcocg": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
     "dfm_solve_pcg_mixed": (_i, [_vp, _vp, _vp, _vp, _d, _u, _up, _dp]),
@@ -597,6 +602,41 @@ def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CO
     return rc, it.value, conv.value
 
 
+def solve_cg(A: Matrix, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
+    """LsSol::Solve_CG (no preconditioner) on device vectors; returns (status, iters, conv)."""
+    it, conv = C.c_uint(), C.c_double()
+    _sync_torch()
+    rc = lib().dfm_solve_cg(A.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    check(rc, "dfm_solve_cg", allow)
+    return rc, it.value, conv.value
+
+
+def vec_dot(ctx: Context, x, y) -> float:
+    """CVector_Blk dot product of two device vectors (deterministic)."""
+    out = C.c_double()
+    _sync_torch()
+    check(lib().dfm_vec_dot(ctx.h, x.numel(), _ptr(x), _ptr(y), C.byref(out)), "dfm_vec_dot")
+    return out.value
+
+
+def vec_axpy(ctx: Context, alpha: float, x, y):
+    """y += alpha x on the context's stream."""
+    _sync_torch()
+    check(lib().dfm_vec_axpy(ctx.h, x.numel(), alpha, _ptr(x), _ptr(y)), "dfm_vec_axpy")
+
+
+def vec_scal(ctx: Context, alpha: float, x):
+    """x *= alpha on the context's stream."""
+    _sync_torch()
+    check(lib().dfm_vec_scal(ctx.h, x.numel(), alpha, _ptr(x)), "dfm_vec_scal")
+
+
+def vec_copy(ctx: Context, x, y):
+    """y := x on the context's stream."""
+    _sync_torch()
+    check(lib().dfm_vec_copy(ctx.h, x.numel(), _ptr(x), _ptr(y)), "dfm_vec_copy")
+
+
 def solve_pbicgstab(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):
     """LsSol::Solve_PBiCGSTAB on device vectors; returns (status, iters, conv)."""
     it, conv = C.c_uint(), C.c_double()
@@ -638,7 +678,8 @@ def solve_host(A: Matrix, M: ILU, b, method=PCG, tol=1e-10, maxit=10000, allow=(
     b = np.ascontiguousarray(b, np.float64)
     x = np.zeros_like(b)
     it, conv = C.c_uint(), C.c_double()
-    rc = lib().dfm_solve_host(A.h, M.h, method, _ptr(b), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
+    rc = lib().dfm_solve_host(A.h, M.h if M is not None else None, method, _ptr(b), _ptr(x), tol, maxit,
+                              C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_host", allow)
     return rc, x, it.value, conv.value
 

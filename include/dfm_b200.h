@@ -52,7 +52,7 @@ typedef enum dfm_status {
 
 enum { DFM_REAL = 0, DFM_COMPLEX = 1 };
 enum { DFM_HOST = 0, DFM_DEVICE = 1 };
-enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2, DFM_PCG_MIXED = 3, DFM_PCOCG_MIXED = 4 };
+enum { DFM_PCG = 0, DFM_PBICGSTAB = 1, DFM_PCOCG = 2, DFM_PCG_MIXED = 3, DFM_PCOCG_MIXED = 4, DFM_CG = 5 };
 
 typedef struct dfm_ctx_s* dfm_ctx;
 typedef struct dfm_mat_s* dfm_mat;
@@ -88,6 +88,19 @@ DFM_API int dfm_buf_alloc(dfm_ctx ctx, size_t bytes, void** out);
 DFM_API int dfm_buf_free(dfm_ctx ctx, void* p);
 DFM_API int dfm_buf_copy(dfm_ctx ctx, void* dst, const void* src, size_t bytes, int direction);
 DFM_API int dfm_buf_zero(dfm_ctx ctx, void* p, size_t bytes);
+
+/* ---- vector operations: CVector_Blk on the device ----------------------- */
+/* The solver-side vector steps of LsSol::CLinearSystem (DOT / COPY / SCAL /
+ * AXPY, src/ls/linearsystem.cpp:298-415, over MatVec::CVector_Blk,
+ * src/matvec/vector_blk.cpp:37-112) on device arrays of n doubles, issued on
+ * the context's stream.  dfm_vec_dot returns the value on the host (it
+ * synchronises; fixed summation order, so equal inputs give equal bits);
+ * the others only enqueue.  dfm_vec_scal multiplies (NaN * 0 stays NaN, as
+ * in the reference). */
+DFM_API int dfm_vec_dot(dfm_ctx ctx, size_t n, const double* x, const double* y, double* out);
+DFM_API int dfm_vec_copy(dfm_ctx ctx, size_t n, const double* x, double* y);          /* y := x */
+DFM_API int dfm_vec_scal(dfm_ctx ctx, size_t n, double alpha, double* x);             /* x := alpha x */
+DFM_API int dfm_vec_axpy(dfm_ctx ctx, size_t n, double alpha, const double* x, double* y); /* y += alpha x */
 
 /* ---- matrix: CMatDia_BlkCrs on the device ------------------------------ */
 /* Pattern from host arrays; validated (monotone rowptr, in-range, strictly
@@ -248,14 +261,17 @@ DFM_API int dfm_ilu_apply(dfm_ilu M, const double* r, double* z);
 DFM_API int dfm_time_ilu_apply(dfm_ilu M, const double* r, double* z, int reps, float* ms);
 /* No counterpart in the reference.  The same z = U^-1 L^-1 r as dfm_ilu_apply,
  * for callers that cannot allocate device memory at the point of use (code
- * inside a stream-ordered region that must not synchronise, a host framework
- * that owns every device allocation, callbacks under an allocator lock): it
- * allocates nothing, keeping its intermediate vector in a static device array
- * of 4 MiB (N * doubles-per-row <= 524,288, else DFM_ERR_INVALID) that every
- * GPU loading the library holds until exit.  All calls share that array, so
- * calls whose kernels overlap on the GPU race on it.  The first call on a
- * device looks up the array's address with that device current; make it
- * before any stream capture.  Runs the one-CTA level-barrier schedule. */
+ * that enqueues work on a stream it must not stall - cudaMalloc and cudaFree
+ * can synchronise the device -, a host framework that owns every device
+ * allocation, callbacks under an allocator lock): it allocates nothing,
+ * keeping its intermediate vector in a static device array of 4 MiB
+ * (N * doubles-per-row <= 524,288, else DFM_ERR_INVALID) that every GPU
+ * loading the library holds until exit.  It enqueues the two sweeps on the
+ * context's stream and returns without waiting; device-side errors surface
+ * through dfm_ctx_take_error.  All calls share the array, so calls whose
+ * kernels overlap on the GPU race on it.  The first call on a context looks
+ * up the array's address with the context's device current; make it before
+ * any stream capture.  Runs the one-CTA level-barrier schedule. */
 DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
 /* Sweep schedule: 0 = autotuned, 1 = sync-free across the GPU, 2 = one CTA with
  * level barriers, 3 = contiguous row ranges per CTA (shared-memory slice, TMA-
@@ -303,6 +319,13 @@ DFM_API int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sl
  * *iters follows the reference: the 0-based index of the converged iteration. */
 DFM_API int dfm_solve_pcg(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
                   unsigned* iters, double* conv);
+/* LsSol::Solve_CG (src/ls/solver_ls_iter.cpp:31-97): conjugate gradients
+ * without a preconditioner, on A alone.  *iters is the 0-based index of the
+ * converged iteration (max_iter when it is reached: DFM_NOT_CONVERGED here,
+ * where the reference returns true and leaves conv_ratio at the tolerance);
+ * |r0|^2 < 1e-60 returns at once with *conv = |r0|.  Real matrices. */
+DFM_API int dfm_solve_cg(dfm_mat A, double* r, double* x, double tol, unsigned maxit, unsigned* iters,
+                         double* conv);
 /* LsSol::Solve_PBiCGSTAB (src/ls/solver_ls_iter.cpp:291-408): shadow residual
  * r0, *iters 1-based.  Real matrices. */
 DFM_API int dfm_solve_pbicgstab(dfm_mat A, dfm_ilu M, double* r, double* x, double tol, unsigned maxit,
@@ -357,7 +380,7 @@ DFM_API int dfm_batch_solve_pcg(dfm_batch batch, const double* b, int b_where, d
                         double tol, unsigned maxit, unsigned* iters, double* conv, int* status);
 
 /* End-to-end variants with HOST buffers (b copied in, x copied out, inside the
- * call); method is any DFM_PCG ... DFM_PCOCG_MIXED. */
+ * call); method is any DFM_PCG ... DFM_CG (M is ignored for DFM_CG). */
 DFM_API int dfm_solve_host(dfm_mat A, dfm_ilu M, int method, const double* b_host, double* x_host, double tol,
                    unsigned maxit, unsigned* iters, double* conv);
 DFM_API int dfm_solve_pcg_host(dfm_mat A, dfm_ilu M, const double* b_host, double* x_host, double tol,

@@ -760,6 +760,47 @@ int dfo_pcg_fill(unsigned N, unsigned b, const unsigned* rowptr, const unsigned*
   return 0;
 }
 
+/* LsSol::Solve_CG (src/ls/solver_ls_iter.cpp:31-97): no preconditioner.
+   x = 0 (SCAL by 0); |r0|^2 < 1e-60 returns true with num_iter = 0 and
+   conv_ratio = |r0|; the loop index is num_iter; at max_iter the loop ends
+   with num_iter = max_iter, conv_ratio untouched and true returned. */
+int dfo_cg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+           const double* off, double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv) {
+  const size_t n = (size_t)N * b;
+  double* p = (double*)calloc(n ? n : 1, sizeof(double));
+  double* Ap = (double*)calloc(n ? n : 1, sizeof(double));
+  vscal(n, 0.0, x);
+  double sq = vdot(n, r, r);
+  if (sq < 1.0e-60) {
+    *iters = 0;
+    *conv = sqrt(sq);
+    free(p); free(Ap);
+    return 1;
+  }
+  const double inv0 = 1.0 / sq;
+  memcpy(p, r, n * sizeof(double));
+  unsigned it;
+  for (it = 0; it < maxit; it++) {
+    dfo_spmv(N, b, rowptr, colind, diag, off, 1.0, p, 0.0, Ap);
+    const double alpha = sq / vdot(n, p, Ap);
+    vaxpy(n, alpha, p, x);
+    vaxpy(n, -alpha, Ap, r);
+    const double sq_new = vdot(n, r, r);
+    if (sq_new * inv0 < tol * tol) {
+      *conv = sqrt(sq_new * inv0);
+      break;
+    }
+    const double beta = sq_new / sq;
+    sq = sq_new;
+    vscal(n, beta, p);
+    vaxpy(n, 1.0, r, p);
+  }
+  if (it == maxit) *conv = tol;
+  *iters = it;
+  free(p); free(Ap);
+  return 1;
+}
+
 int dfo_pbicgstab(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                   const unsigned* diaind, const double* diag, const double* off,
                   const double* fdiag, const double* foff, double* r, double* x, double tol,

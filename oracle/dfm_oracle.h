@@ -103,6 +103,9 @@ int dfo_pcg_fill(unsigned N, unsigned b, const unsigned* rowptr, const unsigned*
                  unsigned* iters, double* conv, double* hist);
 /* LsSol::Solve_PBiCGSTAB (src/ls/solver_ls_iter.cpp:291-408); *iters is the
  * 1-based iitr at convergence, as in the reference. */
+/* LsSol::Solve_CG (no preconditioner), returns the reference's bool. */
+int dfo_cg(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+           const double* off, double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv);
 int dfo_pbicgstab(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                   const unsigned* diaind, const double* diag, const double* off,
                   const double* fdiag, const double* foff, double* r, double* x, double tol,

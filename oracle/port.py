@@ -54,6 +54,7 @@ def lib():
         L.dfo_iluk_init.argtypes = [U, U, up, up, dp, dp, up, up, dp, dp]
         L.dfo_pcg_fill.argtypes = [U, U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp, dp]
         L.dfo_pbicgstab.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp]
+        L.dfo_cg.argtypes = [U, U, up, up, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_zspmv.argtypes = [U, up, up, dp, dp, D, dp, D, dp]
         L.dfo_zilu0.argtypes = [U, up, up, up, dp, dp]
         L.dfo_zilu0.restype = U
@@ -232,6 +233,15 @@ class System:
         ok = lib().dfo_pcg_fill(self.N, self.b, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off),
                                 _u(fr), _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(r), _d(x), tol, maxit,
                                 C.byref(it), C.byref(conv), None)
+        return dict(ok=bool(ok), x=x, iters=it.value, conv=conv.value, r=r)
+
+    def solve_cg(self, rhs=None, tol=1e-10, maxit=10000):
+        """Solve_CG (no preconditioner) from x = 0."""
+        r = np.array(self.rhs if rhs is None else rhs, dtype=np.float64, copy=True)
+        x = np.zeros_like(r)
+        it, conv = C.c_uint(), C.c_double()
+        ok = lib().dfo_cg(self.N, self.b, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off), _d(r),
+                          _d(x), tol, maxit, C.byref(it), C.byref(conv))
         return dict(ok=bool(ok), x=x, iters=it.value, conv=conv.value, r=r)
 
     def fwd(self, fd, fo, v):

@@ -597,7 +597,8 @@ int dfm_ref_mat_solve_lev(unsigned N, unsigned b, const unsigned* rowptr, const 
   unsigned it = maxit;
   t0 = now_s();
   bool ok = (method == DFM_REF_PBICGSTAB) ? LsSol::Solve_PBiCGSTAB(c, it, lsp)
-                                          : LsSol::Solve_PCG(c, it, lsp);
+            : (method == DFM_REF_CG)        ? LsSol::Solve_CG(c, it, ls)
+                                            : LsSol::Solve_PCG(c, it, lsp);
   t1 = now_s();
   if (t_solve) *t_solve = t1 - t0;
   MatVec::CVector_Blk& u = ls.GetVector(-2, 0);

@@ -30,7 +30,7 @@ enum {
   DFM_REF_SOLID3D = 3,     /* Fem::Eqn::AddLinSys_LinearSolid3D_Static, P1 tet, b=3 */
   DFM_REF_HELMHOLTZ2D = 4  /* Fem::Eqn::AddLinSys_Helmholtz + SommerfeltRadiationBC, complex b=1 */
 };
-enum { DFM_REF_PCG = 0, DFM_REF_PBICGSTAB = 1, DFM_REF_PCOCG = 2 };
+enum { DFM_REF_PCG = 0, DFM_REF_PBICGSTAB = 1, DFM_REF_PCOCG = 2, DFM_REF_CG = 3 /* matrix level only */ };
 
 typedef struct dfm_ref_sys dfm_ref_sys;
 

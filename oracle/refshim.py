@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "_ref", "libdfm_refshim.so")
 REF_DIR = "/root/reference"
 
 POISSON2D, SOLID2D, SOLID3D, HELMHOLTZ2D = 1, 2, 3, 4
-PCG, PBICGSTAB, PCOCG = 0, 1, 2
+PCG, PBICGSTAB, PCOCG, CG = 0, 1, 2, 3
 
 _lib = None
 

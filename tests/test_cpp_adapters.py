@@ -36,9 +36,11 @@ def test_adapter_program_compiles_and_links(demo):
 @pytest.mark.gpu
 def test_adapter_reads_complex_matrix_text(demo, tmp_path):
     """CMatDia_BlkCrs::FromTextFile (CZMatDia_BlkCrs(file_path)) + PCOCG from a
-    C++ program, against the oracle's COCG on the same system."""
+    C++ program, against the oracle's COCG on the same system.  The disk has 40
+    rings (N = 4,921; the oracle's COCG converges in 368 iterations), where
+    the iteration count is set by the spectrum, not by rounding."""
     from tests import cases
-    m, S = cases.helmholtz(8)
+    m, S = cases.helmholtz(40)
     mp, bp = tmp_path / "z.txt", tmp_path / "b.txt"
     cases.write_zmat_text(str(mp), S.rowptr, S.colind, S.diag, S.off)
     bp.write_text("\n".join(repr(float(v)) for v in S.rhs) + "\n")
@@ -47,10 +49,10 @@ def test_adapter_reads_complex_matrix_text(demo, tmp_path):
     out = json.loads(r.stdout)
     ns, fd, fo = S.ilu0()
     ref = S.solve(fd, fo, method="pcocg", tol=1e-10, maxit=3000)
+    assert ref["ok"] and ref["iters"] < 1000
     x = np.array(out["x_file"])
-    # a long COCG run: the device's summation order moves the count a little
-    assert out["pcocg_ok"] and abs(out["pcocg_iters"] - ref["iters"]) <= max(3, ref["iters"] // 20)
-    assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
+    assert out["pcocg_ok"] and np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
+    assert abs(out["pcocg_iters"] - ref["iters"]) <= max(3, ref["iters"] // 20), (out["pcocg_iters"], ref["iters"])
 
 
 @pytest.mark.gpu

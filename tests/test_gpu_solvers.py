@@ -192,3 +192,72 @@ def test_solvers_with_each_spmv_kernel(ctx, kernel, method):
         assert _rel(xg, ref["x"]) <= 1e-7
     else:
         assert _rel(xg, ref["x"]) <= X_TOL
+
+
+CG_SYSTEMS = ["poisson20", "poisson_coef", "solid2d", "solid3d"]
+
+
+@pytest.mark.parametrize("name", CG_SYSTEMS)
+def test_cg_matches_oracle(ctx, name):
+    """LsSol::Solve_CG (no preconditioner) on the device against the oracle's
+    restatement (pinned to the reference's Solve_CG)."""
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS[name]()
+    ref = S.solve_cg(tol=1e-10, maxit=5000)
+    assert ref["ok"] and ref["iters"] < 5000
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_cg(A, r, x, tol=1e-10, maxit=5000)
+    assert rc == lib.OK, (rc, it, conv)
+    assert abs(it - ref["iters"]) <= max(3, ref["iters"] // 20), (it, ref["iters"])
+    assert conv < 1e-10
+    assert _rel(x.cpu().numpy(), ref["x"]) <= X_TOL
+    rc, xh, it2, conv2 = lib.solve_host(A, None, S.rhs, lib.CG, tol=1e-10, maxit=5000)
+    assert rc == lib.OK and it2 == it and np.array_equal(xh, x.cpu().numpy())  # deterministic
+
+
+def test_cg_maxit_and_zero_rhs(ctx):
+    from delfem_b200 import lib
+    S = REAL_SYSTEMS["solid2d"]()
+    ref = S.solve_cg(tol=1e-10, maxit=7)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    r = _dev(S.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_cg(A, r, x, tol=1e-10, maxit=7)
+    # the reference returns true with num_iter = max_iter and conv_ratio left at the tolerance
+    assert rc == lib.NOT_CONVERGED and it == 7 == ref["iters"] and ref["conv"] == 1e-10
+    assert conv == pytest.approx(np.linalg.norm(ref["r"]) / np.linalg.norm(S.rhs), rel=1e-6)
+    assert _rel(x.cpu().numpy(), ref["x"]) <= 1e-9
+    r = torch.zeros_like(r)
+    x = torch.full_like(r, 5.0)
+    rc, it, conv = lib.solve_cg(A, r, x)
+    assert rc == lib.OK and it == 0 and conv == 0.0 and float(x.abs().max()) == 0.0
+
+
+def test_vector_ops_match_numpy(ctx):
+    """dfm_vec_dot / axpy / scal / copy (CVector_Blk through CLinearSystem's
+    DOT, AXPY, SCAL, COPY): dot to rounding and bit-reproducible, the
+    elementwise ones exact; SCAL by 0 keeps NaN as the reference's product does."""
+    from delfem_b200 import lib
+    rng = np.random.default_rng(5)
+    for n in (1, 255, 256, 257, 100003, 3 * 337881):
+        xh, yh = rng.standard_normal(n), rng.standard_normal(n)
+        x, y = _dev(xh), _dev(yh)
+        d = lib.vec_dot(ctx, x, y)
+        assert d == pytest.approx(float(np.dot(xh, yh)), rel=1e-12, abs=1e-12 * n)
+        assert lib.vec_dot(ctx, x, y) == d
+        lib.vec_axpy(ctx, -0.75, x, y)
+        ctx.sync()
+        assert np.array_equal(y.cpu().numpy(), yh + -0.75 * xh)
+        lib.vec_scal(ctx, 1.5, y)
+        lib.vec_copy(ctx, y, x)
+        ctx.sync()
+        assert np.array_equal(x.cpu().numpy(), (yh + -0.75 * xh) * 1.5)
+    v = _dev(np.array([1.0, np.nan, 2.0]))
+    lib.vec_scal(ctx, 0.0, v)
+    ctx.sync()
+    out = v.cpu().numpy()
+    assert out[0] == 0.0 and np.isnan(out[1]) and out[2] == 0.0

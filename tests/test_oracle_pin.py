@@ -107,3 +107,20 @@ def test_iluk_pcg_pinned_to_reference(lev):
                                         lev=lev)
     assert rc == 0 and o["ok"]
     assert o["iters"] == it and _eq(o["x"], x) and o["conv"] == conv
+
+
+@pytest.mark.parametrize("name,maxit", [("poisson", 5000), ("solid3d", 5000), ("solid2d", 5000), ("solid2d", 7)])
+def test_cg_pinned_to_reference(name, maxit):
+    """LsSol::Solve_CG (no preconditioner) through the reference's own
+    CLinearSystem, against the oracle's restatement: x, iteration index and
+    ratio bit-identical, including the max_iter exit (true, ratio left at the
+    tolerance)."""
+    S = {"poisson": lambda: cases.poisson(20)[1], "solid3d": lambda: cases.solid3d(6, 2, 2)[1],
+         "solid2d": lambda: cases.solid2d(10)[1]}[name]()
+    o = S.solve_cg(tol=1e-10, maxit=maxit)
+    rc, x, it, conv, _, _ = R.mat_solve(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, S.rhs, method=R.CG, tol=1e-10,
+                                        maxit=maxit)
+    assert rc == 0 and o["ok"]
+    assert it == o["iters"] and _eq(conv, o["conv"]) and _eq(x, o["x"])
+    if maxit == 7:
+        assert it == 7 and conv == 1e-10

@@ -83,6 +83,7 @@ def test_reader_edge_cases(tmp_path):
     "3 2\n0 1 1 0\n0 1 2 0\n",             # repeated off-diagonal entry
     "3 1\n0 1 x 0\n",                      # unparsable value
     "-1 0\n",                              # negative size
+    "3 999999999999999\n0 0 1 0\n",        # a count the file cannot hold (no allocation sized by it)
 ])
 def test_reader_rejects_malformed(tmp_path, text):
     from delfem_b200 import lib

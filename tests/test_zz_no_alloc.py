@@ -1,12 +1,15 @@
 """dfm_ilu_apply_static, the allocation-free preconditioner application.
 
 It exists for callers that cannot allocate device memory where they apply the
-preconditioner (stream-ordered code that must not synchronise, frameworks that
-own every device allocation, callbacks under an allocator lock): it keeps its
-intermediate vector in a static device array instead.  These tests call it
-through the C ABI, twice in a row per system, and compare with dfm_ilu_apply
-at the tolerance the other sweep tests use.  The file is named to be collected
-last and creates its own context, so it runs the same alone or after the rest.
+preconditioner (code that enqueues work on a stream it must not stall,
+frameworks that own every device allocation, callbacks under an allocator
+lock): it keeps its intermediate vector in a static device array instead, and
+only enqueues its sweeps.  These tests call it through the C ABI, twice in a
+row per system, and compare it with the existing entry point dfm_ilu_apply at
+the tolerance the other sweep tests use, and with the oracle's ILU(0)
+application (forward + backward substitution of the reference's factor).  The
+file is named to be collected last and creates its own context, so it runs the
+same alone or after the rest.
 """
 import ctypes
 
@@ -19,6 +22,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 MAX_DOUBLES = 1 << 19  # size of the static scratch array (4 MiB)
+RTOL = 1e-11           # the sweep tests' tolerance (summation order differs)
 
 
 def _dev(a):
@@ -41,10 +45,15 @@ SYSTEMS = {
 }
 
 
+def _close(got, ref):
+    return np.allclose(got, ref, rtol=RTOL, atol=RTOL * np.abs(ref).max())
+
+
 @pytest.mark.parametrize("name", list(SYSTEMS))
 def test_static_apply_matches_apply_twice(nctx, name):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
+    ns, fd, fo = S.ilu0()
     A = lib.Matrix(nctx, S.rowptr, S.colind, S.b, lib.COMPLEX if S.cplx else lib.REAL)
     A.set_values(S.diag, S.off)
     M = lib.ILU(A)
@@ -52,16 +61,19 @@ def test_static_apply_matches_apply_twice(nctx, name):
     rng = np.random.default_rng(17)
     L = lib.lib()
     for call in range(2):  # two calls in a row share the static array
-        r = _dev(rng.standard_normal(S.N * S.xw))
+        rh = rng.standard_normal(S.N * S.xw)
+        r = _dev(rh)
         z_ref = torch.zeros_like(r)
         M.apply(r, z_ref)
         z = torch.full_like(r, float("nan"))
         torch.cuda.synchronize()
         rc = L.dfm_ilu_apply_static(M.h, ctypes.c_void_p(r.data_ptr()), ctypes.c_void_p(z.data_ptr()))
         assert rc == lib.OK, (name, call, rc)
-        ref = z_ref.cpu().numpy()
+        nctx.sync()  # the call only enqueues its sweeps on the context's stream
+        assert nctx.take_error() == (0, 0)
         got = z.cpu().numpy()
-        assert np.allclose(got, ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max()), (name, call)
+        assert _close(got, z_ref.cpu().numpy()), (name, call)
+        assert _close(got, S.precond(fd, fo, rh)), (name, call)
 
 
 def test_static_apply_rejects_systems_beyond_the_array(nctx):
