@@ -153,6 +153,17 @@ def reference_runs():
     return json.load(open(p)) if os.path.exists(p) else {}
 
 
+def reference_solution(name):
+    """The reference's own solution of a benchmark system at a stride of
+    entries, with its norm and iteration count (tests/golden/
+    reference_solutions.npz, made by tests/golden/make_reference_solutions.py)."""
+    p = os.path.join(ROOT, "tests", "golden", "reference_solutions.npz")
+    if not os.path.exists(p):
+        return None
+    g = np.load(p)
+    return {k[len(name) + 1:]: g[k] for k in g.files if k.startswith(name + "_")} or None
+
+
 def cpu_reference_sample(N, b, rowptr, colind, diag, off, rhs, sample_iters):
     """The reference's own ILU(0) + Solve_PCG (oracle/_ref, built from its
     sources) on a bounded sample: the ILU(0) and `sample_iters` PCG iterations
@@ -162,11 +173,18 @@ def cpu_reference_sample(N, b, rowptr, colind, diag, off, rhs, sample_iters):
     return t_ilu, t_solve / max(sample_iters, 1)
 
 
+C2_CONFIG = {"workload": "c2 3D elasticity cantilever 200x40x40 hexes x 6 P1 tets, ILU(0) + PCG to "
+                         "rel.res 1e-8 (plain FP64)", "N": 337881, "b": 3, "ncrs": 4586160, "dof": 1013643,
+             "l2": "inputs larger than L2 (K = 330 MB)"}
+
+
 def run_reference(args, rank):
-    """The reference's stock CPU path on c2 (oracle/_ref): its own pattern,
-    element assembly, ILU(0) and Solve_PCG.  Each step is a bounded sample (the
-    ILU(0) and 5 PCG iterations) scaled to the reference's iteration count to
-    1e-8 (tests/golden/reference_runs.json, measured from the reference)."""
+    """The reference's stock CPU path on c2 (oracle/_ref, built from the
+    DelFEM sources): its own pattern, element assembly, ILU(0)
+    (CPreconditioner_ILU::SetValue) and LsSol::Solve_PCG, single-threaded.
+    One complete solve to 1e-8 is timed in this run and gives the value; the
+    K timed steps are bounded samples (the ILU(0) and 5 PCG iterations) whose
+    scaled time is reported beside it as a cross-check."""
     if rank != 0:
         return
     from oracle import refshim as R
@@ -176,25 +194,39 @@ def run_reference(args, rank):
     m = c2_mesh()
     s = R.RefSystem(R.SOLID3D, m)
     _, t_asm = s.assemble([LAM3, MYU3, 1.0, 0.0, 0.0, -1.0])
-    n_full = reference_runs().get("c2", {}).get(f"tol{TOL:g}", {}).get("iterations")
     d, o, rhs = s.system()
     rp, ci = s.pattern()
-    per_step = []
+    per_step, samples = [], []
     for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         t_ilu, t_iter = cpu_reference_sample(s.N, s.b, rp, ci, d, o, rhs, 5)
         if k >= args.warmup:
-            per_step.append(t_ilu + (n_full or 1) * t_iter)
-    t = statistics.median(per_step)
-    v = 1.0 / t
+            per_step.append(time.perf_counter() - t0)
+            samples.append((t_ilu, t_iter))
+    # one complete solve: the field-level ILU(0) and Solve_PCG to 1e-8
+    rc_i, t_ilu_full = s.ilu()
+    rc, x, it, conv, t_pcg = s.solve(R.PCG, TOL, 20000)
+    t_full = t_ilu_full + t_pcg
+    n_full = it + 1
+    t_ilu_med = statistics.median(a for a, _ in samples)
+    t_iter_med = statistics.median(b_ for _, b_ in samples)
+    v = 1.0 / t_full
+    cfg = dict(C2_CONFIG, parallelism=f"replicas x{args.gpus}")  # the same dict as our arm's
     print(json.dumps({
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "c2 3D elasticity 200x40x40x6 tets, ILU(0)+PCG to 1e-8", "N": s.N, "b": 3,
-                   "ncrs": s.ncrs, "reference_assembly_s": t_asm},
+        "warmup": args.warmup, "ms_per_step": statistics.median(per_step) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": cfg,
+        "value_basis": f"one complete reference solve timed in this run: ILU(0) {t_ilu_full:.2f}s + Solve_PCG "
+                       f"{t_pcg:.1f}s ({n_full} iterations to {TOL:g}); ms_per_step is the median bounded "
+                       f"sample (ILU(0) + 5 iterations)",
+        "full_solve": {"ilu_s": t_ilu_full, "pcg_s": t_pcg, "iterations": n_full, "conv": conv, "ok": rc == 0,
+                       "s_per_iteration": t_pcg / n_full},
+        "sample_scaled_solve_s": t_ilu_med + n_full * t_iter_med,
+        "reference_assembly_s": t_asm,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"per step: the reference's ILU(0) + 5 Solve_PCG iterations on one core "
-                                   f"(the reference is single-threaded), scaled to its {n_full} iterations to 1e-8"},
+                         "sample": f"one full solve ({n_full} iterations) on one host core; steps: the "
+                                   f"reference's ILU(0) + 5 Solve_PCG iterations each"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
@@ -282,6 +314,61 @@ def run_c3(ctx, torch, dev, stream, timed, steps):
     for h in (B, M, A):
         h.close()
     return res
+
+
+def run_c3_sharded(torch, dev, stream, steps):
+    """c3 over all ranks (bench.py --gpus N > 1): the 512 instances shard by a
+    greedy balance of (n+1)^2 (delfem_b200.shard), every rank solves its share
+    as one batch, the time of a batched solve is the max over ranks (CUDA events
+    on this rank's stream, all-reduce over NCCL); the per-instance results are
+    gathered to rank 0.  No data-path collective: weak scaling by instances."""
+    from delfem_b200 import lib, meshes, shard
+    sizes = meshes.batch_sizes(C3_COUNT, C3_LO, C3_HI, C3_SEED)
+    nel = 2 * sizes.astype(np.int64) ** 2
+    eoff = np.concatenate([[0], np.cumsum(nel)])
+    kappa_all = np.random.default_rng(C3_SEED + 1).lognormal(0.0, 1.0, int(eoff[-1]))  # the 1-GPU c3 stream
+
+    def solve_local(idx):
+        ctx = lib.Context(dev)
+        ms = [meshes.unit_square_tri(int(sizes[k])) for k in idx]
+        big, noff, _ = meshes.concat(ms)
+        kappa = np.concatenate([kappa_all[eoff[k]:eoff[k + 1]] for k in idx])
+        G = lib.Mesh(ctx, big.coord, big.elem)
+        rp, ci = G.pattern()
+        A = lib.Matrix(ctx, rp, ci, 1)
+        rhs = torch.empty(big.nnode, dtype=torch.float64, device=f"cuda:{dev}")
+        fl = np.zeros(big.nnode, np.int32)
+        fl[np.unique(big.bnd.ravel())] = 1
+        G.assemble_poisson(A, 1.0, 1.0, rhs, coef=torch.from_numpy(kappa).cuda(dev))
+        lib.apply_dirichlet(A, torch.from_numpy(fl).cuda(dev), rhs)
+        M = lib.ILU(A)
+        M.factor()
+        B = lib.Batch(M, noff.astype(np.uint32))
+        x = torch.zeros_like(rhs)
+        B.solve(rhs, x, tol=TOL)  # warm-up: autotuning
+        ts = []
+        for _ in range(max(2, min(steps, 3))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            rc, _, it, conv, st = B.solve(rhs, x, tol=TOL)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        res = [(int(it[j]), int(st[j])) for j in range(len(idx))]
+        for h in (B, M, A, G):
+            h.close()
+        ctx.close()
+        return statistics.median(ts), res
+
+    out = shard.timed_sharded([(int(n) + 1) ** 2 for n in sizes], solve_local, device=f"cuda:{dev}")
+    if out is None:
+        return {}
+    its = [r[0] for r in out["results"]]
+    return {"instances": int(len(sizes)), "per_rank_instances": out["per_rank_instances"],
+            "per_rank_s": out["per_rank_seconds"], "batched_s_max_over_ranks": out["seconds"],
+            "instances_per_s": len(sizes) / out["seconds"], "max_iterations": int(max(its)),
+            "all_converged": all(r[1] == 0 for r in out["results"]), "scaling": "weak (instances)"}
 
 
 # ------------------------------------------------------------- profile run
@@ -416,15 +503,89 @@ def run_c5(ctx, torch, dev, timed):
     A.spmv(1.0, x, 0.0, y)
     torch.cuda.synchronize()
     res_m = float(torch.linalg.norm(b - y) / torch.linalg.norm(b))
+    ref = reference_solution("c5")
+    if ref is not None and int(ref["N"]) == A.N:
+        xr = ref["x"]
+        pick = lambda v: v.cpu().numpy().reshape(-1, 2)[ref["idx"]]  # noqa: E731
+        ref_cmp = {"reference_iterations": int(ref["iters"]),
+                   "complex128_rel_err_vs_reference": float(np.linalg.norm(pick(x128) - xr) / np.linalg.norm(xr)),
+                   "complex64_rel_err_vs_reference": float(np.linalg.norm(pick(x) - xr) / np.linalg.norm(xr)),
+                   "reference_sample": f"{ref['idx'].size} entries of the reference's Solve_PCOCG solution "
+                                       f"(complex128, rel.res 1e-8)"}
+    else:
+        ref_cmp = {"reference": "fixture absent"}
     out = {"workload": f"c5 Helmholtz k=20 unit disk, {m.nnode} nodes (band numbering), complex ILU(0)-COCG to "
                        f"rel.res 1e-8", "sweep_mode": M.sweep,
            "complex128_s": t_plain, "iterations": it, "status": rc,
            "complex64_inner_s": t_mixed, "complex64_iterations": it_m, "complex64_status": rc_m,
            "complex64_speedup": t_plain / t_mixed, "complex64_true_rel_residual": res_m,
-           "complex64_rel_err_vs_complex128": float(torch.linalg.norm(x - x128) / torch.linalg.norm(x128))}
+           "complex64_rel_err_vs_complex128": float(torch.linalg.norm(x - x128) / torch.linalg.norm(x128)),
+           **ref_cmp}
     for h in (M, A, G):
         h.close()
     return out
+
+
+def run_c4(torch, dev):
+    """c4: the adjoint of 2-D plane-stress elasticity (128x128 grid of P1
+    triangles, 2x2 blocks, nu = 0.3, per-element Young's modulus theta ~
+    lognormal(0, 0.5), left edge clamped, traction (0, -1) on the right edge,
+    L = 1/2 sum over 256 observed nodes |u - u_target|^2 with u_target from a
+    second seeded theta).  One step = the forward solve (device assembly,
+    elimination, ILU(0), PCG to 1e-12) and the backward (adjoint PCG with the
+    same factorization, element kernel) through torch.autograd, timed on the
+    host clock (the library synchronises).  Checked against an FP64 direct
+    adjoint gradient and central finite differences (h = 1e-6) on 64 sampled
+    elements, both FP64 on the host (tests/adjoint_ref.py)."""
+    from delfem_b200 import adjoint, lib
+    from tests import cases
+    from tests.adjoint_ref import Reference
+    ctx = lib.Context(dev)
+    m, theta, theta_t, obs, fixed, load = cases.adjoint_case(128, seed=0)
+    R = Reference(m.coord, m.elem, fixed, load, cases.LAM2_PS, cases.MYU2)
+    ut = R.solve(theta_t)[1]
+    idx = np.concatenate([2 * obs, 2 * obs + 1])
+    prob = adjoint.PlaneStressProblem(ctx, m.coord, m.elem, fixed, load, cases.LAM2_PS, cases.MYU2, tol=1e-12)
+    idx_t = torch.from_numpy(idx).cuda(dev)
+    ut_t = torch.from_numpy(ut).cuda(dev)
+
+    def step():
+        prob._theta = None  # every step assembles and factors K(theta) again
+        th = torch.tensor(theta, dtype=torch.float64, device=f"cuda:{dev}", requires_grad=True)
+        u = adjoint.elastic_solve(th, prob)
+        loss = 0.5 * torch.sum((u[idx_t] - ut_t[idx_t]) ** 2)
+        loss.backward()
+        return float(loss.item()), th.grad
+
+    step()
+    ts = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, g = step()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    g_dev = g.cpu().numpy()
+
+    def gfun(uu):
+        gg = np.zeros_like(uu)
+        gg[idx] = uu[idx] - ut[idx]
+        return 0.5 * np.sum((uu[idx] - ut[idx]) ** 2), gg
+
+    t0 = time.perf_counter()
+    L_ref, g_ref = R.grad(theta, gfun)
+    elems = np.random.default_rng(100).choice(m.elem.shape[0], 64, replace=False)
+    fd = R.fd(theta, idx, ut, elems, h=1e-6)
+    t_check = time.perf_counter() - t0
+    ctx.close()
+    return {"workload": "c4 plane-stress adjoint 128x128 P1 (N = 16,641, b = 2, 32,768 elements), 256 observed "
+                        "nodes, forward + backward per step",
+            "forward_backward_s": statistics.median(ts), "forward_iterations": prob.last_iters + 1,
+            "loss": loss, "loss_rel_err_vs_fp64": abs(loss - L_ref) / abs(L_ref),
+            "grad_rel_err_vs_fp64_adjoint": float(np.linalg.norm(g_dev - g_ref) / np.linalg.norm(g_ref)),
+            "grad_rel_err_vs_central_fd": float(np.linalg.norm(g_dev[elems] - fd) / np.linalg.norm(fd)),
+            "fd": "central differences, h = 1e-6, 64 sampled elements, FP64 direct solves on the host",
+            "host_check_s": t_check}
 
 
 # -------------------------------------------------------------------- our arm
@@ -438,6 +599,7 @@ def run_ours(args, rank, world):
     lib.check(lib.lib().dfm_ctx_set_stream(ctx.h, lib.C.c_void_p(stream.cuda_stream)))
     m, G, A, b_dev, t_asm = build_c2(ctx, torch, dev)
     N, b, ncrs = A.N, A.b, A.ncrs
+    assert (N, b, ncrs) == (C2_CONFIG["N"], C2_CONFIG["b"], C2_CONFIG["ncrs"])
     M = lib.ILU(A)
     # range-sweep CTAs as patches across the beam's long axis (the autotuner
     # times this partition beside balanced ranges of the natural order)
@@ -494,6 +656,25 @@ def run_ours(args, rank, world):
         return float(torch.linalg.norm(b_dev - y) / torch.linalg.norm(b_dev))
 
     rr = true_rel_residual(x64)
+
+    # ---- parity at scale: the c2 solve to 1e-10 against the reference's own x ----
+    parity = {}
+    ref = reference_solution("c2")
+    if ref is not None and rank == 0:
+        x10 = torch.zeros_like(b_dev)
+        r.copy_(b_dev)
+        rc10, it10, conv10 = lib.solve_pcg(A, M, r, x10, tol=1e-10, maxit=20000)
+        xh = x10.cpu().numpy()
+        parity = {"tol": 1e-10, "iterations": it10 + 1, "reference_iterations": int(ref["iters"]) + 1,
+                  "rel_err_vs_reference_sampled": float(np.linalg.norm(xh[ref["idx"]] - ref["x"]) /
+                                                        np.linalg.norm(ref["x"])),
+                  "rel_norm_diff_vs_reference": float(abs(np.linalg.norm(xh) - float(ref["xnorm"])) /
+                                                      float(ref["xnorm"])),
+                  "sample": f"{ref['idx'].size} entries (every {int(ref['idx'][1])}th DOF) of the reference's "
+                            f"Solve_PCG solution, and its 2-norm",
+                  "true_rel_residual": true_rel_residual(x10)}
+        log(f"[bench] c2 at 1e-10: {it10 + 1} iterations (reference {int(ref['iters']) + 1}), rel err vs the "
+            f"reference's x {parity['rel_err_vs_reference_sampled']:.2e}")
 
     # ---- kernel breakdown (CUDA events on the library stream) ----
     y = torch.empty_like(b_dev)
@@ -604,10 +785,14 @@ def run_ours(args, rank, world):
     batched = {}
     if not args.skip_batched and world == 1:
         batched = run_c3(ctx, torch, dev, stream, timed, args.steps)
+    elif not args.skip_batched:
+        batched = {"sharded": run_c3_sharded(torch, dev, stream, args.steps)}
     c1 = {}
+    c4 = {}
     c5 = {}
     if not args.skip_extra and world == 1:
         c1 = run_c1(ctx, torch, dev, timed, rank == 0 and not args.no_cpu_baseline)
+        c4 = run_c4(torch, dev)
         c5 = run_c5(ctx, torch, dev, timed)
 
     cpu = None
@@ -630,11 +815,9 @@ def run_ours(args, rank, world):
             "metric": METRIC, "value": world / t_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "c2 3D elasticity cantilever 200x40x40 hexes x 6 P1 tets, ILU(0) + PCG to "
-                                   "rel.res 1e-8 (plain FP64)", "N": N, "b": b, "ncrs": ncrs,
-                       "dof": N * b, "l2": "inputs larger than L2 (K = %.0f MB)" % (off_d.nbytes / 1e6),
-                       "parallelism": f"replicas x{world}"},
+            "config": dict(C2_CONFIG, parallelism=f"replicas x{world}"),
             "iterations": n_it, "conv": conv, "true_rel_residual": rr, "solve_time_s": t_step,
+            "parity_c2_1e-10": parity,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": dk["gbs"], "peak": hbm, "unit": "GB/s",
                          "frac": dk["frac"], "traffic": traffic, "peak_source": peak_src},
             "spmv_roofline": {"achieved": kernels["spmv_bcrs_b3"]["gbs"], "peak": hbm, "unit": "GB/s",
@@ -644,6 +827,7 @@ def run_ours(args, rank, world):
             "ilu1": iluk,
             "batched": batched,
             "c1": c1,
+            "c4": c4,
             "c5": c5,
             "e2e": {"value": 1.0 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": t_e2e * 1e3},

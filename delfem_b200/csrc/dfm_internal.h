@@ -187,11 +187,18 @@ int set_poll_sleep(unsigned ns);
 // first are substituted by products with the factor; see sweep.cu)
 // part: the CTAs are the parts of the ILU's row partition (G must be its
 // part count) instead of balanced ranges of the natural row order
+// halo: the plan of the shared-memory-only schedule (sweep_halo.cu; unmerged,
+// FP64 vectors)
 int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge = false,
-                     bool part = false);
+                     bool part = false, bool halo = false);
+// sweep_halo.cu
+int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part);
+cudaError_t sweep_halo_launch(dfm_ilu M, bool fwd, const SweepPlan* P, const double* in, double* out,
+                              const double* rdot, double* part, KrylovScalars* sc, const double* rr_part, int rr_n,
+                              bool f32);
 void sweep_plan_free(SweepPlan* P);
 int sweep_plan_refresh(dfm_ilu M, SweepPlan* P);
-int ilu_set_ranges(dfm_ilu M, int G, bool merge = false);
+int ilu_set_ranges(dfm_ilu M, int G, bool merge = false, bool halo = false);
 int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, const double* rdot, double* part,
                         KrylovScalars* sc, const double* rr_part, int rr_n, bool f32 = false);
 // krylov.cu

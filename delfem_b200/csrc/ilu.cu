@@ -826,9 +826,12 @@ int ilu_prepare(dfm_ilu M, bool f32) {
     for (int f = 0; f < 2; f++) {
       SweepPlan& P64 = f ? M->plan_b : M->plan_f;
       SweepPlan& P32 = f ? M->plan32_b : M->plan32_f;
-      if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr || P32.merged != P64.merged) {
-        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32, P64.merged, P64.part))) return rc;
+      if (!P32.valid || P32.G != P64.G || P32.lpr != P64.lpr || P32.merged != P64.merged ||
+          P32.halo != P64.halo || P32.cw != P64.cw || P32.hw != P64.hw) {
+        if ((rc = sweep_plan_build(M, f == 0, P64.G, 4, 8, &P32, P64.merged, P64.part, P64.halo))) return rc;
         P32.lpr = P64.lpr;
+        P32.cw = P64.cw;
+        P32.hw = P64.hw;
         M->plan_gen++;  // captured graphs hold the old plan's buffers
       }
       P32.nb = P64.nb && P32.nb_ok;
@@ -985,6 +988,67 @@ int ilu_autotune(dfm_ilu M) {
         }
       }
     }
+    // the shared-memory-only schedule (mode 9) at the partition and at one
+    // CTA per SM: compute warps x lanes per row, producer warps
+    {
+      const unsigned bx = M->vt == DFM_COMPLEX ? 2u : M->b;
+      struct Cfg { int cw, lpr, hw; };
+      const Cfg cfgs3[] = {{1, 4, 4}, {2, 4, 4}, {4, 4, 4}, {4, 8, 4}, {2, 8, 4}, {4, 4, 8}};
+      const Cfg cfgs1[] = {{1, 2, 4}, {1, 4, 4}, {2, 4, 4}, {4, 4, 4}, {2, 2, 4}, {4, 4, 8}};
+      const Cfg* cfgs = bx == 1 ? cfgs1 : cfgs3;
+      auto try_halo = [&](int G, bool part) -> int {
+        SweepPlan pf, pb;
+        if (sweep_plan_build(M, true, G, 8, 8, &pf, false, part, true) != DFM_OK ||
+            sweep_plan_build(M, false, G, 8, 8, &pb, false, part, true) != DFM_OK) {
+          sweep_plan_free(&pf);
+          sweep_plan_free(&pb);
+          cudaGetLastError();
+          return DFM_OK;
+        }
+        std::swap(M->plan_f, pf);
+        std::swap(M->plan_b, pb);
+        float ms = 1e30f;
+        Cfg bc = cfgs[0];
+        int rc = DFM_OK;
+        for (int q = 0; q < 6 && rc == DFM_OK; q++) {
+          M->plan_f.cw = M->plan_b.cw = cfgs[q].cw;
+          M->plan_f.lpr = M->plan_b.lpr = cfgs[q].lpr;
+          M->plan_f.hw = M->plan_b.hw = cfgs[q].hw;
+          float t = 1e30f;
+          rc = time_mode(3, &t);
+          if (rc == DFM_OK && t < ms) { ms = t; bc = cfgs[q]; }
+          if (rc == DFM_ERR_CUDA || rc == DFM_ERR_UNSUPPORTED) {  // a launch this configuration cannot have
+            cudaGetLastError();
+            rc = DFM_OK;
+          }
+        }
+        M->plan_f.cw = M->plan_b.cw = bc.cw;
+        M->plan_f.lpr = M->plan_b.lpr = bc.lpr;
+        M->plan_f.hw = M->plan_b.hw = bc.hw;
+        std::swap(M->plan_f, pf);
+        std::swap(M->plan_b, pb);
+        if (rc == DFM_OK && ms < best) {
+          best = ms;
+          best_mode = 3;
+          sweep_plan_free(&best_f);
+          sweep_plan_free(&best_b);
+          std::swap(best_f, pf);
+          std::swap(best_b, pb);
+        } else {
+          sweep_plan_free(&pf);
+          sweep_plan_free(&pb);
+        }
+        return rc == DFM_ERR_UNSUPPORTED ? DFM_OK : rc;
+      };
+      int rc = DFM_OK;
+      if (M->nparts > 0 && M->nparts <= (unsigned)nsm) rc = try_halo((int)M->nparts, true);
+      if (rc == DFM_OK) rc = try_halo(nsm, false);
+      if (rc) {
+        sweep_plan_free(&best_f);
+        sweep_plan_free(&best_b);
+        return rc;
+      }
+    }
     std::swap(M->plan_f, best_f);
     std::swap(M->plan_b, best_b);
     M->plan_gen++;
@@ -999,12 +1063,12 @@ int ilu_autotune(dfm_ilu M) {
   return DFM_OK;
 }
 
-int ilu_set_ranges(dfm_ilu M, int G, bool merge) {
+int ilu_set_ranges(dfm_ilu M, int G, bool merge, bool halo) {
   SweepPlan pf, pb;
   const bool part = M->nparts > 0;  // a row partition, when set, fixes the CTAs
   if (part) G = (int)M->nparts;
-  int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge, part);
-  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge, part);
+  int rc = sweep_plan_build(M, true, G, 8, 8, &pf, merge, part, halo);
+  if (!rc) rc = sweep_plan_build(M, false, G, 8, 8, &pb, merge, part, halo);
   if (rc) {
     sweep_plan_free(&pf);
     sweep_plan_free(&pb);

@@ -724,7 +724,11 @@ void sweep_plan_free(SweepPlan* P) {
 }
 
 int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge,
-                     bool part) {
+                     bool part, bool halo) {
+  if (halo) {
+    if (merge || vec_bytes != 8) return DFM_ERR_UNSUPPORTED;
+    return sweep_halo_plan_build(M, fwd, G, val_bytes, P, part);
+  }
   const unsigned N = M->N;
   const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks
   const unsigned bb = b * b;
@@ -1077,6 +1081,10 @@ int sweep_ranges_launch(dfm_ilu M, bool fwd, const double* in, double* out, cons
   if (P->stale) {
     int rc = sweep_plan_refresh(M, P);
     if (rc) return rc;
+  }
+  if (P->halo) {
+    DFM_CUDA_TRY(sweep_halo_launch(M, fwd, P, in, out, rdot, part, sc, rr_part, rr_n, f32));
+    return DFM_OK;
   }
   DFM_CUDA_TRY(f32 ? launch_ranges_b<float>(M, fwd, P, in, out, rdot, part, sc, rr_part, rr_n)
                    : launch_ranges_b<double>(M, fwd, P, in, out, rdot, part, sc, rr_part, rr_n));

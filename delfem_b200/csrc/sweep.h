@@ -84,6 +84,12 @@ struct SweepPlan {
   uint4* d_recipe = nullptr;        // per packed block: {base slot, term range, sign}
   uint4* d_terms = nullptr;         // {s1, j, s2, 0}: F[s1] (D_j^-1) (F[s2])
   bool merged = false;              // steps are pairs of levels
+  // halo plans (sweep_halo.cu, schedule mode 9): compute warps read shared memory only
+  bool halo = false;
+  unsigned x_slice = 0;             // elements of the range slice at the start of X
+  unsigned halo_stride = 0;         // elements of one stage's halo area
+  int cw = 4;                       // compute warps
+  int hw = 4;                       // producer warps
 };
 
 }  // namespace dfm

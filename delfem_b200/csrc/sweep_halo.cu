@@ -1,0 +1,635 @@
+// Range-partitioned ILU triangular sweeps whose level path reads shared
+// memory only (schedule mode 9).
+//
+// The rows are split among co-resident CTAs as in the range schedule
+// (sweep.cu): contiguous ranges of the natural order, or the parts of the
+// caller's row partition.  A CTA walks its rows level by level.  What differs
+// is who waits for what:
+//
+//  * A few compute warps (1, 2 or 4) take the rows of a level, LPR lanes per
+//    row, and read every operand from shared memory: a row of the CTA's own
+//    range from its vector slice, a row of another CTA from the level's halo,
+//    a small per-stage area filled ahead of time.  Between levels they meet
+//    at a named barrier of their own (bar.sync 1, or __syncwarp for a single
+//    warp) instead of a barrier of the whole CTA.
+//  * Producer warps run ahead of them.  Producer p takes the CTA's chunks
+//    (a level, or a slice of one) p, p + P, p + 2P, ...: it waits until the
+//    compute warps have released the chunk's stage, copies the chunk (row
+//    descriptors, operand offsets, halo row ids, factor blocks, D^-1 rows)
+//    into the stage with one TMA bulk copy (cp.async.bulk, no multicast),
+//    waits for it to land, then polls the halo rows' published values in
+//    global memory (NaN sentinel = not yet written) until all are in, copies
+//    them into the stage's halo area and marks the stage ready for that chunk.
+//
+// The critical path of a level is then the compute warps' own work plus a
+// barrier of at most four warps; the L2 round trips for other CTAs' rows and
+// the copies of the level data overlap with earlier levels, up to the depth of
+// the stage ring.
+//
+// Every operand is addressed by a precomputed element offset into X =
+// [slice | halo area of stage 0 | ... | halo area of stage nstage-1]; a chunk's
+// halo offsets name the stage the chunk lands in (its index within the CTA's
+// chunks modulo nstage), so the compute warps never branch on where a value
+// lives.
+//
+// Progress: a row waits only for rows of lower level; every CTA takes its
+// chunks in level order and all CTAs are co-resident (cooperative launch), so
+// every wait ends.  All waits are bounded as well: past the context's limit a
+// wait records DFM_WAIT_TIMEOUT, the CTA stops computing (every compute warp
+// still passes each level's barrier, so no warp is left behind at a barrier),
+// and copies in flight land before the CTA exits.
+#include <algorithm>
+#include <cstring>
+
+#include "dfm_internal.h"
+#include "sweep.h"
+#include "sweep_dev.cuh"
+
+namespace dfm {
+
+constexpr int kHaloMaxStages = 16;
+constexpr int kHaloMaxWarps = 16;
+constexpr int kHaloMaxThreads = 32 * kHaloMaxWarps;
+
+// Header of a chunk of a halo plan: 32 bytes, then the row descriptors at +32
+// as in every plan (the factor gather of sweep.cu serves both).
+struct HaloHeader {
+  unsigned nrows, xoff, vals, dinv, hids, nhalo, pad0, pad1;
+};
+static_assert(sizeof(HaloHeader) == 32, "halo chunk header is 32 bytes");
+
+DFM_DEVINL int ld_volatile_i(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+DFM_DEVINL void st_volatile_i(int* p, int v) { *reinterpret_cast<volatile int*>(p) = v; }
+
+DFM_DEVINL void compute_barrier(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Deterministic block sum of the CTA's share of (rdot, out) over its finished
+// slice, for any block size (fixed order: threads, then warps).  DOT 2:
+// complex rows as real 2x2 blocks, the unconjugated product, re / im parts in
+// part[] and part[kMaxBlocks + ...].
+template <int B, int DOT>
+DFM_DEVINL void halo_dot(const double* __restrict__ rdot, const double* X, unsigned a0, unsigned len, double* part,
+                         const unsigned* rows) {
+  __shared__ double s_w[2][kHaloMaxWarps];
+  double re = 0.0, im = 0.0;
+  if constexpr (DOT == 2) {
+    for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
+      const size_t gi = slot_row(rows, a0 + k);
+      const double rr = rdot[gi * 2], ri = rdot[gi * 2 + 1];
+      const double xr = X[2 * k], xi = X[2 * k + 1];
+      re += rr * xr - ri * xi;
+      im += rr * xi + ri * xr;
+    }
+  } else {
+    for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
+      re += rdot[slot_row(rows, a0 + k / B) * B + k % B] * X[k];
+  }
+  re = group_sum<32>(re);
+  im = group_sum<32>(im);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
+  if (l == 0) {
+    s_w[0][w] = re;
+    s_w[1][w] = im;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double t0 = l < nw ? s_w[0][l] : 0.0, t1 = l < nw ? s_w[1][l] : 0.0;
+    t0 = group_sum<32>(t0);
+    t1 = group_sum<32>(t1);
+    if (l == 0) {
+      part[blockIdx.x] = t0;
+      if (DOT == 2) part[kMaxBlocks + blockIdx.x] = t1;
+    }
+  }
+}
+
+template <int B, int LPR, typename TV, bool FWD, int DOT>
+__global__ void __launch_bounds__(kHaloMaxThreads, 1)
+k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
+             const unsigned* __restrict__ range, const unsigned* __restrict__ rows, const char* __restrict__ blob,
+             unsigned stage_bytes, int nstage, unsigned x_bytes, unsigned x_slice, unsigned halo_stride, int ncw,
+             const double* __restrict__ in, double* out, const double* __restrict__ rdot, double* part,
+             KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st, uint64_t wait_ns) {
+  constexpr int BB = B * B;
+  extern __shared__ __align__(128) char smem[];
+  __shared__ int s_alive;
+  __shared__ int s_released;               // chunks the compute warps are done with
+  __shared__ int s_ready[kHaloMaxStages];  // the chunk whose data and halo a stage holds (-1: none)
+  if (sc) {
+    if (block_flag(&sc->done)) return;
+    if (FWD && rr_part) {
+      const double rr = reduce_partials(rr_part, rr_nparts);
+      if (rr * sc->inv0 < sc->tol2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          sc->conv = sqrt(rr * sc->inv0);
+          sc->conv_it = sc->it;
+          sc->done = sc->conv_code;
+        }
+        return;
+      }
+    }
+  }
+  const unsigned a0 = range[blockIdx.x], a1 = range[blockIdx.x + 1];
+  const unsigned q0 = cta_chunk[blockIdx.x], q1 = cta_chunk[blockIdx.x + 1];
+  const unsigned K = q1 - q0, len = a1 - a0;
+  double* X = reinterpret_cast<double*>(smem);
+  char* stages = smem + x_bytes;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
+
+  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[slot_row(rows, a0 + k / B) * B + k % B];
+  if (threadIdx.x == 0) {
+    s_alive = 1;
+    s_released = 0;
+    for (int s = 0; s < nstage; s++) {
+      mbar_init(&bar[s], 1);
+      s_ready[s] = -1;
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int warp = (int)(threadIdx.x >> 5), wl = (int)(threadIdx.x & 31);
+  const int nwarps = (int)(blockDim.x >> 5);
+
+  if (warp >= ncw) {
+    // ------------------------------------------------------------ producer
+    const int pw = warp - ncw, npw = nwarps - ncw;
+    for (unsigned k = (unsigned)pw; k < K; k += (unsigned)npw) {
+      if (__any_sync(0xffffffffu, !ld_volatile_i(&s_alive))) break;  // warp-uniform
+      const int s = (int)(k % (unsigned)nstage);
+      // the stage is free once the compute warps are done with chunk k - nstage
+      bool ok = true;
+      if (k >= (unsigned)nstage && ld_volatile_i(&s_released) < (int)(k - nstage + 1)) {
+        SpinGuard g(wait_ns);
+        while (ld_volatile_i(&s_released) < (int)(k - nstage + 1)) {
+          if (!ld_volatile_i(&s_alive)) { ok = false; break; }
+          if (g.expired()) {
+            raise_error(st, DFM_WAIT_TIMEOUT, 20);
+            st_volatile_i(&s_alive, 0);
+            ok = false;
+            break;
+          }
+        }
+      }
+      if (!__all_sync(0xffffffffu, ok)) break;  // every lane votes, waited or not
+      __threadfence_block();
+      const ChunkDesc cd = chunks[q0 + k];
+      char* sb = stages + (size_t)s * stage_bytes;
+      if (wl == 0) {
+        fence_proxy_async_smem();  // the compute warps' reads of the stage precede the copy into it
+        mbar_arrive_tx(&bar[s], cd.bytes);
+        bulk_g2s(sb, blob + cd.off, cd.bytes, &bar[s]);
+      }
+      __syncwarp();
+      const unsigned par = (k / (unsigned)nstage) & 1u;
+      if (!mbar_try_wait(&bar[s], par)) {
+        SpinGuard g(wait_ns);
+        while (!mbar_try_wait(&bar[s], par)) {
+          if (g.expired()) {
+            raise_error(st, DFM_WAIT_TIMEOUT, 21);
+            st_volatile_i(&s_alive, 0);
+            ok = false;
+            break;
+          }
+        }
+      }
+      if (!__all_sync(0xffffffffu, ok)) {
+        // the copy must land before the CTA exits (bounded again)
+        if (wl == 0) (void)wait_stage(&bar[s], par, st, wait_ns);
+        break;
+      }
+      // halo: the other CTAs' rows this chunk reads, polled until published
+      const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
+      const unsigned nh = hdr->nhalo;
+      const unsigned* hids = reinterpret_cast<const unsigned*>(sb + hdr->hids);
+      double* H = X + x_slice + (size_t)s * halo_stride;
+      for (unsigned e = (unsigned)wl; e < nh; e += 32) {
+        const size_t row = hids[e];
+        double v[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) v[c] = ld_relaxed(out + row * B + c);
+        bool miss = false;
+#pragma unroll
+        for (int c = 0; c < B; c++) miss |= Sent<double>::is(v[c]);
+        if (miss) {
+          SpinGuard g(wait_ns);
+          while (miss) {
+            miss = false;
+#pragma unroll
+            for (int c = 0; c < B; c++)
+              if (Sent<double>::is(v[c])) {
+                v[c] = ld_relaxed(out + row * B + c);
+                miss |= Sent<double>::is(v[c]);
+              }
+            if (!miss) break;
+            if (g.expired() || ((g.n & 1023u) == 0 && !ld_volatile_i(&s_alive))) {
+              if (g.expired()) raise_error(st, DFM_WAIT_TIMEOUT, 22);
+              st_volatile_i(&s_alive, 0);
+              ok = false;
+              break;
+            }
+          }
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int c = 0; c < B; c++) H[e * B + c] = v[c];
+      }
+      if (!__all_sync(0xffffffffu, ok)) break;
+      if (wl == 0) {
+        __threadfence_block();
+        st_volatile_i(&s_ready[s], (int)k);
+      }
+    }
+  } else {
+    // ------------------------------------------------------------- compute
+    const int nct = ncw * 32;
+    const int lane = (int)threadIdx.x % LPR;
+    const unsigned g = threadIdx.x / LPR, ng = (unsigned)nct / LPR;
+    const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
+    bool alive = true;
+    for (unsigned k = 0; k < K; k++) {
+      const int s = (int)(k % (unsigned)nstage);
+      if (alive && ld_volatile_i(&s_ready[s]) != (int)k) {
+        SpinGuard gd(wait_ns);
+        while (ld_volatile_i(&s_ready[s]) != (int)k) {
+          if (!ld_volatile_i(&s_alive)) { alive = false; break; }
+          if (gd.expired()) {
+            raise_error(st, DFM_WAIT_TIMEOUT, 23);
+            st_volatile_i(&s_alive, 0);
+            alive = false;
+            break;
+          }
+        }
+      }
+      __threadfence_block();
+      const char* sb = stages + (size_t)s * stage_bytes;
+      if (alive) {
+        // the stage's copy completed (observed by its producer): acquire it here too
+        const unsigned par = (k / (unsigned)nstage) & 1u;
+        if (!mbar_try_wait(&bar[s], par)) {
+          SpinGuard gd(wait_ns);
+          while (!mbar_try_wait(&bar[s], par))
+            if (gd.expired()) {
+              raise_error(st, DFM_WAIT_TIMEOUT, 24);
+              st_volatile_i(&s_alive, 0);
+              alive = false;
+              break;
+            }
+        }
+      }
+      alive = __all_sync(0xffffffffu, alive);  // the lanes of a row's group agree
+      if (alive) {
+        const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
+        const unsigned nrows = hdr->nrows;
+        const uint4* rdesc = reinterpret_cast<const uint4*>(sb + 32);
+        const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+        const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+        for (unsigned r = g; r < nrows; r += ng) {
+          const uint4 rd = rdesc[r];
+          double acc[B];
+#pragma unroll
+          for (int c = 0; c < B; c++) acc[c] = 0.0;
+          unsigned kk = rd.y + (unsigned)lane;
+          for (; kk + LPR < rd.z; kk += 2 * LPR) {  // two operands in flight per lane
+            const unsigned o0 = xoff[kk], o1 = xoff[kk + LPR];
+            double x0[B], x1[B];
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              x0[c] = X[o0 + c];
+              x1[c] = X[o1 + c];
+            }
+            const TV* m0 = vals + (size_t)kk * BB;
+            const TV* m1 = vals + (size_t)(kk + LPR) * BB;
+#pragma unroll
+            for (int rr = 0; rr < B; rr++)
+#pragma unroll
+              for (int c = 0; c < B; c++) acc[rr] += (double)m0[rr * B + c] * x0[c];
+#pragma unroll
+            for (int rr = 0; rr < B; rr++)
+#pragma unroll
+              for (int c = 0; c < B; c++) acc[rr] += (double)m1[rr * B + c] * x1[c];
+          }
+          if (kk < rd.z) {
+            const unsigned o0 = xoff[kk];
+            const TV* m0 = vals + (size_t)kk * BB;
+#pragma unroll
+            for (int rr = 0; rr < B; rr++)
+#pragma unroll
+              for (int c = 0; c < B; c++) acc[rr] += (double)m0[rr * B + c] * X[o0 + c];
+          }
+          if (LPR > 1) {
+#pragma unroll
+            for (int rr = 0; rr < B; rr++)
+#pragma unroll
+              for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
+          }
+          if (lane == 0) {
+            double* xi = X + (size_t)rd.x * B;
+            double t[B];
+#pragma unroll
+            for (int rr = 0; rr < B; rr++) t[rr] = xi[rr] - acc[rr];
+            double o[B];
+            if (FWD) {
+              const double* d = reinterpret_cast<const double*>(sb + hdr->dinv) + (size_t)r * BB;
+#pragma unroll
+              for (int rr = 0; rr < B; rr++) {
+                double v = 0.0;
+#pragma unroll
+                for (int c = 0; c < B; c++) v += d[rr * B + c] * t[c];
+                o[rr] = v;
+              }
+            } else {
+#pragma unroll
+              for (int rr = 0; rr < B; rr++) o[rr] = t[rr];
+            }
+#pragma unroll
+            for (int rr = 0; rr < B; rr++) {
+              xi[rr] = o[rr];
+              st_relaxed(out + (size_t)rd.w * B + rr, o[rr]);
+            }
+          }
+        }
+      }
+      // every compute warp passes every level's barrier, alive or not
+      if (ncw > 1) compute_barrier(nct);
+      else __syncwarp();
+      if (threadIdx.x == 0) {
+        __threadfence_block();
+        st_volatile_i(&s_released, (int)k + 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (DOT) halo_dot<B, DOT>(rdot, X, a0, len, part, rows);
+}
+
+// ------------------------------------------------------------------ plan
+// The halo plan of one sweep direction over G CTAs (contiguous ranges of the
+// natural order balanced by dependency blocks, or the ILU's row partition):
+// chunks per level with their halo row lists, operand offsets into X.
+int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part) {
+  const unsigned N = M->N;
+  const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks
+  const unsigned bb = b * b;
+  const unsigned vblk = (unsigned)val_bytes * bb;
+  const unsigned drow = fwd ? 8u * bb : 0u;
+  const std::vector<unsigned>& rp = M->A->h_rowptr;
+  const std::vector<unsigned>& ci = M->A->h_colind;
+  const std::vector<unsigned>& dia = M->h_diaind;
+  const std::vector<unsigned>& lev = fwd ? M->lev_f : M->lev_b;
+  sweep_plan_free(P);
+  if (N >= 0x40000000u) return DFM_ERR_UNSUPPORTED;
+  std::vector<unsigned> order, pos, range;
+  if (part) {
+    if ((unsigned)G != M->nparts || M->part_of.size() != N) return DFM_ERR_INVALID;
+    range.assign(G + 1, 0);
+    for (unsigned i = 0; i < N; i++) range[M->part_of[i] + 1]++;
+    for (int c = 0; c < G; c++) range[c + 1] += range[c];
+    order.assign(N, 0);
+    pos.assign(N, 0);
+    std::vector<unsigned> fill(range.begin(), range.end() - 1);
+    for (unsigned i = 0; i < N; i++) {
+      pos[i] = fill[M->part_of[i]]++;
+      order[pos[i]] = i;
+    }
+  } else {
+    if (G < 1) G = 1;
+    if ((unsigned)G > std::max(N, 1u)) G = (int)std::max(N, 1u);
+    std::vector<unsigned long long> wpre(N + 1, 0);
+    for (unsigned i = 0; i < N; i++) {
+      const unsigned nb = fwd ? dia[i] - rp[i] : rp[i + 1] - dia[i];
+      wpre[i + 1] = wpre[i] + nb + 1;
+    }
+    range.assign(G + 1, N);
+    range[0] = 0;
+    for (int c = 1; c < G; c++) {
+      const unsigned long long target = wpre[N] * (unsigned long long)c / (unsigned)G;
+      range[c] = (unsigned)(std::lower_bound(wpre.begin(), wpre.end(), target) - wpre.begin());
+      range[c] = std::max(range[c], range[c - 1]);
+    }
+  }
+  const auto pos_of = [&](unsigned row) { return pos.empty() ? row : pos[row]; };
+  const auto row_at = [&](unsigned p) { return order.empty() ? p : order[p]; };
+  unsigned maxlen = 0;
+  for (int c = 0; c < G; c++) maxlen = std::max(maxlen, range[c + 1] - range[c]);
+  const size_t x_slice = (size_t)maxlen * b;
+  if (x_slice * 8 + 8 * 1024 > kSweepSmemBudget) return DFM_ERR_UNSUPPORTED;  // use more CTAs
+
+  struct Pend {
+    std::vector<uint4> rd;
+    std::vector<unsigned> xo, hids;
+  };
+  std::vector<ChunkDesc> chunks;
+  std::vector<Pend> pend;
+  std::vector<unsigned> cta_chunk(G + 1, 0);
+  std::vector<uint4> recipe;
+  std::vector<unsigned> hmap(N, 0xffffffffu);  // scratch: remote row -> halo index in the current chunk
+  unsigned maxhalo = 1, stage_max = 32;
+  for (int c = 0; c < G; c++) {
+    cta_chunk[c] = (unsigned)chunks.size();
+    const unsigned a0 = range[c], a1 = range[c + 1];
+    std::vector<unsigned> rows(a1 - a0);
+    for (unsigned q = a0; q < a1; q++) rows[q - a0] = row_at(fwd ? q : (a1 - 1 - (q - a0)));
+    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return lev[x] < lev[y]; });
+    size_t p = 0;
+    while (p < rows.size()) {
+      const unsigned L = lev[rows[p]];
+      Pend pd;
+      unsigned nblk = 0;
+      const size_t rec0 = recipe.size();
+      while (p < rows.size() && lev[rows[p]] == L) {
+        const unsigned i = rows[p];
+        const unsigned s0 = fwd ? rp[i] : dia[i], s1 = fwd ? dia[i] : rp[i + 1];
+        unsigned newh = 0;
+        for (unsigned s = s0; s < s1; s++) {
+          const unsigned pc = pos_of(ci[s]);
+          if (!(pc >= a0 && pc < a1) && hmap[ci[s]] == 0xffffffffu) newh++;
+        }
+        const unsigned nb = s1 - s0;
+        const ChunkLayout est = chunk_layout((unsigned)pd.rd.size() + 1, ((nblk + nb) + 3) & ~3u,
+                                             (unsigned)pd.hids.size() + newh, vblk, drow);
+        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) break;
+        pd.rd.push_back(make_uint4(pos_of(i) - a0, nblk, nblk + nb, i));  // {slot, blocks, global row}
+        for (unsigned s = s0; s < s1; s++) {
+          const unsigned col = ci[s], pc = pos_of(col);
+          unsigned code;
+          if (pc >= a0 && pc < a1) {
+            code = (pc - a0) * b;
+          } else {
+            if (hmap[col] == 0xffffffffu) {
+              hmap[col] = (unsigned)pd.hids.size();
+              pd.hids.push_back(col);
+            }
+            code = 0x80000000u | hmap[col];
+          }
+          pd.xo.push_back(code);
+          recipe.push_back(make_uint4(s, 0u, 0u, 0u));
+        }
+        nblk += nb;
+        p++;
+      }
+      for (unsigned h : pd.hids) hmap[h] = 0xffffffffu;
+      const unsigned nblk_pad = (nblk + 3) & ~3u;
+      for (unsigned k = nblk; k < nblk_pad; k++) {
+        pd.xo.push_back(0);  // padding: outside every row's block range
+        recipe.push_back(make_uint4(0xffffffffu, 0u, 0u, 0u));
+      }
+      ChunkDesc cd = {};
+      cd.nrows = (unsigned)pd.rd.size();
+      cd.nblk_pad = nblk_pad;
+      cd.nhalo = (unsigned)pd.hids.size();
+      cd.blk0 = (unsigned)rec0;
+      cd.row0 = a0;
+      const ChunkLayout cl = chunk_layout(cd.nrows, nblk_pad, cd.nhalo, vblk, drow);
+      cd.vals_off = cl.vals;
+      cd.dinv_off = cl.dinv;
+      cd.bytes = cl.bytes;
+      maxhalo = std::max(maxhalo, cd.nhalo);
+      stage_max = std::max(stage_max, cl.bytes);
+      chunks.push_back(cd);
+      pend.push_back(std::move(pd));
+    }
+  }
+  cta_chunk[G] = (unsigned)chunks.size();
+  const unsigned stage_bytes = (stage_max + 15u) & ~15u;
+  const size_t bar_bytes = 8 * (size_t)kHaloMaxStages;
+  const size_t halo_stride = (size_t)maxhalo * b;
+  auto xbytes = [&](int t) { return ((x_slice + (size_t)t * halo_stride) * 8 + 127) & ~(size_t)127; };
+  int ns = 0;
+  for (int t = kHaloMaxStages; t >= 2; t--)
+    if (xbytes(t) + (size_t)t * stage_bytes + bar_bytes <= kSweepSmemBudget) { ns = t; break; }
+  if (ns < 2) return DFM_ERR_UNSUPPORTED;
+  if (x_slice + (size_t)ns * halo_stride >= 0x80000000ull) return DFM_ERR_UNSUPPORTED;
+
+  size_t blob_size = 0;
+  for (ChunkDesc& cd : chunks) {
+    cd.off = blob_size;
+    blob_size += cd.bytes;
+  }
+  std::vector<char> hblob(std::max<size_t>(blob_size, 16), 0);
+  for (int c = 0; c < G; c++) {
+    for (unsigned q = cta_chunk[c]; q < cta_chunk[c + 1]; q++) {
+      const ChunkDesc& cd = chunks[q];
+      const ChunkLayout cl = chunk_layout(cd.nrows, cd.nblk_pad, cd.nhalo, vblk, drow);
+      const size_t hbase = x_slice + (size_t)((q - cta_chunk[c]) % (unsigned)ns) * halo_stride;
+      Pend& pd = pend[q];
+      for (unsigned& code : pd.xo)
+        if (code & 0x80000000u) code = (unsigned)(hbase + (size_t)(code & 0x7fffffffu) * b);
+      char* base = hblob.data() + cd.off;
+      HaloHeader hdr = {cd.nrows, cl.xoff, cl.vals, cl.dinv, cl.hids, cd.nhalo, 0u, 0u};
+      std::memcpy(base, &hdr, sizeof(hdr));
+      std::memcpy(base + cl.roff, pd.rd.data(), 16 * pd.rd.size());
+      std::memcpy(base + cl.xoff, pd.xo.data(), 4 * pd.xo.size());
+      if (!pd.hids.empty()) std::memcpy(base + cl.hids, pd.hids.data(), 4 * pd.hids.size());
+    }
+  }
+  P->G = G;
+  P->fwd = fwd;
+  P->halo = true;
+  P->nchunks = (unsigned)chunks.size();
+  P->stage_bytes = stage_bytes;
+  P->x_bytes = (unsigned)xbytes(ns);
+  P->x_slice = (unsigned)x_slice;
+  P->halo_stride = (unsigned)halo_stride;
+  P->val_bytes = val_bytes;
+  P->vec_bytes = 8;
+  P->nstage = ns;
+  P->smem = xbytes(ns) + (size_t)ns * stage_bytes + bar_bytes;
+  for (int c = 0; c < G; c++) P->max_cta_chunks = std::max(P->max_cta_chunks, cta_chunk[c + 1] - cta_chunk[c]);
+  P->lpr = b == 1 ? 2 : 4;
+  P->cw = 4;
+  P->hw = 4;
+  cudaStream_t s = M->ctx->stream;
+  DFM_CUDA_TRY(cudaMalloc(&P->d_chunks, sizeof(ChunkDesc) * std::max<size_t>(chunks.size(), 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_cta_chunk, sizeof(unsigned) * (G + 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_range, sizeof(unsigned) * (G + 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_blob, hblob.size()));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_recipe, sizeof(uint4) * std::max<size_t>(recipe.size(), 1)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_terms, sizeof(uint4)));
+  if (!chunks.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_chunks, chunks.data(), sizeof(ChunkDesc) * chunks.size(),
+                                 cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_cta_chunk, cta_chunk.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_range, range.data(), sizeof(unsigned) * (G + 1), cudaMemcpyHostToDevice, s));
+  if (!order.empty()) {
+    DFM_CUDA_TRY(cudaMalloc(&P->d_rows, sizeof(unsigned) * order.size()));
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_rows, order.data(), sizeof(unsigned) * order.size(), cudaMemcpyHostToDevice, s));
+  }
+  P->part = part;
+  DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blob, hblob.data(), hblob.size(), cudaMemcpyHostToDevice, s));
+  if (!recipe.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_recipe, recipe.data(), sizeof(uint4) * recipe.size(), cudaMemcpyHostToDevice, s));
+  P->merged = false;
+  DFM_CUDA_TRY(cudaStreamSynchronize(s));
+  P->valid = true;
+  P->stale = true;
+  return DFM_OK;
+}
+
+// ---------------------------------------------------------------- launch
+template <int B, int LPR, typename TV, bool FWD, int DK>
+static cudaError_t launch_halo(dfm_ilu M, const SweepPlan* P, const double* in, double* out, const double* rdot,
+                               double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  dfm_ctx c = M->ctx;
+  const int ncw = P->cw, nhw = P->hw;
+  if (ncw < 1 || nhw < 1 || ncw + nhw > kHaloMaxWarps || (ncw * 32) % LPR) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P->G);
+  cfg.blockDim = dim3(32 * (ncw + nhw));
+  cfg.dynamicSmemBytes = P->smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  auto go = [&](auto fn) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, fn, (const ChunkDesc*)P->d_chunks, (const unsigned*)P->d_cta_chunk,
+                              (const unsigned*)P->d_range, (const unsigned*)P->d_rows, (const char*)P->d_blob,
+                              P->stage_bytes, P->nstage, P->x_bytes, P->x_slice, P->halo_stride, ncw, in, out, rdot,
+                              part, sc, rr_part, rr_n, c->d_status, (uint64_t)c->wait_ns);
+  };
+  // forward sweeps carry no fused dot; backward ones take it when asked
+  if constexpr (FWD) {
+    return go(k_sweep_halo<B, LPR, TV, true, 0>);
+  } else {
+    if (part) return go(k_sweep_halo<B, LPR, TV, false, DK>);
+    return go(k_sweep_halo<B, LPR, TV, false, 0>);
+  }
+}
+
+template <int B, typename TV, bool FWD, int DK>
+static cudaError_t launch_halo_lpr(dfm_ilu M, const SweepPlan* P, const double* in, double* out, const double* rdot,
+                                   double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  switch (P->lpr) {
+    case 2: return launch_halo<B, 2, TV, FWD, DK>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 4: return launch_halo<B, 4, TV, FWD, DK>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    default: return launch_halo<B, 8, TV, FWD, DK>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  }
+}
+
+template <typename TV, bool FWD>
+static cudaError_t launch_halo_b(dfm_ilu M, const SweepPlan* P, const double* in, double* out, const double* rdot,
+                                 double* part, KrylovScalars* sc, const double* rr_part, int rr_n) {
+  if (M->vt == DFM_COMPLEX) return launch_halo_lpr<2, TV, FWD, 2>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  switch (M->b) {
+    case 1: return launch_halo_lpr<1, TV, FWD, 1>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    case 2: return launch_halo_lpr<2, TV, FWD, 1>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+    default: return launch_halo_lpr<3, TV, FWD, 1>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  }
+}
+
+cudaError_t sweep_halo_launch(dfm_ilu M, bool fwd, const SweepPlan* P, const double* in, double* out,
+                              const double* rdot, double* part, KrylovScalars* sc, const double* rr_part, int rr_n,
+                              bool f32) {
+  if (f32)
+    return fwd ? launch_halo_b<float, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+               : launch_halo_b<float, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+  return fwd ? launch_halo_b<double, true>(M, P, in, out, rdot, part, sc, rr_part, rr_n)
+             : launch_halo_b<double, false>(M, P, in, out, rdot, part, sc, rr_part, rr_n);
+}
+
+}  // namespace dfm

@@ -61,6 +61,9 @@ PROTOS = {
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
+    "dfm_mat_zero_rows": (_i, [_vp, _vp]),
+    "dfm_newmark_residual": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dp]),
+    "dfm_newmark_update": (_i, [_vp, C.c_size_t, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp]),
     "dfm_boundary_matrix": (_i, [_u, _u, _up, _up, _dp, _dp, _ip, _up, _up, _dp, _dp, _up]),
     "dfm_mesh_create": (_i, [_vp, _i, _u, _dp, _u, _u, _ip, _u, _ip, C.POINTER(_vp)]),
     "dfm_mesh_destroy": (_i, [_vp]),
@@ -600,6 +603,28 @@ def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CO
     rc = lib().dfm_solve_pcg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_pcg", allow)
     return rc, it.value, conv.value
+
+
+def mat_zero_rows(B: Matrix, flags):
+    """CMat_BlkCrs::SetBoundaryCondition_Row: zero the rows of fixed DOFs (device flags)."""
+    _sync_torch()
+    check(lib().dfm_mat_zero_rows(B.h, _ptr(flags)), "dfm_mat_zero_rows")
+
+
+def newmark_residual(B: Matrix, scheme, dt, gamma, beta, force, u, v, a, flags, t, r) -> float:
+    """MakeResidual of CLinearSystem_SaveDiaM_Newmark (scheme 1) / _NewmarkBeta (2); returns |r|."""
+    nrm = C.c_double()
+    _sync_torch()
+    check(lib().dfm_newmark_residual(B.h, int(scheme), dt, gamma, beta, _ptr(force), _ptr(u), _ptr(v), _ptr(a),
+                                     _ptr(flags), _ptr(t), _ptr(r), C.byref(nrm)), "dfm_newmark_residual")
+    return nrm.value
+
+
+def newmark_update(ctx: Context, scheme, dt, gamma, beta, flags, x, u, v, a=None):
+    """UpdateValueOfField of the Newmark (1) / Newmark-beta (2) stored systems."""
+    _sync_torch()
+    check(lib().dfm_newmark_update(ctx.h, x.numel(), int(scheme), dt, gamma, beta, _ptr(flags), _ptr(x), _ptr(u),
+                                   _ptr(v), _ptr(a)), "dfm_newmark_update")
 
 
 def solve_cg(A: Matrix, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CONVERGED)):

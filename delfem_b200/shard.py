@@ -67,3 +67,43 @@ def solve_sharded(instances, work, solve_local, group=None):
         for k, res in part:
             out[k] = res
     return out
+
+
+def timed_sharded(work, solve_local, device="cpu", group=None):
+    """Each rank solves its share of the instances and times it; the time of
+    the job is the maximum over ranks.
+
+    solve_local(indices) -> (seconds, results): solves the instances with the
+    given indices (this rank's share, ascending) and returns its time and one
+    picklable result per instance.  device: where the max-reduction tensor
+    lives ("cpu" for gloo, "cuda:<n>" for NCCL).  Every rank takes the same
+    collective steps (an all-reduce of the time, a gather of the results).
+    Returns, on rank 0, {"seconds": max over ranks, "per_rank_instances": [...],
+    "per_rank_seconds": [...], "results": [per instance, original order]}
+    (None on the other ranks)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    parts = partition(work, world)
+    mine = parts[rank]
+    secs, local = solve_local(mine) if mine else (0.0, [])
+    if len(local) != len(mine):
+        raise RuntimeError("solve_local returned a wrong number of results")
+    t = torch.tensor([float(secs)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    payload = (float(secs), list(zip(mine, local)))
+    if world == 1:
+        gathered = [payload]
+    else:
+        gathered = [None] * world if rank == 0 else None
+        dist.gather_object(payload, gathered, dst=0, group=group)
+    if rank != 0:
+        return None
+    out = [None] * len(work)
+    for _, part in gathered:
+        for k, res in part:
+            out[k] = res
+    return {"seconds": float(t.item()), "per_rank_instances": [len(p) for p in parts],
+            "per_rank_seconds": [g[0] for g in gathered], "results": out}

@@ -178,6 +178,31 @@ DFM_API int dfm_boundary_matrix(unsigned N, unsigned b, const unsigned* rowptr, 
                                 const double* diag, const double* off, const int* flags, unsigned* brow,
                                 unsigned* bcol, double* bdiag, double* boff, unsigned* bncrs);
 
+/* ---- time integration with a stored matrix ------------------------------- */
+/* Fem::Ls::CLinearSystem_SaveDiaM_Newmark (first order, scheme 1: the update
+ * is the velocity) and CLinearSystem_SaveDiaM_NewmarkBeta (second order,
+ * scheme 2: the update is the acceleration), src/femls/linearsystem_fieldsave.
+ * cpp:367-880.  B is their stored matrix: the element matrices K_e merged
+ * into the full pattern (diagonal blocks included), with the rows of fixed
+ * DOFs zeroed by dfm_mat_zero_rows (CMat_BlkCrs::SetBoundaryCondition_Row,
+ * src/matvec/mat_blkcrs.cpp:910-951) in FinalizeMarge.  Device vectors of
+ * N*b doubles; flags: device int[N*b], nonzero = fixed.  Real matrices. */
+DFM_API int dfm_mat_zero_rows(dfm_mat B, const int* flags);
+/* MakeResidual (:446-520, :706-794): t = u + dt(1-gamma) v (scheme 1) or
+ * t = u + dt v + dt^2(1/2-beta) a (scheme 2; a unused by scheme 1), then
+ * r = force - B t with r = 0 at fixed DOFs; *norm (nullable) = |r|.  t is the
+ * caller's work vector; r may alias force.  Synchronises (the norm). */
+DFM_API int dfm_newmark_residual(dfm_mat B, int scheme, double dt, double gamma, double beta, const double* force,
+                                 const double* u, const double* v, const double* a, const int* flags, double* t,
+                                 double* r, double* norm);
+/* UpdateValueOfField (:522-566, :796-877) after the solve of the update x:
+ * scheme 1: free DOFs u += dt(1-gamma) v + dt gamma x, fixed DOFs x = v, then
+ * v = x; scheme 2: free DOFs u += dt v + dt^2(1/2-beta) a + dt^2 beta x and
+ * v += dt(1-gamma) a + gamma dt x, fixed DOFs x = a, then a = x.  The
+ * reference's arithmetic term by term (bit-identical). */
+DFM_API int dfm_newmark_update(dfm_ctx ctx, size_t n, int scheme, double dt, double gamma, double beta,
+                               const int* flags, double* x, double* u, double* v, double* a);
+
 /* ---- element assembly: CLinearSystem_Field + Fem::Eqn::AddLinSys_* ------- */
 /* A P1 mesh resident on the device: coord[nnode*ndim], elem[nelem*nnoel]
  * (triangles nnoel = 3 in 2D, tetrahedra 4 in 3D) and optional boundary bars
@@ -283,8 +308,12 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * factorization: half the sequential steps, results equal to rounding), 7 and
  * 8 = 3 and 5 with the row groups in two halves taking alternate levels, the
  * idle half fetching its next row's operands before the level barrier (same
- * results as 3 and 5).  Complex matrices run 3-8 as real 2x2 blocks
- * [re -im; im re]. */
+ * results as 3 and 5), 9 = the row ranges of 3 with the level path in shared
+ * memory only: a few compute warps synchronised by a named barrier take the
+ * rows of each level while producer warps stream the level data by TMA and
+ * prefetch the operands owned by other CTAs into a shared-memory halo (results
+ * equal to those of 3 to rounding).  Complex matrices
+ * run 3-9 as real 2x2 blocks [re -im; im re]. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 /* No counterpart in the reference (its sweeps are sequential).  A row
  * partition for the range-partitioned sweep schedules: CTA c takes the rows

@@ -1004,3 +1004,90 @@ int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const 
   free(p); free(Ap); free(w);
   return 1; /* and Solve_PCOCG returns true (src/femls/zsolver_ls_iter.cpp:213-266) */
 }
+
+/* ------------------------------------------------ stored-matrix Newmark systems */
+
+/* CMat_BlkCrs::SetBoundaryCondition_Row (src/matvec/mat_blkcrs.cpp:910-951):
+   the rows of fixed DOFs zeroed in every block of the row (library layout:
+   the diagonal block separate). */
+void dfo_mat_zero_rows(unsigned N, unsigned b, const unsigned* rowptr, const int* flags, double* diag, double* off) {
+  const unsigned bb = b * b;
+  for (unsigned i = 0; i < N; i++)
+    for (unsigned d = 0; d < b; d++) {
+      if (!flags[(size_t)i * b + d]) continue;
+      for (unsigned c = 0; c < b; c++) diag[(size_t)i * bb + d * b + c] = 0.0;
+      for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++)
+        for (unsigned c = 0; c < b; c++) off[(size_t)s * bb + d * b + c] = 0.0;
+    }
+}
+
+/* One stored-matrix block entry of CMat_BlkCrs::MatVec with alpha = -1 and
+   beta = 1 (src/matvec/mat_blkcrs.cpp:955-1175): y += (alpha * m) * x term by
+   term. */
+static void nm_entry(unsigned b, const double* m, const double* x, double* y) {
+  for (unsigned i = 0; i < b; i++)
+    for (unsigned j = 0; j < b; j++) y[i] += (-1.0 * m[i * b + j]) * x[j];
+}
+
+/* MakeResidual of CLinearSystem_SaveDiaM_Newmark (scheme 1, :446-520) and
+   CLinearSystem_SaveDiaM_NewmarkBeta (scheme 2, :706-794): the predictor
+   t = u + v*(dt*(1-gamma)) or t = (u + v*dt) + a*((dt*dt)*(0.5-beta))
+   (CNodeAry::AddValueFromNodeSegment adds val*alpha), r = force - B t in the
+   reference's entry order - its stored matrix has the pattern of
+   CMat_BlkCrs::SetPatternDia (:1267-1318): the diagonal block first when the
+   row has a column below it, else last - then r = 0 at fixed DOFs and
+   *norm = sqrt(r.r).  t is work space. */
+void dfo_newmark_residual(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                          const double* off, int scheme, double dt, double gamma, double beta, const double* force,
+                          const double* u, const double* v, const double* a, const int* flags, double* t, double* r,
+                          double* norm) {
+  const size_t n = (size_t)N * b;
+  const unsigned bb = b * b;
+  const double c1 = scheme == 1 ? dt * (1 - gamma) : dt;
+  const double c2 = dt * dt * (0.5 - beta);
+  for (size_t k = 0; k < n; k++) {
+    t[k] = u[k] + v[k] * c1;
+    if (scheme == 2) t[k] = t[k] + a[k] * c2;
+  }
+  for (size_t k = 0; k < n; k++) r[k] = force[k];
+  for (unsigned i = 0; i < N; i++) {
+    const int dia_first = rowptr[i + 1] > rowptr[i] && colind[rowptr[i]] < i;
+    double* y = r + (size_t)i * b;
+    if (dia_first) nm_entry(b, diag + (size_t)i * bb, t + (size_t)i * b, y);
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) nm_entry(b, off + (size_t)s * bb, t + (size_t)colind[s] * b, y);
+    if (!dia_first) nm_entry(b, diag + (size_t)i * bb, t + (size_t)i * b, y);
+  }
+  double s = 0.0;
+  for (size_t k = 0; k < n; k++) {
+    if (flags[k]) r[k] = 0.0;
+    s += r[k] * r[k];
+  }
+  *norm = sqrt(s);
+}
+
+/* UpdateValueOfField of the two (:522-566, :796-877), x the solved update. */
+void dfo_newmark_update(size_t n, int scheme, double dt, double gamma, double beta, const int* flags, double* x,
+                        double* u, double* v, double* a) {
+  for (size_t k = 0; k < n; k++) {
+    if (scheme == 1) {
+      const double velo0 = v[k];
+      if (flags[k] == 0) {
+        const double velo1 = x[k];
+        u[k] += dt * (1 - gamma) * velo0 + dt * gamma * velo1;
+      } else {
+        x[k] = velo0;
+      }
+      v[k] = x[k];
+    } else {
+      const double velo0 = v[k], acc0 = a[k];
+      if (flags[k] == 0) {
+        const double acc1 = x[k];
+        u[k] += dt * velo0 + dt * dt * (0.5 - beta) * acc0 + dt * dt * beta * acc1;
+        v[k] += dt * (1 - gamma) * acc0 + gamma * dt * acc1;
+      } else {
+        x[k] = acc0;
+      }
+      a[k] = x[k];
+    }
+  }
+}

@@ -12,6 +12,7 @@
  * Block sizes b = 1, 2, 3 (the closed-form paths of the reference). */
 #ifndef DFM_ORACLE_H
 #define DFM_ORACLE_H
+#include <stddef.h>
 #include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
@@ -127,6 +128,17 @@ void dfo_zfwdbwd(unsigned N, const unsigned* rowptr, const unsigned* colind,
 int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const unsigned* diaind,
               const double* diag, const double* off, const double* fdiag, const double* foff,
               double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv);
+
+/* Stored-matrix Newmark systems: SetBoundaryCondition_Row, MakeResidual and
+   UpdateValueOfField of CLinearSystem_SaveDiaM_Newmark (scheme 1) and
+   _NewmarkBeta (scheme 2). */
+void dfo_mat_zero_rows(unsigned N, unsigned b, const unsigned* rowptr, const int* flags, double* diag, double* off);
+void dfo_newmark_residual(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                          const double* off, int scheme, double dt, double gamma, double beta, const double* force,
+                          const double* u, const double* v, const double* a, const int* flags, double* t, double* r,
+                          double* norm);
+void dfo_newmark_update(size_t n, int scheme, double dt, double gamma, double beta, const int* flags, double* x,
+                        double* u, double* v, double* a);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,9 @@ def lib():
         L.dfo_pcg_fill.argtypes = [U, U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp, dp]
         L.dfo_pbicgstab.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_cg.argtypes = [U, U, up, up, dp, dp, dp, dp, D, U, up, dp]
+        L.dfo_mat_zero_rows.argtypes = [U, U, up, ip, dp, dp]
+        L.dfo_newmark_residual.argtypes = [U, U, up, up, dp, dp, C.c_int, D, D, D, dp, dp, dp, dp, ip, dp, dp, dp]
+        L.dfo_newmark_update.argtypes = [C.c_size_t, C.c_int, D, D, D, ip, dp, dp, dp, dp]
         L.dfo_zspmv.argtypes = [U, up, up, dp, dp, D, dp, D, dp]
         L.dfo_zilu0.argtypes = [U, up, up, up, dp, dp]
         L.dfo_zilu0.restype = U
@@ -288,3 +291,36 @@ def bc_flags_from_bnd(nnode, b, bnd):
     if bnd.size:
         f[np.unique(bnd.ravel())] = 1
     return f.ravel()
+
+
+def mat_zero_rows(N, b, rowptr, flags, diag, off):
+    """CMat_BlkCrs::SetBoundaryCondition_Row on copies of (diag, off)."""
+    d, o = np.array(diag, np.float64, copy=True), np.array(off, np.float64, copy=True)
+    fl = np.ascontiguousarray(flags, np.int32)
+    lib().dfo_mat_zero_rows(N, b, _u(np.ascontiguousarray(rowptr, np.uint32)), fl.ctypes.data_as(ip), _d(d), _dz(o))
+    return d, o
+
+
+def newmark_residual(N, b, rowptr, colind, diag, off, scheme, dt, gamma, beta, force, u, v, a, flags):
+    """MakeResidual of the Newmark stored systems: (r, |r|)."""
+    n = N * b
+    t, r, nrm = np.zeros(n), np.zeros(n), C.c_double()
+    a = np.zeros(n) if a is None else np.ascontiguousarray(a, np.float64)
+    ci = np.ascontiguousarray(colind, np.uint32)
+    fl = np.ascontiguousarray(flags, np.int32)
+    lib().dfo_newmark_residual(N, b, _u(np.ascontiguousarray(rowptr, np.uint32)), _u(ci if ci.size else
+                               np.zeros(1, np.uint32)), _d(np.ascontiguousarray(diag, np.float64)),
+                               _dz(np.ascontiguousarray(off, np.float64)), scheme, dt, gamma, beta,
+                               _d(np.ascontiguousarray(force, np.float64)), _d(np.ascontiguousarray(u, np.float64)),
+                               _d(np.ascontiguousarray(v, np.float64)), _d(a), fl.ctypes.data_as(ip), _d(t), _d(r),
+                               C.byref(nrm))
+    return r, nrm.value
+
+
+def newmark_update(scheme, dt, gamma, beta, flags, x, u, v, a=None):
+    """UpdateValueOfField of the Newmark stored systems on copies: (x, u, v, a)."""
+    x, u, v = (np.array(t, np.float64, copy=True) for t in (x, u, v))
+    a = np.zeros_like(u) if a is None else np.array(a, np.float64, copy=True)
+    fl = np.ascontiguousarray(flags, np.int32)
+    lib().dfo_newmark_update(u.size, scheme, dt, gamma, beta, fl.ctypes.data_as(ip), _d(x), _d(u), _d(v), _d(a))
+    return x, u, v, a

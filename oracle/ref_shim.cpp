@@ -23,12 +23,14 @@
 #include "delfem/mesh3d.h"
 #include "delfem/mesh_interface.h"
 #include "delfem/mesher2d.h"
+#include "delfem/femeqn/eqn_diffusion.h"
 #include "delfem/femeqn/eqn_helmholtz.h"
 #include "delfem/femeqn/eqn_linear_solid2d.h"
 #include "delfem/femeqn/eqn_linear_solid3d.h"
 #include "delfem/femeqn/eqn_poisson.h"
 #include "delfem/femeqn/ker_emat_tri.h"
 #include "delfem/femls/linearsystem_field.h"
+#include "delfem/femls/linearsystem_fieldsave.h"
 #include "delfem/femls/zlinearsystem.h"
 #include "delfem/femls/zpreconditioner.h"
 #include "delfem/femls/zsolver_ls_iter.h"
@@ -756,6 +758,116 @@ int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned c
     for (int k = 0; k < *nnoel; k++)
       elem[(size_t)*nnoel * e + k] =
           hex ? (int)m.GetHexArySet()[0].m_aHex[e].v[k] : (int)m.GetTetArySet()[0].m_aTet[e].v[k];
+  return 0;
+}
+
+
+// The stored-matrix Newmark systems through the reference's own classes
+// (src/femls/linearsystem_fieldsave.cpp:367-880).  Scheme 1:
+// CLinearSystem_SaveDiaM_Newmark + AddLinSys_Diffusion (scalar field with
+// velocity; p = rho, alpha, source).  Scheme 2: CLinearSystem_SaveDiaM_NewmarkBeta
+// + AddLinSys_LinearSolid2D_NonStatic_Save_NewmarkBeta (2-D displacement with
+// velocity and acceleration; p = lambda, myu, rho, gx, gy).  P1 triangles;
+// the boundary bars fix every DOF of their nodes.
+int dfm_ref_newmark(int scheme, int nnode, const double* coord, int nelem, const int* elem, int nbnd,
+                    const int* bnd, const double* p, double dt, double gamma, double beta, double* u, double* v,
+                    double* a, double* x, double* bdiag, double* boff, double* force, int* flags, double* r,
+                    double* norm) {
+  if (scheme != 1 && scheme != 2) return 1;
+  Quiet q;
+  ArrayMesh mesh;
+  mesh.ndim = 2;
+  mesh.coord.assign(coord, coord + (size_t)nnode * 2);
+  mesh.vol.assign(elem, elem + (size_t)nelem * 3);
+  mesh.bnd.assign(bnd, bnd + (size_t)nbnd * 2);
+  CFieldWorld world;
+  const unsigned id_base = world.AddMesh(mesh);
+  const CIDConvEAMshCad conv = world.GetIDConverter(id_base);
+  const unsigned b = scheme == 1 ? 1 : 2;
+  const int fdt = scheme == 1 ? (VALUE | VELOCITY) : (VALUE | VELOCITY | ACCELERATION);
+  const unsigned id_field = world.MakeField_FieldElemDim(id_base, 2, scheme == 1 ? SCALAR : VECTOR2, fdt, CORNER);
+  const unsigned id_bnd = world.GetPartialField(id_field, conv.GetIdEA_fromMsh(2));
+  {  // the field's current state
+    CField& f = world.GetField(id_field);
+    CNodeAry::CNodeSeg& nu = f.GetNodeSeg(CORNER, true, world, VALUE);
+    CNodeAry::CNodeSeg& nv = f.GetNodeSeg(CORNER, true, world, VELOCITY);
+    for (int i = 0; i < nnode; i++)
+      for (unsigned d = 0; d < b; d++) {
+        nu.SetValue(i, d, u[(size_t)i * b + d]);
+        nv.SetValue(i, d, v[(size_t)i * b + d]);
+      }
+    if (scheme == 2) {
+      CNodeAry::CNodeSeg& na = f.GetNodeSeg(CORNER, true, world, ACCELERATION);
+      for (int i = 0; i < nnode; i++)
+        for (unsigned d = 0; d < b; d++) na.SetValue(i, d, a[(size_t)i * b + d]);
+    }
+  }
+  Fem::Ls::CLinearSystem_SaveDiaM_Newmark ls1;
+  Fem::Ls::CLinearSystem_SaveDiaM_NewmarkBeta ls2;
+  Fem::Ls::CLinearSystem_Save& ls = scheme == 1 ? static_cast<Fem::Ls::CLinearSystem_Save&>(ls1)
+                                                : static_cast<Fem::Ls::CLinearSystem_Save&>(ls2);
+  ls.AddPattern_Field(id_field, world);
+  ls.SetFixedBoundaryCondition_Field(id_bnd, world);
+  if (scheme == 1) ls1.SetNewmarkParameter(gamma, dt);
+  else ls2.SetNewmarkParameter(beta, gamma, dt);
+  ls.InitializeMarge();
+  if (scheme == 1) Fem::Eqn::AddLinSys_Diffusion(ls1, p[0], p[1], p[2], world, id_field);
+  else Fem::Eqn::AddLinSys_LinearSolid2D_NonStatic_Save_NewmarkBeta(ls2, p[0], p[1], p[2], p[3], p[4], world, id_field);
+  ls.FinalizeMarge();
+  const unsigned bb = b * b;
+  {  // the stored matrix in the library's layout: diagonal block apart, the rest in column order
+    MatVec::CMat_BlkCrs& B = ls.GetMatrix_Boundary(id_field, CORNER, id_field, CORNER, world);
+    size_t pos = 0;
+    for (int i = 0; i < nnode; i++) {
+      unsigned np = 0;
+      const unsigned* ind = B.GetPtrIndPSuP(i, np);
+      unsigned nv = 0;
+      const double* val = B.GetPtrValPSuP(i, nv);
+      for (unsigned k = 0; k < np; k++) {
+        double* dst = (ind[k] == (unsigned)i) ? bdiag + (size_t)i * bb : boff + (pos++) * bb;
+        std::memcpy(dst, val + (size_t)k * bb, sizeof(double) * bb);
+      }
+    }
+    MatVec::CVector_Blk& F = ls.GetForce(id_field, CORNER, world);
+    MatVec::CBCFlag& bc = ls.m_ls.GetBCFlag(0);
+    for (int i = 0; i < nnode; i++)
+      for (unsigned d = 0; d < b; d++) {
+        force[(size_t)i * b + d] = F.GetValue(i, d);
+        flags[(size_t)i * b + d] = bc.GetBCFlag(i, d);
+      }
+  }
+  *norm = ls.MakeResidual(world);
+  {
+    MatVec::CVector_Blk& R = ls.m_ls.GetVector(-1, 0);
+    MatVec::CVector_Blk& U = ls.m_ls.GetVector(-2, 0);
+    for (int i = 0; i < nnode; i++)
+      for (unsigned d = 0; d < b; d++) {
+        r[(size_t)i * b + d] = R.GetValue(i, d);
+        U.SetValue(i, d, x[(size_t)i * b + d]);  // the solved update
+      }
+  }
+  ls.UpdateValueOfField(id_field, world, scheme == 1 ? VELOCITY : ACCELERATION);
+  {
+    CField& f = world.GetField(id_field);
+    CNodeAry::CNodeSeg& nu = f.GetNodeSeg(CORNER, true, world, VALUE);
+    CNodeAry::CNodeSeg& nv = f.GetNodeSeg(CORNER, true, world, VELOCITY);
+    MatVec::CVector_Blk& U = ls.m_ls.GetVector(-2, 0);
+    std::vector<double> t(b);
+    for (int i = 0; i < nnode; i++) {
+      nu.GetValue(i, t.data());
+      for (unsigned d = 0; d < b; d++) u[(size_t)i * b + d] = t[d];
+      nv.GetValue(i, t.data());
+      for (unsigned d = 0; d < b; d++) v[(size_t)i * b + d] = t[d];
+      for (unsigned d = 0; d < b; d++) x[(size_t)i * b + d] = U.GetValue(i, d);
+    }
+    if (scheme == 2) {
+      CNodeAry::CNodeSeg& na = f.GetNodeSeg(CORNER, true, world, ACCELERATION);
+      for (int i = 0; i < nnode; i++) {
+        na.GetValue(i, t.data());
+        for (unsigned d = 0; d < b; d++) a[(size_t)i * b + d] = t[d];
+      }
+    }
+  }
   return 0;
 }
 

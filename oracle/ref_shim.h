@@ -114,6 +114,20 @@ int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned c
 int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, double* fdiag, double* foff);
 
+/* The stored-matrix Newmark systems through the reference's classes:
+ * scheme 1 CLinearSystem_SaveDiaM_Newmark + AddLinSys_Diffusion (p = rho,
+ * alpha, source; b = 1), scheme 2 CLinearSystem_SaveDiaM_NewmarkBeta +
+ * AddLinSys_LinearSolid2D_NonStatic_Save_NewmarkBeta (p = lambda, myu, rho, gx,
+ * gy; b = 2) on P1 triangles, the boundary bars fixed.  The field is set from
+ * u, v (a), assembled, finalized; out: the stored matrix (library layout over
+ * the mesh pattern), force, BC flags, MakeResidual's r and norm.  Then the
+ * update vector is set to x and UpdateValueOfField runs: u, v, a and x are
+ * overwritten with the field's new state and the final update vector. */
+int dfm_ref_newmark(int scheme, int nnode, const double* coord, int nelem, const int* elem, int nbnd,
+                    const int* bnd, const double* p, double dt, double gamma, double beta, double* u, double* v,
+                    double* a, double* x, double* bdiag, double* boff, double* force, int* flags, double* r,
+                    double* norm);
+
 #ifdef __cplusplus
 }
 #endif

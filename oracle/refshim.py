@@ -12,7 +12,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libdfm_refshim.so")
-REF_DIR = "/root/reference"
+REF_DIR = os.environ.get("DELFEM_REFERENCE", "/root/reference")  # the reference source tree
 
 POISSON2D, SOLID2D, SOLID3D, HELMHOLTZ2D = 1, 2, 3, 4
 PCG, PBICGSTAB, PCOCG, CG = 0, 1, 2, 3
@@ -68,6 +68,8 @@ def lib():
         L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
+        L.dfm_ref_newmark.argtypes = [C.c_int, C.c_int, dp, C.c_int, ip, C.c_int, ip, dp, C.c_double, C.c_double,
+                                      C.c_double, dp, dp, dp, dp, dp, dp, dp, ip, dp, dp]
         _lib = L
     return _lib
 
@@ -258,3 +260,26 @@ def boundary_residual(N, b, rowptr, colind, diag, off, flags, force, u):
     bval = np.zeros(max(n.value, 1) * b * b)
     lib().dfm_ref_boundary_residual(*args, n.value, _u(brow), _u(bcol), _d(bval), C.byref(n), _d(r))
     return brow, bcol[: n.value], bval[: n.value * b * b], r
+
+
+def newmark(scheme, mesh, params, dt, gamma, beta, u, v, a, x, ncrs):
+    """The reference's CLinearSystem_SaveDiaM_Newmark (scheme 1, diffusion) /
+    _NewmarkBeta (scheme 2, 2-D solid) on a P1 triangle mesh whose boundary
+    bars are fixed: its stored matrix (library layout over the mesh pattern,
+    ncrs off-diagonal blocks), force, flags, MakeResidual's r and norm, and the
+    state after UpdateValueOfField with the update x.  Returns a dict."""
+    b = 1 if scheme == 1 else 2
+    N = mesh.nnode
+    u, v, x = (np.array(t, np.float64, copy=True).ravel() for t in (u, v, x))
+    a = np.array(a if a is not None else np.zeros(N * b), np.float64, copy=True).ravel()
+    bd, bo = np.zeros(N * b * b), np.zeros(max(ncrs, 1) * b * b)
+    force, r, fl = np.zeros(N * b), np.zeros(N * b), np.zeros(N * b, np.int32)
+    nrm = C.c_double()
+    elem = np.ascontiguousarray(mesh.elem, np.int32)
+    bnd = np.ascontiguousarray(mesh.bnd, np.int32)
+    rc = lib().dfm_ref_newmark(scheme, N, _d(np.ascontiguousarray(mesh.coord, np.float64)), elem.shape[0], _i(elem),
+                               bnd.shape[0], _i(bnd), _d(np.ascontiguousarray(params, np.float64)), dt, gamma, beta,
+                               _d(u), _d(v), _d(a), _d(x), _d(bd), _d(bo), _d(force), _i(fl), _d(r), C.byref(nrm))
+    if rc:
+        raise RuntimeError(f"dfm_ref_newmark failed ({rc})")
+    return dict(bdiag=bd, boff=bo[: ncrs * b * b], force=force, flags=fl, r=r, norm=nrm.value, u=u, v=v, a=a, x=x)

@@ -74,7 +74,7 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -93,7 +93,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -117,7 +117,7 @@ def test_pcg_matches_oracle(ctx, name, sweep):
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1", "helmholtz_bands"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
-@pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8, 9])
 def test_range_sweep_cta_counts(ctx, name, ctas, mode):
     """Modes 3-8 with every CTA count: same result as the oracle's sweeps."""
     from delfem_b200 import lib

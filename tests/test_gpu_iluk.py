@@ -54,7 +54,7 @@ def test_iluk_pattern_levels_and_factor(ctx, name, lev):
 
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_iluk_apply_every_schedule(ctx, name, sweep):
     S = SYSTEMS[name]()
     A, M = _setup(ctx, S, 1)

@@ -45,7 +45,7 @@ REAL_SYSTEMS = {
 
 
 @pytest.mark.parametrize("name", list(REAL_SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_pbicgstab_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = REAL_SYSTEMS[name]()
@@ -97,7 +97,7 @@ def test_pbicgstab_host_entry(ctx):
 
 
 PCOCG_CASES = [(40, "rings", sw) for sw in (1, 2, 3)] + [(60, "rings", sw) for sw in (1, 2)] + \
-    [(60, "bands", sw) for sw in range(1, 9)]
+    [(60, "bands", sw) for sw in range(1, 10)]
 
 
 @pytest.mark.parametrize("nring,numbering,sweep", PCOCG_CASES)

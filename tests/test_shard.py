@@ -94,3 +94,53 @@ def test_sharded_solve_gathers_in_order_over_two_gloo_ranks(tmp_path):
         ns, fd, fo = S.ilu0()
         o = S.solve(fd, fo, tol=1e-10, maxit=1000)
         assert got[k, 2] == o["iters"] and got[k, 3] == o["x"].max()
+
+
+def _timed_worker(rank, world, port, sizes, out_path):
+    import datetime
+    import time as _t
+
+    import torch.distributed as dist
+
+    from delfem_b200 import meshes
+    from oracle import port as P
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+
+    def solve_local(idx):
+        t0 = _t.perf_counter()
+        res = []
+        for k in idx:
+            m = meshes.unit_square_tri(int(sizes[k]))
+            S = P.System(*P.pattern(m.nnode, m.elem), 1)
+            S.asm_poisson(m, 1.0, 1.0)
+            S.apply_bc(P.bc_flags_from_bnd(m.nnode, 1, m.bnd))
+            ns, fd, fo = S.ilu0()
+            o = S.solve(fd, fo, tol=1e-10, maxit=1000)
+            res.append((rank, o["iters"]))
+        return _t.perf_counter() - t0 + 0.01 * (rank + 1), res  # a rank-dependent time to check the max
+
+    out = shard.timed_sharded([(n + 1) ** 2 for n in sizes], solve_local)
+    if rank == 0:
+        np.save(out_path, np.array([out["seconds"], *out["per_rank_seconds"], *out["per_rank_instances"]] +
+                                   [v for r in out["results"] for v in r], dtype=np.float64))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_timed_sharded_max_over_two_gloo_ranks(tmp_path):
+    """The bench's sharded batch (bench.py at --gpus N): per-rank shares, the
+    job time as the max over ranks, per-instance results gathered in order."""
+    sizes = [10, 3, 14, 6, 8]
+    out_path = str(tmp_path / "t.npy")
+    mp.spawn(_timed_worker, args=(2, _free_port(), sizes, out_path), nprocs=2, join=True)
+    v = np.load(out_path)
+    t_max, t0, t1, n0, n1 = v[:5]
+    assert t_max == max(t0, t1) and t1 >= 0.02
+    parts = shard.partition([(n + 1) ** 2 for n in sizes], 2)
+    assert (n0, n1) == (len(parts[0]), len(parts[1])) and n0 + n1 == len(sizes)
+    res = v[5:].reshape(-1, 2)
+    for r, p in enumerate(parts):
+        assert all(int(res[k, 0]) == r for k in p)
+    assert all(res[:, 1] > 0)
