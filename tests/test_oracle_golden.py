@@ -13,7 +13,7 @@ from oracle import port as P
 
 _ALL = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 ILUK = [p for p in _ALL if os.path.basename(p).startswith("iluk")]
-GOLDEN = [p for p in _ALL if p not in ILUK and not os.path.basename(p).startswith(("zmatref", "gidref"))]
+GOLDEN = [p for p in _ALL if p not in ILUK and not os.path.basename(p).startswith(("zmatref", "gidref", "reference_solutions"))]
 METHOD = {0: "pcg", 1: "pbicgstab", 2: "pcocg"}
 POISSON2D, SOLID2D, SOLID3D, HELMHOLTZ2D = 1, 2, 3, 4
 
