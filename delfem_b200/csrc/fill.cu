@@ -116,7 +116,9 @@ int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out) {
   if (!A || !out || lev < -1) return DFM_ERR_INVALID;
   *out = nullptr;
   if (lev == 0) return dfm_ilu_create(A, out);
-  if (A->vt != DFM_REAL) return DFM_ERR_UNSUPPORTED;  // CZPreconditioner_ILU is ILU(0) here
+  // complex matrices: CZPreconditioner_ILU::SetFillInLevel, whose fill pattern
+  // (CZMatDiaFrac_BlkCrs::AddFracPtn, src/matvec/zmatdiafrac_blkcrs.cpp:263-441)
+  // is the real one's
   std::vector<unsigned> frp, fci;
   int rc = ilu_fill_pattern(A->N, A->h_rowptr, A->h_colind, lev, frp, fci);
   if (rc) return rc;

@@ -7,7 +7,8 @@
 //
 // The dot product is deterministic: a fixed grid of blocks writes one partial
 // each (fixed order inside a block), one warp sums the partials in order.
-// Elementwise operations are streaming, one double per thread per step.
+// Elementwise operations are streaming, one double per thread per step, and
+// bit-identical to the reference's loops.
 #include <algorithm>
 
 #include "dfm_internal.h"
@@ -36,15 +37,16 @@ __global__ void k_vec_dot_final(const double* part, int np, double* out) {
   if (threadIdx.x == 0) *out = s;
 }
 
-// y += alpha x   (CVector_Blk::AXPY)
+// y += alpha x   (CVector_Blk::AXPY: the product rounded, then the sum - no
+// fused multiply-add, as the reference computes it)
 __global__ void __launch_bounds__(kVecOpThreads)
 k_vec_axpy(size_t n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
-  VEC_LOOP(k, n) y[k] += alpha * x[k];
+  VEC_LOOP(k, n) y[k] = __dadd_rn(y[k], __dmul_rn(alpha, x[k]));
 }
 
 // x *= alpha   (CVector_Blk::operator*=: a product, so NaN * 0 stays NaN)
 __global__ void __launch_bounds__(kVecOpThreads) k_vec_scal(size_t n, double alpha, double* __restrict__ x) {
-  VEC_LOOP(k, n) x[k] *= alpha;
+  VEC_LOOP(k, n) x[k] = __dmul_rn(x[k], alpha);
 }
 
 }  // namespace dfm

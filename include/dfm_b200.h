@@ -263,8 +263,11 @@ DFM_API int dfm_ilu_create(dfm_mat A, dfm_ilu* out);
  * entries of CMatDiaFrac_BlkCrs::AddFracPtn (src/matvec/matdiafrac_blkcrs.cpp:
  * 1249-1377) up to level lev (-1: no limit), identical to the reference's;
  * dfm_ilu_factor then starts from A's values in it (SetValue_Initialize) and
- * factors over it.  lev = 0 is dfm_ilu_create.  Real matrices only; batches
- * (dfm_batch_create) take ILU(0) objects only. */
+ * factors over it.  lev = 0 is dfm_ilu_create.  Complex matrices too
+ * (CZPreconditioner_ILU::SetFillInLevel, include/delfem/femls/zpreconditioner.h:75,
+ * whose CZMatDiaFrac_BlkCrs::AddFracPtn, src/matvec/zmatdiafrac_blkcrs.cpp:
+ * 263-441, fills as the real one does).  Batches (dfm_batch_create) take
+ * ILU(0) objects only. */
 DFM_API int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out);
 /* The factor's pattern (host arrays, nullable): rowptr[N+1], colind[*ncrs];
  * the off-diagonal values of dfm_ilu_get_values/set_values follow it. */

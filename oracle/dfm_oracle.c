@@ -957,9 +957,10 @@ static void zaxpy(unsigned n, zc alpha, const double* x, double* y) {
   for (unsigned i = 0; i < n; i++) zst(y + 2 * i, zadd(zld(y + 2 * i), zmul(alpha, zld(x + 2 * i))));
 }
 
-int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const unsigned* diaind,
-              const double* diag, const double* off, const double* fdiag, const double* foff,
-              double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv) {
+int dfo_pcocg_fill(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                   const double* off, const unsigned* frowptr, const unsigned* fcolind, const unsigned* fdiaind,
+                   const double* fdiag, const double* foff, double* r, double* x, double tol, unsigned maxit,
+                   unsigned* iters, double* conv) {
   const size_t n2 = 2 * (size_t)N;
   double* p = (double*)calloc(n2 ? n2 : 1, sizeof(double));
   double* Ap = (double*)calloc(n2 ? n2 : 1, sizeof(double));
@@ -973,7 +974,7 @@ int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const 
   }
   const double inv0 = 1.0 / sq0;
   memcpy(w, r, n2 * sizeof(double));
-  dfo_zfwdbwd(N, rowptr, colind, diaind, fdiag, foff, w);
+  dfo_zfwdbwd(N, frowptr, fcolind, fdiaind, fdiag, foff, w);
   memcpy(p, w, n2 * sizeof(double));
   zc rw = zdot(N, r, w);
   *iters = maxit;
@@ -992,7 +993,7 @@ int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const 
       return 1;
     }
     memcpy(w, r, n2 * sizeof(double));
-    dfo_zfwdbwd(N, rowptr, colind, diaind, fdiag, foff, w);
+    dfo_zfwdbwd(N, frowptr, fcolind, fdiaind, fdiag, foff, w);
     const zc rw2 = zdot(N, r, w);
     const zc beta = zdiv(rw2, rw);
     rw = rw2;
@@ -1003,6 +1004,13 @@ int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const 
   *conv = tol; /* max_iter reached: conv_ratio keeps its input (the tolerance) */
   free(p); free(Ap); free(w);
   return 1; /* and Solve_PCOCG returns true (src/femls/zsolver_ls_iter.cpp:213-266) */
+}
+
+int dfo_pcocg(unsigned N, const unsigned* rowptr, const unsigned* colind, const unsigned* diaind,
+              const double* diag, const double* off, const double* fdiag, const double* foff,
+              double* r, double* x, double tol, unsigned maxit, unsigned* iters, double* conv) {
+  return dfo_pcocg_fill(N, rowptr, colind, diag, off, rowptr, colind, diaind, fdiag, foff, r, x, tol, maxit, iters,
+                        conv);
 }
 
 /* ------------------------------------------------ stored-matrix Newmark systems */
@@ -1088,6 +1096,25 @@ void dfo_newmark_update(size_t n, int scheme, double dt, double gamma, double be
         x[k] = acc0;
       }
       a[k] = x[k];
+    }
+  }
+}
+
+/* ------------------------------------------------ complex ILU(k) */
+
+/* CZMatDiaFrac_BlkCrs::SetValue_Initialize over a filled pattern (complex
+   scalars as (re, im) pairs): A's entries at their slots, zero elsewhere. */
+void dfo_ziluk_init(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                    const double* off, const unsigned* frowptr, const unsigned* fcolind, double* fdiag,
+                    double* foff) {
+  memcpy(fdiag, diag, sizeof(double) * 2 * N);
+  memset(foff, 0, sizeof(double) * 2 * frowptr[N]);
+  for (unsigned i = 0; i < N; i++) {
+    unsigned t = frowptr[i];
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) {
+      while (fcolind[t] != colind[s]) t++; /* A's row is a sorted subset of the factor's */
+      foff[2 * (size_t)t] = off[2 * (size_t)s];
+      foff[2 * (size_t)t + 1] = off[2 * (size_t)s + 1];
     }
   }
 }

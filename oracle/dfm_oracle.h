@@ -140,6 +140,16 @@ void dfo_newmark_residual(unsigned N, unsigned b, const unsigned* rowptr, const 
 void dfo_newmark_update(size_t n, int scheme, double dt, double gamma, double beta, const int* flags, double* x,
                         double* u, double* v, double* a);
 
+/* Complex ILU(k): SetValue_Initialize over the filled pattern, and
+   Fem::Ls::Solve_PCOCG with a factor in its own pattern. */
+void dfo_ziluk_init(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                    const double* off, const unsigned* frowptr, const unsigned* fcolind, double* fdiag,
+                    double* foff);
+int dfo_pcocg_fill(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                   const double* off, const unsigned* frowptr, const unsigned* fcolind, const unsigned* fdiaind,
+                   const double* fdiag, const double* foff, double* r, double* x, double tol, unsigned maxit,
+                   unsigned* iters, double* conv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,8 @@ def lib():
         L.dfo_pcg_fill.argtypes = [U, U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp, dp]
         L.dfo_pbicgstab.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_cg.argtypes = [U, U, up, up, dp, dp, dp, dp, D, U, up, dp]
+        L.dfo_ziluk_init.argtypes = [U, up, up, dp, dp, up, up, dp, dp]
+        L.dfo_pcocg_fill.argtypes = [U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_mat_zero_rows.argtypes = [U, U, up, ip, dp, dp]
         L.dfo_newmark_residual.argtypes = [U, U, up, up, dp, dp, C.c_int, D, D, D, dp, dp, dp, dp, ip, dp, dp, dp]
         L.dfo_newmark_update.argtypes = [C.c_size_t, C.c_int, D, D, D, ip, dp, dp, dp, dp]
@@ -215,9 +217,16 @@ class System:
     def iluk(self, lev_fill):
         """ILU(lev_fill): fill pattern, SetValue_Initialize, DoILUDecomp on it.
         Returns (ns, fpat, fd, fo) with fpat = (frowptr, fcolind, fdiaind)."""
-        assert not self.cplx
         fr, fc, _ = iluk_pattern(self.rowptr, self.colind, lev_fill)
         fdia = diaind(fr, fc)
+        if self.cplx:  # CZMatDiaFrac_BlkCrs(lev, A): the same fill pattern, complex values
+            fd = np.zeros_like(self.diag)
+            fo = np.zeros(max(fc.size, 1) * 2)
+            fcz = fc if fc.size else np.zeros(1, np.uint32)
+            lib().dfo_ziluk_init(self.N, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off), _u(fr),
+                                 _u(fcz), _d(fd), _d(fo))
+            ns = lib().dfo_zilu0(self.N, _u(fr), _u(fcz), _u(fdia), _d(fd), _d(fo))
+            return int(ns), (fr, fc, fdia), fd, fo[: fc.size * 2]
         fd = np.zeros_like(self.diag)
         fo = np.zeros(max(fc.size, 1) * self.b * self.b)
         fcz = fc if fc.size else np.zeros(1, np.uint32)
@@ -227,12 +236,18 @@ class System:
         return int(ns), (fr, fc, fdia), fd, fo[: fc.size * self.b * self.b]
 
     def solve_fill(self, fpat, fd, fo, rhs=None, tol=1e-10, maxit=10000):
-        """Solve_PCG with a factor in its own pattern fpat = (frowptr, fcolind, fdiaind)."""
+        """Solve_PCG (Solve_PCOCG for complex systems) with a factor in its own
+        pattern fpat = (frowptr, fcolind, fdiaind)."""
         fr, fc, fdia = fpat
         r = np.array(self.rhs if rhs is None else rhs, dtype=np.float64, copy=True)
         x = np.zeros_like(r)
         it, conv = C.c_uint(), C.c_double()
         fcz = fc if fc.size else np.zeros(1, np.uint32)
+        if self.cplx:
+            ok = lib().dfo_pcocg_fill(self.N, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off), _u(fr),
+                                      _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(r), _d(x), tol, maxit, C.byref(it),
+                                      C.byref(conv))
+            return dict(ok=bool(ok), x=x, iters=it.value, conv=conv.value, r=r)
         ok = lib().dfo_pcg_fill(self.N, self.b, _u(self.rowptr), _u(self._ci), _d(self.diag), _dz(self.off),
                                 _u(fr), _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(r), _d(x), tol, maxit,
                                 C.byref(it), C.byref(conv), None)
@@ -255,6 +270,18 @@ class System:
     def bwd(self, fo, v):
         v = np.array(v, dtype=np.float64, copy=True)
         lib().dfo_bwd(self.N, self.b, _u(self.rowptr), _u(self._ci), _u(self.dia), _dz(fo), _d(v))
+        return v
+
+    def precond_fill(self, fpat, fd, fo, v):
+        """The ILU(k) preconditioner with a factor in its own pattern."""
+        fr, fc, fdia = fpat
+        fcz = fc if fc.size else np.zeros(1, np.uint32)
+        v = np.array(v, dtype=np.float64, copy=True)
+        if self.cplx:
+            lib().dfo_zfwdbwd(self.N, _u(fr), _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(v))
+            return v
+        lib().dfo_fwd(self.N, self.b, _u(fr), _u(fcz), _u(fdia), _d(fd), _dz(fo), _d(v))
+        lib().dfo_bwd(self.N, self.b, _u(fr), _u(fcz), _u(fdia), _dz(fo), _d(v))
         return v
 
     def precond(self, fd, fo, v):

@@ -871,4 +871,49 @@ int dfm_ref_newmark(int scheme, int nnode, const double* coord, int nelem, const
   return 0;
 }
 
+
+// CZMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp
+// (src/matvec/zmatdiafrac_blkcrs.cpp:77-107, :263-441): the complex ILU(k)
+// pattern and factor, as dfm_ref_mat_iluk for real matrices.
+int dfm_ref_zmat_iluk(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                      const double* off, int lev, unsigned cap, unsigned* frowptr, unsigned* fcolind, double* fdiag,
+                      double* foff, unsigned* fncrs) {
+  Quiet q;
+  MatVec::CZMatDia_BlkCrs* m = make_zmat(N, rowptr, colind, diag, off);
+  MatVec::CZMatDiaFrac_BlkCrs f(lev, *m);
+  *fncrs = f.NCrs();
+  if (!frowptr || f.NCrs() > cap) {
+    delete m;
+    return 2;
+  }
+  frowptr[0] = 0;
+  for (unsigned i = 0; i < N; i++) {
+    unsigned n = 0;
+    const unsigned* c = f.GetPtrIndPSuP(i, n);
+    if (n) std::memcpy(fcolind + frowptr[i], c, sizeof(unsigned) * n);
+    frowptr[i + 1] = frowptr[i] + n;
+  }
+  f.SetValue_Initialize(*m);
+  f.DoILUDecomp();
+  read_zmat(f, fdiag, foff);
+  delete m;
+  return 0;
+}
+
+// The field-level system's preconditioner at fill level lev
+// (CPreconditioner_ILU / CZPreconditioner_ILU SetFillInLevel + SetLinearSystem);
+// the next dfm_ref_ilu factors it.
+int dfm_ref_set_fill(dfm_ref_sys* s, int lev) {
+  Quiet q;
+  if (s->complex_kind()) {
+    s->zprec.SetFillInLevel((unsigned)lev);
+    s->zprec.SetLinearSystem(s->zls);
+  } else {
+    s->prec.Clear();
+    s->prec.SetFillInLevel(lev);
+    s->prec.SetLinearSystem(s->ls.m_ls);
+  }
+  return 0;
+}
+
 }  // extern "C"

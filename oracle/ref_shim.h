@@ -128,6 +128,15 @@ int dfm_ref_newmark(int scheme, int nnode, const double* coord, int nelem, const
                     double* a, double* x, double* bdiag, double* boff, double* force, int* flags, double* r,
                     double* norm);
 
+/* Complex ILU(k): CZMatDiaFrac_BlkCrs(lev, A) pattern and factor (as
+ * dfm_ref_mat_iluk). */
+int dfm_ref_zmat_iluk(unsigned N, const unsigned* rowptr, const unsigned* colind, const double* diag,
+                      const double* off, int lev, unsigned cap, unsigned* frowptr, unsigned* fcolind, double* fdiag,
+                      double* foff, unsigned* fncrs);
+/* The field-level system's preconditioner at fill level lev (SetFillInLevel +
+ * SetLinearSystem); factored by the next dfm_ref_ilu. */
+int dfm_ref_set_fill(dfm_ref_sys* s, int lev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,8 @@ def lib():
         L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
+        L.dfm_ref_zmat_iluk.argtypes = [C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
+        L.dfm_ref_set_fill.argtypes = [P, C.c_int]
         L.dfm_ref_newmark.argtypes = [C.c_int, C.c_int, dp, C.c_int, ip, C.c_int, ip, dp, C.c_double, C.c_double,
                                       C.c_double, dp, dp, dp, dp, dp, dp, dp, ip, dp, dp]
         _lib = L
@@ -139,6 +141,10 @@ class RefSystem:
         f = np.zeros(self.N * self.b, np.int32)
         lib().dfm_ref_get_bcflag(self.h, _i(f))
         return f
+
+    def set_fill(self, lev):
+        """SetFillInLevel(lev) + SetLinearSystem of the system's preconditioner."""
+        lib().dfm_ref_set_fill(self.h, int(lev))
 
     def ilu(self):
         sec = C.c_double()
@@ -283,3 +289,19 @@ def newmark(scheme, mesh, params, dt, gamma, beta, u, v, a, x, ncrs):
     if rc:
         raise RuntimeError(f"dfm_ref_newmark failed ({rc})")
     return dict(bdiag=bd, boff=bo[: ncrs * b * b], force=force, flags=fl, r=r, norm=nrm.value, u=u, v=v, a=a, x=x)
+
+
+def zmat_iluk(N, rowptr, colind, diag, off, lev):
+    """CZMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp:
+    (rc, frowptr, fcolind, fdiag, foff), complex values interleaved."""
+    n = C.c_uint()
+    o = off if off.size else np.zeros(2)
+    ci = colind if colind.size else np.zeros(1, np.uint32)
+    lib().dfm_ref_zmat_iluk(N, _u(rowptr), _u(ci), _d(diag), _d(o), lev, 0, None, None, None, None, C.byref(n))
+    fr = np.zeros(N + 1, np.uint32)
+    fc = np.zeros(max(n.value, 1), np.uint32)
+    fd = np.zeros(2 * N)
+    fo = np.zeros(max(n.value, 1) * 2)
+    rc = lib().dfm_ref_zmat_iluk(N, _u(rowptr), _u(ci), _d(diag), _d(o), lev, n.value, _u(fr), _u(fc), _d(fd),
+                                 _d(fo), C.byref(n))
+    return rc, fr, fc[: n.value], fd, fo[: 2 * n.value]

@@ -138,13 +138,9 @@ def test_iluk_mixed_and_bicgstab(ctx):
 
 
 def test_iluk_limits(ctx):
-    """Complex systems and batches take ILU(0) only; lev < -1 is rejected; a
-    solve with another matrix than the preconditioner's is rejected."""
+    """lev < -1 is rejected; a solve with another matrix than the
+    preconditioner's is rejected."""
     from delfem_b200 import lib
-    Z = cases.helmholtz(6)[1]
-    AZ = lib.Matrix(ctx, Z.rowptr, Z.colind, 1, lib.COMPLEX)
-    with pytest.raises(lib.DfmError):
-        lib.ILU(AZ, fill_level=1)
     S = SYSTEMS["poisson16"]()
     A, M = _setup(ctx, S, 1)
     with pytest.raises(lib.DfmError):
@@ -156,3 +152,36 @@ def test_iluk_limits(ctx):
     x = torch.zeros_like(r)
     with pytest.raises(lib.DfmError):
         lib.solve_pcg(B, M, r, x, tol=1e-10, maxit=100, allow=(lib.OK,))
+
+
+@pytest.mark.parametrize("nring,lev", [(16, 1), (40, 1), (24, 2)])
+def test_complex_iluk_factor_and_cocg(ctx, nring, lev):
+    """CZPreconditioner_ILU::SetFillInLevel(lev) on the device: the fill pattern
+    and the complex factor bit-identical to the oracle (pinned to the
+    reference's CZMatDiaFrac_BlkCrs), the preconditioner to 1e-11 in the range
+    schedules, and ILU(k)-COCG to 1e-8 of the oracle's x."""
+    from delfem_b200 import lib
+    m, Z = cases.helmholtz(nring)
+    A = lib.Matrix(ctx, Z.rowptr, Z.colind, 1, lib.COMPLEX)
+    A.set_values(Z.diag, Z.off)
+    M = lib.ILU(A, fill_level=lev)
+    M.factor()
+    ns, (fr, fc, fdia), fd, fo = Z.iluk(lev)
+    grp, gci = M.pattern()
+    assert np.array_equal(grp, fr) and np.array_equal(gci, fc)
+    gd, go = M.get_values()
+    assert np.array_equal(gd, fd) and np.array_equal(go, fo)
+    rng = np.random.default_rng(3)
+    rv = rng.standard_normal(2 * Z.N)
+    ref = Z.precond_fill((fr, fc, fdia), fd, fo, rv)
+    for sweep in (1, 2, 3, 9):
+        M.sweep = sweep
+        z = torch.zeros(2 * Z.N, dtype=torch.float64, device="cuda")
+        M.apply(_dev(rv), z)
+        assert np.allclose(z.cpu().numpy(), ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max()), sweep
+    o = Z.solve_fill((fr, fc, fdia), fd, fo, tol=1e-10, maxit=3000)
+    r = _dev(Z.rhs)
+    x = torch.zeros_like(r)
+    rc, it, conv = lib.solve_pcocg(A, M, r, x, tol=1e-10, maxit=3000)
+    assert rc == lib.OK and o["ok"]
+    assert np.linalg.norm(x.cpu().numpy() - o["x"]) <= 1e-8 * np.linalg.norm(o["x"])

@@ -124,3 +124,34 @@ def test_cg_pinned_to_reference(name, maxit):
     assert it == o["iters"] and _eq(conv, o["conv"]) and _eq(x, o["x"])
     if maxit == 7:
         assert it == 7 and conv == 1e-10
+
+
+@pytest.mark.parametrize("nring,lev", [(16, 1), (16, 2), (40, 1), (24, -1)])
+def test_complex_iluk_pinned_to_reference(nring, lev):
+    """CZMatDiaFrac_BlkCrs(lev, A) (the fill path of CZPreconditioner_ILU::
+    SetFillInLevel, src/matvec/zmatdiafrac_blkcrs.cpp:77-107, :263-441):
+    pattern and factor of the oracle bit-identical to the reference's."""
+    m, S = cases.helmholtz(nring)
+    rc, fr, fc, fd, fo = R.zmat_iluk(S.N, S.rowptr, S.colind, S.diag, S.off, lev)
+    ns, (pr, pc, pdia), od, oo = S.iluk(lev)
+    assert np.array_equal(fr, pr) and np.array_equal(fc, pc)
+    assert fc.size > S.colind.size  # fill entries exist
+    assert _eq(fd, od) and _eq(fo, oo)
+
+
+def test_complex_ilu1_cocg_pinned_to_reference():
+    """The reference's Helmholtz demo runs CZPreconditioner_ILU with fill level
+    1 (test_glut/helmholtz2d/main.cpp:87): its field-level ILU(1) + Solve_PCOCG
+    against the oracle's, x, iteration count and ratio bit-identical."""
+    m = meshes.unit_disk_tri(40)
+    ref = R.RefSystem(R.HELMHOLTZ2D, m)
+    ref.assemble([cases.WAVE_LENGTH], None, meshes.gaussian_source_load(m))
+    ref.set_fill(1)
+    ref.ilu()
+    rc, x, it, conv, _ = ref.solve(R.PCOCG, 1e-10, 3000)
+    m2, S = cases.helmholtz(40)
+    ns, fpat, fd, fo = S.iluk(1)
+    o = S.solve_fill(fpat, fd, fo, tol=1e-10, maxit=3000)
+    assert rc == 0 and o["ok"]
+    assert it == o["iters"] and _eq(conv, o["conv"]) and _eq(x, o["x"])
+    assert fpat[1].size > S.colind.size  # a filled factor, not ILU(0)
