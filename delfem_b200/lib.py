@@ -62,6 +62,10 @@ PROTOS = {
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
     "dfm_mat_zero_rows": (_i, [_vp, _vp]),
+    "dfm_rmat_create": (_i, [_vp, _u, _u, _u, _u, _up, _up, C.POINTER(_vp)]),
+    "dfm_rmat_destroy": (_i, [_vp]),
+    "dfm_rmat_set_values": (_i, [_vp, _vp, _i]),
+    "dfm_rmat_spmv": (_i, [_vp, _d, _vp, _d, _vp]),
     "dfm_newmark_residual": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dp]),
     "dfm_newmark_update": (_i, [_vp, C.c_size_t, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp]),
     "dfm_boundary_matrix": (_i, [_u, _u, _up, _up, _dp, _dp, _ip, _up, _up, _dp, _dp, _up]),
@@ -603,6 +607,40 @@ def solve_pcg(A: Matrix, M: ILU, r, x, tol=1e-10, maxit=10000, allow=(OK, NOT_CO
     rc = lib().dfm_solve_pcg(A.h, M.h, _ptr(r), _ptr(x), tol, maxit, C.byref(it), C.byref(conv))
     check(rc, "dfm_solve_pcg", allow)
     return rc, it.value, conv.value
+
+
+class RMatrix:
+    """A rectangular block-CRS matrix on the device (CMat_BlkCrs: a coupling
+    of two segments), nrow x ncol blocks of brow x bcol."""
+
+    def __init__(self, ctx: Context, nrow, ncol, brow, bcol, rowptr, colind):
+        self.ctx = ctx
+        rp = np.ascontiguousarray(rowptr, np.uint32)
+        ci = np.ascontiguousarray(colind, np.uint32) if len(colind) else np.zeros(1, np.uint32)
+        h = C.c_void_p()
+        check(lib().dfm_rmat_create(ctx.h, int(nrow), int(ncol), int(brow), int(bcol), rp.ctypes.data_as(_up),
+                                    ci.ctypes.data_as(_up), C.byref(h)), "dfm_rmat_create")
+        self.h = h
+        self.nrow, self.ncol, self.brow, self.bcol = int(nrow), int(ncol), int(brow), int(bcol)
+
+    def set_values(self, val):
+        v = np.ascontiguousarray(val, np.float64)
+        check(lib().dfm_rmat_set_values(self.h, v.ctypes.data_as(C.c_void_p), HOST), "dfm_rmat_set_values")
+
+    def spmv(self, alpha, x, beta, y):
+        _sync_torch()
+        check(lib().dfm_rmat_spmv(self.h, alpha, _ptr(x), beta, _ptr(y)), "dfm_rmat_spmv")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfm_rmat_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def mat_zero_rows(B: Matrix, flags):

@@ -59,6 +59,7 @@ typedef struct dfm_mat_s* dfm_mat;
 typedef struct dfm_ilu_s* dfm_ilu;
 typedef struct dfm_mesh_s* dfm_mesh;
 typedef struct dfm_batch_s* dfm_batch;
+typedef struct dfm_rmat_s* dfm_rmat;
 
 DFM_API const char* dfm_status_string(int status);
 DFM_API int dfm_abi_version(void);
@@ -135,6 +136,21 @@ DFM_API int dfm_spmv(dfm_mat A, double alpha, const double* x, double beta, doub
  * launches of y = A x (the tuned kernel) on the context's stream between one
  * pair of CUDA events, after one untimed launch; *ms = average per launch. */
 DFM_API int dfm_time_spmv(dfm_mat A, const double* x, double* y, int reps, float* ms);
+
+/* ---- rectangular block matrices: CMat_BlkCrs (segment couplings) -------- */
+/* MatVec::CMat_BlkCrs (include/delfem/matvec/mat_blkcrs.h:44-190), the
+ * coupling of two segments of a linear system (CLinearSystem::GetMatrix(i, j),
+ * i != j): nrow x ncol blocks of brow x bcol values (1..3 each), every block
+ * in the CRS list, row-major blocks; pattern from host arrays (rowptr[nrow+1],
+ * colind ascending per row, no repeats; validated). */
+DFM_API int dfm_rmat_create(dfm_ctx ctx, unsigned nrow, unsigned ncol, unsigned brow, unsigned bcol,
+                            const unsigned* rowptr, const unsigned* colind, dfm_rmat* out);
+DFM_API int dfm_rmat_destroy(dfm_rmat R);
+/* val[nnz*brow*bcol] at DFM_HOST or DFM_DEVICE. */
+DFM_API int dfm_rmat_set_values(dfm_rmat R, const double* val, int where);
+/* y (nrow*brow) = beta y + alpha R x (x: ncol*bcol), CMat_BlkCrs::MatVec
+ * (src/matvec/mat_blkcrs.cpp:955-1175); beta == 0 writes y without reading it. */
+DFM_API int dfm_rmat_spmv(dfm_rmat R, double alpha, const double* x, double beta, double* y);
 
 /* Reads a complex matrix with scalar blocks from the reference's text format
  * (CZMatDia_BlkCrs(const std::string& file_path), src/matvec/zmatdia_blkcrs.cpp:

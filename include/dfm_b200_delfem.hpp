@@ -42,18 +42,22 @@
 // it too, one device operation per step; call SyncToHost() (or let lsp go out
 // of scope) before reading -1 / -2 on the host after such a solve.
 //
-// Scope: one linear-system segment with fixed b x b blocks, b in {1, 2, 3}
-// (the CMatDia_BlkCrs of a single field).  Errors other than the reference's
-// boolean results throw dfm_lsol::Error.
+// Scope: fixed b x b blocks, b in {1, 2, 3}, in one segment (the
+// CMatDia_BlkCrs of a single field) or in several (a combined field, bubble
+// DOFs: CLinearSystem::AddLinSysSeg with couplings GetMatrix(i, j)); several
+// segments are joined into one device matrix (detail::Layout) and take ILU(0).
+// Errors other than the reference's boolean results throw dfm_lsol::Error.
 #ifndef DFM_B200_DELFEM_HPP
 #define DFM_B200_DELFEM_HPP
 
+#include <algorithm>
 #include <memory>
 #include <vector>
 
 #include "delfem/ls/linearsystem.h"
 #include "delfem/ls/linearsystem_interface_solver.h"
 #include "delfem/ls/preconditioner.h"
+#include "delfem/matvec/mat_blkcrs.h"
 #include "delfem/matvec/matdia_blkcrs.h"
 #include "delfem/matvec/vector_blk.h"
 #include "dfm_b200.h"
@@ -67,16 +71,150 @@ using dfm_lsol::DeviceVector;
 using dfm_lsol::Error;
 
 namespace detail {
-// The single segment's matrix as the device library takes it.
-inline const MatVec::CMatDia_BlkCrs& segment_matrix(const LsSol::CLinearSystem& ls) {
-  if (ls.GetNLinSysSeg() != 1 || !ls.IsMatrix(0, 0)) throw Error(DFM_ERR_UNSUPPORTED, "one segment expected");
-  const MatVec::CMatDia_BlkCrs& m = ls.GetMatrix(0);
-  if (m.LenBlkCol() < 1 || m.LenBlkCol() > 3) throw Error(DFM_ERR_UNSUPPORTED, "block size");
-  return m;
-}
 // Contiguous values of a fixed-length CVector_Blk.
 inline double* values(MatVec::CVector_Blk& v) { return v.NBlk() ? v.GetValuePtr(0) : nullptr; }
 inline const double* values(const MatVec::CVector_Blk& v) { return v.NBlk() ? v.GetValuePtr(0) : nullptr; }
+
+// The segments of a CLinearSystem (src/ls/linearsystem.cpp: AddLinSysSeg,
+// AddMat_Dia, AddMat_NonDia) joined into one square matrix for the device:
+// segment i's rows follow segment i-1's, its diagonal matrix GetMatrix(i)
+// and its couplings GetMatrix(i, j) (CMat_BlkCrs, rows in segment i, columns
+// in segment j) become one block row each.  Segments of one block length b
+// keep b x b blocks; segments of different lengths are joined one row per
+// DOF (b = 1).  Either way the joined vector is the segments' vectors one
+// after the other, and the joined pattern is the union of the segments'
+// patterns, so ILU(0) of the joined matrix is the reference's segment-wise
+// block ILU(0) (src/ls/preconditioner.cpp:57-335: the same incomplete
+// factorization on the same block pattern, summed in another order).
+struct Layout {
+  unsigned nseg = 0;
+  std::vector<unsigned> nblk, len;
+  std::vector<size_t> dof0;  // first joined vector entry of each segment
+  unsigned b = 1, N = 0;     // joined block size and block rows
+  bool scalar = false;       // segments of different lengths: one row per DOF
+  size_t ndof = 0;
+  std::vector<unsigned> rowptr, colind;
+
+  void build(const LsSol::CLinearSystem& ls) {
+    nseg = ls.GetNLinSysSeg();
+    if (nseg == 0) throw Error(DFM_ERR_INVALID, "a linear system without segments");
+    nblk.assign(nseg, 0);
+    len.assign(nseg, 0);
+    dof0.assign(nseg + 1, 0);
+    for (unsigned i = 0; i < nseg; i++) {
+      if (!ls.IsMatrix(i, i)) throw Error(DFM_ERR_UNSUPPORTED, "a segment without its diagonal matrix");
+      const MatVec::CMatDia_BlkCrs& m = ls.GetMatrix(i);
+      if (m.LenBlkCol() < 1 || m.LenBlkCol() > 3) throw Error(DFM_ERR_UNSUPPORTED, "block size");
+      nblk[i] = m.NBlkMatCol();
+      len[i] = (unsigned)m.LenBlkCol();
+      dof0[i + 1] = dof0[i] + (size_t)nblk[i] * len[i];
+    }
+    ndof = dof0[nseg];
+    scalar = false;
+    for (unsigned i = 1; i < nseg; i++) scalar |= len[i] != len[0];
+    b = scalar ? 1u : len[0];
+    N = (unsigned)(ndof / b);
+    std::vector<double> d, o;
+    walk(ls, false, d, o);
+  }
+
+  // pattern (always) and values (with_values) of the joined matrix, row by row
+  // in ascending columns
+  void walk(const LsSol::CLinearSystem& ls, bool with_values, std::vector<double>& diag, std::vector<double>& off) {
+    std::vector<unsigned>& rp = rowptr;
+    std::vector<unsigned>& ci = colind;
+    const size_t bb = (size_t)b * b;
+    if (!with_values) {
+      rp.assign(N + 1, 0);
+      ci.clear();
+    } else {
+      diag.assign((size_t)N * bb, 0.0);
+      off.assign(colind.size() * bb, 0.0);
+    }
+    size_t k = 0;  // off-diagonal slot
+    auto put = [&](unsigned col, const double* v) {
+      if (!with_values) ci.push_back(col);
+      else std::copy(v, v + bb, off.begin() + k * bb);
+      k++;
+    };
+    unsigned row = 0;
+    for (unsigned i = 0; i < nseg; i++) {
+      const MatVec::CMatDia_BlkCrs& A = ls.GetMatrix(i);
+      const unsigned Li = len[i];
+      for (unsigned p = 0; p < nblk[i]; p++) {
+        unsigned nd = 0, nv = 0;
+        const unsigned* dcol = A.GetPtrIndPSuP(p, nd);
+        const double* dval = A.GetPtrValPSuP(p, nv);
+        const double* dia = A.GetPtrValDia(p);
+        for (unsigned d = 0; d < (scalar ? Li : 1u); d++) {
+          // one joined row: block row p of segment i, or its DOF d
+          for (unsigned j = 0; j < nseg; j++) {
+            if (j == i) {
+              bool dia_done = false;
+              auto put_dia = [&]() {  // the rest of the diagonal block (scalar rows only)
+                for (unsigned e = 0; e < Li; e++)
+                  if (e != d) {
+                    double v = dia[d * Li + e];
+                    put((unsigned)(dof0[i] + (size_t)p * Li + e), &v);
+                  }
+                dia_done = true;
+              };
+              for (unsigned t = 0; t < nd; t++) {
+                const unsigned c = dcol[t];
+                if (scalar && !dia_done && c > p) put_dia();
+                if (!scalar) {
+                  put((unsigned)(dof0[i] / b + c), dval + (size_t)t * bb);
+                } else {
+                  for (unsigned e = 0; e < Li; e++) {
+                    double v = dval[(size_t)t * Li * Li + d * Li + e];
+                    put((unsigned)(dof0[i] + (size_t)c * Li + e), &v);
+                  }
+                }
+              }
+              if (scalar && !dia_done) put_dia();
+            } else if (ls.IsMatrix(i, j)) {
+              const MatVec::CMat_BlkCrs& C = ls.GetMatrix(i, j);
+              const unsigned Lj = len[j];
+              unsigned nc = 0, ncv = 0;
+              const unsigned* ccol = C.GetPtrIndPSuP(p, nc);
+              const double* cval = C.GetPtrValPSuP(p, ncv);
+              for (unsigned t = 0; t < nc; t++) {
+                if (!scalar) {
+                  put((unsigned)(dof0[j] / b + ccol[t]), cval + (size_t)t * bb);
+                } else {
+                  for (unsigned e = 0; e < Lj; e++) {
+                    double v = cval[(size_t)t * Li * Lj + d * Lj + e];
+                    put((unsigned)(dof0[j] + (size_t)ccol[t] * Lj + e), &v);
+                  }
+                }
+              }
+            }
+          }
+          if (with_values) {
+            if (!scalar) std::copy(dia, dia + bb, diag.begin() + (size_t)row * bb);
+            else diag[row] = dia[d * Li + d];
+          }
+          row++;
+          if (!with_values) rp[row] = (unsigned)k;
+        }
+      }
+    }
+  }
+
+  // the CLinearSystem's vector iv, segments one after the other
+  void gather(const LsSol::CLinearSystem& ls, int iv, double* out) const {
+    for (unsigned i = 0; i < nseg; i++) {
+      const double* v = values(ls.GetVector(iv, i));
+      if (v) std::copy(v, v + (dof0[i + 1] - dof0[i]), out + dof0[i]);
+    }
+  }
+  void scatter(LsSol::CLinearSystem& ls, int iv, const double* in) const {
+    for (unsigned i = 0; i < nseg; i++) {
+      double* v = values(ls.GetVector(iv, i));
+      if (v) std::copy(in + dof0[i], in + dof0[i + 1], v);
+    }
+  }
+};
 }  // namespace detail
 
 // LsSol::CPreconditioner_ILU on the device: ILU(0), or ILU(k) after
@@ -101,55 +239,59 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     tmp_r_.reset();
     tmp_z_.reset();
   }
-  // the fill-in level of the next SetLinearSystem (-1: no limit); one
-  // segment, so ilss0 must be -1 or 0
+  // the fill-in level of the next SetLinearSystem (-1: no limit); ilss0 must
+  // be -1 or 0, and systems of several segments take level 0 only
   void SetFillInLevel(int lev, int ilss0 = -1) {
     if (ilss0 != -1 && ilss0 != 0) throw Error(DFM_ERR_UNSUPPORTED, "SetFillInLevel");
     if (lev < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
     lev_ = lev;
   }
-  // pattern of the system matrix on the device, fill pattern and level sets
+  // pattern of the (joined) system matrix on the device, fill pattern and
+  // level sets
   void SetLinearSystem(const LsSol::CLinearSystem& ls) override {
     Clear();
-    const MatVec::CMatDia_BlkCrs& m = detail::segment_matrix(ls);
-    nblk_ = m.NBlkMatCol();
-    len_ = (unsigned)m.LenBlkCol();
-    std::vector<unsigned> rp(nblk_ + 1, 0), ci;
-    ci.reserve(m.NCrs());
-    for (unsigned i = 0; i < nblk_; i++) {
-      unsigned np = 0;
-      const unsigned* p = m.GetPtrIndPSuP(i, np);
-      rp[i + 1] = rp[i] + np;
-      ci.insert(ci.end(), p, p + np);
-    }
-    check(dfm_mat_create(ctx_->get(), nblk_, len_, DFM_REAL, rp.data(), ci.data(), &mat_), "SetLinearSystem");
+    lay_.build(ls);
+    if (lay_.nseg > 1 && lev_ != 0) throw Error(DFM_ERR_UNSUPPORTED, "fill-in across segments");
+    check(dfm_mat_create(ctx_->get(), lay_.N, lay_.b, DFM_REAL, lay_.rowptr.data(), lay_.colind.data(), &mat_),
+          "SetLinearSystem");
     check(dfm_ilu_create_fill(mat_, lev_, &ilu_), "SetLinearSystem");
   }
   // the system's current values to the device and the numeric factorisation;
   // false when more than 10 pivots were singular (the reference's result)
   bool SetValue(const LsSol::CLinearSystem& ls) override {
     if (!mat_) throw Error(DFM_ERR_INVALID, "SetValue before SetLinearSystem");
-    const MatVec::CMatDia_BlkCrs& m = detail::segment_matrix(ls);
-    if (m.NBlkMatCol() != nblk_ || (unsigned)m.LenBlkCol() != len_) throw Error(DFM_ERR_INVALID, "SetValue");
-    unsigned np = 0;
-    const double* off = m.NCrs() ? m.GetPtrValPSuP(0, np) : nullptr;  // row-ordered, contiguous
-    const double* dia = nblk_ ? m.GetPtrValDia(0) : nullptr;
-    check(dfm_mat_set_values(mat_, dia, off, DFM_HOST), "SetValue");
+    if (ls.GetNLinSysSeg() != lay_.nseg) throw Error(DFM_ERR_INVALID, "SetValue");
+    for (unsigned i = 0; i < lay_.nseg; i++)
+      if (ls.GetMatrix(i).NBlkMatCol() != lay_.nblk[i] || (unsigned)ls.GetMatrix(i).LenBlkCol() != lay_.len[i])
+        throw Error(DFM_ERR_INVALID, "SetValue");
+    if (lay_.nseg == 1) {  // one segment: the reference's arrays are the library's layout
+      const MatVec::CMatDia_BlkCrs& m = ls.GetMatrix(0);
+      unsigned np = 0;
+      const double* off = m.NCrs() ? m.GetPtrValPSuP(0, np) : nullptr;  // row-ordered, contiguous
+      const double* dia = lay_.N ? m.GetPtrValDia(0) : nullptr;
+      check(dfm_mat_set_values(mat_, dia, off, DFM_HOST), "SetValue");
+    } else {
+      std::vector<double> d, o;
+      lay_.walk(ls, true, d, o);
+      check(dfm_mat_set_values(mat_, d.data(), o.data(), DFM_HOST), "SetValue");
+    }
     unsigned ns = 0;
     return check(dfm_ilu_factor(ilu_, mat_, &ns), "SetValue", DFM_SINGULAR_PIVOT) == DFM_OK;
   }
-  // {iv} := (LU)^-1 {iv} on the CLinearSystem's host vector (copied to the
+  // {iv} := (LU)^-1 {iv} on the CLinearSystem's host vectors (copied to the
   // device and back); solvers over CLinearSystemGPU apply it on the device
   bool SolvePrecond(LsSol::CLinearSystem& ls, unsigned int iv) override {
-    MatVec::CVector_Blk& v = ls.GetVector((int)iv, 0);
     const size_t n = VectorSize();
     if (!tmp_r_) {
       tmp_r_.reset(new DeviceVector(*ctx_, n));
       tmp_z_.reset(new DeviceVector(*ctx_, n));
     }
-    tmp_r_->upload(detail::values(v));
+    std::vector<double> h(n);
+    lay_.gather(ls, (int)iv, h.data());
+    tmp_r_->upload(h.data());
     ApplyDevice(tmp_r_->data(), tmp_z_->data());
-    tmp_z_->download(detail::values(v));
+    tmp_z_->download(h.data());
+    lay_.scatter(ls, (int)iv, h.data());
     return true;
   }
   // z := (LU)^-1 r on device arrays (r != z)
@@ -158,14 +300,15 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   dfm_mat matrix() const { return mat_; }
   dfm_ilu ilu() const { return ilu_; }
   Context& context() const { return *ctx_; }
-  size_t VectorSize() const { return (size_t)nblk_ * len_; }
+  size_t VectorSize() const { return lay_.ndof; }
+  const detail::Layout& layout() const { return lay_; }
 
  private:
   Context* ctx_;
   dfm_mat mat_ = nullptr;
   dfm_ilu ilu_ = nullptr;
   int lev_ = 0;
-  unsigned nblk_ = 0, len_ = 1;
+  detail::Layout lay_;
   std::unique_ptr<DeviceVector> tmp_r_, tmp_z_;
 };
 
@@ -178,8 +321,11 @@ class CLinearSystemGPU : public LsSol::ILinearSystemPreconditioner_Sol, public L
   CLinearSystemGPU(LsSol::CLinearSystem& ls, CPreconditioner_ILU_GPU& prec)
       : ls_(&ls), prec_(&prec), n_(prec.VectorSize()), r_(prec.context(), n_), u_(prec.context(), n_) {
     if (!prec.matrix()) throw Error(DFM_ERR_INVALID, "preconditioner without SetLinearSystem");
-    const MatVec::CMatDia_BlkCrs& m = detail::segment_matrix(ls);
-    if ((size_t)m.NBlkMatCol() * (unsigned)m.LenBlkCol() != n_) throw Error(DFM_ERR_INVALID, "CLinearSystemGPU");
+    const detail::Layout& L = prec.layout();
+    if (ls.GetNLinSysSeg() != L.nseg) throw Error(DFM_ERR_INVALID, "CLinearSystemGPU");
+    for (unsigned i = 0; i < L.nseg; i++)
+      if ((size_t)ls.GetVector(-1, i).NBlk() * L.len[i] != L.dof0[i + 1] - L.dof0[i])
+        throw Error(DFM_ERR_INVALID, "CLinearSystemGPU");
     SyncFromHost();
   }
   ~CLinearSystemGPU() {
@@ -193,12 +339,18 @@ class CLinearSystemGPU : public LsSol::ILinearSystemPreconditioner_Sol, public L
 
   // the CLinearSystem's residual (-1) and update (-2) to / from the device
   void SyncFromHost() {
-    r_.upload(detail::values(ls_->GetVector(-1, 0)));
-    u_.upload(detail::values(ls_->GetVector(-2, 0)));
+    std::vector<double> h(n_);
+    prec_->layout().gather(*ls_, -1, h.data());
+    r_.upload(h.data());
+    prec_->layout().gather(*ls_, -2, h.data());
+    u_.upload(h.data());
   }
   void SyncToHost() {
-    r_.download(detail::values(ls_->GetVector(-1, 0)));
-    u_.download(detail::values(ls_->GetVector(-2, 0)));
+    std::vector<double> h(n_);
+    r_.download(h.data());
+    prec_->layout().scatter(*ls_, -1, h.data());
+    u_.download(h.data());
+    prec_->layout().scatter(*ls_, -2, h.data());
   }
 
   unsigned int GetTmpVectorArySize() const override { return (unsigned)tmp_.size(); }

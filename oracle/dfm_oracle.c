@@ -1118,3 +1118,35 @@ void dfo_ziluk_init(unsigned N, const unsigned* rowptr, const unsigned* colind, 
     }
   }
 }
+
+/* ------------------------------------------------ rectangular block matrices */
+
+/* CMat_BlkCrs::MatVec, not transposed (src/matvec/mat_blkcrs.cpp:955-1175):
+   per block row, y *= beta, then for every block and entry
+   y += alpha * m * x (left to right); 1 x 1 blocks with beta == 0 start
+   from y = 0 as the reference does. */
+void dfo_rmat_spmv(unsigned nrow, unsigned brow, unsigned bcol, const unsigned* rowptr, const unsigned* colind,
+                   const double* val, double alpha, const double* x, double beta, double* y) {
+  const unsigned bb = brow * bcol;
+  for (unsigned i = 0; i < nrow; i++) {
+    double* yi = y + (size_t)i * brow;
+    if (bb == 1 && beta == 0.0) yi[0] = 0.0;
+    else
+      for (unsigned r = 0; r < brow; r++) yi[r] *= beta;
+    for (unsigned s = rowptr[i]; s < rowptr[i + 1]; s++) {
+      const double* m = val + (size_t)s * bb;
+      const double* xj = x + (size_t)colind[s] * bcol;
+      if (brow == 1 && bcol > 1 && bcol <= 3) { /* the reference's unrolled 1 x 2 and 1 x 3 rows */
+        double t = m[0] * xj[0] + m[1] * xj[1];
+        if (bcol == 3) t = m[0] * xj[0] + m[1] * xj[1] + m[2] * xj[2];
+        yi[0] += alpha * t;
+      } else if (bcol == 1 && brow > 1 && brow <= 3) { /* 2 x 1 and 3 x 1: x scaled first */
+        const double ax = xj[0] * alpha;
+        for (unsigned r = 0; r < brow; r++) yi[r] += m[r] * ax;
+      } else {
+        for (unsigned r = 0; r < brow; r++)
+          for (unsigned c = 0; c < bcol; c++) yi[r] += alpha * m[r * bcol + c] * xj[c];
+      }
+    }
+  }
+}

@@ -150,6 +150,10 @@ int dfo_pcocg_fill(unsigned N, const unsigned* rowptr, const unsigned* colind, c
                    const double* fdiag, const double* foff, double* r, double* x, double tol, unsigned maxit,
                    unsigned* iters, double* conv);
 
+/* CMat_BlkCrs::MatVec (rectangular block-CRS, not transposed). */
+void dfo_rmat_spmv(unsigned nrow, unsigned brow, unsigned bcol, const unsigned* rowptr, const unsigned* colind,
+                   const double* val, double alpha, const double* x, double beta, double* y);
+
 #ifdef __cplusplus
 }
 #endif

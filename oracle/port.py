@@ -57,6 +57,7 @@ def lib():
         L.dfo_cg.argtypes = [U, U, up, up, dp, dp, dp, dp, D, U, up, dp]
         L.dfo_ziluk_init.argtypes = [U, up, up, dp, dp, up, up, dp, dp]
         L.dfo_pcocg_fill.argtypes = [U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp]
+        L.dfo_rmat_spmv.argtypes = [U, U, U, up, up, dp, D, dp, D, dp]
         L.dfo_mat_zero_rows.argtypes = [U, U, up, ip, dp, dp]
         L.dfo_newmark_residual.argtypes = [U, U, up, up, dp, dp, C.c_int, D, D, D, dp, dp, dp, dp, ip, dp, dp, dp]
         L.dfo_newmark_update.argtypes = [C.c_size_t, C.c_int, D, D, D, ip, dp, dp, dp, dp]
@@ -351,3 +352,13 @@ def newmark_update(scheme, dt, gamma, beta, flags, x, u, v, a=None):
     fl = np.ascontiguousarray(flags, np.int32)
     lib().dfo_newmark_update(u.size, scheme, dt, gamma, beta, fl.ctypes.data_as(ip), _d(x), _d(u), _d(v), _d(a))
     return x, u, v, a
+
+
+def rmat_spmv(nrow, brow, bcol, rowptr, colind, val, alpha, x, beta, y):
+    """CMat_BlkCrs::MatVec restated: returns the new y."""
+    y = np.array(y, np.float64, copy=True)
+    ci = np.ascontiguousarray(colind, np.uint32) if len(colind) else np.zeros(1, np.uint32)
+    lib().dfo_rmat_spmv(nrow, brow, bcol, _u(np.ascontiguousarray(rowptr, np.uint32)), _u(ci),
+                        _dz(np.ascontiguousarray(val, np.float64)), alpha, _d(np.ascontiguousarray(x, np.float64)),
+                        beta, _d(y))
+    return y

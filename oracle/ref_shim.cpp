@@ -916,4 +916,34 @@ int dfm_ref_set_fill(dfm_ref_sys* s, int lev) {
   return 0;
 }
 
+
+// CMat_BlkCrs(nrow, brow, ncol, bcol) with the given pattern and values, then
+// MatVec(alpha, x, beta, y) (src/matvec/mat_blkcrs.cpp:955-1175).
+int dfm_ref_rmat_spmv(unsigned nrow, unsigned ncol, unsigned brow, unsigned bcol, const unsigned* rowptr,
+                      const unsigned* colind, const double* val, double alpha, const double* x, double beta,
+                      double* y) {
+  Quiet q;
+  MatVec::CMat_BlkCrs m(nrow, brow, ncol, bcol);
+  Com::CIndexedArray crs;
+  crs.index.assign(rowptr, rowptr + nrow + 1);
+  crs.array.assign(colind, colind + rowptr[nrow]);
+  m.AddPattern(crs);
+  m.SetZero();
+  const unsigned bb = brow * bcol;
+  for (unsigned i = 0; i < nrow; i++) {
+    unsigned np = 0;
+    double* p = m.GetPtrValPSuP(i, np);
+    if (np) std::memcpy(p, val + (size_t)rowptr[i] * bb, sizeof(double) * bb * np);
+  }
+  MatVec::CVector_Blk vx(ncol, bcol), vy(nrow, brow);
+  for (unsigned j = 0; j < ncol; j++)
+    for (unsigned c = 0; c < bcol; c++) vx.SetValue(j, c, x[(size_t)j * bcol + c]);
+  for (unsigned i = 0; i < nrow; i++)
+    for (unsigned r = 0; r < brow; r++) vy.SetValue(i, r, y[(size_t)i * brow + r]);
+  m.MatVec(alpha, vx, beta, vy, true);
+  for (unsigned i = 0; i < nrow; i++)
+    for (unsigned r = 0; r < brow; r++) y[(size_t)i * brow + r] = vy.GetValue(i, r);
+  return 0;
+}
+
 }  // extern "C"

@@ -137,6 +137,12 @@ int dfm_ref_zmat_iluk(unsigned N, const unsigned* rowptr, const unsigned* colind
  * SetLinearSystem); factored by the next dfm_ref_ilu. */
 int dfm_ref_set_fill(dfm_ref_sys* s, int lev);
 
+/* CMat_BlkCrs::MatVec on a rectangular block matrix (nrow x ncol blocks of
+ * brow x bcol), y updated in place. */
+int dfm_ref_rmat_spmv(unsigned nrow, unsigned ncol, unsigned brow, unsigned bcol, const unsigned* rowptr,
+                      const unsigned* colind, const double* val, double alpha, const double* x, double beta,
+                      double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,8 @@ def lib():
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
         L.dfm_ref_zmat_iluk.argtypes = [C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
         L.dfm_ref_set_fill.argtypes = [P, C.c_int]
+        L.dfm_ref_rmat_spmv.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint, up, up, dp, C.c_double, dp,
+                                        C.c_double, dp]
         L.dfm_ref_newmark.argtypes = [C.c_int, C.c_int, dp, C.c_int, ip, C.c_int, ip, dp, C.c_double, C.c_double,
                                       C.c_double, dp, dp, dp, dp, dp, dp, dp, ip, dp, dp]
         _lib = L
@@ -305,3 +307,13 @@ def zmat_iluk(N, rowptr, colind, diag, off, lev):
     rc = lib().dfm_ref_zmat_iluk(N, _u(rowptr), _u(ci), _d(diag), _d(o), lev, n.value, _u(fr), _u(fc), _d(fd),
                                  _d(fo), C.byref(n))
     return rc, fr, fc[: n.value], fd, fo[: 2 * n.value]
+
+
+def rmat_spmv(nrow, ncol, brow, bcol, rowptr, colind, val, alpha, x, beta, y):
+    """The reference's CMat_BlkCrs::MatVec: returns the new y."""
+    y = np.array(y, np.float64, copy=True)
+    ci = np.ascontiguousarray(colind, np.uint32) if len(colind) else np.zeros(1, np.uint32)
+    v = np.ascontiguousarray(val, np.float64) if len(val) else np.zeros(1)
+    lib().dfm_ref_rmat_spmv(nrow, ncol, brow, bcol, _u(np.ascontiguousarray(rowptr, np.uint32)), _u(ci), _d(v), alpha,
+                            _d(np.ascontiguousarray(x, np.float64)), beta, _d(y))
+    return y

@@ -9,16 +9,22 @@
 //   delfem_dropin poisson N     2-D Poisson -lap u = 1 on an N x N grid of P1 triangles, u = 0 on the boundary
 //   delfem_dropin solid3d NX NY NZ   3-D linear elasticity of a box (Kuhn tetrahedra), x = 0 face clamped,
 //                                    unit body force in -z
+//   delfem_dropin twoseg N M L0 L1   a linear system of two segments built at the matrix level
+//                                    (LsSol::CLinearSystem::AddLinSysSeg / AddMat_Dia / AddMat_NonDia):
+//                                    an N x N grid of L0 x L0 blocks and a chain of M nodes of L1 x L1
+//                                    blocks, coupled both ways; symmetric positive definite
 //   [lev]                       optional last argument: ILU fill-in level (SetFillInLevel), default 0
 //
 // Every run builds the problem from scratch, solves, calls the reference's
-// UpdateValueOfField and reads the field back.  Runs:
+// UpdateValueOfField and reads the field back (the segments' update vectors
+// for twoseg).  Runs:
 //   ref_pcg, ref_bicg, ref_cg  the reference's LsSol solvers with LsSol::CPreconditioner_ILU
 //   gpu_pcg, gpu_bicg, gpu_cg  dfm_delfem::Solve_*_GPU over dfm_delfem::CLinearSystemGPU
 //   ref_over_gpu               the reference's LsSol::Solve_PCG driving CLinearSystemGPU step by step
 //   glue_gpu_prec              the reference's CLinearSystemPreconditioner glue with
 //                              dfm_delfem::CPreconditioner_ILU_GPU as its LsSol::CPreconditioner
 // and prints one JSON object: per run ok, iterations, conv and the field values.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -38,6 +44,9 @@
 #include "delfem/ls/linearsystem.h"
 #include "delfem/ls/preconditioner.h"
 #include "delfem/ls/solver_ls_iter.h"
+#include "delfem/matvec/mat_blkcrs.h"
+#include "delfem/matvec/matdia_blkcrs.h"
+#include "delfem/matvec/vector_blk.h"
 #include "delfem/mesh_interface.h"
 #include "dfm_b200_delfem.hpp"
 
@@ -151,8 +160,17 @@ GridMesh solid_mesh(int nx, int ny, int nz) {
   return m;
 }
 
+// One fresh linear system to solve: the solver-side CLinearSystem, its
+// assembly, and the solution after the solve.
+struct Sys {
+  virtual ~Sys() {}
+  virtual LsSol::CLinearSystem& lin() = 0;
+  virtual void assemble() = 0;
+  virtual std::vector<double> result() = 0;
+};
+
 // One fresh DelFEM problem: field world, field, boundary, linear system.
-struct Problem {
+struct Problem : Sys {
   std::string kind;
   GridMesh mesh;
   CFieldWorld world;
@@ -168,7 +186,7 @@ struct Problem {
     ls.AddPattern_Field(id_field, world);
     ls.SetFixedBoundaryCondition_Field(id_bnd, world);
   }
-  void assemble() {
+  void assemble() override {
     Quiet q;
     ls.InitializeMarge();
     if (kind == "poisson") {
@@ -179,9 +197,13 @@ struct Problem {
     }
     ls.FinalizeMarge();
   }
-  void update_field() {
-    Quiet q;
-    ls.UpdateValueOfField(id_field, world, VALUE);
+  LsSol::CLinearSystem& lin() override { return ls.m_ls; }
+  std::vector<double> result() override {
+    {
+      Quiet q;
+      ls.UpdateValueOfField(id_field, world, VALUE);
+    }
+    return field();
   }
   std::vector<double> field() const {
     const CField& f = world.GetField(id_field);
@@ -190,6 +212,115 @@ struct Problem {
     std::vector<double> out((size_t)ns.Size() * len);
     for (unsigned i = 0; i < ns.Size(); i++) ns.GetValue(i, &out[(size_t)i * len]);
     return out;
+  }
+};
+
+// Two segments at the matrix level: segment 0 an n x n grid (4 neighbours) of
+// L0 x L0 blocks, segment 1 a chain of m nodes of L1 x L1 blocks, node k of the
+// chain coupled to two grid nodes; couplings C (rows in segment 1) and C^T.
+struct TwoSeg : Sys {
+  unsigned n, m, L0, L1, N0;
+  LsSol::CLinearSystem ls;
+  std::vector<std::vector<unsigned>> grid, chain, cpl, cplT;
+
+  TwoSeg(unsigned n_, unsigned m_, unsigned l0, unsigned l1) : n(n_), m(m_), L0(l0), L1(l1), N0(n_ * n_) {
+    grid.resize(N0);
+    for (unsigned j = 0; j < n; j++)
+      for (unsigned i = 0; i < n; i++) {
+        auto& g = grid[i + j * n];
+        if (j > 0) g.push_back(i + (j - 1) * n);
+        if (i > 0) g.push_back(i - 1 + j * n);
+        if (i + 1 < n) g.push_back(i + 1 + j * n);
+        if (j + 1 < n) g.push_back(i + (j + 1) * n);
+      }
+    chain.resize(m);
+    cpl.resize(m);
+    cplT.resize(N0);
+    for (unsigned k = 0; k < m; k++) {
+      if (k > 0) chain[k].push_back(k - 1);
+      if (k + 1 < m) chain[k].push_back(k + 1);
+      unsigned a = (3 * k) % N0, b = (7 * k + 1) % N0;
+      if (a > b) std::swap(a, b);
+      cpl[k].push_back(a);
+      if (b != a) cpl[k].push_back(b);
+      for (unsigned c : cpl[k]) cplT[c].push_back(k);
+    }
+    Quiet q;
+    ls.AddLinSysSeg(N0, L0);
+    ls.AddLinSysSeg(m, L1);
+    ls.AddMat_Dia(0, crs(grid));
+    ls.AddMat_Dia(1, crs(chain));
+    ls.AddMat_NonDia(1, 0, crs(cpl));
+    ls.AddMat_NonDia(0, 1, crs(cplT));
+  }
+  static Com::CIndexedArray crs(const std::vector<std::vector<unsigned>>& rows) {
+    Com::CIndexedArray a;
+    a.index.assign(1, 0);
+    for (const auto& r : rows) {
+      a.array.insert(a.array.end(), r.begin(), r.end());
+      a.index.push_back((unsigned)a.array.size());
+    }
+    return a;
+  }
+  // symmetric coupling block values: entry (r, c) of C's block (k, g)
+  static double cval(unsigned k, unsigned g, unsigned r, unsigned c) { return -0.1 - 0.01 * ((k + 2 * g + r + 3 * c) % 5); }
+  LsSol::CLinearSystem& lin() override { return ls; }
+  void assemble() override {
+    Quiet q;
+    ls.InitializeMarge();
+    MatVec::CMatDia_BlkCrs& A0 = ls.GetMatrix(0);
+    MatVec::CMatDia_BlkCrs& A1 = ls.GetMatrix(1);
+    for (unsigned p = 0; p < N0; p++) {
+      double* d = A0.GetPtrValDia(p);
+      for (unsigned r = 0; r < L0; r++)
+        for (unsigned c = 0; c < L0; c++) d[r * L0 + c] = (r == c ? 4.0 + 0.5 * L0 : 0.0) + 0.1;
+      unsigned np = 0;
+      double* o = A0.GetPtrValPSuP(p, np);
+      for (unsigned t = 0; t < np * L0 * L0; t++) o[t] = ((t % (L0 * L0)) % (L0 + 1) == 0 ? -1.0 : 0.0) - 0.05;
+    }
+    for (unsigned k = 0; k < m; k++) {
+      double* d = A1.GetPtrValDia(k);
+      for (unsigned r = 0; r < L1; r++)
+        for (unsigned c = 0; c < L1; c++) d[r * L1 + c] = (r == c ? 2.2 + 0.4 * L0 + 0.2 * L1 : 0.0) + 0.1;
+      unsigned np = 0;
+      double* o = A1.GetPtrValPSuP(k, np);
+      for (unsigned t = 0; t < np * L1 * L1; t++) o[t] = ((t % (L1 * L1)) % (L1 + 1) == 0 ? -1.0 : 0.0) - 0.05;
+    }
+    {  // C: rows in the chain, columns in the grid; C^T: the transpose, block by block
+      MatVec::CMat_BlkCrs& C = ls.GetMatrix(1, 0);
+      MatVec::CMat_BlkCrs& CT = ls.GetMatrix(0, 1);
+      for (unsigned k = 0; k < m; k++) {
+        unsigned np = 0;
+        double* o = C.GetPtrValPSuP(k, np);
+        for (unsigned t = 0; t < np; t++)
+          for (unsigned r = 0; r < L1; r++)
+            for (unsigned c = 0; c < L0; c++) o[(t * L1 + r) * L0 + c] = cval(k, cpl[k][t], r, c);
+      }
+      for (unsigned g = 0; g < N0; g++) {
+        unsigned np = 0;
+        double* o = CT.GetPtrValPSuP(g, np);
+        for (unsigned t = 0; t < np; t++)
+          for (unsigned r = 0; r < L0; r++)
+            for (unsigned c = 0; c < L1; c++) o[(t * L0 + r) * L1 + c] = cval(cplT[g][t], g, c, r);
+      }
+    }
+    for (unsigned s = 0; s < 2; s++) {
+      MatVec::CVector_Blk& f = ls.GetVector(-1, s);
+      const unsigned L = s ? L1 : L0;
+      for (unsigned i = 0; i < f.NBlk(); i++)
+        for (unsigned d = 0; d < L; d++) f.SetValue(i, d, std::sin(0.37 * i + 1.3 * d + 0.5 * s) + 0.2);
+    }
+    ls.FinalizeMarge();
+  }
+  std::vector<double> result() override {
+    std::vector<double> x;
+    for (unsigned s = 0; s < 2; s++) {
+      const MatVec::CVector_Blk& u = ls.GetVector(-2, s);
+      const unsigned L = s ? L1 : L0;
+      for (unsigned i = 0; i < u.NBlk(); i++)
+        for (unsigned d = 0; d < L; d++) x.push_back(u.GetValue(i, d));
+    }
+    return x;
   }
 };
 
@@ -205,18 +336,24 @@ struct Run {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev] | twoseg N M L0 L1\n", argv[0]);
     return 2;
   }
   const std::string kind = argv[1];
   GridMesh mesh;
   int lev = 0;
+  std::function<std::unique_ptr<Sys>()> make;
   if (kind == "poisson") {
     mesh = poisson_mesh(std::atoi(argv[2]));
     if (argc > 3) lev = std::atoi(argv[3]);
+    make = [&]() { return std::unique_ptr<Sys>(new Problem(kind, mesh)); };
   } else if (kind == "solid3d" && argc >= 5) {
     mesh = solid_mesh(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]));
     if (argc > 5) lev = std::atoi(argv[5]);
+    make = [&]() { return std::unique_ptr<Sys>(new Problem(kind, mesh)); };
+  } else if (kind == "twoseg" && argc >= 6) {
+    const unsigned n = std::atoi(argv[2]), m = std::atoi(argv[3]), l0 = std::atoi(argv[4]), l1 = std::atoi(argv[5]);
+    make = [=]() { return std::unique_ptr<Sys>(new TwoSeg(n, m, l0, l1)); };
   } else {
     return 2;
   }
@@ -227,39 +364,38 @@ int main(int argc, char** argv) {
     dfm_lsol::Context ctx(0);
     // the reference's path: LsSol::CPreconditioner_ILU + LsSol solvers
     auto ref_run = [&](const char* name, int method) {
-      Problem P(kind, mesh);
+      std::unique_ptr<Sys> P = make();
       Run r;
       r.name = name;
       r.conv = tol;
       r.it = maxit;
       Quiet q;
       LsSol::CPreconditioner_ILU prec;
-      prec.SetFillInLevel(lev);
-      prec.SetLinearSystem(P.ls.m_ls);
-      P.assemble();
-      prec.SetValue(P.ls.m_ls);
-      LsSol::CLinearSystemPreconditioner lsp(P.ls.m_ls, prec);
+      if (lev) prec.SetFillInLevel(lev);
+      prec.SetLinearSystem(P->lin());
+      P->assemble();
+      prec.SetValue(P->lin());
+      LsSol::CLinearSystemPreconditioner lsp(P->lin(), prec);
       if (method == 0) r.ok = LsSol::Solve_PCG(r.conv, r.it, lsp);
       else if (method == 1) r.ok = LsSol::Solve_PBiCGSTAB(r.conv, r.it, lsp);
-      else r.ok = LsSol::Solve_CG(r.conv, r.it, P.ls.m_ls);
-      P.update_field();
-      r.x = P.field();
+      else r.ok = LsSol::Solve_CG(r.conv, r.it, P->lin());
+      r.x = P->result();
       runs.push_back(r);
     };
     // the drop-in: only the preconditioner, the interface object and the solver change
     auto gpu_run = [&](const char* name, int method) {
-      Problem P(kind, mesh);
+      std::unique_ptr<Sys> P = make();
       Run r;
       r.name = name;
       r.conv = tol;
       r.it = maxit;
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
-      prec.SetLinearSystem(P.ls.m_ls);
-      P.assemble();
-      if (!prec.SetValue(P.ls.m_ls)) throw dfm_lsol::Error(DFM_SINGULAR_PIVOT, name);
+      prec.SetLinearSystem(P->lin());
+      P->assemble();
+      if (!prec.SetValue(P->lin())) throw dfm_lsol::Error(DFM_SINGULAR_PIVOT, name);
       {
-        dfm_delfem::CLinearSystemGPU lsp(P.ls.m_ls, prec);
+        dfm_delfem::CLinearSystemGPU lsp(P->lin(), prec);
         if (method == 0) r.ok = dfm_delfem::Solve_PCG_GPU(r.conv, r.it, lsp);
         else if (method == 1) r.ok = dfm_delfem::Solve_PBiCGSTAB_GPU(r.conv, r.it, lsp);
         else if (method == 2) r.ok = dfm_delfem::Solve_CG_GPU(r.conv, r.it, lsp);
@@ -269,8 +405,7 @@ int main(int argc, char** argv) {
           lsp.SyncToHost();
         }
       }
-      P.update_field();
-      r.x = P.field();
+      r.x = P->result();
       runs.push_back(r);
     };
     ref_run("ref_pcg", 0);
@@ -281,7 +416,7 @@ int main(int argc, char** argv) {
     gpu_run("gpu_cg", 2);
     gpu_run("ref_over_gpu", 3);
     {  // the reference's glue class with the device preconditioner as its LsSol::CPreconditioner
-      Problem P(kind, mesh);
+      std::unique_ptr<Sys> P = make();
       Run r;
       r.name = "glue_gpu_prec";
       r.conv = tol;
@@ -289,16 +424,15 @@ int main(int argc, char** argv) {
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
       LsSol::CPreconditioner& base = prec;
-      base.SetLinearSystem(P.ls.m_ls);
-      P.assemble();
-      base.SetValue(P.ls.m_ls);
-      LsSol::CLinearSystemPreconditioner lsp(P.ls.m_ls, base);
+      base.SetLinearSystem(P->lin());
+      P->assemble();
+      base.SetValue(P->lin());
+      LsSol::CLinearSystemPreconditioner lsp(P->lin(), base);
       {
         Quiet q;
         r.ok = LsSol::Solve_PCG(r.conv, r.it, lsp);
       }
-      P.update_field();
-      r.x = P.field();
+      r.x = P->result();
       runs.push_back(r);
     }
   } catch (const dfm_lsol::Error& e) {

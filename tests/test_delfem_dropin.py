@@ -4,7 +4,10 @@ reference's headers and library by `make -C oracle dropin`): the reference's
 field world, assembly, Dirichlet elimination and UpdateValueOfField, with
 dfm_delfem::CPreconditioner_ILU_GPU, CLinearSystemGPU and Solve_*_GPU in place
 of LsSol's classes.  The same program runs the reference's own solvers on the
-same problem; the field after UpdateValueOfField must agree to 1e-8 relative
+same problem (a system of two segments - the reference's block ILU over
+segments, src/ls/preconditioner.cpp:57-335, against the drop-in's ILU(0) of
+the joined matrix - among them); the field after UpdateValueOfField (the
+segments' updates for the two-segment system) must agree to 1e-8 relative
 at a relative residual of 1e-10, and the iteration counts within the few that
 the device's summation order moves them."""
 import json
@@ -43,7 +46,11 @@ def _rel(a, b):
 
 
 CASES = [("poisson", ["poisson", "32"]), ("poisson_ilu1", ["poisson", "24", "1"]),
-         ("solid3d", ["solid3d", "10", "3", "3"]), ("solid3d_ilu1", ["solid3d", "8", "2", "2", "1"])]
+         ("solid3d", ["solid3d", "10", "3", "3"]), ("solid3d_ilu1", ["solid3d", "8", "2", "2", "1"]),
+         # two segments (LsSol::CLinearSystem::AddLinSysSeg x 2 with couplings both ways): equal block
+         # lengths, and different ones (joined one row per DOF)
+         ("twoseg_2_2", ["twoseg", "40", "200", "2", "2"]), ("twoseg_2_1", ["twoseg", "40", "200", "2", "1"]),
+         ("twoseg_1_3", ["twoseg", "40", "200", "1", "3"])]
 
 
 @pytest.mark.gpu
