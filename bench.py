@@ -373,12 +373,15 @@ def run_c3_sharded(torch, dev, stream, steps):
 
 # ------------------------------------------------------------- profile run
 def run_profile():
-    """A short c2 workload for profiler captures: device assembly, ILU(0), a
-    32-iteration PCG that autotunes the kernels, then inside the NVTX range
-    "steady": 3 SpMVs, 3 ILU applications and a 32-iteration PCG (no timing
-    output)."""
+    """A short workload for profiler captures: every kernel family of the path
+    runs a few times inside the NVTX range "steady" (after the autotuners),
+    each family in a sub-range of its own: c2 assembly + Dirichlet
+    elimination, ILU(0) factor, SpMV, ILU applications (FP64 and the FP32
+    copy of the mixed solve), a 32-iteration PCG (Krylov update kernels);
+    the c5 Helmholtz system (complex assembly, factor, SpMV, sweeps); a batch
+    of 64 c3 instances (batched kernels).  No timing output."""
     import torch
-    from delfem_b200 import lib
+    from delfem_b200 import lib, meshes
     ctx = lib.Context(0)
     m, G, A, b_dev, _ = build_c2(ctx, torch, 0)
     M = lib.ILU(A)
@@ -389,17 +392,85 @@ def run_profile():
     y = torch.empty_like(b_dev)
     r = b_dev.clone()
     rc, it, conv = lib.solve_pcg(A, M, r, x, tol=TOL, maxit=32)  # autotunes SpMV lanes and the sweep schedule
+    r.copy_(b_dev)
+    lib.solve_pcg_mixed(A, M, r, x, tol=TOL, maxit=16)  # FP32 factor copy and its plans
+    flags = np.zeros((m.nnode, 3), np.int32)
+    flags[np.unique(m.bnd.ravel())] = 1
+    flags_d = torch.from_numpy(flags.ravel()).cuda()
+    # c5 and a c3 subset, tuned before the range
+    mz = meshes.unit_disk_tri(258, numbering="bands")
+    GZ = lib.Mesh(ctx, mz.coord, mz.elem, mz.bnd)
+    AZ = lib.Matrix(ctx, *GZ.pattern(), 1, lib.COMPLEX)
+    bz = torch.empty(2 * mz.nnode, dtype=torch.float64, device="cuda")
+    loadz = torch.from_numpy(meshes.gaussian_source_load(mz).ravel()).cuda()
+    GZ.assemble_helmholtz(AZ, 2 * 3.1416 / 20, bz, load=loadz)
+    MZ = lib.ILU(AZ)
+    MZ.factor()
+    xz, yz, rz = torch.zeros_like(bz), torch.empty_like(bz), bz.clone()
+    lib.solve_pcocg(AZ, MZ, rz, xz, tol=1e-8, maxit=16)
+    sizes = meshes.batch_sizes(C3_COUNT, C3_LO, C3_HI, C3_SEED)[:64]
+    ms = [meshes.unit_square_tri(int(n)) for n in sizes]
+    big, noff, _ = meshes.concat(ms)
+    GB = lib.Mesh(ctx, big.coord, big.elem)
+    AB = lib.Matrix(ctx, *GB.pattern(), 1)
+    bb = torch.empty(big.nnode, dtype=torch.float64, device="cuda")
+    flb = np.zeros(big.nnode, np.int32)
+    flb[np.unique(big.bnd.ravel())] = 1
+    GB.assemble_poisson(AB, 1.0, 1.0, bb)
+    lib.apply_dirichlet(AB, torch.from_numpy(flb).cuda(), bb)
+    MB = lib.ILU(AB)
+    MB.factor()
+    B = lib.Batch(MB, noff.astype(np.uint32))
+    xb = torch.zeros_like(bb)
+    B.solve(bb, xb, tol=TOL)  # autotunes the batch schedule
     torch.cuda.synchronize()
-    torch.cuda.nvtx.range_push("steady")  # profiler filter: the tuned steady state only
+    nv = torch.cuda.nvtx
+    nv.range_push("steady")  # profiler filter: the tuned steady state only
+    nv.range_push("c2_assembly")
+    G.assemble_solid3d(A, LAM3, MYU3, 1.0, 0.0, 0.0, -1.0, b_dev)
+    lib.apply_dirichlet(A, flags_d, b_dev)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c2_factor")
+    M.factor()
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c2_spmv")
     for _ in range(3):
         A.spmv(1.0, b_dev, 0.0, y)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c2_ilu_apply")
     for _ in range(3):
         M.apply(b_dev, y)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c2_pcg")
     r.copy_(b_dev)
     lib.solve_pcg(A, M, r, x, tol=TOL, maxit=32)
     torch.cuda.synchronize()
-    torch.cuda.nvtx.range_pop()
-    log(f"[profile-run] sweep mode {M.sweep}, lanes {A.lanes}, spmv kernel {A.spmv_kernel}")
+    nv.range_pop()
+    nv.range_push("c2_pcg_mixed")
+    r.copy_(b_dev)
+    lib.solve_pcg_mixed(A, M, r, x, tol=TOL, maxit=16)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c5")
+    GZ.assemble_helmholtz(AZ, 2 * 3.1416 / 20, bz, load=loadz)
+    MZ.factor()
+    for _ in range(3):
+        AZ.spmv(1.0, bz, 0.0, yz)
+    for _ in range(3):
+        MZ.apply(bz, yz)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_push("c3_batch")
+    B.solve(bb, xb, tol=TOL)
+    torch.cuda.synchronize()
+    nv.range_pop()
+    nv.range_pop()
+    log(f"[profile-run] c2 sweep mode {M.sweep}, lanes {A.lanes}, spmv kernel {A.spmv_kernel}; c5 sweep mode "
+        f"{MZ.sweep}; c3 batch schedule {B.schedule}")
 
 
 # ------------------------------------------------------- c1 and c5 sections

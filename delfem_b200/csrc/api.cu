@@ -509,6 +509,29 @@ int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
   return DFM_OK;
 }
 
+int dfm_ilu_set_sweep_warps(dfm_ilu M, int compute_warps, int lanes, int producer_warps) {
+  if (!M || (compute_warps != 1 && compute_warps != 2 && compute_warps != 4) ||
+      (lanes != 2 && lanes != 4 && lanes != 8) || producer_warps < 1 || compute_warps + producer_warps > 16)
+    return DFM_ERR_INVALID;
+  if (M->sweep != 3 || !M->plan_f.halo) return DFM_ERR_INVALID;  // mode 9 only
+  for (SweepPlan* P : {&M->plan_f, &M->plan_b, &M->plan32_f, &M->plan32_b}) {
+    P->cw = compute_warps;
+    P->lpr = lanes;
+    P->hw = producer_warps;
+  }
+  M->plan_gen++;  // captured solves hold the old launch shape
+  return DFM_OK;
+}
+
+int dfm_ilu_get_sweep_warps(dfm_ilu M, int* compute_warps, int* lanes, int* producer_warps) {
+  if (!M || !compute_warps || !lanes || !producer_warps) return DFM_ERR_INVALID;
+  if (M->sweep != 3 || !M->plan_f.halo) return DFM_ERR_INVALID;
+  *compute_warps = M->plan_f.cw;
+  *lanes = M->plan_f.lpr;
+  *producer_warps = M->plan_f.hw;
+  return DFM_OK;
+}
+
 int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns) {
   if (!M || max_blocks < 0 || poll_sleep_ns > 100000) return DFM_ERR_INVALID;
   M->sweep_blocks = max_blocks;

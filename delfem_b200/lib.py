@@ -92,6 +92,8 @@ PROTOS = {
     "dfm_ilu_apply_static": (_i, [_vp, _vp, _vp]),
     "dfm_ilu_set_sweep": (_i, [_vp, _i]),
     "dfm_ilu_get_sweep": (_i, [_vp, _ip]),
+    "dfm_ilu_set_sweep_warps": (_i, [_vp, _i, _i, _i]),
+    "dfm_ilu_get_sweep_warps": (_i, [_vp, _ip, _ip, _ip]),
     "dfm_ilu_set_sweep_tuning": (_i, [_vp, _i, _u]),
     "dfm_ilu_set_sweep_partition": (_i, [_vp, _up, _u]),
     "dfm_sweep_partition_patches": (_i, [_u, _i, _dp, _u, _up, _up]),
@@ -535,6 +537,17 @@ class ILU:
     @sweep.setter
     def sweep(self, v):
         check(lib().dfm_ilu_set_sweep(self.h, int(v)))
+
+    @property
+    def sweep_warps(self):
+        """(compute warps, lanes per row, producer warps) of schedule 9."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().dfm_ilu_get_sweep_warps(self.h, C.byref(a), C.byref(b), C.byref(c)), "dfm_ilu_get_sweep_warps")
+        return a.value, b.value, c.value
+
+    @sweep_warps.setter
+    def sweep_warps(self, v):
+        check(lib().dfm_ilu_set_sweep_warps(self.h, *(int(t) for t in v)), "dfm_ilu_set_sweep_warps")
 
 
 class Batch:

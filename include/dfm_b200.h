@@ -351,6 +351,13 @@ DFM_API int dfm_ilu_set_sweep_partition(dfm_ilu M, const unsigned* part, unsigne
 DFM_API int dfm_sweep_partition_patches(unsigned nnode, int ndim, const double* coord, unsigned max_parts,
                                         unsigned* part, unsigned* nparts);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
+/* No counterpart in the reference.  The launch shape of schedule 9 (valid
+ * while it is the schedule): compute warps 1, 2 or 4, lanes per row 2, 4 or 8,
+ * producer warps (compute + producer <= 16).  The autotuner picks one; this
+ * pins it (a row's sum runs over `lanes` lanes, so the lanes decide its
+ * summation order). */
+DFM_API int dfm_ilu_set_sweep_warps(dfm_ilu M, int compute_warps, int lanes, int producer_warps);
+DFM_API int dfm_ilu_get_sweep_warps(dfm_ilu M, int* compute_warps, int* lanes, int* producer_warps);
 /* Sync-free schedule knobs: cap on the number of co-resident blocks (0 = all
  * that fit) and the back-off between polls of a waiting lane in ns (global). */
 DFM_API int dfm_ilu_set_sweep_tuning(dfm_ilu M, int max_blocks, unsigned poll_sleep_ns);

@@ -208,3 +208,30 @@ def test_spmv_large_rows_and_tiles(ctx, kernel):
     A.spmv(1.0, dev(x), 0.0, y)
     ref = S.spmv(1.0, x, 0.0, np.zeros_like(x))
     assert np.allclose(y.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("name", ["solid3d", "poisson_coef", "helmholtz_bands", "random_b3"])
+@pytest.mark.parametrize("warps", [(1, 2, 1), (1, 4, 4), (2, 8, 2), (4, 4, 12)])
+def test_halo_sweep_every_warp_split(ctx, name, warps):
+    """Schedule 9 with each split of compute warps, lanes per row and producer
+    warps: the preconditioner to 1e-11 of the oracle, before and after a
+    refactorization (the packed level data follow the factor)."""
+    from delfem_b200 import lib
+    S = SYSTEMS[name]()
+    A = make(ctx, S)
+    M = lib.ILU(A)
+    M.factor()
+    M.sweep = 9
+    M.sweep_warps = warps
+    assert M.sweep == 9 and M.sweep_warps == warps
+    _, fd, fo = S.ilu0()
+    r = np.random.default_rng(9).standard_normal(S.N * S.xw)
+    ref = S.precond(fd, fo, r)
+    z = torch.zeros(S.N * S.xw, dtype=torch.float64, device="cuda")
+    M.apply(dev(r), z)
+    assert np.allclose(z.cpu().numpy(), ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
+    A.set_values(S.diag * 2.0, S.off * 2.0)
+    M.factor()
+    M.apply(dev(r), z)
+    assert np.allclose(z.cpu().numpy(), ref / 2.0, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
+    assert ctx.take_error() == (0, 0)
