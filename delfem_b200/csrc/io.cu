@@ -166,8 +166,8 @@ int zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, unsigned* rowp
 // the axis of that smallest variance is dropped, the other two kept in cyclic
 // order (y,z / z,x / x,y); with ndim 2 the lines carry x y.  The volume
 // elements and coordinates are what the pattern and the assembly need; the
-// boundary facets the reference derives (outer bars / colour-coded
-// triangles) are not produced.
+// boundary facets the reference derives from them are dfm_gid_boundary's
+// (boundary.cu).
 namespace dfm {
 namespace {
 struct Lines {

@@ -61,6 +61,7 @@ PROTOS = {
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
+    "dfm_gid_boundary": (_i, [_i, _u, _dp, _i, _u, _ip, _d, _ip, _up, _up, _up, _up, _up, _up, _up, _up]),
     "dfm_mat_zero_rows": (_i, [_vp, _vp]),
     "dfm_rmat_create": (_i, [_vp, _u, _u, _u, _u, _up, _up, C.POINTER(_vp)]),
     "dfm_rmat_destroy": (_i, [_vp]),
@@ -414,6 +415,38 @@ def read_gid_mesh(path):
     check(L.dfm_gid_read_mesh(p, C.byref(nd), C.byref(nn), coord.ctypes.data_as(_dp), C.byref(no), C.byref(ne),
                               elem.ctypes.data_as(_ip)), "dfm_gid_read_mesh")
     return coord, elem
+
+
+def gid_boundary(coord, elem, crt_dot=None):
+    """The boundary facets the reference's GiD readers derive from a mesh
+    (dfm_gid_boundary): a dict with ``facets`` [nfacet, nnofa] (boundary
+    triangles of a tetrahedral mesh, outer bars of a planar one), ``groups``
+    (per colour / bar chain, the facet indices in the reference's order),
+    ``vertices`` (planar: the chains' end nodes, ascending) and ``ends``
+    [ngroup, 2] (planar: each chain's first and last vertex index).
+    ``crt_dot`` defaults to the reference's thresholds, 0.2 for the
+    triangles' normals and 0.8 for the bars' directions."""
+    coord = np.ascontiguousarray(coord, np.float64)
+    elem = np.ascontiguousarray(elem, np.int32)
+    ndim, nnoel = coord.shape[1], elem.shape[1]
+    if crt_dot is None:
+        crt_dot = 0.2 if ndim == 3 else 0.8
+    L = lib()
+    nf, nfa, ng, nv = C.c_int(), C.c_uint(), C.c_uint(), C.c_uint()
+    args = (int(ndim), coord.shape[0], coord.ctypes.data_as(_dp), int(nnoel), elem.shape[0], elem.ctypes.data_as(_ip),
+            float(crt_dot), C.byref(nf), C.byref(nfa))
+    check(L.dfm_gid_boundary(*args, None, C.byref(ng), None, None, C.byref(nv), None, None), "dfm_gid_boundary")
+    facet = np.zeros((nfa.value, nf.value), np.uint32)
+    gptr = np.zeros(ng.value + 1, np.uint32)
+    gfac = np.zeros(max(nfa.value, 1), np.uint32)
+    vert = np.zeros(max(nv.value, 1), np.uint32)
+    ends = np.zeros((max(ng.value, 1), 2), np.uint32)
+    check(L.dfm_gid_boundary(*args, facet.ctypes.data_as(_up), C.byref(ng), gptr.ctypes.data_as(_up),
+                             gfac.ctypes.data_as(_up), C.byref(nv), vert.ctypes.data_as(_up),
+                             ends.ctypes.data_as(_up)), "dfm_gid_boundary")
+    groups = [gfac[gptr[g]:gptr[g + 1]].copy() for g in range(ng.value)]
+    return {"facets": facet, "groups": groups, "vertices": vert[:nv.value].copy(),
+            "ends": ends[:ng.value].copy() if ndim == 2 else np.zeros((0, 2), np.uint32)}
 
 
 def boundary_matrix(rowptr, colind, diag, off, flags, b):

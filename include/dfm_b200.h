@@ -173,11 +173,43 @@ DFM_API int dfm_zmat_read_text(const char* path, unsigned* N, unsigned* ncrs, un
  * dropping its axis of least variance as the 2-D mesher does (a non-planar
  * one is DFM_ERR_INVALID).  With coord == NULL it reports *ndim, *nnode,
  * *nnoel and *nelem; then coord[nnode*ndim] and elem[nelem*nnoel] (0-based,
- * nullable) receive the mesh, ready for dfm_mesh_create.  Boundary facets are
- * not derived.  Malformed input is DFM_ERR_INVALID, an unreadable file
- * DFM_ERR_IO. */
+ * nullable) receive the mesh, ready for dfm_mesh_create; dfm_gid_boundary
+ * derives the reference's boundary facets from it.  Malformed input is
+ * DFM_ERR_INVALID, an unreadable file DFM_ERR_IO. */
 DFM_API int dfm_gid_read_mesh(const char* path, int* ndim, unsigned* nnode, double* coord, int* nnoel,
                               unsigned* nelem, int* elem);
+
+/* The boundary facets the reference's GiD readers derive from the elements
+ * (host only), on a mesh as dfm_gid_read_mesh returns it:
+ *  - ndim 3, nnoel 4 (tetrahedra; Msh::CMesh3D::ReadFromFile_GiDMsh,
+ *    src/msh/mesh3d.cpp:744-778): facets are the triangles of faces that no
+ *    other tetrahedron shares with the opposite orientation (Msh::MakeTetSurTet
+ *    + MakeOuterBoundTet, src/msh/meshkernel3d.cpp:102-230, 514-539), in
+ *    (tetrahedron, face) order, nodes counter-clockwise from outside; groups
+ *    are the colours of Msh::MakeColorCoding_Tri3D (:905-947): flat patches
+ *    grown across shared edges whose unit normals have a dot product above
+ *    crt_dot (0.2 in the reader), each group's facets ascending;
+ *  - ndim 2, nnoel 3 or 4 (Msh::CMesher2D::ReadFromFile_GiDMsh,
+ *    src/msh/mesher2d.cpp:2581-2760): facets are the outer bars (edges no
+ *    other element shares; MakeOuterBoundTri / Quad,
+ *    src/msh/meshkernel2d.cpp:1272-1323) in (element, edge) order; groups are
+ *    the bar arrays of Msh::ColorCodeBarAry (:1941-2018): chains in walking
+ *    order that end at a node without exactly two bars or where successive
+ *    unit directions have a dot product at most crt_dot (0.8 there);
+ *    vertex[] holds the chains' end nodes ascending (the reader's vertices)
+ *    and group_ends[2 g] / [2 g + 1] the indices into vertex[] of chain g's
+ *    first and last node (the bar array's id_se);
+ *  - ndim 3, nnoel 8 (hexahedra): no facets (the reference derives none).
+ * The reference numbers the element array 1, then the groups 2, 3, ... and
+ * (2-D) the vertices after them.  With facet == NULL it reports *nnofa (nodes
+ * per facet), *nfacet, *ngroup and *nvertex; then facet[nfacet*nnofa],
+ * group_ptr[ngroup+1], group_facet[nfacet], vertex[nvertex] and
+ * group_ends[2*ngroup] (each but facet nullable) receive them.  Node indices
+ * out of range or an element with a repeated node are DFM_ERR_INVALID. */
+DFM_API int dfm_gid_boundary(int ndim, unsigned nnode, const double* coord, int nnoel, unsigned nelem,
+                             const int* elem, double crt_dot, int* nnofa, unsigned* nfacet, unsigned* facet,
+                             unsigned* ngroup, unsigned* group_ptr, unsigned* group_facet, unsigned* nvertex,
+                             unsigned* vertex, unsigned* group_ends);
 
 /* The stored boundary matrix B of Fem::Ls::CLinearSystem_Save
  * (src/femls/linearsystem_fieldsave.cpp:64-260; pattern CMat_BlkCrs::

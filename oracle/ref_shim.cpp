@@ -11,6 +11,7 @@
 //                  MatVec::CMatDiaFrac_BlkCrs (src/matvec/matdiafrac_blkcrs.cpp:227-287, :769).
 #include "ref_shim.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <iostream>
@@ -761,6 +762,61 @@ int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned c
   return 0;
 }
 
+
+// The boundary facets the reference's GiD readers derive and store: 3-D
+// (CMesh3D), the colour-coded triangle arrays; 2-D (CMesher2D), the bar arrays
+// (chains of outer bars) and the vertices at their ends.  Facets come out
+// grouped, group by group in the readers' order, with each group's array id;
+// 2-D vertices with their node and id, and each chain's id_se as indices into
+// the vertex list.
+int dfm_ref_gid_boundary(const char* path, int want2d, unsigned cap_facet, unsigned cap_group, unsigned cap_vertex,
+                         unsigned* nfacet, unsigned* ngroup, unsigned* nvertex, unsigned* facet, unsigned* group_ptr,
+                         unsigned* group_id, unsigned* vertex, unsigned* vertex_id, unsigned* group_ends) {
+  Quiet q;
+  std::vector<unsigned> f, gp(1, 0), gid, vx, vid, ge;
+  if (want2d) {
+    Msh::CMesher2D m;
+    if (!m.ReadFromFile_GiDMsh(path)) return 1;
+    for (const Msh::SVertex& v : m.GetVertexAry()) {
+      vx.push_back(v.v);
+      vid.push_back(v.id);
+    }
+    for (const Msh::CBarAry& a : m.GetBarArySet()) {
+      for (const Msh::SBar& b : a.m_aBar) {
+        f.push_back(b.v[0]);
+        f.push_back(b.v[1]);
+      }
+      gp.push_back((unsigned)(f.size() / 2));
+      gid.push_back(a.id);
+      for (int k = 0; k < 2; k++) {
+        unsigned idx = ~0u;
+        for (size_t i = 0; i < vid.size(); i++)
+          if (vid[i] == a.id_se[k]) idx = (unsigned)i;
+        ge.push_back(idx);
+      }
+    }
+  } else {
+    Msh::CMesh3D m;
+    if (!m.ReadFromFile_GiDMsh(path)) return 1;
+    for (const Msh::CTriAry3D& a : m.GetTriArySet()) {
+      for (const Msh::STri3D& t : a.m_aTri)
+        for (int k = 0; k < 3; k++) f.push_back(t.v[k]);
+      gp.push_back((unsigned)(f.size() / 3));
+      gid.push_back(a.id);
+    }
+  }
+  *nfacet = gp.back();
+  *ngroup = (unsigned)gid.size();
+  *nvertex = (unsigned)vx.size();
+  if (!facet || *nfacet > cap_facet || *ngroup > cap_group || *nvertex > cap_vertex) return 2;
+  std::copy(f.begin(), f.end(), facet);
+  std::copy(gp.begin(), gp.end(), group_ptr);
+  std::copy(gid.begin(), gid.end(), group_id);
+  std::copy(vx.begin(), vx.end(), vertex);
+  std::copy(vid.begin(), vid.end(), vertex_id);
+  std::copy(ge.begin(), ge.end(), group_ends);
+  return 0;
+}
 
 // The stored-matrix Newmark systems through the reference's own classes
 // (src/femls/linearsystem_fieldsave.cpp:367-880).  Scheme 1:

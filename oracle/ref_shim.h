@@ -111,6 +111,9 @@ int dfm_ref_boundary_residual(unsigned N, unsigned b, const unsigned* rowptr, co
  * reference's reader returned false. */
 int dfm_ref_gid_read(const char* path, int want2d, unsigned cap_node, unsigned cap_elem, unsigned* nnode,
                      unsigned* nelem, int* nnoel, double* coord, int* elem);
+int dfm_ref_gid_boundary(const char* path, int want2d, unsigned cap_facet, unsigned cap_group, unsigned cap_vertex,
+                         unsigned* nfacet, unsigned* ngroup, unsigned* nvertex, unsigned* facet, unsigned* group_ptr,
+                         unsigned* group_id, unsigned* vertex, unsigned* vertex_id, unsigned* group_ends);
 int dfm_ref_zmat_ilu0(unsigned N, const unsigned* rowptr, const unsigned* colind,
                       const double* diag, const double* off, double* fdiag, double* foff);
 

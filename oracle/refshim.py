@@ -65,6 +65,8 @@ def lib():
         L.dfm_ref_boundary_residual.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, ip, dp, dp, C.c_uint, up, up,
                                                 dp, up, dp]
         L.dfm_ref_gid_read.argtypes = [C.c_char_p, C.c_int, C.c_uint, C.c_uint, up, up, ip, dp, ip]
+        L.dfm_ref_gid_boundary.argtypes = [C.c_char_p, C.c_int, C.c_uint, C.c_uint, C.c_uint, up, up, up, up, up, up,
+                                            up, up, up]
         L.dfm_ref_zmat_read.argtypes = [C.c_char_p, C.c_uint, up, up, up, up, dp, dp]
         L.dfm_ref_zmat_spmv.argtypes = [C.c_uint, up, up, dp, dp, C.c_double, dp, C.c_double, dp]
         L.dfm_ref_zmat_ilu0.argtypes = [C.c_uint, up, up, dp, dp, dp, dp]
@@ -250,6 +252,35 @@ def gid_read(path, want2d):
     rc = lib().dfm_ref_gid_read(p, int(want2d), nn.value, ne.value, C.byref(nn), C.byref(ne), C.byref(no),
                                 _d(coord.reshape(-1)), _i(elem.reshape(-1)))
     return rc, coord, elem
+
+
+def gid_boundary(path, want2d):
+    """The boundary facets the reference's GiD readers derive and store: a
+    dict with ``facets`` (grouped, [nfacet, 3] triangles or [nfacet, 2] bars),
+    ``groups`` (index ranges of each colour / bar array into ``facets``),
+    ``group_ids``, and for 2-D ``vertices`` (nodes), ``vertex_ids`` and
+    ``ends`` (each chain's id_se as indices into ``vertices``); None when the
+    reader refuses the file."""
+    p = os.fsencode(path)
+    nf, ng, nv = C.c_uint(), C.c_uint(), C.c_uint()
+    z = None
+    rc = lib().dfm_ref_gid_boundary(p, int(want2d), 0, 0, 0, C.byref(nf), C.byref(ng), C.byref(nv), z, z, z, z, z, z)
+    if rc == 1:
+        return None
+    k = 2 if want2d else 3
+    facet = np.zeros((max(nf.value, 1), k), np.uint32)
+    gptr = np.zeros(ng.value + 1, np.uint32)
+    gid = np.zeros(max(ng.value, 1), np.uint32)
+    vert = np.zeros(max(nv.value, 1), np.uint32)
+    vid = np.zeros(max(nv.value, 1), np.uint32)
+    ends = np.zeros((max(ng.value, 1), 2), np.uint32)
+    rc = lib().dfm_ref_gid_boundary(p, int(want2d), nf.value, ng.value, nv.value, C.byref(nf), C.byref(ng),
+                                    C.byref(nv), _u(facet.reshape(-1)), _u(gptr), _u(gid), _u(vert), _u(vid),
+                                    _u(ends.reshape(-1)))
+    assert rc == 0
+    return {"facets": facet[:nf.value], "groups": [np.arange(gptr[g], gptr[g + 1]) for g in range(ng.value)],
+            "group_ids": gid[:ng.value], "vertices": vert[:nv.value], "vertex_ids": vid[:nv.value],
+            "ends": ends[:ng.value] if want2d else np.zeros((0, 2), np.uint32)}
 
 
 def boundary_residual(N, b, rowptr, colind, diag, off, flags, force, u):

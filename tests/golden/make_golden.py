@@ -121,7 +121,8 @@ def generate_gid(path=HERE):
     """Two GiD ASCII meshes (a tetrahedral box, scaled by pi so that the
     coordinates use every digit; a triangulated square on the plane x = 0.25
     in 3-D) and what the reference's readers (Msh::CMesh3D and
-    Msh::CMesher2D ReadFromFile_GiDMsh) build from them."""
+    Msh::CMesher2D ReadFromFile_GiDMsh) build from them: nodes, elements and
+    the boundary facets they derive."""
     m = meshes.box_tet(3, 2, 2)
     f3 = os.path.join(path, "gid_box_tet.msh")
     cases.write_gid_mesh(f3, m.coord * np.pi, m.elem, "Tetrahedra")
@@ -134,8 +135,16 @@ def generate_gid(path=HERE):
     cases.write_gid_mesh(f2, p3, t.elem, "Triangle")
     rc, c2, e2 = R.gid_read(f2, want2d=True)
     assert rc == 0
+    # the boundary facets the readers derive: grouped facets, group offsets, 2-D vertices and chain ends
+    b3, b2 = R.gid_boundary(f3, want2d=False), R.gid_boundary(f2, want2d=True)
+    bnd = {}
+    for tag, b in (("tet", b3), ("tri", b2)):
+        bnd[f"{tag}_bnd_facets"] = b["facets"]
+        bnd[f"{tag}_bnd_group_ptr"] = np.cumsum([0] + [len(k) for k in b["groups"]])
+        bnd[f"{tag}_bnd_vertices"] = b["vertices"]
+        bnd[f"{tag}_bnd_ends"] = b["ends"]
     np.savez_compressed(os.path.join(path, "gidref_meshes.npz"), tet_coord=c3, tet_elem=e3, tri_coord=c2,
-                        tri_elem=e2)
+                        tri_elem=e2, **bnd)
     print(f"gid: {c3.shape[0]} nodes / {e3.shape[0]} tets, {c2.shape[0]} nodes / {e2.shape[0]} triangles")
 
 
