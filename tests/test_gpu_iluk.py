@@ -154,12 +154,15 @@ def test_iluk_limits(ctx):
         lib.solve_pcg(B, M, r, x, tol=1e-10, maxit=100, allow=(lib.OK,))
 
 
-@pytest.mark.parametrize("nring,lev", [(16, 1), (40, 1), (24, 2)])
-def test_complex_iluk_factor_and_cocg(ctx, nring, lev):
+@pytest.mark.parametrize("nring,lev,solve", [(16, 1, False), (40, 1, True), (24, 2, False), (60, 2, True)])
+def test_complex_iluk_factor_and_cocg(ctx, nring, lev, solve):
     """CZPreconditioner_ILU::SetFillInLevel(lev) on the device: the fill pattern
     and the complex factor bit-identical to the oracle (pinned to the
     reference's CZMatDiaFrac_BlkCrs), the preconditioner to 1e-11 in the range
-    schedules, and ILU(k)-COCG to 1e-8 of the oracle's x."""
+    schedules, and ILU(k)-COCG to 1e-8 of the oracle's x on the cases where
+    COCG converges (on rings 16 / lev 1 and 24 / lev 2 it stalls above 1e-10
+    for 3000 iterations, the reference's Solve_PCOCG as well, and its
+    iterates there are rounding noise)."""
     from delfem_b200 import lib
     m, Z = cases.helmholtz(nring)
     A = lib.Matrix(ctx, Z.rowptr, Z.colind, 1, lib.COMPLEX)
@@ -179,7 +182,10 @@ def test_complex_iluk_factor_and_cocg(ctx, nring, lev):
         z = torch.zeros(2 * Z.N, dtype=torch.float64, device="cuda")
         M.apply(_dev(rv), z)
         assert np.allclose(z.cpu().numpy(), ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max()), sweep
+    if not solve:
+        return
     o = Z.solve_fill((fr, fc, fdia), fd, fo, tol=1e-10, maxit=3000)
+    assert o["iters"] < 3000  # converged (Solve_PCOCG returns true at max_iter too)
     r = _dev(Z.rhs)
     x = torch.zeros_like(r)
     rc, it, conv = lib.solve_pcocg(A, M, r, x, tol=1e-10, maxit=3000)
