@@ -52,6 +52,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "delfem/ls/linearsystem.h"
@@ -219,7 +220,12 @@ struct Layout {
 
 // LsSol::CPreconditioner_ILU on the device: ILU(0), or ILU(k) after
 // SetFillInLevel(k), in the natural ordering.  It also owns the device copy of
-// the system matrix, which CLinearSystemGPU multiplies with.
+// the system matrix, which CLinearSystemGPU multiplies with.  A system of
+// several segments is factored as one joined matrix (segments one after the
+// other; one row per DOF when their block lengths differ): ILU(k) of the
+// joined matrix is the reference's segment-wise block ILU(k)
+// (src/ls/preconditioner.cpp:57-335) when every segment pair has the same
+// level, since both are the incomplete factorisation on the same fill pattern.
 class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
  public:
   explicit CPreconditioner_ILU_GPU(Context& ctx) : ctx_(&ctx) {}
@@ -227,34 +233,47 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     SetFillInLevel((int)nlev);
     SetLinearSystem(ls);
   }
-  ~CPreconditioner_ILU_GPU() override { Clear(); }
+  ~CPreconditioner_ILU_GPU() override { release(); }
   CPreconditioner_ILU_GPU(const CPreconditioner_ILU_GPU&) = delete;
   CPreconditioner_ILU_GPU& operator=(const CPreconditioner_ILU_GPU&) = delete;
 
+  // the device objects and the fill-level requests (as the reference's Clear)
   void Clear() {
-    if (ilu_) dfm_ilu_destroy(ilu_);
-    if (mat_) dfm_mat_destroy(mat_);
-    ilu_ = nullptr;
-    mat_ = nullptr;
-    tmp_r_.reset();
-    tmp_z_.reset();
+    release();
+    lev_in_.clear();
   }
-  // the fill-in level of the next SetLinearSystem (-1: no limit); ilss0 must
-  // be -1 or 0, and systems of several segments take level 0 only
+  // a fill-in level request for the next SetLinearSystem (-1: no limit), for
+  // every segment pair (ilss0 == -1) or the pairs of segment ilss0; requests
+  // apply in order, later ones over earlier ones (the reference's alev table)
   void SetFillInLevel(int lev, int ilss0 = -1) {
-    if (ilss0 != -1 && ilss0 != 0) throw Error(DFM_ERR_UNSUPPORTED, "SetFillInLevel");
-    if (lev < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
-    lev_ = lev;
+    if (lev < -1 || ilss0 < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
+    lev_in_.emplace_back(lev, ilss0);
   }
   // pattern of the (joined) system matrix on the device, fill pattern and
   // level sets
   void SetLinearSystem(const LsSol::CLinearSystem& ls) override {
-    Clear();
+    release();
     lay_.build(ls);
-    if (lay_.nseg > 1 && lev_ != 0) throw Error(DFM_ERR_UNSUPPORTED, "fill-in across segments");
+    lev_ = fill_level(lay_.nseg);
     check(dfm_mat_create(ctx_->get(), lay_.N, lay_.b, DFM_REAL, lay_.rowptr.data(), lay_.colind.data(), &mat_),
           "SetLinearSystem");
     check(dfm_ilu_create_fill(mat_, lev_, &ilu_), "SetLinearSystem");
+  }
+  // the fill level of every segment pair after the requests; different levels
+  // for different pairs are not supported
+  int fill_level(unsigned nseg) const {
+    std::vector<int> alev((size_t)nseg * nseg, 0);
+    for (const auto& r : lev_in_) {
+      if (r.second == -1) {
+        std::fill(alev.begin(), alev.end(), r.first);
+        continue;
+      }
+      if ((unsigned)r.second >= nseg) throw Error(DFM_ERR_INVALID, "SetFillInLevel: segment index");
+      for (unsigned i = 0; i < nseg; i++) alev[(size_t)i * nseg + r.second] = alev[(size_t)r.second * nseg + i] = r.first;
+    }
+    for (int v : alev)
+      if (v != alev[0]) throw Error(DFM_ERR_UNSUPPORTED, "different fill-in levels for different segment pairs");
+    return alev.empty() ? 0 : alev[0];
   }
   // the system's current values to the device and the numeric factorisation;
   // false when more than 10 pivots were singular (the reference's result)
@@ -304,9 +323,19 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   const detail::Layout& layout() const { return lay_; }
 
  private:
+  void release() {
+    if (ilu_) dfm_ilu_destroy(ilu_);
+    if (mat_) dfm_mat_destroy(mat_);
+    ilu_ = nullptr;
+    mat_ = nullptr;
+    tmp_r_.reset();
+    tmp_z_.reset();
+  }
+
   Context* ctx_;
   dfm_mat mat_ = nullptr;
   dfm_ilu ilu_ = nullptr;
+  std::vector<std::pair<int, int>> lev_in_;
   int lev_ = 0;
   detail::Layout lay_;
   std::unique_ptr<DeviceVector> tmp_r_, tmp_z_;

@@ -9,7 +9,7 @@
 //   delfem_dropin poisson N     2-D Poisson -lap u = 1 on an N x N grid of P1 triangles, u = 0 on the boundary
 //   delfem_dropin solid3d NX NY NZ   3-D linear elasticity of a box (Kuhn tetrahedra), x = 0 face clamped,
 //                                    unit body force in -z
-//   delfem_dropin twoseg N M L0 L1   a linear system of two segments built at the matrix level
+//   delfem_dropin twoseg N M L0 L1 [lev]   a linear system of two segments built at the matrix level
 //                                    (LsSol::CLinearSystem::AddLinSysSeg / AddMat_Dia / AddMat_NonDia):
 //                                    an N x N grid of L0 x L0 blocks and a chain of M nodes of L1 x L1
 //                                    blocks, coupled both ways; symmetric positive definite
@@ -336,7 +336,7 @@ struct Run {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev] | twoseg N M L0 L1\n", argv[0]);
+    std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev] | twoseg N M L0 L1 [lev]\n", argv[0]);
     return 2;
   }
   const std::string kind = argv[1];
@@ -353,6 +353,7 @@ int main(int argc, char** argv) {
     make = [&]() { return std::unique_ptr<Sys>(new Problem(kind, mesh)); };
   } else if (kind == "twoseg" && argc >= 6) {
     const unsigned n = std::atoi(argv[2]), m = std::atoi(argv[3]), l0 = std::atoi(argv[4]), l1 = std::atoi(argv[5]);
+    if (argc > 6) lev = std::atoi(argv[6]);
     make = [=]() { return std::unique_ptr<Sys>(new TwoSeg(n, m, l0, l1)); };
   } else {
     return 2;

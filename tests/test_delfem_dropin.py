@@ -50,7 +50,10 @@ CASES = [("poisson", ["poisson", "32"]), ("poisson_ilu1", ["poisson", "24", "1"]
          # two segments (LsSol::CLinearSystem::AddLinSysSeg x 2 with couplings both ways): equal block
          # lengths, and different ones (joined one row per DOF)
          ("twoseg_2_2", ["twoseg", "40", "200", "2", "2"]), ("twoseg_2_1", ["twoseg", "40", "200", "2", "1"]),
-         ("twoseg_1_3", ["twoseg", "40", "200", "1", "3"])]
+         ("twoseg_1_3", ["twoseg", "40", "200", "1", "3"]),
+         # ILU(k) across the segments: the joined matrix's ILU(k) against the reference's segment-wise one
+         ("twoseg_2_2_ilu1", ["twoseg", "40", "200", "2", "2", "1"]),
+         ("twoseg_2_1_ilu2", ["twoseg", "40", "200", "2", "1", "2"])]
 
 
 @pytest.mark.gpu
