@@ -10,8 +10,14 @@
 
 namespace dfm {
 
+// the CUDA error behind the last DFM_ERR_CUDA / DFM_ERR_NOMEM of this host
+// thread and the runtime call that returned it (a string literal)
+thread_local cudaError_t g_cuda_err = cudaSuccess;
+thread_local const char* g_cuda_what = "";
+
 int cuda_fail(cudaError_t e, const char* what) {
-  (void)what;
+  g_cuda_err = e;
+  g_cuda_what = what;
   if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); return DFM_ERR_NOMEM; }
   return DFM_ERR_CUDA;
 }
@@ -100,6 +106,11 @@ static int time_launches(cudaStream_t s, int reps, float* ms, F launch) {
 using namespace dfm;
 
 extern "C" {
+
+int dfm_last_cuda_error(char* buf, size_t n) {
+  if (buf && n) std::snprintf(buf, n, "%s: %s", g_cuda_what, cudaGetErrorName(g_cuda_err));
+  return (int)g_cuda_err;
+}
 
 const char* dfm_status_string(int s) {
   switch (s) {

@@ -61,6 +61,7 @@ PROTOS = {
     "dfm_time_spmv": (_i, [_vp, _vp, _vp, _i, C.POINTER(C.c_float)]),
     "dfm_zmat_read_text": (_i, [C.c_char_p, _up, _up, _up, _up, _dp, _dp]),
     "dfm_gid_read_mesh": (_i, [C.c_char_p, _ip, _up, _dp, _ip, _up, _ip]),
+    "dfm_last_cuda_error": (_i, [C.c_char_p, C.c_size_t]),
     "dfm_gid_boundary": (_i, [_i, _u, _dp, _i, _u, _ip, _d, _ip, _up, _up, _up, _up, _up, _up, _up, _up]),
     "dfm_mat_zero_rows": (_i, [_vp, _vp]),
     "dfm_rmat_create": (_i, [_vp, _u, _u, _u, _u, _up, _up, C.POINTER(_vp)]),
@@ -120,6 +121,10 @@ class DfmError(RuntimeError):
     def __init__(self, code: int, where: str = ""):
         self.code = code
         msg = lib().dfm_status_string(code).decode() if _lib is not None else str(code)
+        if _lib is not None and code in (ERR_CUDA, ERR_NOMEM):  # the runtime call and its error
+            buf = C.create_string_buffer(256)
+            if _lib.dfm_last_cuda_error(buf, 256):
+                msg += f" [{buf.value.decode(errors='replace')}]"
         super().__init__(f"{where}: {msg} ({code})")
 
 

@@ -62,6 +62,11 @@ typedef struct dfm_batch_s* dfm_batch;
 typedef struct dfm_rmat_s* dfm_rmat;
 
 DFM_API const char* dfm_status_string(int status);
+/* The CUDA error code behind this host thread's last DFM_ERR_CUDA or
+ * DFM_ERR_NOMEM (cudaSuccess if none), with "<runtime call>: <error name>"
+ * written to buf[n] (nullable).  No reference counterpart: the reference has
+ * no device code. */
+DFM_API int dfm_last_cuda_error(char* buf, size_t n);
 DFM_API int dfm_abi_version(void);
 
 /* ---- context: device, stream, device status word ---------------------- */

@@ -120,7 +120,8 @@ struct Layout {
   }
 
   // pattern (always) and values (with_values) of the joined matrix, row by row
-  // in ascending columns
+  // in ascending columns; the pattern pass reads no values (a CLinearSystem
+  // has none before its first InitializeMarge)
   void walk(const LsSol::CLinearSystem& ls, bool with_values, std::vector<double>& diag, std::vector<double>& off) {
     std::vector<unsigned>& rp = rowptr;
     std::vector<unsigned>& ci = colind;
@@ -155,7 +156,7 @@ struct Layout {
               auto put_dia = [&]() {  // the rest of the diagonal block (scalar rows only)
                 for (unsigned e = 0; e < Li; e++)
                   if (e != d) {
-                    double v = dia[d * Li + e];
+                    const double v = with_values ? dia[d * Li + e] : 0.0;
                     put((unsigned)(dof0[i] + (size_t)p * Li + e), &v);
                   }
                 dia_done = true;
@@ -167,7 +168,7 @@ struct Layout {
                   put((unsigned)(dof0[i] / b + c), dval + (size_t)t * bb);
                 } else {
                   for (unsigned e = 0; e < Li; e++) {
-                    double v = dval[(size_t)t * Li * Li + d * Li + e];
+                    const double v = with_values ? dval[(size_t)t * Li * Li + d * Li + e] : 0.0;
                     put((unsigned)(dof0[i] + (size_t)c * Li + e), &v);
                   }
                 }
@@ -184,7 +185,7 @@ struct Layout {
                   put((unsigned)(dof0[j] / b + ccol[t]), cval + (size_t)t * bb);
                 } else {
                   for (unsigned e = 0; e < Lj; e++) {
-                    double v = cval[(size_t)t * Li * Lj + d * Lj + e];
+                    const double v = with_values ? cval[(size_t)t * Li * Lj + d * Lj + e] : 0.0;
                     put((unsigned)(dof0[j] + (size_t)ccol[t] * Lj + e), &v);
                   }
                 }
