@@ -153,7 +153,17 @@ int dfm_ctx_create(int device, dfm_ctx* out) {
 }
 
 int dfm_ctx_destroy(dfm_ctx c) {
-  if (!c) return DFM_OK;
+  if (c) ctx_release(c);
+  return DFM_OK;
+}
+
+}  // extern "C"
+
+namespace dfm {
+void ctx_retain(dfm_ctx c) { c->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void ctx_release(dfm_ctx c) {
+  if (c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
   cudaSetDevice(c->device);
   if (c->own) cudaStreamSynchronize(c->own);
   cudaFree(c->d_status);
@@ -162,8 +172,10 @@ int dfm_ctx_destroy(dfm_ctx c) {
   if (c->h_scal) cudaFreeHost(c->h_scal);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
-  return DFM_OK;
 }
+}  // namespace dfm
+
+extern "C" {
 
 int dfm_ctx_set_stream(dfm_ctx c, void* stream) {
   if (!c) return DFM_ERR_INVALID;
@@ -276,6 +288,7 @@ int dfm_mat_create(dfm_ctx c, unsigned N, unsigned b, int vt, const unsigned* ro
   dfm_mat A = new (std::nothrow) dfm_mat_s();
   if (!A) return DFM_ERR_NOMEM;
   A->ctx = c;
+  ctx_retain(c);
   A->N = N;
   A->b = b;
   A->vt = vt;
@@ -307,7 +320,9 @@ int dfm_mat_destroy(dfm_mat A) {
   cudaFree(A->d_diag32);
   cudaFree(A->d_off32);
   spmv_free_tiles(A);
+  dfm_ctx c = A->ctx;
   delete A;
+  ctx_release(c);
   return DFM_OK;
 }
 
@@ -401,6 +416,7 @@ int dfm_ilu_create(dfm_mat A, dfm_ilu* out) {
   dfm_ilu M = new (std::nothrow) dfm_ilu_s();
   if (!M) return DFM_ERR_NOMEM;
   M->ctx = A->ctx;
+  ctx_retain(M->ctx);
   M->A = A;
   M->user = A;
   M->N = A->N;
@@ -458,7 +474,9 @@ int dfm_ilu_destroy(dfm_ilu M) {
   cudaFree(M->d_tmp);
   cudaFree(M->d_fillmap);
   if (M->fillpat) dfm_mat_destroy(M->fillpat);
+  dfm_ctx c = M->ctx;
   delete M;
+  ctx_release(c);
   return DFM_OK;
 }
 

@@ -463,6 +463,7 @@ int dfm_mesh_create(dfm_ctx c, int ndim, unsigned nnode, const double* coord, un
   dfm_mesh G = new (std::nothrow) dfm_mesh_s();
   if (!G) return DFM_ERR_NOMEM;
   G->ctx = c;
+  ctx_retain(c);
   G->ndim = ndim;
   G->nnode = nnode;
   G->nnoel = nnoel;
@@ -532,7 +533,9 @@ int dfm_mesh_destroy(dfm_mesh G) {
   cudaFree(G->d_esup);
   cudaFree(G->d_bsup_ptr);
   cudaFree(G->d_bsup);
+  dfm_ctx c = G->ctx;
   delete G;
+  ctx_release(c);
   return DFM_OK;
 }
 

@@ -862,6 +862,7 @@ int dfm_batch_create(dfm_ilu M, unsigned ninst, const unsigned* row_off, dfm_bat
   dfm_batch B = new (std::nothrow) dfm_batch_s();
   if (!B) return DFM_ERR_NOMEM;
   B->ctx = A->ctx;
+  ctx_retain(B->ctx);
   B->A = A;
   B->M = M;
   B->ninst = ninst;
@@ -903,7 +904,9 @@ int dfm_batch_destroy(dfm_batch B) {
     cudaFree(v);
   if (B->h_scal) cudaFreeHost(B->h_scal);
   if (B->h_ndone) cudaFreeHost(B->h_ndone);
+  dfm_ctx c = B->ctx;
   delete B;
+  ctx_release(c);
   return DFM_OK;
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -19,6 +20,8 @@
 namespace dfm {
 
 int cuda_fail(cudaError_t e, const char* what);
+void ctx_retain(dfm_ctx c);
+void ctx_release(dfm_ctx c);
 int take_code(dfm_ctx c);
 // Host (DFM_HOST, then synchronises) or device source -> device memory.
 int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t s);
@@ -66,6 +69,10 @@ struct SpmvTiles {
 
 struct dfm_ctx_s;
 struct dfm_ctx_s {
+  // one reference for the caller's handle and one per object created on the
+  // context; dfm_ctx_destroy drops the caller's, the last one frees it (so
+  // objects may outlive the handle and be destroyed in any order)
+  std::atomic<int> refs{1};
   int device = 0;
   int nsm = 148;
   cudaStream_t own = nullptr;

@@ -127,6 +127,7 @@ int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out) {
   if (!P) return DFM_ERR_NOMEM;
   dfm_ctx c = A->ctx;
   P->ctx = c;
+  ctx_retain(c);
   P->N = A->N;
   P->b = A->b;
   P->vt = A->vt;

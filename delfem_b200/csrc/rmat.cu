@@ -105,6 +105,7 @@ int dfm_rmat_create(dfm_ctx ctx, unsigned nrow, unsigned ncol, unsigned brow, un
   dfm_rmat R = new (std::nothrow) dfm_rmat_s();
   if (!R) return DFM_ERR_NOMEM;
   R->ctx = ctx;
+  ctx_retain(ctx);
   R->nrow = nrow;
   R->ncol = ncol;
   R->brow = brow;
@@ -119,10 +120,7 @@ int dfm_rmat_create(dfm_ctx ctx, unsigned nrow, unsigned ncol, unsigned brow, un
   if (!rc && R->nnz) rc = copy_in(R->d_colind, colind, sizeof(unsigned) * R->nnz, DFM_HOST, ctx->stream);
   if (!rc && cudaMemsetAsync(R->d_val, 0, sizeof(double) * nval, ctx->stream) != cudaSuccess) rc = DFM_ERR_CUDA;
   if (rc) {
-    cudaFree(R->d_rowptr);
-    cudaFree(R->d_colind);
-    cudaFree(R->d_val);
-    delete R;
+    dfm_rmat_destroy(R);
     return rc;
   }
   *out = R;
@@ -131,11 +129,13 @@ int dfm_rmat_create(dfm_ctx ctx, unsigned nrow, unsigned ncol, unsigned brow, un
 
 int dfm_rmat_destroy(dfm_rmat R) {
   if (!R) return DFM_OK;
+  dfm_ctx ctx = R->ctx;
   cudaStreamSynchronize(R->ctx->stream);
   cudaFree(R->d_rowptr);
   cudaFree(R->d_colind);
   cudaFree(R->d_val);
   delete R;
+  ctx_release(ctx);
   return DFM_OK;
 }
 

@@ -105,6 +105,135 @@ DFM_DEVINL void halo_dot(const double* __restrict__ rdot, const double* X, unsig
   }
 }
 
+// What a lane needs of one row that does not depend on the level before it:
+// the row descriptor, its first two blocks and their operand offsets, and for
+// the lanes that finish components (lane c takes components c, c + LPR, ...)
+// the row's right-hand side and (forward) those rows of its D^-1.  Loaded
+// ahead, before the previous level's barrier where the stage is ready, so
+// that only the reads of X follow that barrier.
+template <int B, int LPR, typename TV>
+struct RowPre {
+  static constexpr int NC = (B + LPR - 1) / LPR;  // components per finishing lane
+  uint4 rd;
+  unsigned o0, o1;
+  bool h0, h1;
+  TV m0[B * B], m1[B * B];
+  double xr[B], dr[NC][B];
+};
+
+template <int B, int LPR, typename TV, bool FWD>
+DFM_DEVINL void row_prefetch(RowPre<B, LPR, TV>& P, const char* sb, const double* X, unsigned r, int lane) {
+  constexpr int BB = B * B;
+  const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
+  const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+  const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+  P.rd = reinterpret_cast<const uint4*>(sb + 32)[r];
+  const unsigned k0 = P.rd.y + (unsigned)lane, k1 = k0 + LPR;
+  P.h0 = k0 < P.rd.z;
+  P.h1 = k1 < P.rd.z;
+  if (P.h0) {
+    P.o0 = xoff[k0];
+#pragma unroll
+    for (int e = 0; e < BB; e++) P.m0[e] = vals[(size_t)k0 * BB + e];
+  }
+  if (P.h1) {
+    P.o1 = xoff[k1];
+#pragma unroll
+    for (int e = 0; e < BB; e++) P.m1[e] = vals[(size_t)k1 * BB + e];
+  }
+  if (lane < B) {
+    const double* xi = X + (size_t)P.rd.x * B;  // the row's right-hand side: only this row writes it
+#pragma unroll
+    for (int c = 0; c < B; c++) P.xr[c] = xi[c];
+    if (FWD) {
+      const double* d = reinterpret_cast<const double*>(sb + hdr->dinv) + (size_t)r * BB;
+#pragma unroll
+      for (int j = 0; j < P.NC; j++) {
+        const int cc = lane + j * LPR;
+        if (cc < B)
+#pragma unroll
+          for (int c = 0; c < B; c++) P.dr[j][c] = d[cc * B + c];
+      }
+    }
+  }
+}
+
+// One row from its prefetched part: the operand reads, the lane sums (blocks
+// kk, kk + LPR, ... in order), the butterfly over the row's lanes (every lane
+// ends with the same sum), then lane c finishes components c, c + LPR, ... < B:
+// x_i[c] = (D^-1 (b_i - sum))[c] forward, (b_i - sum)[c] backward, into the
+// slice and published to `out`.  The same operations in the same order as
+// the reference's row loop (up to the lanes' summation order).
+template <int B, int LPR, typename TV, bool FWD>
+DFM_DEVINL void row_finish(const RowPre<B, LPR, TV>& P, const char* sb, double* X, double* out, int lane,
+                           unsigned gmask) {
+  constexpr int BB = B * B;
+  double acc[B];
+#pragma unroll
+  for (int c = 0; c < B; c++) acc[c] = 0.0;
+  if (P.h0) {
+    double x0[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) x0[c] = X[P.o0 + c];
+#pragma unroll
+    for (int rr = 0; rr < B; rr++)
+#pragma unroll
+      for (int c = 0; c < B; c++) acc[rr] += (double)P.m0[rr * B + c] * x0[c];
+  }
+  if (P.h1) {
+    double x1[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) x1[c] = X[P.o1 + c];
+#pragma unroll
+    for (int rr = 0; rr < B; rr++)
+#pragma unroll
+      for (int c = 0; c < B; c++) acc[rr] += (double)P.m1[rr * B + c] * x1[c];
+  }
+  if (P.h1) {  // rows with more than 2 LPR blocks
+    const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
+    const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
+    const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+    for (unsigned kk = P.rd.y + (unsigned)lane + 2 * LPR; kk < P.rd.z; kk += LPR) {
+      const unsigned o = xoff[kk];
+      const TV* m = vals + (size_t)kk * BB;
+#pragma unroll
+      for (int rr = 0; rr < B; rr++)
+#pragma unroll
+        for (int c = 0; c < B; c++) acc[rr] += (double)m[rr * B + c] * X[o + c];
+    }
+  }
+  if (LPR > 1) {
+#pragma unroll
+    for (int rr = 0; rr < B; rr++)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
+  }
+  if (lane < B) {
+    double t[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) t[c] = P.xr[c] - acc[c];
+#pragma unroll
+    for (int j = 0; j < P.NC; j++) {
+      const int cc = lane + j * LPR;
+      if (cc < B) {
+        double v;
+        if (FWD) {
+          v = 0.0;
+#pragma unroll
+          for (int c = 0; c < B; c++) v += P.dr[j][c] * t[c];
+        } else {
+          v = t[0];
+#pragma unroll
+          for (int c = 1; c < B; c++)
+            if (c == cc) v = t[c];
+        }
+        X[(size_t)P.rd.x * B + cc] = v;
+        st_relaxed(out + (size_t)P.rd.w * B + cc, v);
+      }
+    }
+  }
+}
+
 template <int B, int LPR, typename TV, bool FWD, int DOT>
 __global__ void __launch_bounds__(kHaloMaxThreads, 1)
 k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
@@ -112,7 +241,6 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
              unsigned stage_bytes, int nstage, unsigned x_bytes, unsigned x_slice, unsigned halo_stride, int ncw,
              const double* __restrict__ in, double* out, const double* __restrict__ rdot, double* part,
              KrylovScalars* sc, const double* rr_part, int rr_nparts, DevStatus* st, uint64_t wait_ns) {
-  constexpr int BB = B * B;
   extern __shared__ __align__(128) char smem[];
   __shared__ int s_alive;
   __shared__ int s_released;               // chunks the compute warps are done with
@@ -236,6 +364,7 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
         for (int c = 0; c < B; c++) H[e * B + c] = v[c];
       }
       if (!__all_sync(0xffffffffu, ok)) break;
+      __syncwarp();  // every lane's halo stores precede lane 0's release
       if (wl == 0) {
         __threadfence_block();
         st_volatile_i(&s_ready[s], (int)k);
@@ -248,26 +377,27 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
     const unsigned g = threadIdx.x / LPR, ng = (unsigned)nct / LPR;
     const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) / LPR * LPR));
     bool alive = true;
+    RowPre<B, LPR, TV> pre;
+    bool have_pre = false;     // pre holds row g of chunk k (loaded before chunk k-1's barrier)
+    unsigned s = 0, par = 0;   // chunk k's stage and that stage's phase parity
     for (unsigned k = 0; k < K; k++) {
-      const int s = (int)(k % (unsigned)nstage);
-      if (alive && ld_volatile_i(&s_ready[s]) != (int)k) {
-        SpinGuard gd(wait_ns);
-        while (ld_volatile_i(&s_ready[s]) != (int)k) {
-          if (!ld_volatile_i(&s_alive)) { alive = false; break; }
-          if (gd.expired()) {
-            raise_error(st, DFM_WAIT_TIMEOUT, 23);
-            st_volatile_i(&s_alive, 0);
-            alive = false;
-            break;
+      const char* sb = stages + (size_t)s * stage_bytes;
+      if (!have_pre) {
+        // wait until the producer marked the stage ready for chunk k, then
+        // acquire the stage's copy (its phase has completed: a probe suffices)
+        if (alive && ld_acquire_cta(&s_ready[s]) != (int)k) {
+          SpinGuard gd(wait_ns);
+          while (ld_acquire_cta(&s_ready[s]) != (int)k) {
+            if (!ld_volatile_i(&s_alive)) { alive = false; break; }
+            if (gd.expired()) {
+              raise_error(st, DFM_WAIT_TIMEOUT, 23);
+              st_volatile_i(&s_alive, 0);
+              alive = false;
+              break;
+            }
           }
         }
-      }
-      __threadfence_block();
-      const char* sb = stages + (size_t)s * stage_bytes;
-      if (alive) {
-        // the stage's copy completed (observed by its producer): acquire it here too
-        const unsigned par = (k / (unsigned)nstage) & 1u;
-        if (!mbar_try_wait(&bar[s], par)) {
+        if (alive && !mbar_test_wait(&bar[s], par)) {
           SpinGuard gd(wait_ns);
           while (!mbar_try_wait(&bar[s], par))
             if (gd.expired()) {
@@ -277,87 +407,40 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
               break;
             }
         }
+        alive = __all_sync(0xffffffffu, alive);  // the lanes of a row's group agree
+        if (alive && g < reinterpret_cast<const HaloHeader*>(sb)->nrows)
+          row_prefetch<B, LPR, TV, FWD>(pre, sb, X, g, lane);
       }
-      alive = __all_sync(0xffffffffu, alive);  // the lanes of a row's group agree
       if (alive) {
-        const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
-        const unsigned nrows = hdr->nrows;
-        const uint4* rdesc = reinterpret_cast<const uint4*>(sb + 32);
-        const unsigned* xoff = reinterpret_cast<const unsigned*>(sb + hdr->xoff);
-        const TV* vals = reinterpret_cast<const TV*>(sb + hdr->vals);
+        const unsigned nrows = reinterpret_cast<const HaloHeader*>(sb)->nrows;
         for (unsigned r = g; r < nrows; r += ng) {
-          const uint4 rd = rdesc[r];
-          double acc[B];
-#pragma unroll
-          for (int c = 0; c < B; c++) acc[c] = 0.0;
-          unsigned kk = rd.y + (unsigned)lane;
-          for (; kk + LPR < rd.z; kk += 2 * LPR) {  // two operands in flight per lane
-            const unsigned o0 = xoff[kk], o1 = xoff[kk + LPR];
-            double x0[B], x1[B];
-#pragma unroll
-            for (int c = 0; c < B; c++) {
-              x0[c] = X[o0 + c];
-              x1[c] = X[o1 + c];
-            }
-            const TV* m0 = vals + (size_t)kk * BB;
-            const TV* m1 = vals + (size_t)(kk + LPR) * BB;
-#pragma unroll
-            for (int rr = 0; rr < B; rr++)
-#pragma unroll
-              for (int c = 0; c < B; c++) acc[rr] += (double)m0[rr * B + c] * x0[c];
-#pragma unroll
-            for (int rr = 0; rr < B; rr++)
-#pragma unroll
-              for (int c = 0; c < B; c++) acc[rr] += (double)m1[rr * B + c] * x1[c];
-          }
-          if (kk < rd.z) {
-            const unsigned o0 = xoff[kk];
-            const TV* m0 = vals + (size_t)kk * BB;
-#pragma unroll
-            for (int rr = 0; rr < B; rr++)
-#pragma unroll
-              for (int c = 0; c < B; c++) acc[rr] += (double)m0[rr * B + c] * X[o0 + c];
-          }
-          if (LPR > 1) {
-#pragma unroll
-            for (int rr = 0; rr < B; rr++)
-#pragma unroll
-              for (int o = LPR / 2; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(gmask, acc[rr], o);
-          }
-          if (lane == 0) {
-            double* xi = X + (size_t)rd.x * B;
-            double t[B];
-#pragma unroll
-            for (int rr = 0; rr < B; rr++) t[rr] = xi[rr] - acc[rr];
-            double o[B];
-            if (FWD) {
-              const double* d = reinterpret_cast<const double*>(sb + hdr->dinv) + (size_t)r * BB;
-#pragma unroll
-              for (int rr = 0; rr < B; rr++) {
-                double v = 0.0;
-#pragma unroll
-                for (int c = 0; c < B; c++) v += d[rr * B + c] * t[c];
-                o[rr] = v;
-              }
-            } else {
-#pragma unroll
-              for (int rr = 0; rr < B; rr++) o[rr] = t[rr];
-            }
-#pragma unroll
-            for (int rr = 0; rr < B; rr++) {
-              xi[rr] = o[rr];
-              st_relaxed(out + (size_t)rd.w * B + rr, o[rr]);
-            }
-          }
+          if (r != g) row_prefetch<B, LPR, TV, FWD>(pre, sb, X, r, lane);
+          row_finish<B, LPR, TV, FWD>(pre, sb, X, out, lane, gmask);
+        }
+      }
+      // look ahead: chunk k + 1's first row, if the producer already made its
+      // stage ready (nothing is waited for here)
+      unsigned s1 = s + 1, par1 = par;
+      if (s1 == (unsigned)nstage) {
+        s1 = 0;
+        par1 ^= 1u;
+      }
+      have_pre = false;
+      if (alive && k + 1 < K) {
+        bool rdy = ld_acquire_cta(&s_ready[s1]) == (int)(k + 1) && mbar_test_wait(&bar[s1], par1);
+        rdy = __all_sync(0xffffffffu, rdy);
+        if (rdy) {
+          const char* sb1 = stages + (size_t)s1 * stage_bytes;
+          if (g < reinterpret_cast<const HaloHeader*>(sb1)->nrows) row_prefetch<B, LPR, TV, FWD>(pre, sb1, X, g, lane);
+          have_pre = true;
         }
       }
       // every compute warp passes every level's barrier, alive or not
       if (ncw > 1) compute_barrier(nct);
       else __syncwarp();
-      if (threadIdx.x == 0) {
-        __threadfence_block();
-        st_volatile_i(&s_released, (int)k + 1);
-      }
+      if (threadIdx.x == 0) st_release_cta(&s_released, (int)k + 1);
+      s = s1;
+      par = par1;
     }
   }
   __syncthreads();

@@ -71,6 +71,10 @@ DFM_API int dfm_abi_version(void);
 
 /* ---- context: device, stream, device status word ---------------------- */
 DFM_API int dfm_ctx_create(int device, dfm_ctx* out);
+/* Releases the caller's handle.  Every matrix, ILU, mesh, batch and
+ * rectangular matrix created on the context holds it too, so they may be
+ * destroyed before or after it, in any order; the context's stream and
+ * buffers go with the last of them. */
 DFM_API int dfm_ctx_destroy(dfm_ctx ctx);
 /* Issue work on `stream` (a cudaStream_t; NULL restores the context's own). */
 DFM_API int dfm_ctx_set_stream(dfm_ctx ctx, void* stream);
