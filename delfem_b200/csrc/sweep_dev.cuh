@@ -31,26 +31,6 @@ DFM_DEVINL bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Non-blocking probe of the same phase (no suspend hint): true once it completed.
-DFM_DEVINL bool mbar_test_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, "
-      "p;\n}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// CTA-scope acquire load / release store of a shared-memory flag.
-DFM_DEVINL int ld_acquire_cta(const int* p) {
-  int v;
-  asm volatile("ld.acquire.cta.shared::cta.s32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)) : "memory");
-  return v;
-}
-DFM_DEVINL void st_release_cta(int* p, int v) {
-  asm volatile("st.release.cta.shared::cta.s32 [%0], %1;" ::"r"(smem_addr(p)), "r"(v) : "memory");
-}
 // 1-D bulk copy global -> this CTA's shared memory (addresses and size 16-byte multiples).
 DFM_DEVINL void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(

@@ -379,15 +379,15 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
     bool alive = true;
     RowPre<B, LPR, TV> pre;
     bool have_pre = false;     // pre holds row g of chunk k (loaded before chunk k-1's barrier)
-    unsigned s = 0, par = 0;   // chunk k's stage and that stage's phase parity
+    unsigned nrows = 0;        // chunk k's rows, read with the look-ahead
+    unsigned s = 0;            // chunk k's stage
     for (unsigned k = 0; k < K; k++) {
       const char* sb = stages + (size_t)s * stage_bytes;
       if (!have_pre) {
-        // wait until the producer marked the stage ready for chunk k, then
-        // acquire the stage's copy (its phase has completed: a probe suffices)
-        if (alive && ld_acquire_cta(&s_ready[s]) != (int)k) {
+        // wait until the producer marked the stage ready for chunk k
+        if (alive && ld_volatile_i(&s_ready[s]) != (int)k) {
           SpinGuard gd(wait_ns);
-          while (ld_acquire_cta(&s_ready[s]) != (int)k) {
+          while (ld_volatile_i(&s_ready[s]) != (int)k) {
             if (!ld_volatile_i(&s_alive)) { alive = false; break; }
             if (gd.expired()) {
               raise_error(st, DFM_WAIT_TIMEOUT, 23);
@@ -397,22 +397,14 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
             }
           }
         }
-        if (alive && !mbar_test_wait(&bar[s], par)) {
-          SpinGuard gd(wait_ns);
-          while (!mbar_try_wait(&bar[s], par))
-            if (gd.expired()) {
-              raise_error(st, DFM_WAIT_TIMEOUT, 24);
-              st_volatile_i(&s_alive, 0);
-              alive = false;
-              break;
-            }
-        }
+        // the stage's copy landed before the producer released the flag (it
+        // waited for the copy's mbarrier phase), so the fence suffices here
+        __threadfence_block();
         alive = __all_sync(0xffffffffu, alive);  // the lanes of a row's group agree
-        if (alive && g < reinterpret_cast<const HaloHeader*>(sb)->nrows)
-          row_prefetch<B, LPR, TV, FWD>(pre, sb, X, g, lane);
+        nrows = alive ? reinterpret_cast<const HaloHeader*>(sb)->nrows : 0u;
+        if (g < nrows) row_prefetch<B, LPR, TV, FWD>(pre, sb, X, g, lane);
       }
       if (alive) {
-        const unsigned nrows = reinterpret_cast<const HaloHeader*>(sb)->nrows;
         for (unsigned r = g; r < nrows; r += ng) {
           if (r != g) row_prefetch<B, LPR, TV, FWD>(pre, sb, X, r, lane);
           row_finish<B, LPR, TV, FWD>(pre, sb, X, out, lane, gmask);
@@ -420,27 +412,26 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
       }
       // look ahead: chunk k + 1's first row, if the producer already made its
       // stage ready (nothing is waited for here)
-      unsigned s1 = s + 1, par1 = par;
-      if (s1 == (unsigned)nstage) {
-        s1 = 0;
-        par1 ^= 1u;
-      }
+      const unsigned s1 = s + 1 == (unsigned)nstage ? 0u : s + 1;
       have_pre = false;
       if (alive && k + 1 < K) {
-        bool rdy = ld_acquire_cta(&s_ready[s1]) == (int)(k + 1) && mbar_test_wait(&bar[s1], par1);
+        bool rdy = ld_volatile_i(&s_ready[s1]) == (int)(k + 1);
+        __threadfence_block();
         rdy = __all_sync(0xffffffffu, rdy);
         if (rdy) {
-          const char* sb1 = stages + (size_t)s1 * stage_bytes;
-          if (g < reinterpret_cast<const HaloHeader*>(sb1)->nrows) row_prefetch<B, LPR, TV, FWD>(pre, sb1, X, g, lane);
+          nrows = reinterpret_cast<const HaloHeader*>(stages + (size_t)s1 * stage_bytes)->nrows;
+          if (g < nrows) row_prefetch<B, LPR, TV, FWD>(pre, stages + (size_t)s1 * stage_bytes, X, g, lane);
           have_pre = true;
         }
       }
       // every compute warp passes every level's barrier, alive or not
       if (ncw > 1) compute_barrier(nct);
       else __syncwarp();
-      if (threadIdx.x == 0) st_release_cta(&s_released, (int)k + 1);
+      if (threadIdx.x == 0) {
+        __threadfence_block();
+        st_volatile_i(&s_released, (int)k + 1);
+      }
       s = s1;
-      par = par1;
     }
   }
   __syncthreads();
