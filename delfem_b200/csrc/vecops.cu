@@ -49,6 +49,14 @@ __global__ void __launch_bounds__(kVecOpThreads) k_vec_scal(size_t n, double alp
   VEC_LOOP(k, n) x[k] = __dmul_rn(x[k], alpha);
 }
 
+// y[i] := x[idx[i]] block by block (b doubles per block): a vector into or
+// out of a block ordering (COrdering_Blk::OrderingVector_OldToNew / _NewToOld)
+__global__ void __launch_bounds__(kVecOpThreads)
+k_vec_gather(size_t nblk, unsigned b, const unsigned* __restrict__ idx, const double* __restrict__ x,
+             double* __restrict__ y) {
+  VEC_LOOP(k, nblk * b) y[k] = x[(size_t)idx[k / b] * b + k % b];
+}
+
 }  // namespace dfm
 
 using namespace dfm;
@@ -86,6 +94,14 @@ int dfm_vec_scal(dfm_ctx ctx, size_t n, double alpha, double* x) {
   if (!ctx || (n && !x)) return DFM_ERR_INVALID;
   if (n == 0) return DFM_OK;
   k_vec_scal<<<vecop_grid(n), kVecOpThreads, 0, ctx->stream>>>(n, alpha, x);
+  DFM_CUDA_TRY(cudaGetLastError());
+  return DFM_OK;
+}
+
+int dfm_vec_gather(dfm_ctx ctx, size_t nblk, unsigned b, const unsigned* idx, const double* x, double* y) {
+  if (!ctx || b < 1 || (nblk && (!idx || !x || !y)) || (const double*)y == x) return DFM_ERR_INVALID;
+  if (nblk == 0) return DFM_OK;
+  k_vec_gather<<<vecop_grid(nblk * b), kVecOpThreads, 0, ctx->stream>>>(nblk, b, idx, x, y);
   DFM_CUDA_TRY(cudaGetLastError());
   return DFM_OK;
 }

@@ -46,6 +46,7 @@ PROTOS = {
     "dfm_vec_copy": (_i, [_vp, C.c_size_t, _vp, _vp]),
     "dfm_vec_scal": (_i, [_vp, C.c_size_t, _d, _vp]),
     "dfm_vec_axpy": (_i, [_vp, C.c_size_t, _d, _vp, _vp]),
+    "dfm_vec_gather": (_i, [_vp, C.c_size_t, _u, _vp, _vp, _vp]),
     "dfm_mat_create": (_i, [_vp, _u, _u, _i, _up, _up, C.POINTER(_vp)]),
     "dfm_mat_destroy": (_i, [_vp]),
     "dfm_mat_info": (_i, [_vp, _up, _up, _up, _ip]),
@@ -731,6 +732,13 @@ def vec_dot(ctx: Context, x, y) -> float:
     _sync_torch()
     check(lib().dfm_vec_dot(ctx.h, x.numel(), _ptr(x), _ptr(y), C.byref(out)), "dfm_vec_dot")
     return out.value
+
+
+def vec_gather(ctx, b, idx, x, y):
+    """y[i b + c] := x[idx[i] b + c] (dfm_vec_gather): idx a device uint32
+    tensor of block indices, x and y device float64 tensors."""
+    _sync_torch()
+    check(lib().dfm_vec_gather(ctx.h, idx.numel(), int(b), _ptr(idx), _ptr(x), _ptr(y)), "dfm_vec_gather")
 
 
 def vec_axpy(ctx: Context, alpha: float, x, y):

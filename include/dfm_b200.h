@@ -111,6 +111,12 @@ DFM_API int dfm_vec_dot(dfm_ctx ctx, size_t n, const double* x, const double* y,
 DFM_API int dfm_vec_copy(dfm_ctx ctx, size_t n, const double* x, double* y);          /* y := x */
 DFM_API int dfm_vec_scal(dfm_ctx ctx, size_t n, double alpha, double* x);             /* x := alpha x */
 DFM_API int dfm_vec_axpy(dfm_ctx ctx, size_t n, double alpha, const double* x, double* y); /* y += alpha x */
+/* y[i b + c] := x[idx[i] b + c] for the nblk blocks of b doubles (idx a
+ * device array of nblk block indices, y not aliasing x): a vector into or out
+ * of a block ordering, as COrdering_Blk::OrderingVector_OldToNew / _NewToOld
+ * (src/matvec/ordering_blk.cpp:136-170) with idx the new-to-old or the
+ * old-to-new map.  Enqueued on the context's stream. */
+DFM_API int dfm_vec_gather(dfm_ctx ctx, size_t nblk, unsigned b, const unsigned* idx, const double* x, double* y);
 
 /* ---- matrix: CMatDia_BlkCrs on the device ------------------------------ */
 /* Pattern from host arrays; validated (monotone rowptr, in-range, strictly

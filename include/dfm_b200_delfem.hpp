@@ -58,6 +58,7 @@
 #include "delfem/ls/linearsystem.h"
 #include "delfem/ls/linearsystem_interface_solver.h"
 #include "delfem/ls/preconditioner.h"
+#include "delfem/ls/solver_ls_iter.h"
 #include "delfem/matvec/mat_blkcrs.h"
 #include "delfem/matvec/matdia_blkcrs.h"
 #include "delfem/matvec/vector_blk.h"
@@ -243,6 +244,13 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     release();
     lev_in_.clear();
   }
+  // CPreconditioner_ILU::SetOrdering (include/delfem/ls/preconditioner.h:93-97):
+  // for the next SetLinearSystem, factor the system with its block rows and
+  // columns renumbered, aind[new] = old (COrdering_Blk); empty: off.  As the
+  // reference's ordered path (src/ls/preconditioner.cpp:60-82, 224-229,
+  // 305-311) it is ILU(0) of one segment, whatever the fill level.
+  void SetOrdering(const std::vector<int>& aind) { order_ = aind; }
+  bool ordered() const { return !order_.empty(); }
   // a fill-in level request for the next SetLinearSystem (-1: no limit), for
   // every segment pair (ilss0 == -1) or the pairs of segment ilss0; requests
   // apply in order, later ones over earlier ones (the reference's alev table)
@@ -258,7 +266,12 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     lev_ = fill_level(lay_.nseg);
     check(dfm_mat_create(ctx_->get(), lay_.N, lay_.b, DFM_REAL, lay_.rowptr.data(), lay_.colind.data(), &mat_),
           "SetLinearSystem");
-    check(dfm_ilu_create_fill(mat_, lev_, &ilu_), "SetLinearSystem");
+    if (ordered()) {
+      make_ordered();
+      check(dfm_ilu_create(pmat_, &ilu_), "SetLinearSystem");
+    } else {
+      check(dfm_ilu_create_fill(mat_, lev_, &ilu_), "SetLinearSystem");
+    }
   }
   // the fill level of every segment pair after the requests; different levels
   // for different pairs are not supported
@@ -290,13 +303,21 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
       const double* off = m.NCrs() ? m.GetPtrValPSuP(0, np) : nullptr;  // row-ordered, contiguous
       const double* dia = lay_.N ? m.GetPtrValDia(0) : nullptr;
       check(dfm_mat_set_values(mat_, dia, off, DFM_HOST), "SetValue");
+      if (ordered()) {  // the renumbered matrix: block i of row i' from block n2o(i) of row n2o(i')
+        const size_t bb = (size_t)lay_.b * lay_.b;
+        std::vector<double> pd((size_t)lay_.N * bb), po(psrc_.size() * bb);
+        for (unsigned i = 0; i < lay_.N; i++) std::copy(dia + n2o_[i] * bb, dia + (n2o_[i] + 1) * bb, pd.begin() + i * bb);
+        for (size_t t = 0; t < psrc_.size(); t++)
+          std::copy(off + psrc_[t] * bb, off + (psrc_[t] + 1) * bb, po.begin() + t * bb);
+        check(dfm_mat_set_values(pmat_, pd.data(), po.data(), DFM_HOST), "SetValue");
+      }
     } else {
       std::vector<double> d, o;
       lay_.walk(ls, true, d, o);
       check(dfm_mat_set_values(mat_, d.data(), o.data(), DFM_HOST), "SetValue");
     }
     unsigned ns = 0;
-    return check(dfm_ilu_factor(ilu_, mat_, &ns), "SetValue", DFM_SINGULAR_PIVOT) == DFM_OK;
+    return check(dfm_ilu_factor(ilu_, ordered() ? pmat_ : mat_, &ns), "SetValue", DFM_SINGULAR_PIVOT) == DFM_OK;
   }
   // {iv} := (LU)^-1 {iv} on the CLinearSystem's host vectors (copied to the
   // device and back); solvers over CLinearSystemGPU apply it on the device
@@ -314,8 +335,23 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     lay_.scatter(ls, (int)iv, h.data());
     return true;
   }
-  // z := (LU)^-1 r on device arrays (r != z)
-  void ApplyDevice(const double* r, double* z) { check(dfm_ilu_apply(ilu_, r, z), "SolvePrecond"); }
+  // z := (LU)^-1 r on device arrays (r != z); with an ordering the vector is
+  // renumbered in (OrderingVector_OldToNew), swept, and renumbered back
+  void ApplyDevice(const double* r, double* z) {
+    if (!ordered()) {
+      check(dfm_ilu_apply(ilu_, r, z), "SolvePrecond");
+      return;
+    }
+    if (!tmp_o1_) {
+      tmp_o1_.reset(new DeviceVector(*ctx_, lay_.ndof));
+      tmp_o2_.reset(new DeviceVector(*ctx_, lay_.ndof));
+    }
+    check(dfm_vec_gather(ctx_->get(), lay_.N, lay_.b, static_cast<const unsigned*>(d_n2o_), r, tmp_o1_->data()),
+          "SolvePrecond");
+    check(dfm_ilu_apply(ilu_, tmp_o1_->data(), tmp_o2_->data()), "SolvePrecond");
+    check(dfm_vec_gather(ctx_->get(), lay_.N, lay_.b, static_cast<const unsigned*>(d_o2n_), tmp_o2_->data(), z),
+          "SolvePrecond");
+  }
 
   dfm_mat matrix() const { return mat_; }
   dfm_ilu ilu() const { return ilu_; }
@@ -327,10 +363,49 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   void release() {
     if (ilu_) dfm_ilu_destroy(ilu_);
     if (mat_) dfm_mat_destroy(mat_);
+    if (pmat_) dfm_mat_destroy(pmat_);
+    if (d_n2o_) dfm_buf_free(ctx_->get(), d_n2o_);
+    if (d_o2n_) dfm_buf_free(ctx_->get(), d_o2n_);
     ilu_ = nullptr;
-    mat_ = nullptr;
+    mat_ = pmat_ = nullptr;
+    d_n2o_ = d_o2n_ = nullptr;
     tmp_r_.reset();
     tmp_z_.reset();
+    tmp_o1_.reset();
+    tmp_o2_.reset();
+  }
+  // the renumbered pattern (row i = old row n2o[i], columns renumbered and
+  // sorted), where each of its blocks comes from, and the maps on the device
+  void make_ordered() {
+    if (lay_.nseg != 1) throw Error(DFM_ERR_UNSUPPORTED, "SetOrdering with several segments");
+    const unsigned N = lay_.N;
+    if (order_.size() != N) throw Error(DFM_ERR_INVALID, "SetOrdering: one entry per block row");
+    n2o_.assign(N, 0);
+    std::vector<unsigned> o2n(N, ~0u);
+    for (unsigned i = 0; i < N; i++) {
+      const int v = order_[i];
+      if (v < 0 || (unsigned)v >= N || o2n[v] != ~0u) throw Error(DFM_ERR_INVALID, "SetOrdering: not a permutation");
+      n2o_[i] = (unsigned)v;
+      o2n[v] = i;
+    }
+    std::vector<unsigned> prow(N + 1, 0), pcol;
+    psrc_.clear();
+    std::vector<std::pair<unsigned, unsigned>> row;
+    for (unsigned i = 0; i < N; i++) {
+      const unsigned o = n2o_[i];
+      row.clear();
+      for (unsigned t = lay_.rowptr[o]; t < lay_.rowptr[o + 1]; t++) row.emplace_back(o2n[lay_.colind[t]], t);
+      std::sort(row.begin(), row.end());
+      for (const auto& e : row) {
+        pcol.push_back(e.first);
+        psrc_.push_back(e.second);
+      }
+      prow[i + 1] = (unsigned)pcol.size();
+    }
+    check(dfm_mat_create(ctx_->get(), N, lay_.b, DFM_REAL, prow.data(), pcol.data(), &pmat_), "SetOrdering");
+    for (void** d : {&d_n2o_, &d_o2n_}) check(dfm_buf_alloc(ctx_->get(), sizeof(unsigned) * std::max(N, 1u), d), "SetOrdering");
+    check(dfm_buf_copy(ctx_->get(), d_n2o_, n2o_.data(), sizeof(unsigned) * N, DFM_H2D), "SetOrdering");
+    check(dfm_buf_copy(ctx_->get(), d_o2n_, o2n.data(), sizeof(unsigned) * N, DFM_H2D), "SetOrdering");
   }
 
   Context* ctx_;
@@ -338,8 +413,13 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   dfm_ilu ilu_ = nullptr;
   std::vector<std::pair<int, int>> lev_in_;
   int lev_ = 0;
+  std::vector<int> order_;             // SetOrdering: new -> old block row (empty: off)
+  dfm_mat pmat_ = nullptr;             // the renumbered matrix the ordered ILU(0) factors
+  std::vector<unsigned> n2o_, psrc_;   // new -> old row; source slot of each renumbered block
+  void* d_n2o_ = nullptr;              // device copies of new -> old and old -> new
+  void* d_o2n_ = nullptr;
   detail::Layout lay_;
-  std::unique_ptr<DeviceVector> tmp_r_, tmp_z_;
+  std::unique_ptr<DeviceVector> tmp_r_, tmp_z_, tmp_o1_, tmp_o2_;
 };
 
 // The reference's solver interface over device vectors: handle -1 is the
@@ -473,6 +553,11 @@ inline bool run(CLinearSystemGPU& g, Fn fn, double& conv_ratio, unsigned int& it
 inline bool Solve_PCG_GPU(double& conv_ratio, unsigned int& iteration, LsSol::ILinearSystemPreconditioner_Sol& lsp) {
   CLinearSystemGPU& g = detail::gpu_system(lsp, "Solve_PCG_GPU");
   CPreconditioner_ILU_GPU& M = g.preconditioner();
+  if (M.ordered()) {  // the reference's own driver over the device operations (renumbering in SolvePrecond)
+    const bool ok = LsSol::Solve_PCG(conv_ratio, iteration, g);
+    g.SyncToHost();
+    return ok;
+  }
   return detail::run(g, [&](double t, unsigned m, unsigned* it, double* cv) {
     return dfm_solve_pcg(M.matrix(), M.ilu(), g.vec(-1), g.vec(-2), t, m, it, cv);
   }, conv_ratio, iteration, false);
@@ -484,6 +569,11 @@ inline bool Solve_PBiCGSTAB_GPU(double& conv_ratio, unsigned int& num_iter,
                                 LsSol::ILinearSystemPreconditioner_Sol& lsp) {
   CLinearSystemGPU& g = detail::gpu_system(lsp, "Solve_PBiCGSTAB_GPU");
   CPreconditioner_ILU_GPU& M = g.preconditioner();
+  if (M.ordered()) {
+    const bool ok = LsSol::Solve_PBiCGSTAB(conv_ratio, num_iter, g);
+    g.SyncToHost();
+    return ok;
+  }
   return detail::run(g, [&](double t, unsigned m, unsigned* it, double* cv) {
     return dfm_solve_pbicgstab(M.matrix(), M.ilu(), g.vec(-1), g.vec(-2), t, m, it, cv);
   }, conv_ratio, num_iter, true);

@@ -13,7 +13,9 @@
 //                                    (LsSol::CLinearSystem::AddLinSysSeg / AddMat_Dia / AddMat_NonDia):
 //                                    an N x N grid of L0 x L0 blocks and a chain of M nodes of L1 x L1
 //                                    blocks, coupled both ways; symmetric positive definite
-//   [lev]                       optional last argument: ILU fill-in level (SetFillInLevel), default 0
+//   [lev]                       optional: ILU fill-in level (SetFillInLevel), default 0
+//   [rev|rand]                  optional last argument: a block ordering (CPreconditioner_ILU::SetOrdering),
+//                               the rows reversed or shuffled (one-segment problems)
 //
 // Every run builds the problem from scratch, solves, calls the reference's
 // UpdateValueOfField and reads the field back (the segments' update vectors
@@ -24,7 +26,9 @@
 //   glue_gpu_prec              the reference's CLinearSystemPreconditioner glue with
 //                              dfm_delfem::CPreconditioner_ILU_GPU as its LsSol::CPreconditioner
 // and prints one JSON object: per run ok, iterations, conv and the field values.
+#include <algorithm>
 #include <cmath>
+#include <random>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -339,6 +343,8 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev] | twoseg N M L0 L1 [lev]\n", argv[0]);
     return 2;
   }
+  std::string ordk;  // block ordering for SetOrdering
+  if (argc > 3 && (std::string(argv[argc - 1]) == "rev" || std::string(argv[argc - 1]) == "rand")) ordk = argv[--argc];
   const std::string kind = argv[1];
   GridMesh mesh;
   int lev = 0;
@@ -360,6 +366,15 @@ int main(int argc, char** argv) {
   }
   const double tol = 1e-10;
   const unsigned maxit = 5000;
+  // aind[new] = old: the rows reversed, or shuffled with a fixed seed
+  auto ordering = [&](Sys& P) {
+    std::vector<int> a;
+    if (ordk.empty()) return a;
+    const unsigned n = P.lin().GetMatrix(0).NBlkMatCol();
+    for (unsigned i = 0; i < n; i++) a.push_back(ordk == "rev" ? (int)(n - 1 - i) : (int)i);
+    if (ordk == "rand") std::shuffle(a.begin(), a.end(), std::mt19937(7));
+    return a;
+  };
   std::vector<Run> runs;
   try {
     dfm_lsol::Context ctx(0);
@@ -373,6 +388,7 @@ int main(int argc, char** argv) {
       Quiet q;
       LsSol::CPreconditioner_ILU prec;
       if (lev) prec.SetFillInLevel(lev);
+      prec.SetOrdering(ordering(*P));
       prec.SetLinearSystem(P->lin());
       P->assemble();
       prec.SetValue(P->lin());
@@ -392,6 +408,7 @@ int main(int argc, char** argv) {
       r.it = maxit;
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
+      prec.SetOrdering(ordering(*P));
       prec.SetLinearSystem(P->lin());
       P->assemble();
       if (!prec.SetValue(P->lin())) throw dfm_lsol::Error(DFM_SINGULAR_PIVOT, name);
@@ -424,6 +441,7 @@ int main(int argc, char** argv) {
       r.it = maxit;
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
+      prec.SetOrdering(ordering(*P));
       LsSol::CPreconditioner& base = prec;
       base.SetLinearSystem(P->lin());
       P->assemble();

@@ -53,7 +53,10 @@ CASES = [("poisson", ["poisson", "32"]), ("poisson_ilu1", ["poisson", "24", "1"]
          ("twoseg_1_3", ["twoseg", "40", "200", "1", "3"]),
          # ILU(k) across the segments: the joined matrix's ILU(k) against the reference's segment-wise one
          ("twoseg_2_2_ilu1", ["twoseg", "40", "200", "2", "2", "1"]),
-         ("twoseg_2_1_ilu2", ["twoseg", "40", "200", "2", "1", "2"])]
+         ("twoseg_2_1_ilu2", ["twoseg", "40", "200", "2", "1", "2"]),
+         # CPreconditioner_ILU::SetOrdering: the rows reversed or shuffled (ILU(0) of the renumbered matrix)
+         ("poisson_ord_rev", ["poisson", "24", "0", "rev"]), ("poisson_ord_rand", ["poisson", "32", "0", "rand"]),
+         ("solid3d_ord_rand", ["solid3d", "10", "3", "3", "0", "rand"])]
 
 
 @pytest.mark.gpu

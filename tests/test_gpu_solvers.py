@@ -261,3 +261,14 @@ def test_vector_ops_match_numpy(ctx):
     ctx.sync()
     out = v.cpu().numpy()
     assert out[0] == 0.0 and np.isnan(out[1]) and out[2] == 0.0
+    # block renumbering (COrdering_Blk::OrderingVector_*): gather by a permutation and back
+    for nblk, b in ((1, 3), (1000, 1), (4097, 2), (337881, 3)):
+        perm = rng.permutation(nblk).astype(np.uint32)
+        inv = np.argsort(perm).astype(np.uint32)
+        xh = rng.standard_normal(nblk * b)
+        x, y, z = _dev(xh), _dev(np.zeros(nblk * b)), _dev(np.zeros(nblk * b))
+        lib.vec_gather(ctx, b, torch.from_numpy(perm).cuda(), x, y)
+        lib.vec_gather(ctx, b, torch.from_numpy(inv).cuda(), y, z)
+        ctx.sync()
+        assert np.array_equal(y.cpu().numpy(), xh.reshape(nblk, b)[perm].ravel())
+        assert np.array_equal(z.cpu().numpy(), xh)
