@@ -176,7 +176,7 @@ struct Result {
   std::vector<unsigned> group_ends;  // 2 per group (2-D)
 };
 
-void tet_boundary(unsigned nnode, const double* coord, unsigned ntet, const int* tet, double crt, Result& R) {
+void tet_boundary(const double* coord, unsigned ntet, const int* tet, double crt, Result& R) {
   R.nnofa = 3;
   const std::vector<char> linked = tet_face_linked(ntet, tet);
   for (unsigned t = 0; t < ntet; t++)
@@ -219,7 +219,6 @@ void tet_boundary(unsigned nnode, const double* coord, unsigned ntet, const int*
   R.group_facet.resize(ntri);
   std::vector<unsigned> fill(R.group_ptr.begin(), R.group_ptr.end() - 1);
   for (size_t t = 0; t < ntri; t++) R.group_facet[fill[color[t]]++] = (unsigned)t;
-  (void)nnode;
 }
 
 void planar_boundary(unsigned nnode, const double* coord, int nnoel, unsigned nelem, const int* elem, double crt,
@@ -345,7 +344,7 @@ int gid_boundary(int ndim, unsigned nnode, const double* coord, int nnoel, unsig
         if (elem[(size_t)nnoel * t + r] == v) return DFM_ERR_INVALID;  // a repeated node
     }
   Result R;
-  if (tet) tet_boundary(nnode, coord, nelem, elem, crt_dot, R);
+  if (tet) tet_boundary(coord, nelem, elem, crt_dot, R);
   else if (planar) planar_boundary(nnode, coord, nnoel, nelem, elem, crt_dot, R);
   else R.group_ptr.assign(1, 0);
   *nnofa = hex ? 4 : R.nnofa;
