@@ -522,8 +522,8 @@ int dfm_ilu_set_values(dfm_ilu M, const double* diag, const double* off, int whe
 }
 
 int dfm_ilu_set_sweep(dfm_ilu M, int mode) {
-  if (!M || mode < 0 || mode > 9) return DFM_ERR_INVALID;
-  if (mode == 9) return ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm, false, true);
+  if (!M || mode < 0 || mode > 10) return DFM_ERR_INVALID;
+  if (mode >= 9) return ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm, mode == 10, true);
   if (mode >= 3) {
     const bool merge = mode == 5 || mode == 6 || mode == 8, nb = mode == 4 || mode == 6, pipe = mode >= 7;
     const int rc = ilu_set_ranges(M, M->sweep_blocks > 0 ? M->sweep_blocks : M->ctx->nsm, merge);
@@ -597,7 +597,7 @@ int dfm_ilu_get_sweep(dfm_ilu M, int* mode) {
   if (!M || !mode) return DFM_ERR_INVALID;
   *mode = M->sweep;
   if (M->sweep == 3 && M->plan_f.halo)
-    *mode = 9;
+    *mode = M->plan_f.merged ? 10 : 9;
   else if (M->sweep == 3)
     *mode = M->plan_f.pipe ? (M->plan_f.merged ? 8 : 7) : (M->plan_f.merged ? 5 : 3) + (M->plan_f.nb ? 1 : 0);
   return DFM_OK;

@@ -199,7 +199,7 @@ int set_poll_sleep(unsigned ns);
 int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge = false,
                      bool part = false, bool halo = false);
 // sweep_halo.cu
-int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part);
+int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part, bool merge = false);
 cudaError_t sweep_halo_launch(dfm_ilu M, bool fwd, const SweepPlan* P, const double* in, double* out,
                               const double* rdot, double* part, KrylovScalars* sc, const double* rr_part, int rr_n,
                               bool f32);

@@ -988,18 +988,18 @@ int ilu_autotune(dfm_ilu M) {
         }
       }
     }
-    // the shared-memory-only schedule (mode 9) at the partition and at one
-    // CTA per SM: compute warps x lanes per row, producer warps
+    // the shared-memory-only schedule (modes 9 and 10) at the partition and at
+    // one CTA per SM: compute warps x lanes per row, producer warps
     {
       const unsigned bx = M->vt == DFM_COMPLEX ? 2u : M->b;
       struct Cfg { int cw, lpr, hw; };
       const Cfg cfgs3[] = {{1, 4, 4}, {2, 4, 4}, {4, 4, 4}, {4, 8, 4}, {2, 8, 4}, {4, 4, 8}};
       const Cfg cfgs1[] = {{1, 2, 4}, {1, 4, 4}, {2, 4, 4}, {4, 4, 4}, {2, 2, 4}, {4, 4, 8}};
       const Cfg* cfgs = bx == 1 ? cfgs1 : cfgs3;
-      auto try_halo = [&](int G, bool part) -> int {
+      auto try_halo = [&](int G, bool part, bool merge) -> int {
         SweepPlan pf, pb;
-        if (sweep_plan_build(M, true, G, 8, 8, &pf, false, part, true) != DFM_OK ||
-            sweep_plan_build(M, false, G, 8, 8, &pb, false, part, true) != DFM_OK) {
+        if (sweep_plan_build(M, true, G, 8, 8, &pf, merge, part, true) != DFM_OK ||
+            sweep_plan_build(M, false, G, 8, 8, &pb, merge, part, true) != DFM_OK) {
           sweep_plan_free(&pf);
           sweep_plan_free(&pb);
           cudaGetLastError();
@@ -1041,8 +1041,10 @@ int ilu_autotune(dfm_ilu M) {
         return rc == DFM_ERR_UNSUPPORTED ? DFM_OK : rc;
       };
       int rc = DFM_OK;
-      if (M->nparts > 0 && M->nparts <= (unsigned)nsm) rc = try_halo((int)M->nparts, true);
-      if (rc == DFM_OK) rc = try_halo(nsm, false);
+      for (int mg = 0; mg < 2 && rc == DFM_OK; mg++) {  // levels one by one (mode 9), in merged pairs (mode 10)
+        if (M->nparts > 0 && M->nparts <= (unsigned)nsm) rc = try_halo((int)M->nparts, true, mg != 0);
+        if (rc == DFM_OK) rc = try_halo(nsm, false, mg != 0);
+      }
       if (rc) {
         sweep_plan_free(&best_f);
         sweep_plan_free(&best_b);

@@ -726,8 +726,8 @@ void sweep_plan_free(SweepPlan* P) {
 int sweep_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, int vec_bytes, SweepPlan* P, bool merge,
                      bool part, bool halo) {
   if (halo) {
-    if (merge || vec_bytes != 8) return DFM_ERR_UNSUPPORTED;
-    return sweep_halo_plan_build(M, fwd, G, val_bytes, P, part);
+    if (vec_bytes != 8) return DFM_ERR_UNSUPPORTED;
+    return sweep_halo_plan_build(M, fwd, G, val_bytes, P, part, merge);
   }
   const unsigned N = M->N;
   const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks

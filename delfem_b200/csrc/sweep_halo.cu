@@ -333,13 +333,21 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
       const unsigned* hids = reinterpret_cast<const unsigned*>(sb + hdr->hids);
       double* H = X + x_slice + (size_t)s * halo_stride;
       for (unsigned e = (unsigned)wl; e < nh; e += 32) {
-        const size_t row = hids[e];
+        const unsigned hid = hids[e];
         double v[B];
-#pragma unroll
-        for (int c = 0; c < B; c++) v[c] = ld_relaxed(out + row * B + c);
         bool miss = false;
+        if (hid & 0x80000000u) {  // an entry of the input vector (merged level pairs): no wait
+          const size_t row = hid & 0x7fffffffu;
 #pragma unroll
-        for (int c = 0; c < B; c++) miss |= Sent<double>::is(v[c]);
+          for (int c = 0; c < B; c++) v[c] = in[row * B + c];
+        } else {
+          const size_t row = hid;
+#pragma unroll
+          for (int c = 0; c < B; c++) v[c] = ld_relaxed(out + row * B + c);
+#pragma unroll
+          for (int c = 0; c < B; c++) miss |= Sent<double>::is(v[c]);
+        }
+        const size_t row = hid & 0x7fffffffu;
         if (miss) {
           SpinGuard g(wait_ns);
           while (miss) {
@@ -442,7 +450,7 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
 // The halo plan of one sweep direction over G CTAs (contiguous ranges of the
 // natural order balanced by dependency blocks, or the ILU's row partition):
 // chunks per level with their halo row lists, operand offsets into X.
-int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part) {
+int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* P, bool part, bool merge) {
   const unsigned N = M->N;
   const unsigned b = M->vt == DFM_COMPLEX ? 2u : M->b;  // complex scalars as real 2x2 blocks
   const unsigned bb = b * b;
@@ -497,53 +505,127 @@ int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* 
   std::vector<ChunkDesc> chunks;
   std::vector<Pend> pend;
   std::vector<unsigned> cta_chunk(G + 1, 0);
-  std::vector<uint4> recipe;
-  std::vector<unsigned> hmap(N, 0xffffffffu);  // scratch: remote row -> halo index in the current chunk
+  std::vector<uint4> recipe, terms;
+  constexpr unsigned NONE = 0xffffffffu;
+  // halo entries: another CTA's output row, or (kInput) an entry of the input
+  // vector, which the second level of a merged pair reads in place of the
+  // first level's output
+  constexpr unsigned kInput = 0x80000000u;
+  std::vector<unsigned> hmap(N, NONE);                   // scratch: output row -> halo index in the chunk
+  std::vector<unsigned> hmap_in(merge ? N : 0u, NONE);   // scratch: input entry -> halo index
   unsigned maxhalo = 1, stage_max = 32;
+  // step of a row: its level, or with merged level pairs its level / 2
+  auto step = [&](unsigned i) { return merge ? lev[i] / 2 : lev[i]; };
+  // operands of row i: kind 0 = a slot of this CTA's slice (v = slot), 1 =
+  // another CTA's output row v, 2 = the input vector's row v; with the recipe
+  // of the packed block (the same substitutions as the range plans, sweep.cu)
+  struct Op {
+    unsigned kind, v;
+    uint4 rc;
+  };
+  std::vector<Op> ops;
+  std::vector<unsigned> kmap(merge ? N : 0u, NONE);  // scratch: column -> position in ops
+  auto slots = [&](unsigned i, unsigned& s0, unsigned& s1) {
+    s0 = fwd ? rp[i] : dia[i];
+    s1 = fwd ? dia[i] : rp[i + 1];
+  };
+  auto row_ops = [&](unsigned i, unsigned a0, unsigned a1) {
+    ops.clear();
+    auto opnd = [&](unsigned col, uint4 rc) -> Op {
+      const unsigned pc = pos_of(col);
+      return (pc >= a0 && pc < a1) ? Op{0u, pc - a0, rc} : Op{1u, col, rc};
+    };
+    unsigned s0, s1;
+    slots(i, s0, s1);
+    if (!(merge && (lev[i] & 1u))) {
+      for (unsigned s = s0; s < s1; s++) ops.push_back(opnd(ci[s], make_uint4(s, 0u, 0u, 0u)));
+      return;
+    }
+    // second level of a pair: operands on the first level are substituted
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned j = ci[s];
+      if (lev[j] + 1 != lev[i]) continue;
+      const unsigned t0 = (unsigned)terms.size();
+      terms.push_back(make_uint4(s, fwd ? j : NONE, NONE, 0u));  // L_ij D_j^-1  |  U'_ij
+      ops.push_back(Op{2u, j, make_uint4(NONE, t0, t0 + 1, 0u)});
+    }
+    const size_t first_c = ops.size();
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned k = ci[s];
+      if (lev[k] + 1 == lev[i]) continue;
+      kmap[k] = (unsigned)ops.size();
+      ops.push_back(opnd(k, make_uint4(s, 0u, 0u, 1u)));
+    }
+    // fill terms F_ij (D_j^-1) F_jk, grouped per column k
+    std::vector<std::vector<uint4>> tl(ops.size() - first_c);
+    for (unsigned s = s0; s < s1; s++) {
+      const unsigned j = ci[s];
+      if (lev[j] + 1 != lev[i]) continue;
+      unsigned t0, t1;
+      slots(j, t0, t1);
+      for (unsigned t = t0; t < t1; t++) {
+        const unsigned k = ci[t];
+        if (kmap[k] == NONE) {
+          kmap[k] = (unsigned)ops.size();
+          ops.push_back(opnd(k, make_uint4(NONE, 0u, 0u, 1u)));
+          tl.emplace_back();
+        }
+        tl[kmap[k] - first_c].push_back(make_uint4(s, fwd ? j : NONE, t, 0u));
+      }
+    }
+    for (size_t q = first_c; q < ops.size(); q++) {
+      ops[q].rc.y = (unsigned)terms.size();
+      for (const uint4& t : tl[q - first_c]) terms.push_back(t);
+      ops[q].rc.z = (unsigned)terms.size();
+      kmap[ops[q].kind == 0 ? row_at(a0 + ops[q].v) : ops[q].v] = NONE;
+    }
+  };
   for (int c = 0; c < G; c++) {
     cta_chunk[c] = (unsigned)chunks.size();
     const unsigned a0 = range[c], a1 = range[c + 1];
     std::vector<unsigned> rows(a1 - a0);
     for (unsigned q = a0; q < a1; q++) rows[q - a0] = row_at(fwd ? q : (a1 - 1 - (q - a0)));
-    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return lev[x] < lev[y]; });
+    std::stable_sort(rows.begin(), rows.end(), [&](unsigned x, unsigned y) { return step(x) < step(y); });
     size_t p = 0;
     while (p < rows.size()) {
-      const unsigned L = lev[rows[p]];
+      const unsigned L = step(rows[p]);
       Pend pd;
       unsigned nblk = 0;
       const size_t rec0 = recipe.size();
-      while (p < rows.size() && lev[rows[p]] == L) {
+      while (p < rows.size() && step(rows[p]) == L) {
         const unsigned i = rows[p];
-        const unsigned s0 = fwd ? rp[i] : dia[i], s1 = fwd ? dia[i] : rp[i + 1];
+        const size_t tmark = terms.size();
+        row_ops(i, a0, a1);
         unsigned newh = 0;
-        for (unsigned s = s0; s < s1; s++) {
-          const unsigned pc = pos_of(ci[s]);
-          if (!(pc >= a0 && pc < a1) && hmap[ci[s]] == 0xffffffffu) newh++;
-        }
-        const unsigned nb = s1 - s0;
+        for (const Op& o : ops)
+          if ((o.kind == 1 && hmap[o.v] == NONE) || (o.kind == 2 && hmap_in[o.v] == NONE)) newh++;
+        const unsigned nb = (unsigned)ops.size();
         const ChunkLayout est = chunk_layout((unsigned)pd.rd.size() + 1, ((nblk + nb) + 3) & ~3u,
                                              (unsigned)pd.hids.size() + newh, vblk, drow);
-        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) break;
+        if (!pd.rd.empty() && (est.bytes > kChunkMaxBytes || pd.rd.size() >= kChunkMaxRows)) {
+          terms.resize(tmark);  // this row starts the next chunk
+          break;
+        }
         pd.rd.push_back(make_uint4(pos_of(i) - a0, nblk, nblk + nb, i));  // {slot, blocks, global row}
-        for (unsigned s = s0; s < s1; s++) {
-          const unsigned col = ci[s], pc = pos_of(col);
+        for (const Op& o : ops) {
           unsigned code;
-          if (pc >= a0 && pc < a1) {
-            code = (pc - a0) * b;
+          if (o.kind == 0) {
+            code = o.v * b;
           } else {
-            if (hmap[col] == 0xffffffffu) {
-              hmap[col] = (unsigned)pd.hids.size();
-              pd.hids.push_back(col);
+            std::vector<unsigned>& hm = o.kind == 1 ? hmap : hmap_in;
+            if (hm[o.v] == NONE) {
+              hm[o.v] = (unsigned)pd.hids.size();
+              pd.hids.push_back(o.kind == 1 ? o.v : (kInput | o.v));
             }
-            code = 0x80000000u | hmap[col];
+            code = 0x80000000u | hm[o.v];
           }
           pd.xo.push_back(code);
-          recipe.push_back(make_uint4(s, 0u, 0u, 0u));
+          recipe.push_back(o.rc);
         }
         nblk += nb;
         p++;
       }
-      for (unsigned h : pd.hids) hmap[h] = 0xffffffffu;
+      for (unsigned h : pd.hids) (h & kInput ? hmap_in[h & ~kInput] : hmap[h]) = NONE;
       const unsigned nblk_pad = (nblk + 3) & ~3u;
       for (unsigned k = nblk; k < nblk_pad; k++) {
         pd.xo.push_back(0);  // padding: outside every row's block range
@@ -620,7 +702,9 @@ int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* 
   DFM_CUDA_TRY(cudaMalloc(&P->d_range, sizeof(unsigned) * (G + 1)));
   DFM_CUDA_TRY(cudaMalloc(&P->d_blob, hblob.size()));
   DFM_CUDA_TRY(cudaMalloc(&P->d_recipe, sizeof(uint4) * std::max<size_t>(recipe.size(), 1)));
-  DFM_CUDA_TRY(cudaMalloc(&P->d_terms, sizeof(uint4)));
+  DFM_CUDA_TRY(cudaMalloc(&P->d_terms, sizeof(uint4) * std::max<size_t>(terms.size(), 1)));
+  if (!terms.empty())
+    DFM_CUDA_TRY(cudaMemcpyAsync(P->d_terms, terms.data(), sizeof(uint4) * terms.size(), cudaMemcpyHostToDevice, s));
   if (!chunks.empty())
     DFM_CUDA_TRY(cudaMemcpyAsync(P->d_chunks, chunks.data(), sizeof(ChunkDesc) * chunks.size(),
                                  cudaMemcpyHostToDevice, s));
@@ -634,7 +718,7 @@ int sweep_halo_plan_build(dfm_ilu M, bool fwd, int G, int val_bytes, SweepPlan* 
   DFM_CUDA_TRY(cudaMemcpyAsync(P->d_blob, hblob.data(), hblob.size(), cudaMemcpyHostToDevice, s));
   if (!recipe.empty())
     DFM_CUDA_TRY(cudaMemcpyAsync(P->d_recipe, recipe.data(), sizeof(uint4) * recipe.size(), cudaMemcpyHostToDevice, s));
-  P->merged = false;
+  P->merged = merge;
   DFM_CUDA_TRY(cudaStreamSynchronize(s));
   P->valid = true;
   P->stale = true;

@@ -378,8 +378,10 @@ DFM_API int dfm_ilu_apply_static(dfm_ilu M, const double* r, double* z);
  * memory only: a few compute warps synchronised by a named barrier take the
  * rows of each level while producer warps stream the level data by TMA and
  * prefetch the operands owned by other CTAs into a shared-memory halo (results
- * equal to those of 3 to rounding).  Complex matrices
- * run 3-9 as real 2x2 blocks [re -im; im re]. */
+ * equal to those of 3 to rounding), 10 = 9 with the levels taken in pairs as
+ * in 5 (half the sequential steps; the second level reads the first level's
+ * right-hand sides through the products with the factor; results equal to
+ * rounding).  Complex matrices run 3-10 as real 2x2 blocks [re -im; im re]. */
 DFM_API int dfm_ilu_set_sweep(dfm_ilu M, int mode);
 /* No counterpart in the reference (its sweeps are sequential).  A row
  * partition for the range-partitioned sweep schedules: CTA c takes the rows
@@ -398,8 +400,8 @@ DFM_API int dfm_ilu_set_sweep_partition(dfm_ilu M, const unsigned* part, unsigne
 DFM_API int dfm_sweep_partition_patches(unsigned nnode, int ndim, const double* coord, unsigned max_parts,
                                         unsigned* part, unsigned* nparts);
 DFM_API int dfm_ilu_get_sweep(dfm_ilu M, int* mode);
-/* No counterpart in the reference.  The launch shape of schedule 9 (valid
- * while it is the schedule): compute warps 1, 2 or 4, lanes per row 2, 4 or 8,
+/* No counterpart in the reference.  The launch shape of schedules 9 and 10
+ * (valid while one of them is the schedule): compute warps 1, 2 or 4, lanes per row 2, 4 or 8,
  * producer warps (compute + producer <= 16).  The autotuner picks one; this
  * pins it (a row's sum runs over `lanes` lanes, so the lanes decide its
  * summation order). */

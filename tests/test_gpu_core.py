@@ -74,7 +74,7 @@ def test_ilu_factor_bit_exact(ctx, name):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_ilu_apply_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -93,7 +93,7 @@ def test_ilu_apply_matches_oracle(ctx, name, sweep):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_pcg_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -117,7 +117,7 @@ def test_pcg_matches_oracle(ctx, name, sweep):
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b1", "helmholtz_bands"])
 @pytest.mark.parametrize("ctas", [1, 3, 7, 148])
-@pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("mode", [3, 4, 5, 6, 7, 8, 9, 10])
 def test_range_sweep_cta_counts(ctx, name, ctas, mode):
     """Modes 3-8 with every CTA count: same result as the oracle's sweeps."""
     from delfem_b200 import lib
@@ -212,18 +212,20 @@ def test_spmv_large_rows_and_tiles(ctx, kernel):
 
 @pytest.mark.parametrize("name", ["solid3d", "poisson_coef", "helmholtz_bands", "random_b3"])
 @pytest.mark.parametrize("warps", [(1, 2, 1), (1, 4, 4), (2, 8, 2), (4, 4, 12)])
-def test_halo_sweep_every_warp_split(ctx, name, warps):
-    """Schedule 9 with each split of compute warps, lanes per row and producer
-    warps: the preconditioner to 1e-11 of the oracle, before and after a
-    refactorization (the packed level data follow the factor)."""
+@pytest.mark.parametrize("mode", [9, 10])
+def test_halo_sweep_every_warp_split(ctx, name, warps, mode):
+    """Schedules 9 and 10 (merged level pairs) with each split of compute
+    warps, lanes per row and producer warps: the preconditioner to 1e-11 of
+    the oracle, before and after a refactorization (the packed level data and
+    the merged pairs' product blocks follow the factor)."""
     from delfem_b200 import lib
     S = SYSTEMS[name]()
     A = make(ctx, S)
     M = lib.ILU(A)
     M.factor()
-    M.sweep = 9
+    M.sweep = mode
     M.sweep_warps = warps
-    assert M.sweep == 9 and M.sweep_warps == warps
+    assert M.sweep == mode and M.sweep_warps == warps
     _, fd, fo = S.ilu0()
     r = np.random.default_rng(9).standard_normal(S.N * S.xw)
     ref = S.precond(fd, fo, r)

@@ -54,7 +54,7 @@ def test_iluk_pattern_levels_and_factor(ctx, name, lev):
 
 
 @pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b3"])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_iluk_apply_every_schedule(ctx, name, sweep):
     S = SYSTEMS[name]()
     A, M = _setup(ctx, S, 1)
@@ -177,7 +177,7 @@ def test_complex_iluk_factor_and_cocg(ctx, nring, lev, solve):
     rng = np.random.default_rng(3)
     rv = rng.standard_normal(2 * Z.N)
     ref = Z.precond_fill((fr, fc, fdia), fd, fo, rv)
-    for sweep in (1, 2, 3, 9):
+    for sweep in (1, 2, 3, 9, 10):
         M.sweep = sweep
         z = torch.zeros(2 * Z.N, dtype=torch.float64, device="cuda")
         M.apply(_dev(rv), z)

@@ -32,7 +32,7 @@ def op32(ctx, request):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7, 9, 10])
 def test_mixed_true_residual_and_solution(ctx, op32, name, sweep):
     from delfem_b200 import lib
     S = SYSTEMS[name]()
@@ -127,7 +127,7 @@ def test_mixed_follows_value_updates(ctx):
 
 
 @pytest.mark.parametrize("nring", [40])
-@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 5, 7, 9, 10])
 def test_cocg_mixed_true_residual(ctx, op32, nring, sweep):
     """complex64 values inside complex128 residual replacement (Helmholtz)."""
     from delfem_b200 import lib

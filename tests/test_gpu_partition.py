@@ -32,7 +32,7 @@ def _make(ctx, S):
 
 
 @pytest.mark.parametrize("name", list(SYSTEMS))
-@pytest.mark.parametrize("sweep", [3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("sweep", [3, 4, 5, 6, 7, 8, 9, 10])
 def test_random_partition_every_range_mode(ctx, name, sweep):
     S = SYSTEMS[name]()
     A, M = _make(ctx, S)
@@ -61,7 +61,7 @@ def test_patch_partition_pcg(ctx):
     M.set_sweep_partition(part, nparts)
     _, fd, fo = S.ilu0()
     ref = S.solve(fd, fo, method="pcg", tol=1e-10, maxit=2000)
-    for sweep in (0, 3, 8, 9):
+    for sweep in (0, 3, 8, 9, 10):
         if sweep:
             M.sweep = sweep
         r = _dev(S.rhs)
@@ -88,7 +88,7 @@ def test_partition_rejected(ctx):
         M.set_sweep_partition(np.zeros(S.N, np.uint32), 100000)  # more parts than co-resident CTAs
 
 
-@pytest.mark.parametrize("sweep", [0, 3, 7, 9])
+@pytest.mark.parametrize("sweep", [0, 3, 7, 9, 10])
 def test_partition_with_fill(ctx, sweep):
     """ILU(1) under the patch partition: the partition applies to the rows of
     the filled factor's pattern the same way; PCG to the oracle's x."""

@@ -45,7 +45,7 @@ REAL_SYSTEMS = {
 
 
 @pytest.mark.parametrize("name", list(REAL_SYSTEMS))
-@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("sweep", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_pbicgstab_matches_oracle(ctx, name, sweep):
     from delfem_b200 import lib
     S = REAL_SYSTEMS[name]()
