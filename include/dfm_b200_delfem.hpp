@@ -239,10 +239,12 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   CPreconditioner_ILU_GPU(const CPreconditioner_ILU_GPU&) = delete;
   CPreconditioner_ILU_GPU& operator=(const CPreconditioner_ILU_GPU&) = delete;
 
-  // the device objects and the fill-level requests (as the reference's Clear)
+  // the device objects, the fill-level requests and the ordering (as the
+  // reference's Clear, src/ls/preconditioner.cpp:31-52)
   void Clear() {
     release();
     lev_in_.clear();
+    order_.clear();
   }
   // CPreconditioner_ILU::SetOrdering (include/delfem/ls/preconditioner.h:93-97):
   // for the next SetLinearSystem, factor the system with its block rows and
