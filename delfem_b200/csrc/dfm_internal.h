@@ -172,7 +172,8 @@ int spmv_grid(dfm_mat A);
 int ilu_factor_launch(dfm_ilu M, dfm_mat A);
 // fill.cu
 int ilu_fill_pattern(unsigned N, const std::vector<unsigned>& rp, const std::vector<unsigned>& ci, int lev,
-                     std::vector<unsigned>& frp, std::vector<unsigned>& fci);
+                     std::vector<unsigned>& frp, std::vector<unsigned>& fci, const std::vector<unsigned char>& unl,
+                     unsigned bound);
 int ilu_fill_values(dfm_ilu M, dfm_mat A);
 // With sc, a forward sweep first stops the solve when |r|^2/|r0|^2 < tol^2
 // (partials in part(2)) unless rr_check is false.

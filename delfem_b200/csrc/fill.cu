@@ -27,16 +27,24 @@ namespace dfm {
 // the level it has (AddFracPtn's sorted list inserts only new columns, see
 // CListRLN::Insert in include/delfem/matvec/matdiafrac_blkcrs.h:207-257), so
 // a column's level is that of the first pivot reaching it.  lev = -1: no limit.
+// Rows flagged in `unl` (CPreconditioner_ILU::SetFillBlk, AddFracPtn(lev,
+// aBlkFill), src/matvec/matdiafrac_blkcrs.cpp:1379-1500) lift the limit: a
+// candidate (i, j) with i, j < bound is kept at any level when row i or row j
+// is flagged, so a pivot cannot be skipped on its own level in a row that may
+// take such fill.  `bound` is the first segment's row count in a joined
+// multi-segment system (only that segment's diagonal matrix gets the list).
 // The row is a linked list over column numbers; `level[c]` is kNone for
 // columns not in it.
 int ilu_fill_pattern(unsigned N, const std::vector<unsigned>& rp, const std::vector<unsigned>& ci, int lev,
-                     std::vector<unsigned>& frp, std::vector<unsigned>& fci) {
+                     std::vector<unsigned>& frp, std::vector<unsigned>& fci, const std::vector<unsigned char>& unl,
+                     unsigned bound) {
   constexpr unsigned kNone = 0xffffffffu;
   const size_t ncrs = rp[N];
   frp.assign(N + 1, 0);
   fci.clear();
   const bool dense = N > 0 && ncrs == (size_t)N * (N - 1);
-  if (lev == 0 || ncrs == 0 || dense) {  // AddFracPtn returns at once
+  const bool flags = !unl.empty();
+  if ((lev == 0 && !flags) || ncrs == 0 || dense) {  // AddFracPtn returns at once
     fci.assign(ci.begin(), ci.begin() + ncrs);
     frp = rp;
     return DFM_OK;
@@ -55,14 +63,16 @@ int ilu_fill_pattern(unsigned N, const std::vector<unsigned>& rp, const std::vec
       (last == kNone ? head : next[last]) = c;
       last = c;
     }
+    const bool may_flag = flags && i < bound, flag_i = may_flag && unl[i];
     for (unsigned k = head; k != kNone; k = next[k]) {
       const unsigned lik = level[k];
-      if (!within(lik)) continue;
+      if (!may_flag && !within(lik)) continue;
       if (k >= i) break;
       unsigned at = k;  // insertion point: every new column lies after k
       for (size_t s = upper[k]; s < frp[k + 1]; s++) {
         const unsigned lkj = flev[s], j = fci[s];
-        if (!within(lkj) || j == i || level[j] != kNone) continue;
+        const bool free_ij = may_flag && j < bound && (flag_i || unl[j]);
+        if (!(free_ij || within(std::max(lik, lkj))) || j == i || level[j] != kNone) continue;
         while (next[at] != kNone && next[at] < j) at = next[at];
         next[j] = next[at];
         next[at] = j;
@@ -112,15 +122,26 @@ using namespace dfm;
 
 extern "C" {
 
-int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out) {
-  if (!A || !out || lev < -1) return DFM_ERR_INVALID;
+int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out) { return dfm_ilu_create_fill_rows(A, lev, nullptr, 0, 0, out); }
+
+int dfm_ilu_create_fill_rows(dfm_mat A, int lev, const unsigned* rows, size_t nrows, unsigned bound, dfm_ilu* out) {
+  if (!A || !out || lev < -1 || (nrows && !rows)) return DFM_ERR_INVALID;
   *out = nullptr;
-  if (lev == 0) return dfm_ilu_create(A, out);
+  std::vector<unsigned char> unl;
+  if (nrows) {
+    if (bound == 0 || bound > A->N) return DFM_ERR_INVALID;
+    unl.assign(A->N, 0);
+    for (size_t t = 0; t < nrows; t++) {
+      if (rows[t] >= bound) return DFM_ERR_INVALID;
+      unl[rows[t]] = 1;
+    }
+  }
+  if (lev == 0 && !nrows) return dfm_ilu_create(A, out);
   // complex matrices: CZPreconditioner_ILU::SetFillInLevel, whose fill pattern
   // (CZMatDiaFrac_BlkCrs::AddFracPtn, src/matvec/zmatdiafrac_blkcrs.cpp:263-441)
   // is the real one's
   std::vector<unsigned> frp, fci;
-  int rc = ilu_fill_pattern(A->N, A->h_rowptr, A->h_colind, lev, frp, fci);
+  int rc = ilu_fill_pattern(A->N, A->h_rowptr, A->h_colind, lev, frp, fci, unl, bound);
   if (rc) return rc;
   // the pattern-only matrix that the factor, level sets and sweep plans use
   dfm_mat P = new (std::nothrow) dfm_mat_s();

@@ -84,6 +84,7 @@ PROTOS = {
     "dfm_coef_grad_solid2d": (_i, [_vp, _d, _d, _vp, _vp, _vp]),
     "dfm_ilu_create": (_i, [_vp, C.POINTER(_vp)]),
     "dfm_ilu_create_fill": (_i, [_vp, _i, C.POINTER(_vp)]),
+    "dfm_ilu_create_fill_rows": (_i, [_vp, _i, _up, C.c_size_t, C.c_uint, C.POINTER(_vp)]),
     "dfm_ilu_pattern": (_i, [_vp, _up, _up, _up]),
     "dfm_ilu_destroy": (_i, [_vp]),
     "dfm_ilu_levels": (_i, [_vp, _up, _up, _up, _up]),
@@ -487,13 +488,20 @@ def apply_dirichlet(A: Matrix, flags, rhs=None):
 
 class ILU:
     """LsSol::CPreconditioner_ILU on the device: ILU(0), or ILU(fill_level)
-    (SetFillInLevel; -1 = no limit) with the factor in its own fill pattern."""
+    (SetFillInLevel; -1 = no limit) with the factor in its own fill pattern.
+    fill_rows: the SetFillBlk list (block rows whose fill has no level limit),
+    acting on pairs of rows below fill_bound (default N)."""
 
-    def __init__(self, A: Matrix, fill_level: int = 0):
+    def __init__(self, A: Matrix, fill_level: int = 0, fill_rows=None, fill_bound=None):
         self.A = A
         self.fill_level = int(fill_level)
         h = C.c_void_p()
-        if self.fill_level == 0:
+        if fill_rows is not None and len(fill_rows):
+            rows = np.ascontiguousarray(fill_rows, np.uint32)
+            bound = A.N if fill_bound is None else int(fill_bound)
+            check(lib().dfm_ilu_create_fill_rows(A.h, self.fill_level, rows.ctypes.data_as(_up), rows.size, bound,
+                                                 C.byref(h)), "dfm_ilu_create_fill_rows")
+        elif self.fill_level == 0:
             check(lib().dfm_ilu_create(A.h, C.byref(h)), "dfm_ilu_create")
         else:
             check(lib().dfm_ilu_create_fill(A.h, self.fill_level, C.byref(h)), "dfm_ilu_create_fill")

@@ -332,6 +332,18 @@ DFM_API int dfm_ilu_create(dfm_mat A, dfm_ilu* out);
  * 263-441, fills as the real one does).  Batches (dfm_batch_create) take
  * ILU(0) objects only. */
 DFM_API int dfm_ilu_create_fill(dfm_mat A, int lev, dfm_ilu* out);
+/* ILU(k) with unlimited fill through some block rows (CPreconditioner_ILU::
+ * SetFillBlk, include/delfem/ls/preconditioner.h:80, applied by
+ * CMatDiaFrac_BlkCrs::AddFracPtn(lev, aBlkFill), src/matvec/
+ * matdiafrac_blkcrs.cpp:1379-1500): a fill candidate (i, j) is kept whatever
+ * its level when row i or row j is one of rows[0..nrows) and i, j < bound;
+ * otherwise the rule of dfm_ilu_create_fill.  bound = N for one matrix; for
+ * segments joined into one matrix, the first segment's block rows (the
+ * reference hands the list to that segment's diagonal matrix only).  Rows may
+ * repeat; a row >= bound is DFM_ERR_INVALID.  nrows = 0 is
+ * dfm_ilu_create_fill. */
+DFM_API int dfm_ilu_create_fill_rows(dfm_mat A, int lev, const unsigned* rows, size_t nrows, unsigned bound,
+                                     dfm_ilu* out);
 /* The factor's pattern (host arrays, nullable): rowptr[N+1], colind[*ncrs];
  * the off-diagonal values of dfm_ilu_get_values/set_values follow it. */
 DFM_API int dfm_ilu_pattern(dfm_ilu M, unsigned* rowptr, unsigned* colind, unsigned* ncrs);

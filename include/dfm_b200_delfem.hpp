@@ -260,6 +260,12 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     if (lev < -1 || ilss0 < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
     lev_in_.emplace_back(lev, ilss0);
   }
+  // CPreconditioner_ILU::SetFillBlk (include/delfem/ls/preconditioner.h:80):
+  // block rows of the first segment whose fill has no level limit at the next
+  // SetLinearSystem (the reference passes the list to that segment's diagonal
+  // matrix, AddFracPtn(lev, aBlkFill), src/ls/preconditioner.cpp:140-142);
+  // Clear keeps it, as the reference's does, and an ordering ignores it
+  void SetFillBlk(const std::vector<unsigned int>& aBlk) { fill_blk_ = aBlk; }
   // pattern of the (joined) system matrix on the device, fill pattern and
   // level sets
   void SetLinearSystem(const LsSol::CLinearSystem& ls) override {
@@ -271,6 +277,19 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
     if (ordered()) {
       make_ordered();
       check(dfm_ilu_create(pmat_, &ilu_), "SetLinearSystem");
+    } else if (!fill_blk_.empty()) {
+      // the listed block rows as rows of the joined matrix (every DOF row of
+      // the block when the join is one row per DOF); the flags act within the
+      // first segment's rows
+      const unsigned L = lay_.scalar ? lay_.len[0] : 1u;
+      std::vector<unsigned> rows;
+      rows.reserve(fill_blk_.size() * L);
+      for (unsigned r : fill_blk_) {
+        if (r >= lay_.nblk[0]) throw Error(DFM_ERR_INVALID, "SetFillBlk: block row out of range");
+        for (unsigned d = 0; d < L; d++) rows.push_back(r * L + d);
+      }
+      check(dfm_ilu_create_fill_rows(mat_, lev_, rows.data(), rows.size(), lay_.nblk[0] * L, &ilu_),
+            "SetLinearSystem");
     } else {
       check(dfm_ilu_create_fill(mat_, lev_, &ilu_), "SetLinearSystem");
     }
@@ -414,6 +433,7 @@ class CPreconditioner_ILU_GPU : public LsSol::CPreconditioner {
   dfm_mat mat_ = nullptr;
   dfm_ilu ilu_ = nullptr;
   std::vector<std::pair<int, int>> lev_in_;
+  std::vector<unsigned int> fill_blk_;  // SetFillBlk: block rows of segment 0 with unlimited fill
   int lev_ = 0;
   std::vector<int> order_;             // SetOrdering: new -> old block row (empty: off)
   dfm_mat pmat_ = nullptr;             // the renumbered matrix the ordered ILU(0) factors

@@ -202,10 +202,13 @@ class CPreconditioner_ILU {
     if (lev < -1) throw Error(DFM_ERR_INVALID, "SetFillInLevel");
     lev_ = lev;
   }
+  // SetFillBlk(aBlk): block rows whose fill has no level limit from the next
+  // SetLinearSystem on (AddFracPtn(lev, aBlkFill)); empty: none
+  void SetFillBlk(const std::vector<unsigned int>& aBlk) { blk_ = aBlk; }
   // fill pattern (ILU(lev)) and level sets of the sweeps
   void SetLinearSystem(const CMatDia_BlkCrs& A) {
     Clear();
-    check(dfm_ilu_create_fill(A.get(), lev_, &h_), "SetLinearSystem");
+    check(dfm_ilu_create_fill_rows(A.get(), lev_, blk_.data(), blk_.size(), A.NBlkMatCol(), &h_), "SetLinearSystem");
   }
   // numeric factorization; false when more than 10 pivots were singular
   bool SetValue(const CMatDia_BlkCrs& A) {
@@ -222,6 +225,7 @@ class CPreconditioner_ILU {
  private:
   dfm_ilu h_ = nullptr;
   int lev_ = 0;
+  std::vector<unsigned int> blk_;
 };
 
 // Fem::Ls::CLinearSystem_Save::MakeResidual: {r} := {force} - [B]{u} with B

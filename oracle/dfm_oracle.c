@@ -83,6 +83,20 @@ void dfo_diaind(unsigned N, const unsigned* rowptr, const unsigned* colind, unsi
 #define DFO_ABSENT 0xffffffffu
 int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
                      unsigned* frowptr, unsigned** fcolind_out, unsigned** flev_out) {
+  return dfo_iluk_pattern_rows(N, rowptr, colind, lev_fill, 0, NULL, N, frowptr, fcolind_out, flev_out);
+}
+
+/* The same with CMatDiaFrac_BlkCrs::AddFracPtn(lev_fill, aBlkFill)
+ * (src/matvec/matdiafrac_blkcrs.cpp:1379-1500): a row listed in aBlkFill has
+ * the fill flag -1, and a candidate (i, j) is dropped only when its level
+ * exceeds lev_fill and neither row i nor row j is flagged; the pivot loop
+ * therefore cannot skip a pivot on its level alone when row i may take
+ * flagged fill.  Flags apply to pairs with i, j < bound (the rows of the
+ * matrix that AddFracPtn saw when this one is a joined system).  The early
+ * return for lev_fill == 0 needs an empty list. */
+int dfo_iluk_pattern_rows(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
+                          unsigned nrows, const unsigned* rows, unsigned bound, unsigned* frowptr,
+                          unsigned** fcolind_out, unsigned** flev_out) {
   const unsigned ncrs0 = rowptr[N];
   size_t cap = (size_t)ncrs0 * 4 + 16, nf = 0;
   unsigned* fcol = (unsigned*)malloc(cap * sizeof(unsigned));
@@ -91,7 +105,15 @@ int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind,
   unsigned* lv = (unsigned*)malloc((N ? N : 1) * sizeof(unsigned));
   unsigned* nx = (unsigned*)malloc((N ? N : 1) * sizeof(unsigned));
   const unsigned END = DFO_ABSENT;
-  const int no_fill = lev_fill == 0 || ncrs0 == 0 || (size_t)ncrs0 == (size_t)N * (N ? N - 1 : 0);
+  unsigned char* flag = (unsigned char*)calloc(N ? N : 1, 1);
+  for (unsigned t = 0; t < nrows; t++) {
+    if (rows[t] >= bound || bound > N) {
+      free(fcol); free(flev); free(fdia); free(lv); free(nx); free(flag);
+      return -1;
+    }
+    flag[rows[t]] = 1;
+  }
+  const int no_fill = (lev_fill == 0 && nrows == 0) || ncrs0 == 0 || (size_t)ncrs0 == (size_t)N * (N ? N - 1 : 0);
   for (unsigned j = 0; j < N; j++) lv[j] = DFO_ABSENT;
   frowptr[0] = 0;
   for (unsigned i = 0; i < N; i++) {
@@ -105,15 +127,19 @@ int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind,
       tail = c;
     }
     if (!no_fill) {
+      const int flagged_i = i < bound && flag[i];
+      const int may_flag = nrows > 0 && i < bound;  /* row i can take fill of a flagged row j */
       for (unsigned k = head; k != END; k = nx[k]) {
         const unsigned lik = lv[k];
-        if (lev_fill != -1 && lik + 1 > (unsigned)lev_fill) continue;
+        if (!may_flag && lev_fill != -1 && lik + 1 > (unsigned)lev_fill) continue;
         if (k >= i) break;
         unsigned hint = k; /* every new j lies after k */
         for (unsigned s = fdia[k]; s < frowptr[k + 1]; s++) {
           const unsigned lkj = flev[s];
-          if (lev_fill != -1 && lkj + 1 > (unsigned)lev_fill) continue;
           const unsigned j = fcol[s];
+          const unsigned lmax = lik > lkj ? lik : lkj;
+          const int unlimited = lev_fill == -1 || (j < bound && (flagged_i || flag[j]));
+          if (!unlimited && lmax + 1 > (unsigned)lev_fill) continue;
           if (j == i || lv[j] != DFO_ABSENT) continue;
           while (nx[hint] != END && nx[hint] < j) hint = nx[hint];
           nx[j] = nx[hint];
@@ -143,6 +169,7 @@ int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind,
   free(fdia);
   free(lv);
   free(nx);
+  free(flag);
   *fcolind_out = fcol;
   if (flev_out) *flev_out = flev; else free(flev);
   return 0;

@@ -31,6 +31,12 @@ void dfo_diaind(unsigned N, const unsigned* rowptr, const unsigned* colind, unsi
  * lev_fill = -1: no limit. */
 int dfo_iluk_pattern(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
                      unsigned* frowptr, unsigned** fcolind, unsigned** flev);
+/* AddFracPtn(lev_fill, aBlkFill) (src/matvec/matdiafrac_blkcrs.cpp:1379-1500,
+ * CPreconditioner_ILU::SetFillBlk): fill through a listed row, or into one, is
+ * kept at any level; flags act on pairs i, j < bound.  -1: a row >= bound. */
+int dfo_iluk_pattern_rows(unsigned N, const unsigned* rowptr, const unsigned* colind, int lev_fill,
+                          unsigned nrows, const unsigned* rows, unsigned bound, unsigned* frowptr,
+                          unsigned** fcolind, unsigned** flev);
 void dfo_free(void* p);
 /* SetValue_Initialize (include/delfem/matvec/matdiafrac_blkcrs.h:90-117): A's
  * values into the fill pattern, zero elsewhere. */

@@ -50,6 +50,7 @@ def lib():
         L.dfo_bwd.argtypes = [U, U, up, up, up, dp, dp]
         L.dfo_pcg.argtypes = [U, U, up, up, up, dp, dp, dp, dp, dp, dp, D, U, up, dp, dp]
         L.dfo_iluk_pattern.argtypes = [U, up, up, C.c_int, up, C.POINTER(up), C.POINTER(up)]
+        L.dfo_iluk_pattern_rows.argtypes = [U, up, up, C.c_int, U, up, U, up, C.POINTER(up), C.POINTER(up)]
         L.dfo_free.argtypes = [C.c_void_p]
         L.dfo_iluk_init.argtypes = [U, U, up, up, dp, dp, up, up, dp, dp]
         L.dfo_pcg_fill.argtypes = [U, U, up, up, dp, dp, up, up, up, dp, dp, dp, dp, D, U, up, dp, dp]
@@ -110,15 +111,21 @@ def diaind(rowptr, colind):
     return d[:N]
 
 
-def iluk_pattern(rowptr, colind, lev_fill):
-    """ILU(k) fill pattern (CMatDiaFrac_BlkCrs::AddFracPtn): (frowptr, fcolind, flev)."""
+def iluk_pattern(rowptr, colind, lev_fill, rows=None, bound=None):
+    """ILU(k) fill pattern (CMatDiaFrac_BlkCrs::AddFracPtn): (frowptr, fcolind, flev).
+    rows: block rows with unlimited fill (AddFracPtn(lev, aBlkFill), the
+    SetFillBlk list), acting on pairs of rows below bound (default: all)."""
     rowptr = np.ascontiguousarray(rowptr, np.uint32)
     colind = np.ascontiguousarray(colind, np.uint32)
     N = rowptr.size - 1
     fr = np.zeros(N + 1, np.uint32)
     pc, pl = C.POINTER(C.c_uint)(), C.POINTER(C.c_uint)()
-    lib().dfo_iluk_pattern(N, _u(rowptr), _u(colind if colind.size else np.zeros(1, np.uint32)), int(lev_fill),
-                           _u(fr), C.byref(pc), C.byref(pl))
+    rw = np.ascontiguousarray(rows if rows is not None else [], np.uint32)
+    rc = lib().dfo_iluk_pattern_rows(N, _u(rowptr), _u(colind if colind.size else np.zeros(1, np.uint32)),
+                                     int(lev_fill), rw.size, _u(rw if rw.size else np.zeros(1, np.uint32)),
+                                     N if bound is None else int(bound), _u(fr), C.byref(pc), C.byref(pl))
+    if rc:
+        raise ValueError("fill rows out of range")
     n = int(fr[-1])
     fc = np.ctypeslib.as_array(pc, shape=(max(n, 1),))[:n].copy()
     fl = np.ctypeslib.as_array(pl, shape=(max(n, 1),))[:n].copy()
@@ -215,10 +222,11 @@ class System:
             ns = lib().dfo_ilu0(self.N, self.b, _u(self.rowptr), _u(self._ci), _u(self.dia), _d(fd), _dz(fo))
         return int(ns), fd, fo
 
-    def iluk(self, lev_fill):
+    def iluk(self, lev_fill, rows=None):
         """ILU(lev_fill): fill pattern, SetValue_Initialize, DoILUDecomp on it.
+        rows: the SetFillBlk list (unlimited fill through those block rows).
         Returns (ns, fpat, fd, fo) with fpat = (frowptr, fcolind, fdiaind)."""
-        fr, fc, _ = iluk_pattern(self.rowptr, self.colind, lev_fill)
+        fr, fc, _ = iluk_pattern(self.rowptr, self.colind, lev_fill, rows)
         fdia = diaind(fr, fc)
         if self.cplx:  # CZMatDiaFrac_BlkCrs(lev, A): the same fill pattern, complex values
             fd = np.zeros_like(self.diag)

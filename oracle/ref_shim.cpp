@@ -534,9 +534,25 @@ int dfm_ref_mat_precond(unsigned N, unsigned b, const unsigned* rowptr, const un
 int dfm_ref_mat_iluk(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                      const double* diag, const double* off, int lev, unsigned cap, unsigned* frowptr,
                      unsigned* fcolind, double* fdiag, double* foff, unsigned* fncrs) {
+  return dfm_ref_mat_iluk_rows(N, b, rowptr, colind, diag, off, lev, 0, nullptr, cap, frowptr, fcolind, fdiag, foff,
+                               fncrs);
+}
+
+// With rows: the preconditioner's SetFillBlk path (src/ls/preconditioner.cpp:
+// 91, 140-142): CMatDiaFrac_BlkCrs(0, A), AddFracPtn(lev, aBlkFill), and the
+// pattern finalised as SetValue does (MakePatternFinalize).
+int dfm_ref_mat_iluk_rows(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                          const double* diag, const double* off, int lev, unsigned nrows, const unsigned* rows,
+                          unsigned cap, unsigned* frowptr, unsigned* fcolind, double* fdiag, double* foff,
+                          unsigned* fncrs) {
   Quiet q;
   MatVec::CMatDia_BlkCrs* m = make_mat(N, b, rowptr, colind, diag, off);
-  MatVec::CMatDiaFrac_BlkCrs f(lev, *m);
+  MatVec::CMatDiaFrac_BlkCrs f(nrows ? 0 : lev, *m);
+  if (nrows) {
+    const std::vector<unsigned int> blk(rows, rows + nrows);
+    f.AddFracPtn(lev, blk);
+    f.MakePatternFinalize();
+  }
   *fncrs = f.NCrs();
   if (!frowptr || f.NCrs() > cap) {
     delete m;

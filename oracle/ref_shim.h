@@ -76,6 +76,12 @@ int dfm_ref_mat_precond(unsigned N, unsigned b, const unsigned* rowptr, const un
 int dfm_ref_mat_iluk(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
                      const double* diag, const double* off, int lev, unsigned cap, unsigned* frowptr,
                      unsigned* fcolind, double* fdiag, double* foff, unsigned* fncrs);
+/* The same through CMatDiaFrac_BlkCrs(0, A) + AddFracPtn(lev, aBlkFill) +
+ * MakePatternFinalize (the SetFillBlk path) when nrows > 0. */
+int dfm_ref_mat_iluk_rows(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,
+                          const double* diag, const double* off, int lev, unsigned nrows, const unsigned* rows,
+                          unsigned cap, unsigned* frowptr, unsigned* fcolind, double* fdiag, double* foff,
+                          unsigned* fncrs);
 /* LsSol::CLinearSystem + CPreconditioner_ILU(0) + Solve_PCG / Solve_PBiCGSTAB.
  * Returns 0 when the solver reported convergence, 3 when it did not, 1 on ILU failure. */
 int dfm_ref_mat_solve(unsigned N, unsigned b, const unsigned* rowptr, const unsigned* colind,

@@ -60,6 +60,8 @@ def lib():
         L.dfm_ref_mat_solve.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                         C.c_uint, up, dp, dp, dp, dp]
         L.dfm_ref_mat_iluk.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, up, dp, dp, up]
+        L.dfm_ref_mat_iluk_rows.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, C.c_int, C.c_uint, up, C.c_uint, up,
+                                            up, dp, dp, up]
         L.dfm_ref_mat_solve_lev.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, dp, C.c_int, C.c_double,
                                             C.c_uint, C.c_int, up, dp, dp, dp, dp]
         L.dfm_ref_boundary_residual.argtypes = [C.c_uint, C.c_uint, up, up, dp, dp, ip, dp, dp, C.c_uint, up, up,
@@ -197,19 +199,22 @@ def mat_solve(N, b, rowptr, colind, diag, off, rhs, method=PCG, tol=1e-10, maxit
     return rc, x, it.value, conv.value, ti.value, ts.value
 
 
-def mat_iluk(N, b, rowptr, colind, diag, off, lev):
+def mat_iluk(N, b, rowptr, colind, diag, off, lev, rows=None):
     """CMatDiaFrac_BlkCrs(lev, A) + SetValue_Initialize + DoILUDecomp:
-    (rc, frowptr, fcolind, fdiag, foff)."""
+    (rc, frowptr, fcolind, fdiag, foff).  rows: the SetFillBlk list
+    (AddFracPtn(lev, aBlkFill) over CMatDiaFrac_BlkCrs(0, A))."""
     n = C.c_uint()
     o = off if off.size else np.zeros(1)
-    lib().dfm_ref_mat_iluk(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, 0, None, None, None, None,
-                           C.byref(n))
+    rw = np.ascontiguousarray(rows if rows is not None else [], np.uint32)
+    ra = (rw.size, _u(rw if rw.size else np.zeros(1, np.uint32)))
+    lib().dfm_ref_mat_iluk_rows(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, *ra, 0, None, None, None, None,
+                                C.byref(n))
     fr = np.zeros(N + 1, np.uint32)
     fc = np.zeros(max(n.value, 1), np.uint32)
     fd = np.zeros(N * b * b)
     fo = np.zeros(max(n.value, 1) * b * b)
-    rc = lib().dfm_ref_mat_iluk(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, n.value, _u(fr), _u(fc),
-                                _d(fd), _d(fo), C.byref(n))
+    rc = lib().dfm_ref_mat_iluk_rows(N, b, _u(rowptr), _u(colind), _d(diag), _d(o), lev, *ra, n.value, _u(fr),
+                                     _u(fc), _d(fd), _d(fo), C.byref(n))
     return rc, fr, fc[: n.value], fd, fo[: n.value * b * b]
 
 

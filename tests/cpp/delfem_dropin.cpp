@@ -14,8 +14,10 @@
 //                                    an N x N grid of L0 x L0 blocks and a chain of M nodes of L1 x L1
 //                                    blocks, coupled both ways; symmetric positive definite
 //   [lev]                       optional: ILU fill-in level (SetFillInLevel), default 0
-//   [rev|rand]                  optional last argument: a block ordering (CPreconditioner_ILU::SetOrdering),
+//   [rev|rand]                  optional trailing argument: a block ordering (CPreconditioner_ILU::SetOrdering),
 //                               the rows reversed or shuffled (one-segment problems)
+//   [fill]                      optional trailing argument: CPreconditioner_ILU::SetFillBlk with every 9th
+//                               block row of the first segment's middle fifth (unlimited fill through them)
 //
 // Every run builds the problem from scratch, solves, calls the reference's
 // UpdateValueOfField and reads the field back (the segments' update vectors
@@ -343,8 +345,15 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "usage: %s poisson N [lev] | solid3d NX NY NZ [lev] | twoseg N M L0 L1 [lev]\n", argv[0]);
     return 2;
   }
-  std::string ordk;  // block ordering for SetOrdering
-  if (argc > 3 && (std::string(argv[argc - 1]) == "rev" || std::string(argv[argc - 1]) == "rand")) ordk = argv[--argc];
+  std::string ordk;      // block ordering for SetOrdering
+  bool fillblk = false;  // SetFillBlk
+  while (argc > 3) {
+    const std::string a = argv[argc - 1];
+    if (a == "rev" || a == "rand") ordk = a;
+    else if (a == "fill") fillblk = true;
+    else break;
+    argc--;
+  }
   const std::string kind = argv[1];
   GridMesh mesh;
   int lev = 0;
@@ -375,6 +384,14 @@ int main(int argc, char** argv) {
     if (ordk == "rand") std::shuffle(a.begin(), a.end(), std::mt19937(7));
     return a;
   };
+  // SetFillBlk list: every 9th block row of the first segment's middle fifth
+  auto fill_rows = [&](Sys& P) {
+    std::vector<unsigned int> a;
+    if (!fillblk) return a;
+    const unsigned n = P.lin().GetMatrix(0).NBlkMatCol();
+    for (unsigned i = 2 * n / 5; i < 3 * n / 5; i += 9) a.push_back(i);
+    return a;
+  };
   std::vector<Run> runs;
   try {
     dfm_lsol::Context ctx(0);
@@ -389,6 +406,7 @@ int main(int argc, char** argv) {
       LsSol::CPreconditioner_ILU prec;
       if (lev) prec.SetFillInLevel(lev);
       prec.SetOrdering(ordering(*P));
+      prec.SetFillBlk(fill_rows(*P));
       prec.SetLinearSystem(P->lin());
       P->assemble();
       prec.SetValue(P->lin());
@@ -409,6 +427,7 @@ int main(int argc, char** argv) {
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
       prec.SetOrdering(ordering(*P));
+      prec.SetFillBlk(fill_rows(*P));
       prec.SetLinearSystem(P->lin());
       P->assemble();
       if (!prec.SetValue(P->lin())) throw dfm_lsol::Error(DFM_SINGULAR_PIVOT, name);
@@ -442,6 +461,7 @@ int main(int argc, char** argv) {
       dfm_delfem::CPreconditioner_ILU_GPU prec(ctx);
       prec.SetFillInLevel(lev);
       prec.SetOrdering(ordering(*P));
+      prec.SetFillBlk(fill_rows(*P));
       LsSol::CPreconditioner& base = prec;
       base.SetLinearSystem(P->lin());
       P->assemble();

@@ -71,12 +71,32 @@ int main(int argc, char** argv) {
     const bool ok3 = dfm_lsol::Solve_PCG(conv3, it3, A, M1, r, x3);
     std::vector<double> xh3(A.VectorSize());
     x3.download(xh3.data());
+    // ILU(1) with unlimited fill through every 7th block row of the middle
+    // third: CPreconditioner_ILU::SetFillBlk
+    dfm_lsol::CPreconditioner_ILU M2;
+    M2.SetFillInLevel(1);
+    std::vector<unsigned int> blk;
+    for (unsigned i = A.NBlkMatCol() / 3; i < 2 * A.NBlkMatCol() / 3; i += 7) blk.push_back(i);
+    M2.SetFillBlk(blk);
+    M2.SetLinearSystem(A);
+    if (!M2.SetValue(A)) return 2;
+    double conv4 = 1e-10;
+    unsigned it4 = 1000;
+    dfm_lsol::DeviceVector x4(ctx, A.VectorSize());
+    r.copy_from(f);
+    const bool ok4 = dfm_lsol::Solve_PCG(conv4, it4, A, M2, r, x4);
+    std::vector<double> xh4(A.VectorSize());
+    x4.download(xh4.data());
     std::printf("{\"pcg_ok\": %s, \"pcg_iters\": %u, \"pcg_conv\": %.17g, \"bicg_ok\": %s, \"bicg_iters\": %u, "
-                "\"bicg_conv\": %.17g, \"ilu1_ok\": %s, \"ilu1_iters\": %u, \"x\": [",
-                ok ? "true" : "false", it, conv, ok2 ? "true" : "false", it2, conv2, ok3 ? "true" : "false", it3);
+                "\"bicg_conv\": %.17g, \"ilu1_ok\": %s, \"ilu1_iters\": %u, \"fillblk_ok\": %s, "
+                "\"fillblk_iters\": %u, \"x\": [",
+                ok ? "true" : "false", it, conv, ok2 ? "true" : "false", it2, conv2, ok3 ? "true" : "false", it3,
+                ok4 ? "true" : "false", it4);
     for (size_t k = 0; k < xh.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh[k]);
     std::printf("], \"x_ilu1\": [");
     for (size_t k = 0; k < xh3.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh3[k]);
+    std::printf("], \"x_fillblk\": [");
+    for (size_t k = 0; k < xh4.size(); k++) std::printf("%s%.17g", k ? ", " : "", xh4[k]);
     std::printf("]");
     // optional: a complex matrix in the reference's text format (argv[2]) and
     // its right-hand side (argv[3], one "re im" pair per row), solved by PCOCG

@@ -78,3 +78,9 @@ def test_adapter_program_matches_oracle(demo):
     x1 = np.array(out["x_ilu1"])
     assert out["ilu1_ok"] and abs(out["ilu1_iters"] - ref1["iters"]) <= 1 and ref1["iters"] < ref["iters"]
     assert np.linalg.norm(x1 - ref1["x"]) <= 1e-8 * np.linalg.norm(ref1["x"])
+    n = S.N  # SetFillBlk: every 7th block row of the middle third
+    ns2, fpat2, fd2, fo2 = S.iluk(1, np.arange(n // 3, 2 * n // 3, 7))
+    ref2 = S.solve_fill(fpat2, fd2, fo2, tol=1e-10, maxit=1000)
+    x2 = np.array(out["x_fillblk"])
+    assert out["fillblk_ok"] and abs(out["fillblk_iters"] - ref2["iters"]) <= 1
+    assert np.linalg.norm(x2 - ref2["x"]) <= 1e-8 * np.linalg.norm(ref2["x"])

@@ -56,7 +56,11 @@ CASES = [("poisson", ["poisson", "32"]), ("poisson_ilu1", ["poisson", "24", "1"]
          ("twoseg_2_1_ilu2", ["twoseg", "40", "200", "2", "1", "2"]),
          # CPreconditioner_ILU::SetOrdering: the rows reversed or shuffled (ILU(0) of the renumbered matrix)
          ("poisson_ord_rev", ["poisson", "24", "0", "rev"]), ("poisson_ord_rand", ["poisson", "32", "0", "rand"]),
-         ("solid3d_ord_rand", ["solid3d", "10", "3", "3", "0", "rand"])]
+         ("solid3d_ord_rand", ["solid3d", "10", "3", "3", "0", "rand"]),
+         # CPreconditioner_ILU::SetFillBlk: unlimited fill through listed block rows (AddFracPtn(lev, aBlkFill))
+         ("poisson_fill_ilu1", ["poisson", "32", "1", "fill"]), ("solid3d_fill_ilu0", ["solid3d", "10", "3", "3", "0", "fill"]),
+         ("twoseg_2_2_fill_ilu1", ["twoseg", "40", "200", "2", "2", "1", "fill"]),
+         ("twoseg_2_1_fill_ilu0", ["twoseg", "40", "200", "2", "1", "0", "fill"])]
 
 
 @pytest.mark.gpu

@@ -191,3 +191,53 @@ def test_complex_iluk_factor_and_cocg(ctx, nring, lev, solve):
     rc, it, conv = lib.solve_pcocg(A, M, r, x, tol=1e-10, maxit=3000)
     assert rc == lib.OK and o["ok"]
     assert np.linalg.norm(x.cpu().numpy() - o["x"]) <= 1e-8 * np.linalg.norm(o["x"])
+
+
+def _fill_rows(N, kind):
+    if kind == "scattered":
+        return np.random.default_rng(N).choice(N, size=max(1, N // 15), replace=False).astype(np.uint32)
+    return np.arange(N // 3, N // 3 + max(2, N // 10), dtype=np.uint32)
+
+
+@pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b3"])
+@pytest.mark.parametrize("lev", [0, 1, 2])
+@pytest.mark.parametrize("kind", ["scattered", "run"])
+def test_iluk_fill_rows(ctx, name, lev, kind):
+    """SetFillBlk (AddFracPtn(lev, aBlkFill)): the listed rows take fill at
+    any level; pattern, level sets and factor identical to the oracle's (pinned
+    to the reference's), the range-partitioned sweeps to 1e-11."""
+    from delfem_b200 import lib
+    S = SYSTEMS[name]()
+    rows = _fill_rows(S.N, kind)
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    A.set_values(S.diag, S.off)
+    M = lib.ILU(A, fill_level=lev, fill_rows=rows)
+    ns, (fr, fc, fdia), fd, fo = S.iluk(lev, rows)
+    rp, ci = M.pattern()
+    assert np.array_equal(rp, fr) and np.array_equal(ci, fc)
+    lf, nf, lb, nb = M.levels()
+    olf, onf, olb, onb = P.levels(fr, fc, fdia)
+    assert nf == onf and nb == onb and np.array_equal(lf, olf) and np.array_equal(lb, olb)
+    rc, gns = M.factor()
+    assert gns == ns == 0
+    gd, go = M.get_values()
+    assert np.array_equal(gd, fd) and np.array_equal(go, fo)
+    F = P.System(fr, fc, S.b)
+    r = np.random.default_rng(6).standard_normal(S.N * S.b)
+    ref = F.precond(fd, fo, r)
+    for sweep in (1, 9):
+        M.sweep = sweep
+        z = torch.zeros(S.N * S.b, dtype=torch.float64, device="cuda")
+        M.apply(_dev(r), z)
+        got = z.cpu().numpy()
+        assert np.allclose(got, ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
+
+
+def test_iluk_fill_rows_invalid(ctx):
+    """A listed row at or past the bound, or a zero bound, is DFM_ERR_INVALID."""
+    from delfem_b200 import lib
+    S = SYSTEMS["poisson16"]()
+    A = lib.Matrix(ctx, S.rowptr, S.colind, S.b)
+    for rows, bound in (([S.N], None), ([3], 3), ([0], 0)):
+        with pytest.raises(lib.DfmError):
+            lib.ILU(A, fill_level=1, fill_rows=np.array(rows, np.uint32), fill_bound=bound)

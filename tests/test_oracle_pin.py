@@ -96,6 +96,35 @@ def test_iluk_pinned_to_reference(name, lev):
     assert fc.size >= S.colind.size
 
 
+def _fill_rows(N, kind):
+    """SetFillBlk lists: a few scattered rows, a contiguous run, the last row."""
+    if kind == "scattered":
+        return np.random.default_rng(N).choice(N, size=max(1, N // 15), replace=False).astype(np.uint32)
+    if kind == "run":
+        return np.arange(N // 3, N // 3 + max(2, N // 10), dtype=np.uint32)
+    return np.array([N - 1, N - 1], np.uint32)  # the last row, listed twice
+
+
+@pytest.mark.parametrize("name", ["poisson_coef", "solid2d", "solid3d", "random_b3"])
+@pytest.mark.parametrize("lev", [0, 1, 2])
+@pytest.mark.parametrize("kind", ["scattered", "run", "last"])
+def test_iluk_fill_rows_pinned_to_reference(name, lev, kind):
+    """CPreconditioner_ILU::SetFillBlk: AddFracPtn(lev, aBlkFill), where fill
+    through or into a listed row is kept at any level (flag -1), over
+    CMatDiaFrac_BlkCrs(0, A): the oracle's pattern, values and factor are
+    bit-identical to the reference's."""
+    S = ILUK_SYSTEMS[name]()
+    rows = _fill_rows(S.N, kind)
+    ns, (fr, fc, fdia), fd, fo = S.iluk(lev, rows)
+    rc, rfr, rfc, rfd, rfo = R.mat_iluk(S.N, S.b, S.rowptr, S.colind, S.diag, S.off, lev, rows)
+    assert rc == 0 and ns == 0
+    assert np.array_equal(fr, rfr) and np.array_equal(fc, rfc)
+    assert _eq(fd, rfd) and _eq(fo, rfo)
+    if kind != "last":  # the last row's pivots have no upper part but itself
+        _, (fr0, fc0, _), _, _ = S.iluk(lev)
+        assert fc.size > fc0.size  # the listed rows took fill beyond level lev
+
+
 @pytest.mark.parametrize("lev", [0, 1, 2])
 def test_iluk_pcg_pinned_to_reference(lev):
     """Solve_PCG with CPreconditioner_ILU::SetFillInLevel(lev): the same x,
