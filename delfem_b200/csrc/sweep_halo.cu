@@ -234,6 +234,63 @@ DFM_DEVINL void row_finish(const RowPre<B, LPR, TV>& P, const char* sb, double* 
   }
 }
 
+// One producer lane's halo entries e0, e0 + 32, ... (NP of them, those below
+// nh) into H: every entry's values are read, then each pass re-reads all the
+// values that still hold the sentinel, so a lane's second entry costs no L2
+// round trip of its own after the first.  Entries flagged 0x80000000 are rows
+// of the input vector (merged level pairs) and need no wait.  False when the
+// wait ran out (recorded) or the CTA is shutting down.
+template <int B, int NP>
+DFM_DEVINL bool halo_poll(const unsigned* hids, unsigned e0, unsigned nh, const double* __restrict__ in,
+                          const double* out, double* H, int* s_alive, DevStatus* st, uint64_t wait_ns) {
+  size_t row[NP];
+  bool from_out[NP];
+  double v[NP][B];
+#pragma unroll
+  for (int u = 0; u < NP; u++) {
+    const unsigned e = e0 + 32u * u;
+    const unsigned hid = e < nh ? hids[e] : 0x80000000u;
+    row[u] = hid & 0x7fffffffu;
+    from_out[u] = e < nh && !(hid & 0x80000000u);
+#pragma unroll
+    for (int c = 0; c < B; c++)
+      v[u][c] = e >= nh ? 0.0 : from_out[u] ? ld_relaxed(out + row[u] * B + c) : in[row[u] * B + c];
+  }
+  auto missing = [&]() {
+    bool m = false;
+#pragma unroll
+    for (int u = 0; u < NP; u++)
+#pragma unroll
+      for (int c = 0; c < B; c++) m |= from_out[u] && Sent<double>::is(v[u][c]);
+    return m;
+  };
+  if (missing()) {
+    SpinGuard g(wait_ns);
+    for (;;) {
+#pragma unroll
+      for (int u = 0; u < NP; u++)
+#pragma unroll
+        for (int c = 0; c < B; c++)
+          if (from_out[u] && Sent<double>::is(v[u][c])) v[u][c] = ld_relaxed(out + row[u] * B + c);
+      if (!missing()) break;
+      const bool late = g.expired();
+      if (late || ((g.n & 1023u) == 0 && !ld_volatile_i(s_alive))) {
+        if (late) raise_error(st, DFM_WAIT_TIMEOUT, 22);
+        st_volatile_i(s_alive, 0);
+        return false;
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NP; u++) {
+    const unsigned e = e0 + 32u * u;
+    if (e < nh)
+#pragma unroll
+      for (int c = 0; c < B; c++) H[e * B + c] = v[u][c];
+  }
+  return true;
+}
+
 template <int B, int LPR, typename TV, bool FWD, int DOT>
 __global__ void __launch_bounds__(kHaloMaxThreads, 1)
 k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ cta_chunk,
@@ -327,49 +384,17 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
         if (wl == 0) (void)wait_stage(&bar[s], par, st, wait_ns);
         break;
       }
-      // halo: the other CTAs' rows this chunk reads, polled until published
+      // halo: the other CTAs' rows this chunk reads, polled until published;
+      // a lane takes entries wl, wl + 32, ..., two at a time past 32 entries
       const HaloHeader* hdr = reinterpret_cast<const HaloHeader*>(sb);
       const unsigned nh = hdr->nhalo;
       const unsigned* hids = reinterpret_cast<const unsigned*>(sb + hdr->hids);
       double* H = X + x_slice + (size_t)s * halo_stride;
-      for (unsigned e = (unsigned)wl; e < nh; e += 32) {
-        const unsigned hid = hids[e];
-        double v[B];
-        bool miss = false;
-        if (hid & 0x80000000u) {  // an entry of the input vector (merged level pairs): no wait
-          const size_t row = hid & 0x7fffffffu;
-#pragma unroll
-          for (int c = 0; c < B; c++) v[c] = in[row * B + c];
-        } else {
-          const size_t row = hid;
-#pragma unroll
-          for (int c = 0; c < B; c++) v[c] = ld_relaxed(out + row * B + c);
-#pragma unroll
-          for (int c = 0; c < B; c++) miss |= Sent<double>::is(v[c]);
-        }
-        const size_t row = hid & 0x7fffffffu;
-        if (miss) {
-          SpinGuard g(wait_ns);
-          while (miss) {
-            miss = false;
-#pragma unroll
-            for (int c = 0; c < B; c++)
-              if (Sent<double>::is(v[c])) {
-                v[c] = ld_relaxed(out + row * B + c);
-                miss |= Sent<double>::is(v[c]);
-              }
-            if (!miss) break;
-            if (g.expired() || ((g.n & 1023u) == 0 && !ld_volatile_i(&s_alive))) {
-              if (g.expired()) raise_error(st, DFM_WAIT_TIMEOUT, 22);
-              st_volatile_i(&s_alive, 0);
-              ok = false;
-              break;
-            }
-          }
-        }
-        if (!ok) break;
-#pragma unroll
-        for (int c = 0; c < B; c++) H[e * B + c] = v[c];
+      if (nh > 32u) {
+        for (unsigned e0 = (unsigned)wl; e0 < nh && ok; e0 += 64u)
+          ok = halo_poll<B, 2>(hids, e0, nh, in, out, H, &s_alive, st, wait_ns);
+      } else if ((unsigned)wl < nh) {
+        ok = halo_poll<B, 1>(hids, (unsigned)wl, nh, in, out, H, &s_alive, st, wait_ns);
       }
       if (!__all_sync(0xffffffffu, ok)) break;
       __syncwarp();  // every lane's halo stores precede lane 0's release
