@@ -211,8 +211,6 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
   char* stages = smem + x_bytes;
   uint64_t* bar_data = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
 
-  // X slice <- in[a0:a1) (rows overwrite their entry with the output)
-  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[slot_row(rows, a0 + k / B) * B + k % B];
   unsigned issued_end = q0;  // stage thread: chunks [q0, issued_end) requested
   if (threadIdx.x == kStageThread) {
     s_alive = 1;
@@ -225,8 +223,11 @@ k_sweep_ranges(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict_
       bulk_g2s(stages + (size_t)s * stage_bytes, blob + cd.off, cd.bytes, &bar_data[s]);
       issued_end = q + 1;
     }
-    if (q0 < q1 && !wait_stage(&bar_data[0], 0u, st, wait_ns)) s_alive = 0;
   }
+  // X slice <- in[a0:a1) while the first chunks are in flight (rows
+  // overwrite their entry with the output)
+  load_slice<B, 8>(X, in, rows, a0, len);
+  if (threadIdx.x == kStageThread && q0 < q1 && !wait_stage(&bar_data[0], 0u, st, wait_ns)) s_alive = 0;
   __syncthreads();
   const int lane = threadIdx.x % LPR;
   const unsigned g = threadIdx.x / LPR, ng = kSweepThreads / LPR;

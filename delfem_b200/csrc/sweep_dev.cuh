@@ -102,27 +102,94 @@ DFM_DEVINL bool wait_stage(uint64_t* bar, unsigned parity, DevStatus* st, uint64
 // nullptr for the natural order (row a0 + k).
 DFM_DEVINL size_t slot_row(const unsigned* rows, unsigned p) { return rows ? (size_t)rows[p] : (size_t)p; }
 
+// The CTA's slice X[k] = v[row of slot a0 + k / B][k % B], k < len * B.  A
+// thread takes k = tid, tid + T, ... (T threads) as U independent loads at a
+// time (the slot -> row lookups of a batch, then their values): the slice is
+// read from L2 at the start of every sweep, on the critical path, and one
+// dependent round trip per element would serialise ~len * B / T of them.
+template <int B, int U, typename TX, typename TI>
+DFM_DEVINL void load_slice(TX* X, const TI* __restrict__ v, const unsigned* __restrict__ rows, unsigned a0,
+                           unsigned len) {
+  const unsigned tot = len * B, T = blockDim.x;
+  for (unsigned k0 = threadIdx.x; k0 < tot; k0 += U * T) {
+    TI w[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      w[u] = k < tot ? v[slot_row(rows, a0 + k / B) * B + k % B] : TI(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      if (k < tot) X[k] = w[u];
+    }
+  }
+}
+
+// This thread's share of sum_k rdot[row of slot a0 + k / B][k % B] * X[k]
+// (real) in ascending k, U loads of rdot at a time; the same sum, in the same
+// order, as one load per term.
+template <int B, int U, typename TX, typename TR>
+DFM_DEVINL double slice_dot(const TR* __restrict__ rdot, const TX* X, const unsigned* __restrict__ rows,
+                            unsigned a0, unsigned len) {
+  const unsigned tot = len * B, T = blockDim.x;
+  double acc = 0.0;
+  for (unsigned k0 = threadIdx.x; k0 < tot; k0 += U * T) {
+    TR w[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      w[u] = k < tot ? rdot[slot_row(rows, a0 + k / B) * B + k % B] : TR(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      if (k < tot) acc += (double)w[u] * (double)X[k];
+    }
+  }
+  return acc;
+}
+
+// The complex form (rows as (re, im) pairs): this thread's share of the
+// unconjugated sum_k rdot_k X_k over slots k = tid, tid + T, ..., U at a time.
+template <int U, typename TX, typename TR>
+DFM_DEVINL void slice_zdot(const TR* __restrict__ rdot, const TX* X, const unsigned* __restrict__ rows,
+                           unsigned a0, unsigned len, double& re, double& im) {
+  const unsigned T = blockDim.x;
+  for (unsigned k0 = threadIdx.x; k0 < len; k0 += U * T) {
+    TR wr[U], wi[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      const size_t gi = k < len ? slot_row(rows, a0 + k) : 0;
+      wr[u] = k < len ? rdot[gi * 2] : TR(0);
+      wi[u] = k < len ? rdot[gi * 2 + 1] : TR(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned k = k0 + (unsigned)u * T;
+      if (k < len) {
+        const double rr = (double)wr[u], ri = (double)wi[u];
+        const double xr = (double)X[2 * k], xi = (double)X[2 * k + 1];
+        re += rr * xr - ri * xi;
+        im += rr * xi + ri * xr;
+      }
+    }
+  }
+}
+
 template <int B, int DOT, typename TX>
 DFM_DEVINL void range_dot(const TX* __restrict__ rdot, const TX* X, unsigned a0, unsigned len, bool alive,
                           double* part, const unsigned* rows) {
   if constexpr (DOT == 2) {
     static_assert(B == 2, "complex rows are 2x2 real blocks");
     double re = 0.0, im = 0.0;
-    if (alive)
-      for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
-        const size_t gi = slot_row(rows, a0 + k);
-        const double rr = (double)rdot[gi * 2], ri = (double)rdot[gi * 2 + 1];
-        const double xr = (double)X[2 * k], xi = (double)X[2 * k + 1];
-        re += rr * xr - ri * xi;
-        im += rr * xi + ri * xr;
-      }
+    if (alive) slice_zdot<4>(rdot, X, rows, a0, len, re, im);
     block_partial<kSweepThreads>(re, part);
     block_partial<kSweepThreads>(im, part + kMaxBlocks);
   } else {
     double dacc = 0.0;
-    if (alive)
-      for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
-        dacc += (double)rdot[slot_row(rows, a0 + k / B) * B + k % B] * (double)X[k];
+    if (alive) dacc = slice_dot<B, 8>(rdot, X, rows, a0, len);
     block_partial<kSweepThreads>(dacc, part);
   }
 }

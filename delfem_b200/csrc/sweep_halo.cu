@@ -75,16 +75,9 @@ DFM_DEVINL void halo_dot(const double* __restrict__ rdot, const double* X, unsig
   __shared__ double s_w[2][kHaloMaxWarps];
   double re = 0.0, im = 0.0;
   if constexpr (DOT == 2) {
-    for (unsigned k = threadIdx.x; k < len; k += blockDim.x) {
-      const size_t gi = slot_row(rows, a0 + k);
-      const double rr = rdot[gi * 2], ri = rdot[gi * 2 + 1];
-      const double xr = X[2 * k], xi = X[2 * k + 1];
-      re += rr * xr - ri * xi;
-      im += rr * xi + ri * xr;
-    }
+    slice_zdot<8>(rdot, X, rows, a0, len, re, im);
   } else {
-    for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x)
-      re += rdot[slot_row(rows, a0 + k / B) * B + k % B] * X[k];
+    re = slice_dot<B, 16>(rdot, X, rows, a0, len);
   }
   re = group_sum<32>(re);
   im = group_sum<32>(im);
@@ -323,7 +316,6 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
   char* stages = smem + x_bytes;
   uint64_t* bar = reinterpret_cast<uint64_t*>(stages + (size_t)nstage * stage_bytes);
 
-  for (unsigned k = threadIdx.x; k < len * B; k += blockDim.x) X[k] = in[slot_row(rows, a0 + k / B) * B + k % B];
   if (threadIdx.x == 0) {
     s_alive = 1;
     s_released = 0;
@@ -336,12 +328,25 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
   __syncthreads();
   const int warp = (int)(threadIdx.x >> 5), wl = (int)(threadIdx.x & 31);
   const int nwarps = (int)(blockDim.x >> 5);
+  // A producer's first chunk (pw < nstage: its stage has not been used yet) is
+  // requested before the slice load, so the copy overlaps it.
+  const int pw0 = warp - ncw;
+  const bool pre_issued = warp >= ncw && pw0 < nstage && (unsigned)pw0 < K;
+  if (pre_issued && wl == 0) {
+    const ChunkDesc cd = chunks[q0 + (unsigned)pw0];
+    mbar_arrive_tx(&bar[pw0], cd.bytes);
+    bulk_g2s(stages + (size_t)pw0 * stage_bytes, blob + cd.off, cd.bytes, &bar[pw0]);
+  }
+  load_slice<B, 16>(X, in, rows, a0, len);
+  __syncthreads();
 
   if (warp >= ncw) {
     // ------------------------------------------------------------ producer
     const int pw = warp - ncw, npw = nwarps - ncw;
     for (unsigned k = (unsigned)pw; k < K; k += (unsigned)npw) {
-      if (__any_sync(0xffffffffu, !ld_volatile_i(&s_alive))) break;  // warp-uniform
+      // (the pre-issued first chunk goes on to its landing wait whatever happens)
+      const bool first = pre_issued && k == (unsigned)pw;
+      if (!first && __any_sync(0xffffffffu, !ld_volatile_i(&s_alive))) break;  // warp-uniform
       const int s = (int)(k % (unsigned)nstage);
       // the stage is free once the compute warps are done with chunk k - nstage
       bool ok = true;
@@ -361,7 +366,7 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
       __threadfence_block();
       const ChunkDesc cd = chunks[q0 + k];
       char* sb = stages + (size_t)s * stage_bytes;
-      if (wl == 0) {
+      if (wl == 0 && !first) {
         fence_proxy_async_smem();  // the compute warps' reads of the stage precede the copy into it
         mbar_arrive_tx(&bar[s], cd.bytes);
         bulk_g2s(sb, blob + cd.off, cd.bytes, &bar[s]);
