@@ -329,7 +329,9 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
   const int warp = (int)(threadIdx.x >> 5), wl = (int)(threadIdx.x & 31);
   const int nwarps = (int)(blockDim.x >> 5);
   // A producer's first chunk (pw < nstage: its stage has not been used yet) is
-  // requested before the slice load, so the copy overlaps it.
+  // requested here, at the start.  The slice is not loaded here: the
+  // producers put each chunk's right-hand sides into their slots with the
+  // chunk's halo, off the compute warps' path.
   const int pw0 = warp - ncw;
   const bool pre_issued = warp >= ncw && pw0 < nstage && (unsigned)pw0 < K;
   if (pre_issued && wl == 0) {
@@ -337,8 +339,6 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
     mbar_arrive_tx(&bar[pw0], cd.bytes);
     bulk_g2s(stages + (size_t)pw0 * stage_bytes, blob + cd.off, cd.bytes, &bar[pw0]);
   }
-  load_slice<B, 16>(X, in, rows, a0, len);
-  __syncthreads();
 
   if (warp >= ncw) {
     // ------------------------------------------------------------ producer
@@ -395,11 +395,33 @@ k_sweep_halo(const ChunkDesc* __restrict__ chunks, const unsigned* __restrict__ 
       const unsigned nh = hdr->nhalo;
       const unsigned* hids = reinterpret_cast<const unsigned*>(sb + hdr->hids);
       double* H = X + x_slice + (size_t)s * halo_stride;
+      // the chunk's own right-hand sides (in[] of its rows) go into their slots
+      // of the slice: lane l reads row l's before the halo poll and stores them
+      // after it, rows past 32 follow (the slice is not loaded up front)
+      const unsigned nr = hdr->nrows;
+      const uint4* rdesc = reinterpret_cast<const uint4*>(sb + 32);
+      double rhs[B];
+      const bool has_row = (unsigned)wl < nr;
+      unsigned slot = 0;
+      if (has_row) {
+        const uint4 rd = rdesc[wl];
+        slot = rd.x;
+#pragma unroll
+        for (int c = 0; c < B; c++) rhs[c] = in[(size_t)rd.w * B + c];
+      }
       if (nh > 32u) {
         for (unsigned e0 = (unsigned)wl; e0 < nh && ok; e0 += 64u)
           ok = halo_poll<B, 2>(hids, e0, nh, in, out, H, &s_alive, st, wait_ns);
       } else if ((unsigned)wl < nh) {
         ok = halo_poll<B, 1>(hids, (unsigned)wl, nh, in, out, H, &s_alive, st, wait_ns);
+      }
+      if (has_row)
+#pragma unroll
+        for (int c = 0; c < B; c++) X[(size_t)slot * B + c] = rhs[c];
+      for (unsigned rr = (unsigned)wl + 32u; rr < nr; rr += 32u) {
+        const uint4 rd = rdesc[rr];
+#pragma unroll
+        for (int c = 0; c < B; c++) X[(size_t)rd.x * B + c] = in[(size_t)rd.w * B + c];
       }
       if (!__all_sync(0xffffffffu, ok)) break;
       __syncwarp();  // every lane's halo stores precede lane 0's release
