@@ -19,7 +19,10 @@
 //    into the stage with one TMA bulk copy (cp.async.bulk, no multicast),
 //    waits for it to land, then polls the halo rows' published values in
 //    global memory (NaN sentinel = not yet written) until all are in, copies
-//    them into the stage's halo area and marks the stage ready for that chunk.
+//    them into the stage's halo area, puts the chunk's own right-hand sides
+//    (the input vector's entries of its rows) into their slots of the slice,
+//    and marks the stage ready for that chunk.  The slice is never loaded as a
+//    whole: a launch starts on its first level at once.
 //
 // The critical path of a level is then the compute warps' own work plus a
 // barrier of at most four warps; the L2 round trips for other CTAs' rows and
