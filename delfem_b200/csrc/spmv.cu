@@ -210,6 +210,7 @@ k_spmv_elem(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __r
 // from global memory directly.  The copy starts at the 16-byte boundary below
 // the run and ends at the one above it (the arrays carry kArrayPad spare
 // elements).
+constexpr int kWsUnroll = 2;  // blocks per lane whose column and x loads are issued together
 constexpr int kWsChunks = 8;  // 16-byte chunks per lane and pass: a 4,096-byte slice of off-diagonal values
 
 template <int B, int LPR, typename TV>
@@ -291,17 +292,33 @@ k_spmv_ws(unsigned N, const unsigned* __restrict__ rowptr, const unsigned* __res
       double acc[B];
 #pragma unroll
       for (int r = 0; r < B; r++) acc[r] = 0.0;
-      for (unsigned s = s0 + lane; s <= s1; s += LPR) {
-        const unsigned col = s < s1 ? __ldcs(colind + s) : i;
-        double xv[B];
+      // the lane's blocks s0 + lane, + LPR, ... (the diagonal block last, as
+      // slot s1) in that order, kWsUnroll at a time: their column indices,
+      // then their x entries are requested together before the products
+      constexpr int U = kWsUnroll;
+      for (unsigned sb0 = s0 + lane; sb0 <= s1; sb0 += U * LPR) {
+        unsigned col[U];
 #pragma unroll
-        for (int c = 0; c < B; c++) xv[c] = __ldg(x + (size_t)col * B + c);
-        if (s < s1) {
-          const size_t boff = (size_t)(s - sb) * S::VB + dv;
-          if (boff + S::VB <= S::OFF) ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + boff), xv);
-          else ws_mac<B>(acc, off + (size_t)s * BB, xv);
-        } else {
-          ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + S::OFF + dd + g * S::VB), xv);
+        for (int u = 0; u < U; u++) {
+          const unsigned s = sb0 + u * LPR;
+          col[u] = s < s1 ? __ldcs(colind + s) : i;
+        }
+        double xv[U][B];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (sb0 + u * LPR <= s1)
+#pragma unroll
+            for (int c = 0; c < B; c++) xv[u][c] = __ldg(x + (size_t)col[u] * B + c);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const unsigned s = sb0 + u * LPR;
+          if (s < s1) {
+            const size_t boff = (size_t)(s - sb) * S::VB + dv;
+            if (boff + S::VB <= S::OFF) ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + boff), xv[u]);
+            else ws_mac<B>(acc, off + (size_t)s * BB, xv[u]);
+          } else if (s == s1) {
+            ws_mac<B>(acc, reinterpret_cast<const TV*>(wb + S::OFF + dd + g * S::VB), xv[u]);
+          }
         }
       }
 #pragma unroll
